@@ -1,0 +1,241 @@
+/*
+ * taucs_b200.h -- C ABI of libtaucs_b200.so, a B200 (sm_100a) implementation
+ * of TAUCS's multifrontal supernodal Cholesky factorization and supernodal
+ * triangular solve.
+ *
+ * The first part of this header repeats the reference's public interface for
+ * this path with the same names, argument meanings, ownership and error
+ * returns, so that a C caller of TAUCS can relink against this library:
+ *
+ *   taucs_ccs_matrix ............ src/taucs.h:537-554
+ *   error codes / flags ......... src/taucs.h:90-108
+ *   factor / solve / free ....... src/taucs_private.h:222-257
+ *   taucs_linsolve .............. src/taucs_private.h:16-22
+ *   CCS helpers ................. src/taucs_private.h:44-73
+ *   ordering .................... src/taucs_private.h:97-101
+ *   generators .................. src/taucs_private.h:145-147
+ *   vector permutes ............. src/taucs_private.h:270-273
+ *   logging / timers ............ src/taucs_private.h:280-285
+ *
+ * The numeric factorization and the solve run on the current CUDA device; the
+ * factor handle keeps its L factor in device memory.  Host arrays passed to
+ * these functions are ordinary (pageable or pinned) host memory.  There is no
+ * CPU fallback: when no usable sm_100 device is present the factor functions
+ * return NULL / TAUCS_ERROR and report the CUDA error through taucs_printf.
+ *
+ * The second part (taucs_b200_*) adds what the reference does not have:
+ * device-pointer entry points, multi-RHS solves, stream selection, mixed
+ * precision with iterative refinement, batched factorization of many small
+ * systems, and inspection hooks used by the parity tests.
+ */
+#ifndef TAUCS_B200_H
+#define TAUCS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* reference interface                                                 */
+/* ------------------------------------------------------------------ */
+
+#define TAUCS_SUCCESS           0
+#define TAUCS_ERROR            -1
+#define TAUCS_ERROR_NOMEM      -2
+#define TAUCS_ERROR_BADARGS    -3
+#define TAUCS_ERROR_INDEFINITE -4
+#define TAUCS_ERROR_MAXDEPTH   -5
+
+#define TAUCS_INT       1024
+#define TAUCS_DOUBLE    2048
+#define TAUCS_SINGLE    4096
+#define TAUCS_DCOMPLEX  8192
+#define TAUCS_SCOMPLEX 16384
+
+#define TAUCS_LOWER      1
+#define TAUCS_UPPER      2
+#define TAUCS_TRIANGULAR 4
+#define TAUCS_SYMMETRIC  8
+#define TAUCS_HERMITIAN  16
+#define TAUCS_PATTERN    32
+
+/* Sparse matrix in compressed column storage, 0-based (src/taucs.h:537-554).
+ * Symmetric matrices store the lower triangle including the diagonal; row
+ * indices within a column need not be sorted and duplicates are summed. */
+typedef struct {
+  int  n;       /* columns */
+  int  m;       /* rows */
+  int  flags;
+  int* colptr;  /* n+1 */
+  int* rowind;  /* colptr[n] */
+  union {
+    void*   v;
+    double* d;
+    float*  s;
+  } values;
+} taucs_ccs_matrix;
+
+/* CCS helpers (src/taucs_ccs_base.c:72-132, src/taucs_ccs_ops.c:174-344) */
+taucs_ccs_matrix* taucs_ccs_create(int m, int n, int nnz, int flags);
+taucs_ccs_matrix* taucs_dccs_create(int m, int n, int nnz);
+void              taucs_ccs_free(taucs_ccs_matrix* A);
+void              taucs_dccs_free(taucs_ccs_matrix* A);
+taucs_ccs_matrix* taucs_ccs_permute_symmetrically(taucs_ccs_matrix* A, int* perm, int* invperm);
+taucs_ccs_matrix* taucs_dccs_permute_symmetrically(taucs_ccs_matrix* A, int* perm, int* invperm);
+void              taucs_ccs_times_vec(taucs_ccs_matrix* A, void* X, void* B);
+void              taucs_dccs_times_vec(taucs_ccs_matrix* A, double* X, double* B);
+
+/* vector permutes (src/taucs_vec_base.c:194-206): pv[i] = v[p[i]];
+ * v[invp[i]] = pv[i] */
+void taucs_vec_permute(int n, int flags, void* v, void* pv, int p[]);
+void taucs_vec_ipermute(int n, int flags, void* pv, void* v, int invp[]);
+void taucs_dvec_permute(int n, double v[], double pv[], int p[]);
+void taucs_dvec_ipermute(int n, double pv[], double v[], int invp[]);
+
+/* generators (src/taucs_ccs_generators.c:89-261) */
+taucs_ccs_matrix* taucs_ccs_generate_mesh2d(int n, char* which);
+taucs_ccs_matrix* taucs_ccs_generate_mesh3d(int X, int Y, int Z);
+
+/* fill-reducing ordering (src/taucs_ccs_order.c:843-880): "amd", "identity",
+ * "random" (and "genmmd"/"metis"/"colamd" report failure).  perm and invperm
+ * are allocated with malloc; *perm == NULL on failure. */
+void taucs_ccs_order(taucs_ccs_matrix* A, int** perm, int** invperm, char* which);
+
+/* multifrontal supernodal LL^T (src/taucs_private.h:245-257).  A is the
+ * already permuted lower triangle.  The handle's first member is int flags
+ * (TAUCS_DOUBLE), as in the reference.  NULL on a nonpositive pivot, out of
+ * memory (host or device), or an elimination tree deeper than max_depth. */
+void* taucs_ccs_factor_llt_mf(taucs_ccs_matrix* A);
+void* taucs_ccs_factor_llt_mf_maxdepth(taucs_ccs_matrix* A, int max_depth);
+void* taucs_ccs_factor_llt_symbolic(taucs_ccs_matrix* A);
+void* taucs_ccs_factor_llt_symbolic_maxdepth(taucs_ccs_matrix* A, int max_depth);
+/* 0, or -1 on a nonpositive pivot (numeric part freed) */
+int   taucs_ccs_factor_llt_numeric(taucs_ccs_matrix* A, void* L);
+void* taucs_dccs_factor_llt_mf(taucs_ccs_matrix* A);
+void* taucs_dccs_factor_llt_mf_maxdepth(taucs_ccs_matrix* A, int max_depth);
+void* taucs_dccs_factor_llt_symbolic(taucs_ccs_matrix* A);
+void* taucs_dccs_factor_llt_symbolic_maxdepth(taucs_ccs_matrix* A, int max_depth);
+int   taucs_dccs_factor_llt_numeric(taucs_ccs_matrix* A, void* L);
+
+/* x := (L L^T)^-1 b, one right-hand side, host vectors in permuted order.
+ * b is read only.  0, or -1 on failure. */
+int   taucs_supernodal_solve_llt(void* L, void* x, void* b);
+int   taucs_dsupernodal_solve_llt(void* L, void* x, void* b);
+
+void  taucs_supernodal_factor_free(void* L);
+void  taucs_supernodal_factor_free_numeric(void* L);
+taucs_ccs_matrix* taucs_supernodal_factor_to_ccs(void* L);
+void* taucs_supernodal_factor_get_diag(void* L);
+void  taucs_dsupernodal_factor_free(void* L);
+void  taucs_dsupernodal_factor_free_numeric(void* L);
+taucs_ccs_matrix* taucs_dsupernodal_factor_to_ccs(void* L);
+double* taucs_dsupernodal_factor_get_diag(void* L);
+
+/* unified interface (src/taucs_linsolve.c:189-622).  Options understood:
+ *   taucs.factor=bool taucs.factor.symbolic=bool taucs.factor.numeric=bool
+ *   taucs.factor.LLT=bool taucs.factor.mf=bool taucs.factor.ll=bool
+ *   taucs.factor.ordering=string taucs.maxdepth=number
+ * plus the additions
+ *   taucs.gpu.precision=fp64|mixed   (mixed: FP32 fronts + FP64 refinement)
+ *   taucs.gpu.refine.tol=number      (scaled residual target, default 1e-12)
+ *   taucs.gpu.refine.maxits=number   (default 10)
+ * Values may be written as "=#k" to take opt_arg[k].  Unknown options are
+ * reported through taucs_printf and ignored, as in the reference.  The LLT
+ * factor is always the multifrontal one here (taucs.factor.ll selects it too).
+ * All nrhs columns are solved together. */
+int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, void* B,
+                   char* options[], void* opt_arg[]);
+
+/* logging and timers (src/taucs_logging.c:32-80, src/taucs_timer.c:250-290) */
+void   taucs_logfile(char* file_prefix);
+int    taucs_printf(char* fmt, ...);
+double taucs_wtime(void);
+double taucs_ctime(void);
+
+/* ------------------------------------------------------------------ */
+/* B200 additions (no counterpart in the reference)                    */
+/* ------------------------------------------------------------------ */
+
+/* Stream used by the calling thread's subsequent taucs_* / taucs_b200_*
+ * calls (a cudaStream_t; NULL = the legacy default stream). */
+int taucs_b200_set_stream(void* cuda_stream);
+
+/* Numeric factorization from DEVICE values (nnz doubles in the order of the
+ * matrix the handle was analysed with).  Asynchronous on the current stream
+ * except for the final status read; returns 0 or -1 (nonpositive pivot). */
+int taucs_b200_factor_numeric_device(void* L, const double* d_values);
+
+/* Same as taucs_ccs_factor_llt_numeric but returns without the final status
+ * read: the status is read by the next call to taucs_b200_factor_status. */
+int taucs_b200_factor_numeric_device_async(void* L, const double* d_values);
+int taucs_b200_factor_status(void* L);
+
+/* nrhs right-hand sides, column-major n x nrhs with leading dimension ld, on
+ * the DEVICE, permuted order.  X may alias B. */
+int taucs_b200_solve_device(void* L, int nrhs, double* d_X, const double* d_B, int ld);
+
+/* nrhs right-hand sides in HOST memory (column-major, leading dimension n) */
+int taucs_b200_solve_many(void* L, int nrhs, double* X, const double* B);
+
+/* Precision of the numeric factor: 0 = FP64 fronts (default), 1 = FP32 fronts
+ * (diagonal scaling, FP32 POTRF, FP32-accumulated products) for use with
+ * taucs_b200_solve_refine. */
+int taucs_b200_set_precision(void* L, int precision);
+
+/* Iterative refinement: solves A x = b to scaled residual
+ * ||A x - b||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol with the factor
+ * in L (any precision) and an FP64 residual on the device.  A is the permuted
+ * matrix the factor was computed from.  Host vectors, nrhs columns.  Returns
+ * the number of refinement steps taken (>= 0), or -1 when the target was not
+ * reached within maxits; res_out (nrhs) receives the final scaled residuals. */
+int taucs_b200_solve_refine(void* L, taucs_ccs_matrix* A, int nrhs, double* X,
+                            const double* B, double tol, int maxits, double* res_out);
+
+/* Inspection of the symbolic factor, in the reference's own arrays (slots
+ * 0..n_sn-1, virtual root n_sn) -- used by the parity tests. */
+typedef struct {
+  int    n;
+  int    n_sn;           /* supernode slots, including emptied ones */
+  int    n_live;         /* supernodes with at least one column      */
+  int    n_levels;       /* height of the supernodal tree            */
+  long   struct_len;     /* sum of sn_up_size                        */
+  long   l_values;       /* sum of sn_size * sn_up_size (L doubles)  */
+  double flops;          /* the reference's relaxed flop count       */
+  double l_bytes;        /* device bytes of L panels                 */
+  double u_bytes;        /* device bytes of the update arena (peak)  */
+  double ea_bytes;       /* algorithmic extend-add + assembly bytes  */
+  double solve_bytes;    /* algorithmic bytes of one 1-RHS solve     */
+  int    max_front;      /* largest sn_up_size                       */
+  int    max_sn_size;    /* largest sn_size                          */
+} taucs_b200_info;
+
+int taucs_b200_factor_info(void* L, taucs_b200_info* info);
+int taucs_b200_export_symbolic(void* L, int* sn_size, int* sn_up_size,
+                               int* first_child, int* next_child,
+                               long* struct_ptr, int* struct_idx);
+/* numeric panels as f x s column-major per supernode, rows in sn_struct order
+ * (the reference's order), val_ptr[n_sn+1] offsets */
+int taucs_b200_export_values(void* L, long* val_ptr, double* vals);
+/* elimination tree of a permuted lower CCS matrix (parent[n], root = n) */
+int taucs_b200_etree(taucs_ccs_matrix* A, int* parent);
+
+/* 3D 7-point operator with per-edge conductances exp(sigma*N(0,1)) scaled
+ * by (ax, ay, az) on an X x Y x Z grid, Dirichlet boundary (boundary faces
+ * drawn the same way and added to the diagonal), seeded; lower CCS in the
+ * row order of taucs_ccs_generate_mesh3d.  Z == 0 gives the 2D 5-point
+ * analogue on X x Y. */
+taucs_ccs_matrix* taucs_b200_generate_lognormal(int X, int Y, int Z, double sigma,
+                                                double ax, double ay, double az,
+                                                unsigned long long seed);
+
+/* CUDA kernel launches issued by this library on the calling thread since
+ * the last reset (for launch accounting in benchmarks). */
+long taucs_b200_launch_count(int reset);
+
+/* last CUDA or internal error message of the calling thread ("" if none) */
+const char* taucs_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,510 @@
+// C ABI entry points of libtaucs_b200.so: the reference's factor / solve /
+// free / convert interface (src/taucs_sn_llt.c:2892-3241 generic dispatch,
+// :1979-2209 double instantiations, :2844-2885 solve, :803-1006 helpers) and
+// taucs_linsolve (src/taucs_linsolve.c:189-622), implemented over the device
+// plan and kernels.  There is no CPU numeric path: when CUDA is unavailable
+// the numeric functions fail with the reference's error returns.
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+
+#include "factor.h"
+
+namespace tb {
+
+static thread_local cudaStream_t g_stream = nullptr;
+cudaStream_t current_stream() { return g_stream; }
+
+static std::atomic<long> g_launches{0};
+void count_launch(long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+static bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return false;
+}
+
+template <class T>
+static bool dev_upload(T** dst, const T* src, size_t n, cudaStream_t st) {
+  if (n == 0) n = 1;
+  if (!cuda_ok(cudaMalloc((void**) dst, n * sizeof(T)), "cudaMalloc")) return false;
+  if (src) return cuda_ok(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+  return true;
+}
+
+int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
+  std::vector<int> small, big;
+  std::vector<Tile> tiles;
+  D->small_off.clear(); D->big_off.clear(); D->tile_off.clear();
+  for (const LevelPlan& LP : P.levels) {
+    D->small_off.push_back((int) small.size());
+    D->big_off.push_back((int) big.size());
+    D->tile_off.push_back((int) tiles.size());
+    small.insert(small.end(), LP.small_fronts.begin(), LP.small_fronts.end());
+    big.insert(big.end(), LP.big_fronts.begin(), LP.big_fronts.end());
+    tiles.insert(tiles.end(), LP.build_tiles.begin(), LP.build_tiles.end());
+  }
+  bool ok = dev_upload(&D->fronts, P.fronts.data(), P.fronts.size(), st)
+         && dev_upload(&D->children, P.children.data(), P.children.size(), st)
+         && dev_upload(&D->rows, P.rows.data(), P.rows.size(), st)
+         && dev_upload(&D->maps, P.maps.data(), P.maps.size(), st)
+         && dev_upload(&D->acol_ptr, P.acol_ptr.data(), P.acol_ptr.size(), st)
+         && dev_upload(&D->a_rows, P.a_rows.data(), P.a_rows.size(), st)
+         && dev_upload(&D->a_idx, P.a_idx.data(), P.a_idx.size(), st)
+         && dev_upload(&D->small_list, small.data(), small.size(), st)
+         && dev_upload(&D->big_list, big.data(), big.size(), st)
+         && dev_upload(&D->tiles, tiles.data(), tiles.size(), st);
+  if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "plan upload");
+  return ok ? 0 : -1;
+}
+
+void devplan_free(DevPlan* D) {
+  cudaFree(D->fronts); cudaFree(D->children); cudaFree(D->rows); cudaFree(D->maps);
+  cudaFree(D->acol_ptr); cudaFree(D->a_rows); cudaFree(D->a_idx);
+  cudaFree(D->small_list); cudaFree(D->big_list); cudaFree(D->tiles);
+  *D = DevPlan();
+}
+
+static void free_numeric(Factor* F) {
+  cudaFree(F->dL); F->dL = nullptr;
+  cudaFree(F->dU); F->dU = nullptr;
+  cudaFree(F->dL32); F->dL32 = nullptr;
+  cudaFree(F->dU32); F->dU32 = nullptr;
+  F->has_numeric = false;
+}
+
+static void free_device(Factor* F) {
+  free_numeric(F);
+  if (F->dev_ready) devplan_free(&F->dp);
+  cudaFree(F->dA); F->dA = nullptr;
+  cudaFree(F->dstatus); F->dstatus = nullptr;
+  cudaFree(F->dW); F->dW = nullptr;
+  cudaFree(F->dX); F->dX = nullptr;
+  cudaFree(F->dscale); F->dscale = nullptr;
+  cudaFree(F->dcolptr); F->dcolptr = nullptr;
+  cudaFree(F->drowind); F->drowind = nullptr;
+  if (F->hstatus) cudaFreeHost(F->hstatus);
+  F->hstatus = nullptr;
+  F->dev_ready = false;
+}
+
+// device plan and per-handle buffers, allocated on the first numeric call
+static int ensure_device(Factor* F) {
+  if (F->dev_ready) return 0;
+  int dev = 0;
+  if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) return -1;
+  cudaDeviceProp prop;
+  if (!cuda_ok(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties")) return -1;
+  if (prop.major < 10) {
+    set_error("this library is built for sm_100a (B200); the current device is not");
+    return -1;
+  }
+  F->device = dev;
+  cudaStream_t st = current_stream();
+  if (devplan_upload(F->plan, &F->dp, st)) { devplan_free(&F->dp); return -1; }
+  F->dev_ready = true;
+  const Plan& P = F->plan;
+  bool ok = dev_upload(&F->dA, (const double*) nullptr, (size_t) P.nnz, st)
+         && dev_upload(&F->dstatus, (const int*) nullptr, 1, st)
+         && dev_upload(&F->dW, (const double*) nullptr, (size_t) P.v_len * SOLVE_NRHS, st)
+         && dev_upload(&F->dX, (const double*) nullptr, (size_t) F->n * SOLVE_NRHS, st)
+         && dev_upload(&F->dcolptr, F->colptr.data(), F->colptr.size(), st)
+         && dev_upload(&F->drowind, F->rowind.data(), F->rowind.size(), st)
+         && cuda_ok(cudaMallocHost((void**) &F->hstatus, sizeof(int)), "cudaMallocHost");
+  if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "upload");
+  if (!ok) { free_device(F); return -1; }
+  return 0;
+}
+
+static bool pattern_matches(const Factor* F, const taucs_ccs_matrix* A) {
+  if (A->n != F->n) return false;
+  if (memcmp(A->colptr, F->colptr.data(), sizeof(int) * (F->n + 1))) return false;
+  return !memcmp(A->rowind, F->rowind.data(), sizeof(int) * (size_t) F->colptr[F->n]);
+}
+
+static bool check_matrix(const taucs_ccs_matrix* A, const char* who) {
+  if (!A) { set_error(std::string(who) + ": NULL matrix"); return false; }
+  if (!(A->flags & TAUCS_DOUBLE)) { set_error(std::string(who) + ": only TAUCS_DOUBLE matrices are supported"); return false; }
+  if (!(A->flags & (TAUCS_SYMMETRIC | TAUCS_HERMITIAN)) || !(A->flags & TAUCS_LOWER)) {
+    set_error(std::string(who) + ": the lower triangle of a symmetric matrix is required");
+    return false;
+  }
+  return true;
+}
+
+Factor* symbolic(taucs_ccs_matrix* A, int max_depth) {
+  if (!check_matrix(A, "taucs_ccs_factor_llt_symbolic")) return nullptr;
+  double wt = taucs_wtime();
+  Factor* F = new (std::nothrow) Factor();
+  if (!F) return nullptr;
+  F->n = A->n;
+  int rc = symbolic_analyze(A->n, A->colptr, A->rowind, max_depth, &F->sym);
+  if (rc != TAUCS_SUCCESS) { delete F; return nullptr; }
+  rc = build_plan(F->sym, A->n, A->colptr, A->rowind, &F->plan);
+  if (rc != TAUCS_SUCCESS) { delete F; return nullptr; }
+  F->colptr.assign(A->colptr, A->colptr + A->n + 1);
+  F->rowind.assign(A->rowind, A->rowind + A->colptr[A->n]);
+  tprintf("\t\tSymbolic Analysis            = % 10.3f seconds\n", taucs_wtime() - wt);
+  tprintf("\t\tRelaxed  Analysis of LL^T: %.2e flops, %d supernodes, %d levels\n", F->plan.flops,
+          F->plan.n_fronts, F->plan.n_levels);
+  return F;
+}
+
+int numeric_device(Factor* F, const double* d_vals, bool wait);
+
+int numeric_device(Factor* F, const double* d_vals, bool wait) {
+  if (ensure_device(F)) return -1;
+  cudaStream_t st = current_stream();
+  const Plan& P = F->plan;
+  if (!F->dL && !cuda_ok(cudaMalloc(&F->dL, sizeof(double) * (size_t) P.l_len), "cudaMalloc(L)")) return -1;
+  if (!F->dU && !cuda_ok(cudaMalloc(&F->dU, sizeof(double) * (size_t) P.u_len), "cudaMalloc(U)")) {
+    free_numeric(F);
+    return -1;
+  }
+  int e = launch_numeric_fp64(P, F->dp, d_vals, F->dL, F->dU, F->dstatus, st);
+  if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
+  if (!cuda_ok(cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st), "status")) return -1;
+  F->has_numeric = true;
+  if (!wait) return 0;
+  if (!cuda_ok(cudaStreamSynchronize(st), "numeric factorization")) return -1;
+  if (*F->hstatus != INT_MAX) {
+    tprintf("\t\tLL^T Factorization: Matrix is not positive definite.\n");
+    tprintf("\t\t                    nonpositive pivot in column %d\n", *F->hstatus);
+    free_numeric(F);
+    return -1;
+  }
+  return 0;
+}
+
+int numeric_host(Factor* F, taucs_ccs_matrix* A) {
+  if (!check_matrix(A, "taucs_ccs_factor_llt_numeric")) return -1;
+  if (!pattern_matches(F, A)) {
+    set_error("taucs_ccs_factor_llt_numeric: the matrix pattern differs from the analysed one");
+    return -1;
+  }
+  if (ensure_device(F)) return -1;
+  cudaStream_t st = current_stream();
+  double wt = taucs_wtime();
+  if (!cuda_ok(cudaMemcpyAsync(F->dA, A->values.d, sizeof(double) * (size_t) F->plan.nnz,
+                               cudaMemcpyHostToDevice, st), "values upload")) return -1;
+  int rc = numeric_device(F, F->dA, true);
+  tprintf("\t\tSupernodal Multifrontal LL^T = % 10.3f seconds\n", taucs_wtime() - wt);
+  return rc;
+}
+
+int solve_device(Factor* F, int nrhs, double* dX, const double* dB, int ld) {
+  if (!F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
+  cudaStream_t st = current_stream();
+  int e = launch_solve_fp64(F->plan, F->dp, F->dL, nrhs, dX, dB, ld, F->dW, nullptr, st);
+  return cuda_ok((cudaError_t) e, "solve launch") ? 0 : -1;
+}
+
+int solve_host(Factor* F, int nrhs, double* X, const double* B) {
+  if (!F || !F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
+  cudaStream_t st = current_stream();
+  const int n = F->n;
+  for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
+    const int nq = std::min(SOLVE_NRHS, nrhs - q0);
+    if (!cuda_ok(cudaMemcpyAsync(F->dX, B + (size_t) q0 * n, sizeof(double) * (size_t) n * nq,
+                                 cudaMemcpyHostToDevice, st), "rhs upload")) return -1;
+    if (solve_device(F, nq, F->dX, F->dX, n)) return -1;
+    if (!cuda_ok(cudaMemcpyAsync(X + (size_t) q0 * n, F->dX, sizeof(double) * (size_t) n * nq,
+                                 cudaMemcpyDeviceToHost, st), "solution download")) return -1;
+  }
+  return cuda_ok(cudaStreamSynchronize(st), "solve") ? 0 : -1;
+}
+
+// L panels in the reference's row order (f x s per slot, ld f)
+static int download_ref_panels(Factor* F, std::vector<long>& vptr, std::vector<double>& vals) {
+  if (!F->has_numeric) return -1;
+  const Plan& P = F->plan;
+  const Symbolic& S = F->sym;
+  std::vector<double> hL((size_t) P.l_len);
+  cudaStream_t st = current_stream();
+  if (!cuda_ok(cudaMemcpyAsync(hL.data(), F->dL, sizeof(double) * (size_t) P.l_len, cudaMemcpyDeviceToHost, st), "L download")) return -1;
+  if (!cuda_ok(cudaStreamSynchronize(st), "L download")) return -1;
+  vptr.assign(S.n_sn + 1, 0);
+  long tot = 0;
+  for (int sn = 0; sn < S.n_sn; sn++) { vptr[sn] = tot; tot += (long) S.sn_size[sn] * S.sn_up_size[sn]; }
+  vptr[S.n_sn] = tot;
+  vals.assign(std::max(tot, 1L), 0.0);
+  std::vector<int> local;
+  for (const FrontDesc& Fd : P.fronts) {
+    const int sn = Fd.sn, s = Fd.s, f = Fd.f;
+    const std::vector<int>& st_ = S.sn_struct[sn];
+    const int* rw = P.rows.data() + Fd.rows_off;
+    local.resize(f);
+    for (int k = 0; k < f; k++) local[k] = (int) (std::lower_bound(rw, rw + f, st_[k]) - rw);
+    const double* pan = hL.data() + Fd.l_off;
+    double* out = vals.data() + vptr[sn];
+    for (int jp = 0; jp < s; jp++) {
+      const int lj = local[jp];
+      for (int ip = jp; ip < f; ip++) {
+        const int li = local[ip];
+        out[(size_t) jp * f + ip] = (li >= lj) ? pan[li + (size_t) lj * f] : 0.0;
+      }
+    }
+  }
+  return 0;
+}
+
+static int order_identity(int n, int* p, int* ip) {
+  for (int i = 0; i < n; i++) p[i] = ip[i] = i;
+  return 0;
+}
+
+}  // namespace tb
+
+using namespace tb;
+
+extern "C" {
+
+int taucs_b200_set_stream(void* s) {
+  g_stream = (cudaStream_t) s;
+  return 0;
+}
+
+long taucs_b200_launch_count(int reset) {
+  return reset ? g_launches.exchange(0) : g_launches.load();
+}
+
+void* taucs_dccs_factor_llt_symbolic_maxdepth(taucs_ccs_matrix* A, int max_depth) {
+  return symbolic(A, max_depth);
+}
+void* taucs_dccs_factor_llt_symbolic(taucs_ccs_matrix* A) { return symbolic(A, 0); }
+void* taucs_ccs_factor_llt_symbolic_maxdepth(taucs_ccs_matrix* A, int max_depth) { return symbolic(A, max_depth); }
+void* taucs_ccs_factor_llt_symbolic(taucs_ccs_matrix* A) { return symbolic(A, 0); }
+
+int taucs_dccs_factor_llt_numeric(taucs_ccs_matrix* A, void* L) {
+  if (!L) return -1;
+  return numeric_host((Factor*) L, A);
+}
+int taucs_ccs_factor_llt_numeric(taucs_ccs_matrix* A, void* L) { return taucs_dccs_factor_llt_numeric(A, L); }
+
+void* taucs_dccs_factor_llt_mf_maxdepth(taucs_ccs_matrix* A, int max_depth) {
+  Factor* F = symbolic(A, max_depth);
+  if (!F) return nullptr;
+  if (numeric_host(F, A)) {
+    free_device(F);
+    delete F;
+    return nullptr;
+  }
+  return F;
+}
+void* taucs_dccs_factor_llt_mf(taucs_ccs_matrix* A) { return taucs_dccs_factor_llt_mf_maxdepth(A, 0); }
+void* taucs_ccs_factor_llt_mf_maxdepth(taucs_ccs_matrix* A, int max_depth) { return taucs_dccs_factor_llt_mf_maxdepth(A, max_depth); }
+void* taucs_ccs_factor_llt_mf(taucs_ccs_matrix* A) { return taucs_dccs_factor_llt_mf_maxdepth(A, 0); }
+
+int taucs_dsupernodal_solve_llt(void* L, void* x, void* b) {
+  if (!L || !x || !b) return -1;
+  return solve_host((Factor*) L, 1, (double*) x, (const double*) b);
+}
+int taucs_supernodal_solve_llt(void* L, void* x, void* b) { return taucs_dsupernodal_solve_llt(L, x, b); }
+
+int taucs_b200_solve_many(void* L, int nrhs, double* X, const double* B) {
+  if (!L || nrhs < 0) return -1;
+  if (nrhs == 0) return 0;
+  return solve_host((Factor*) L, nrhs, X, B);
+}
+
+int taucs_b200_factor_numeric_device(void* L, const double* d_values) {
+  if (!L) return -1;
+  return numeric_device((Factor*) L, d_values, true);
+}
+
+int taucs_b200_factor_numeric_device_async(void* L, const double* d_values) {
+  if (!L) return -1;
+  return numeric_device((Factor*) L, d_values, false);
+}
+
+int taucs_b200_factor_status(void* vL) {
+  Factor* F = (Factor*) vL;
+  if (!F || !F->has_numeric) return -1;
+  if (!cuda_ok(cudaStreamSynchronize(current_stream()), "status")) return -1;
+  if (*F->hstatus != INT_MAX) { free_numeric(F); return -1; }
+  return 0;
+}
+
+int taucs_b200_solve_device(void* L, int nrhs, double* d_X, const double* d_B, int ld) {
+  if (!L || nrhs < 0 || ld < ((Factor*) L)->n) return -1;
+  if (nrhs == 0) return 0;
+  return solve_device((Factor*) L, nrhs, d_X, d_B, ld);
+}
+
+void taucs_dsupernodal_factor_free(void* L) {
+  Factor* F = (Factor*) L;
+  if (!F) return;
+  free_device(F);
+  delete F;
+}
+void taucs_supernodal_factor_free(void* L) { taucs_dsupernodal_factor_free(L); }
+
+void taucs_dsupernodal_factor_free_numeric(void* L) {
+  if (L) free_numeric((Factor*) L);
+}
+void taucs_supernodal_factor_free_numeric(void* L) { taucs_dsupernodal_factor_free_numeric(L); }
+
+taucs_ccs_matrix* taucs_dsupernodal_factor_to_ccs(void* vL) {
+  Factor* F = (Factor*) vL;
+  if (!F) return nullptr;
+  std::vector<long> vp;
+  std::vector<double> v;
+  if (download_ref_panels(F, vp, v)) return nullptr;
+  const Symbolic& S = F->sym;
+  const int n = F->n;
+  // same traversal and zero dropping as src/taucs_sn_llt.c:851-978
+  std::vector<int> len(n, 0);
+  long nnz = 0;
+  for (int sn = 0; sn < S.n_sn; sn++) {
+    const int s = S.sn_size[sn], f = S.sn_up_size[sn];
+    const double* pan = v.data() + vp[sn];
+    for (int jp = 0; jp < s; jp++) {
+      int j = S.sn_struct[sn][jp];
+      for (int ip = jp; ip < f; ip++)
+        if (pan[(size_t) jp * f + ip] != 0.0) { len[j]++; nnz++; }
+    }
+  }
+  taucs_ccs_matrix* C = taucs_ccs_create(n, n, (int) nnz, TAUCS_DOUBLE | TAUCS_TRIANGULAR | TAUCS_LOWER);
+  if (!C) return nullptr;
+  C->colptr[0] = 0;
+  for (int j = 0; j < n; j++) C->colptr[j + 1] = C->colptr[j] + len[j];
+  for (int sn = 0; sn < S.n_sn; sn++) {
+    const int s = S.sn_size[sn], f = S.sn_up_size[sn];
+    const double* pan = v.data() + vp[sn];
+    for (int jp = 0; jp < s; jp++) {
+      int j = S.sn_struct[sn][jp];
+      int next = C->colptr[j];
+      for (int ip = jp; ip < f; ip++) {
+        const double x = pan[(size_t) jp * f + ip];
+        if (x == 0.0) continue;
+        C->rowind[next] = S.sn_struct[sn][ip];
+        C->values.d[next] = x;
+        next++;
+      }
+    }
+  }
+  return C;
+}
+taucs_ccs_matrix* taucs_supernodal_factor_to_ccs(void* L) { return taucs_dsupernodal_factor_to_ccs(L); }
+
+double* taucs_dsupernodal_factor_get_diag(void* vL) {
+  Factor* F = (Factor*) vL;
+  if (!F || !F->has_numeric) return nullptr;
+  const Plan& P = F->plan;
+  double* diag = (double*) malloc(sizeof(double) * (size_t) std::max(F->n, 1));
+  if (!diag) return nullptr;
+  cudaStream_t st = current_stream();
+  // one strided copy per front: the diagonal of the panel has stride f+1
+  for (const FrontDesc& Fd : P.fronts) {
+    const int* rw = P.rows.data() + Fd.rows_off;
+    std::vector<double> d(Fd.s);
+    if (!cuda_ok(cudaMemcpy2DAsync(d.data(), sizeof(double), F->dL + Fd.l_off, sizeof(double) * (Fd.f + 1),
+                                   sizeof(double), Fd.s, cudaMemcpyDeviceToHost, st), "diag")) {
+      free(diag);
+      return nullptr;
+    }
+    cudaStreamSynchronize(st);
+    for (int c = 0; c < Fd.s; c++) diag[rw[c]] = d[c];
+  }
+  return diag;
+}
+void* taucs_supernodal_factor_get_diag(void* L) { return taucs_dsupernodal_factor_get_diag(L); }
+
+int taucs_b200_factor_info(void* vL, taucs_b200_info* info) {
+  Factor* F = (Factor*) vL;
+  if (!F || !info) return -1;
+  const Plan& P = F->plan;
+  const Symbolic& S = F->sym;
+  info->n = F->n;
+  info->n_sn = S.n_sn;
+  info->n_live = P.n_fronts;
+  info->n_levels = P.n_levels;
+  long sl = 0, lv = 0;
+  for (int sn = 0; sn < S.n_sn; sn++) { sl += S.sn_up_size[sn]; lv += (long) S.sn_size[sn] * S.sn_up_size[sn]; }
+  info->struct_len = sl;
+  info->l_values = lv;
+  info->flops = P.flops;
+  info->l_bytes = 8.0 * (double) P.l_len;
+  info->u_bytes = 8.0 * (double) P.u_len;
+  info->ea_bytes = P.ea_bytes;
+  info->solve_bytes = P.solve_bytes;
+  info->max_front = P.max_front;
+  info->max_sn_size = P.max_s;
+  return 0;
+}
+
+int taucs_b200_export_symbolic(void* vL, int* sn_size, int* sn_up_size, int* first_child, int* next_child,
+                               long* struct_ptr, int* struct_idx) {
+  Factor* F = (Factor*) vL;
+  if (!F) return -1;
+  const Symbolic& S = F->sym;
+  long p = 0;
+  for (int sn = 0; sn < S.n_sn; sn++) {
+    sn_size[sn] = S.sn_size[sn];
+    sn_up_size[sn] = S.sn_up_size[sn];
+  }
+  for (int sn = 0; sn <= S.n_sn; sn++) {
+    first_child[sn] = S.first_child[sn];
+    next_child[sn] = S.next_child[sn];
+  }
+  for (int sn = 0; sn < S.n_sn; sn++) {
+    struct_ptr[sn] = p;
+    for (int k = 0; k < S.sn_up_size[sn]; k++) struct_idx[p + k] = S.sn_struct[sn][k];
+    p += S.sn_up_size[sn];
+  }
+  struct_ptr[S.n_sn] = p;
+  return 0;
+}
+
+int taucs_b200_export_values(void* vL, long* val_ptr, double* vals) {
+  Factor* F = (Factor*) vL;
+  if (!F) return -1;
+  std::vector<long> vp;
+  std::vector<double> v;
+  if (download_ref_panels(F, vp, v)) return -1;
+  std::copy(vp.begin(), vp.end(), val_ptr);
+  std::copy(v.begin(), v.begin() + vp.back(), vals);
+  return 0;
+}
+
+int taucs_b200_etree(taucs_ccs_matrix* A, int* parent) {
+  if (!A || !parent) return -1;
+  return etree(A->n, A->colptr, A->rowind, parent);
+}
+
+void taucs_ccs_order(taucs_ccs_matrix* A, int** perm, int** invperm, char* which) {
+  *perm = *invperm = nullptr;
+  if (!A || !which) return;
+  const int n = A->n;
+  int* p = (int*) malloc(sizeof(int) * (size_t) std::max(n, 1));
+  int* ip = (int*) malloc(sizeof(int) * (size_t) std::max(n, 1));
+  if (!p || !ip) { free(p); free(ip); return; }
+  int rc = -1;
+  if (!strcmp(which, "identity")) {
+    rc = order_identity(n, p, ip);
+  } else if (!strcmp(which, "random")) {
+    std::mt19937 gen(12345u);
+    for (int i = 0; i < n; i++) p[i] = i;
+    std::shuffle(p, p + n, gen);
+    for (int i = 0; i < n; i++) ip[p[i]] = i;
+    rc = 0;
+  } else if (!strcmp(which, "amd")) {
+    if (!(A->flags & (TAUCS_SYMMETRIC | TAUCS_HERMITIAN)) || !(A->flags & TAUCS_LOWER)) {
+      tprintf("taucs_ccs_amd: the lower part of a symmetric matrix must be represented.\n");
+    } else {
+      rc = amd_order(n, A->colptr, A->rowind, p, ip);
+    }
+  } else {
+    tprintf("taucs_ccs_order: ordering %s is not available in this build\n", which);
+  }
+  if (rc) { free(p); free(ip); return; }
+  *perm = p;
+  *invperm = ip;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// Internal declarations shared by the host and device translation units of
+// libtaucs_b200.so.  Nothing here is part of the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "taucs_b200.h"
+
+namespace tb {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+const char* last_error();
+int tprintf(const char* fmt, ...);
+
+// --------------------------------------------------------------- symbolic
+// The supernodal structure exactly as the reference's symbolic phase leaves
+// it (src/taucs_sn_llt.c:3663-4001): n_sn slots, slot n_sn is the virtual
+// root, emptied slots have sn_size == 0.
+struct Symbolic {
+  int n = 0;
+  int n_sn = 0;
+  std::vector<int> sn_size;        // n_sn
+  std::vector<int> sn_up_size;     // n_sn
+  std::vector<int> first_child;    // n_sn + 1
+  std::vector<int> next_child;     // n_sn + 1
+  std::vector<std::vector<int>> sn_struct;  // n_sn (reference row order)
+};
+
+// etree of a permuted lower CCS pattern: parent[j], root = n
+int etree(int n, const int* colptr, const int* rowind, int* parent);
+// full symbolic phase; returns TAUCS_SUCCESS, TAUCS_ERROR_MAXDEPTH or
+// TAUCS_ERROR_NOMEM
+int symbolic_analyze(int n, const int* colptr, const int* rowind, int max_depth,
+                     Symbolic* out);
+
+// ------------------------------------------------------------ AMD ordering
+int amd_order(int n, const int* colptr, const int* rowind, int* perm, int* invperm);
+
+// ------------------------------------------------------------------- plan
+// Front-build tile: rows [r0, r0+TILE_R) x columns [c0, c0+TILE_C) of the
+// lower part of one front.
+// c0 >= 0: panel region (front-local rows r0.., columns c0..);
+// c0 < 0: update-matrix region, U-local rows r0.., columns -1-c0..
+struct Tile {
+  int front;   // device-order front index
+  int r0, c0;
+};
+
+// Dense-kernel tile for the blocked partial factorization and the update
+// of U (see numeric.cu).
+struct GemmTile {
+  int front;
+  int i0, j0;
+};
+
+// One supernode in device order.
+struct FrontDesc {
+  int64_t l_off;      // panel offset (doubles) in the L arena; panel f x s, ld f
+  int64_t u_off;      // update matrix offset in the U arena; m x m, ld m (-1 if m == 0)
+  int64_t v_off;      // update-vector offset for the solve (m * nrhs_max)
+  int s, f;           // columns, front order (m = f - s)
+  int child_begin;    // range in child list
+  int child_end;
+  int rows_off;       // offset of the sorted global row list (f entries)
+  int map_off;        // offset of this front's map into its parent (m entries)
+  int acol_off;       // offset into the A-column pointer table (s + 1 entries)
+  int level;
+  int parent;         // device-order parent index, -1 for roots
+  int sn;             // reference slot
+};
+
+struct LevelPlan {
+  int front_begin, front_end;      // fronts of this level (device order)
+  // small fronts, fused kernel
+  std::vector<int> small_fronts;
+  // medium/large fronts
+  std::vector<int> big_fronts;
+  std::vector<Tile> build_tiles;
+  int max_s_big = 0;               // largest s among big fronts
+  int max_m_big = 0;
+};
+
+struct Plan {
+  int n = 0;
+  int n_fronts = 0;
+  int n_levels = 0;
+  int64_t l_len = 0;               // doubles in L arena
+  int64_t u_len = 0;               // doubles in U arena (peak of planned lifetimes)
+  int64_t v_len = 0;               // doubles of per-front update vectors (1 rhs)
+  int64_t nnz = 0;
+  std::vector<FrontDesc> fronts;
+  std::vector<int> children;       // device-order child indices
+  std::vector<int> rows;           // per front: f sorted global rows
+  std::vector<int> maps;           // per non-root front: m parent-local indices
+  std::vector<int> acol_ptr;       // per front: s+1 offsets into a_rows/a_idx
+  std::vector<int> a_rows;         // local row of each A entry
+  std::vector<int> a_idx;          // index of that entry in A's value array
+  std::vector<LevelPlan> levels;
+  double flops = 0.0;
+  double ea_bytes = 0.0;
+  double solve_bytes = 0.0;
+  int max_front = 0, max_s = 0;
+};
+
+int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, Plan* P);
+
+}  // namespace tb

@@ -1,0 +1,63 @@
+// Tunables and host-side launchers of the device kernels.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace tb {
+
+// fronts of order <= SMALL_F_MAX are built and factored entirely in shared
+// memory by one CTA (k_small_front); larger ones go through the tiled path
+constexpr int SMALL_F_MAX = 96;
+// front-build tile (rows x columns of one front held in shared memory)
+constexpr int BUILD_TR = 64;
+constexpr int BUILD_TC = 32;
+// block column width of the blocked partial Cholesky of large fronts
+constexpr int PANEL_NB = 64;
+// rows per CTA of the panel POTRF+TRSM kernel
+constexpr int TRSM_ROWS = 64;
+// GEMM tile of the trailing / update-matrix kernels
+constexpr int GEMM_BM = 64;
+constexpr int GEMM_BN = 64;
+constexpr int GEMM_BK = 16;
+// right-hand sides handled per solve pass
+constexpr int SOLVE_NRHS = 8;
+
+// Device copies of the plan arrays.
+struct DevPlan {
+  FrontDesc* fronts = nullptr;
+  int* children = nullptr;
+  int* rows = nullptr;
+  int* maps = nullptr;
+  int* acol_ptr = nullptr;
+  int* a_rows = nullptr;
+  int* a_idx = nullptr;
+  int* small_list = nullptr;   // all levels, concatenated
+  int* big_list = nullptr;
+  Tile* tiles = nullptr;
+  std::vector<int> small_off, big_off, tile_off;  // per level (host)
+  std::vector<int> lvl_max_f_small;               // per level (host)
+};
+
+int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st);
+void devplan_free(DevPlan* D);
+
+// numeric factorization over all levels; vals = A's values (device);
+// status (device int) receives the smallest failing global column, or
+// INT_MAX; returns a cudaError_t code
+int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L,
+                        double* U, int* status, cudaStream_t st);
+
+// multi-RHS solve, device vectors in permuted order: X (n x nrhs, ld) from
+// B (n x nrhs, ld); W scratch of P.v_len * SOLVE_NRHS doubles, Y n *
+// SOLVE_NRHS doubles
+int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
+                      const double* B, int ld, double* W, double* Y, cudaStream_t st);
+
+// launch accounting
+void count_launch(long k = 1);
+
+}  // namespace tb
