@@ -228,6 +228,22 @@ taucs_ccs_matrix* taucs_b200_generate_lognormal(int X, int Y, int Z, double sigm
                                                 double ax, double ay, double az,
                                                 unsigned long long seed);
 
+/* Device timing per kernel class, for benchmarks (off by default).  When
+ * enabled, every launch of the library's kernels is bracketed by CUDA events
+ * on its stream, and the algorithmic flops and bytes of the launch are
+ * recorded.  Enabling or disabling clears the totals. */
+#define TAUCS_B200_KC_SMALL_FRONT 0
+#define TAUCS_B200_KC_BUILD       1
+#define TAUCS_B200_KC_POTRF       2
+#define TAUCS_B200_KC_TRSM        3
+#define TAUCS_B200_KC_GEMM_PANEL  4
+#define TAUCS_B200_KC_GEMM_U      5
+#define TAUCS_B200_KC_SOLVE_FWD   6
+#define TAUCS_B200_KC_SOLVE_BWD   7
+#define TAUCS_B200_KC_OTHER       8
+int taucs_b200_profile(int enable);
+int taucs_b200_profile_read(int kernel_class, double* ms, long* launches, double* flops, double* bytes);
+
 /* CUDA kernel launches issued by this library on the calling thread since
  * the last reset (for launch accounting in benchmarks). */
 long taucs_b200_launch_count(int reset);

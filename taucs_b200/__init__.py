@@ -106,6 +106,9 @@ def lib():
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
         "taucs_b200_etree": (C.c_int, [pc, _i32p]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
+        "taucs_b200_profile": (C.c_int, [C.c_int]),
+        "taucs_b200_profile_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long),
+                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "taucs_b200_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -224,7 +227,10 @@ class Factor:
         self.h = C.c_void_p(handle)
 
     def __del__(self):
-        self.free()
+        try:
+            self.free()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
 
     def free(self):
         if getattr(self, "h", None) and self.h.value:

@@ -40,14 +40,19 @@ static bool dev_upload(T** dst, const T* src, size_t n, cudaStream_t st) {
 int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
   std::vector<int> small, big;
   std::vector<Tile> tiles;
-  D->small_off.clear(); D->big_off.clear(); D->tile_off.clear();
+  std::vector<int2_> sf, sb;
+  D->small_off.clear(); D->big_off.clear(); D->tile_off.clear(); D->sfwd_off.clear(); D->sbwd_off.clear();
   for (const LevelPlan& LP : P.levels) {
     D->small_off.push_back((int) small.size());
     D->big_off.push_back((int) big.size());
     D->tile_off.push_back((int) tiles.size());
+    D->sfwd_off.push_back((int) sf.size());
+    D->sbwd_off.push_back((int) sb.size());
     small.insert(small.end(), LP.small_fronts.begin(), LP.small_fronts.end());
     big.insert(big.end(), LP.big_fronts.begin(), LP.big_fronts.end());
     tiles.insert(tiles.end(), LP.build_tiles.begin(), LP.build_tiles.end());
+    sf.insert(sf.end(), LP.solve_fwd_blocks.begin(), LP.solve_fwd_blocks.end());
+    sb.insert(sb.end(), LP.solve_bwd_blocks.begin(), LP.solve_bwd_blocks.end());
   }
   bool ok = dev_upload(&D->fronts, P.fronts.data(), P.fronts.size(), st)
          && dev_upload(&D->children, P.children.data(), P.children.size(), st)
@@ -58,7 +63,9 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
          && dev_upload(&D->a_idx, P.a_idx.data(), P.a_idx.size(), st)
          && dev_upload(&D->small_list, small.data(), small.size(), st)
          && dev_upload(&D->big_list, big.data(), big.size(), st)
-         && dev_upload(&D->tiles, tiles.data(), tiles.size(), st);
+         && dev_upload(&D->tiles, tiles.data(), tiles.size(), st)
+         && dev_upload(&D->sfwd, sf.data(), sf.size(), st)
+         && dev_upload(&D->sbwd, sb.data(), sb.size(), st);
   if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "plan upload");
   return ok ? 0 : -1;
 }
@@ -67,12 +74,14 @@ void devplan_free(DevPlan* D) {
   cudaFree(D->fronts); cudaFree(D->children); cudaFree(D->rows); cudaFree(D->maps);
   cudaFree(D->acol_ptr); cudaFree(D->a_rows); cudaFree(D->a_idx);
   cudaFree(D->small_list); cudaFree(D->big_list); cudaFree(D->tiles);
+  cudaFree(D->sfwd); cudaFree(D->sbwd);
   *D = DevPlan();
 }
 
 static void free_numeric(Factor* F) {
   cudaFree(F->dL); F->dL = nullptr;
   cudaFree(F->dU); F->dU = nullptr;
+  cudaFree(F->dDinv); F->dDinv = nullptr;
   cudaFree(F->dL32); F->dL32 = nullptr;
   cudaFree(F->dU32); F->dU32 = nullptr;
   F->has_numeric = false;
@@ -88,6 +97,7 @@ static void free_device(Factor* F) {
   cudaFree(F->dscale); F->dscale = nullptr;
   cudaFree(F->dcolptr); F->dcolptr = nullptr;
   cudaFree(F->drowind); F->drowind = nullptr;
+  cudaFree(F->dflags); F->dflags = nullptr;
   if (F->hstatus) cudaFreeHost(F->hstatus);
   F->hstatus = nullptr;
   F->dev_ready = false;
@@ -110,12 +120,14 @@ static int ensure_device(Factor* F) {
   F->dev_ready = true;
   const Plan& P = F->plan;
   bool ok = dev_upload(&F->dA, (const double*) nullptr, (size_t) P.nnz, st)
-         && dev_upload(&F->dstatus, (const int*) nullptr, 1, st)
+         && dev_upload(&F->dstatus, (const int*) nullptr, 2, st)
+         && dev_upload(&F->dflags, (const int*) nullptr, (size_t) P.n_blk, st)
+         && cuda_ok(cudaMemsetAsync(F->dflags, 0, sizeof(int) * (size_t) P.n_blk, st), "flags")
          && dev_upload(&F->dW, (const double*) nullptr, (size_t) P.v_len * SOLVE_NRHS, st)
          && dev_upload(&F->dX, (const double*) nullptr, (size_t) F->n * SOLVE_NRHS, st)
          && dev_upload(&F->dcolptr, F->colptr.data(), F->colptr.size(), st)
          && dev_upload(&F->drowind, F->rowind.data(), F->rowind.size(), st)
-         && cuda_ok(cudaMallocHost((void**) &F->hstatus, sizeof(int)), "cudaMallocHost");
+         && cuda_ok(cudaMallocHost((void**) &F->hstatus, 2 * sizeof(int)), "cudaMallocHost");
   if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "upload");
   if (!ok) { free_device(F); return -1; }
   return 0;
@@ -166,7 +178,11 @@ int numeric_device(Factor* F, const double* d_vals, bool wait) {
     free_numeric(F);
     return -1;
   }
-  int e = launch_numeric_fp64(P, F->dp, d_vals, F->dL, F->dU, F->dstatus, st);
+  if (!F->dDinv && !cuda_ok(cudaMalloc(&F->dDinv, sizeof(double) * (size_t) P.dinv_len), "cudaMalloc(Dinv)")) {
+    free_numeric(F);
+    return -1;
+  }
+  int e = launch_numeric_fp64(P, F->dp, d_vals, F->dL, F->dU, F->dDinv, F->dstatus, st);
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   if (!cuda_ok(cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st), "status")) return -1;
   F->has_numeric = true;
@@ -200,8 +216,22 @@ int numeric_host(Factor* F, taucs_ccs_matrix* A) {
 int solve_device(Factor* F, int nrhs, double* dX, const double* dB, int ld) {
   if (!F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
   cudaStream_t st = current_stream();
-  int e = launch_solve_fp64(F->plan, F->dp, F->dL, nrhs, dX, dB, ld, F->dW, nullptr, st);
+  if (!cuda_ok(cudaMemsetAsync(F->dstatus + 1, 0, sizeof(int), st), "solve status")) return -1;
+  int e = launch_solve_fp64(F->plan, F->dp, F->dL, nrhs, dX, dB, ld, F->dW, F->dflags, &F->epoch,
+                            F->dstatus + 1, st);
   return cuda_ok((cudaError_t) e, "solve launch") ? 0 : -1;
+}
+
+// reads the solve status word after the stream has drained
+static int solve_status(Factor* F, cudaStream_t st) {
+  if (!cuda_ok(cudaMemcpyAsync(F->hstatus + 1, F->dstatus + 1, sizeof(int), cudaMemcpyDeviceToHost, st), "status"))
+    return -1;
+  if (!cuda_ok(cudaStreamSynchronize(st), "solve")) return -1;
+  if (F->hstatus[1] != 0) {
+    set_error("solve: a bounded wait between thread blocks timed out");
+    return -1;
+  }
+  return 0;
 }
 
 int solve_host(Factor* F, int nrhs, double* X, const double* B) {
@@ -216,7 +246,7 @@ int solve_host(Factor* F, int nrhs, double* X, const double* B) {
     if (!cuda_ok(cudaMemcpyAsync(X + (size_t) q0 * n, F->dX, sizeof(double) * (size_t) n * nq,
                                  cudaMemcpyDeviceToHost, st), "solution download")) return -1;
   }
-  return cuda_ok(cudaStreamSynchronize(st), "solve") ? 0 : -1;
+  return solve_status(F, st);
 }
 
 // L panels in the reference's row order (f x s per slot, ld f)

@@ -25,7 +25,10 @@ struct Factor {
   int* dstatus = nullptr;
   double* dW = nullptr;        // solve work vectors (v_len * SOLVE_NRHS)
   double* dX = nullptr;        // solve staging (n * SOLVE_NRHS)
-  int* hstatus = nullptr;      // pinned status readback
+  int* hstatus = nullptr;      // pinned status readback (2 ints: factor, solve)
+  double* dDinv = nullptr;     // inverses of the big fronts' 64x64 diagonal blocks
+  int* dflags = nullptr;       // solve handshake flags (plan.n_blk)
+  int epoch = 0;               // last epoch written into dflags
   bool has_numeric = false;
   int precision = 0;           // 0 FP64, 1 FP32 fronts
 

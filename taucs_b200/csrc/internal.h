@@ -49,6 +49,10 @@ struct Tile {
   int r0, c0;
 };
 
+struct int2_ {
+  int a, b;
+};
+
 // Dense-kernel tile for the blocked partial factorization and the update
 // of U (see numeric.cu).
 struct GemmTile {
@@ -60,7 +64,10 @@ struct GemmTile {
 struct FrontDesc {
   int64_t l_off;      // panel offset (doubles) in the L arena; panel f x s, ld f
   int64_t u_off;      // update matrix offset in the U arena; m x m, ld m (-1 if m == 0)
-  int64_t v_off;      // update-vector offset for the solve (m * nrhs_max)
+  int64_t v_off;      // solve work-vector offset (f entries per right-hand side)
+  int64_t dinv_off;   // inverses of the 64x64 diagonal blocks (big fronts), -1 otherwise
+  int blk_off;        // solve flags: first of ceil(s/64) per big front, -1 otherwise
+  int pad_;
   int s, f;           // columns, front order (m = f - s)
   int child_begin;    // range in child list
   int child_end;
@@ -74,6 +81,9 @@ struct FrontDesc {
 
 struct LevelPlan {
   int front_begin, front_end;      // fronts of this level (device order)
+  // solve: big fronts are split into 64-row blocks, one CTA each
+  std::vector<int2_> solve_fwd_blocks;   // (front, row block)
+  std::vector<int2_> solve_bwd_blocks;   // (front, column block), last block first
   // small fronts, fused kernel
   std::vector<int> small_fronts;
   // medium/large fronts
@@ -89,7 +99,9 @@ struct Plan {
   int n_levels = 0;
   int64_t l_len = 0;               // doubles in L arena
   int64_t u_len = 0;               // doubles in U arena (peak of planned lifetimes)
-  int64_t v_len = 0;               // doubles of per-front update vectors (1 rhs)
+  int64_t v_len = 0;               // doubles of per-front work vectors (1 rhs)
+  int64_t dinv_len = 0;            // doubles of diagonal-block inverses
+  int n_blk = 0;                   // solve flags
   int64_t nnz = 0;
   std::vector<FrontDesc> fronts;
   std::vector<int> children;       // device-order child indices

@@ -38,7 +38,9 @@ struct DevPlan {
   int* small_list = nullptr;   // all levels, concatenated
   int* big_list = nullptr;
   Tile* tiles = nullptr;
-  std::vector<int> small_off, big_off, tile_off;  // per level (host)
+  int2_* sfwd = nullptr;       // solve blocks, all levels concatenated
+  int2_* sbwd = nullptr;
+  std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off;  // per level (host)
   std::vector<int> lvl_max_f_small;               // per level (host)
 };
 
@@ -49,15 +51,29 @@ void devplan_free(DevPlan* D);
 // status (device int) receives the smallest failing global column, or
 // INT_MAX; returns a cudaError_t code
 int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L,
-                        double* U, int* status, cudaStream_t st);
+                        double* U, double* Dinv, int* status, cudaStream_t st);
 
 // multi-RHS solve, device vectors in permuted order: X (n x nrhs, ld) from
 // B (n x nrhs, ld); W scratch of P.v_len * SOLVE_NRHS doubles, Y n *
 // SOLVE_NRHS doubles
+// flags (P.n_blk ints) carry release/acquire handshakes between the CTAs of
+// a big front; epoch must differ from every value they hold; status gets
+// SOLVE_TIMEOUT if a bounded wait gave up
+constexpr int SOLVE_TIMEOUT = -2;
 int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
-                      const double* B, int ld, double* W, double* Y, cudaStream_t st);
+                      const double* B, int ld, double* W, int* flags, int* epoch, int* status,
+                      cudaStream_t st);
 
 // launch accounting
 void count_launch(long k = 1);
+
+// Optional per-kernel-class timing: when enabled, launchers bracket every
+// launch of a class with CUDA events on the launch stream and record the
+// algorithmic flops and bytes of that launch.
+enum KernelClass { KC_SMALL = 0, KC_BUILD, KC_POTRF, KC_TRSM, KC_GEMM_PANEL, KC_GEMM_U, KC_SOLVE_FWD,
+                   KC_SOLVE_BWD, KC_OTHER, KC_COUNT };
+bool prof_enabled();
+void prof_begin(int kc, cudaStream_t st);
+void prof_end(int kc, cudaStream_t st, double flops, double bytes);
 
 }  // namespace tb

@@ -16,8 +16,10 @@
 //                   matrices into shared memory in a fixed child order
 //                   (deterministic, no atomics) and writes the tile once;
 //   k_potrf_diag    blocked partial Cholesky, step kb: one CTA per front
-//                   factors the 64x64 diagonal block in place;
-//   k_trsm          then one CTA per 64-row slab below it solves X L_kk^-T;
+//                   factors the 64x64 diagonal block in place and forms its
+//                   inverse;
+//   k_trsm          then one CTA per 64-row slab below it computes
+//                   X L_kk^-T = X Dinv^T on DMMA;
 //   k_gemm          C -= A B^T on DMMA (mma.sync m16n8k8 f64) tiles: the
 //                   trailing update of the panel after each step, and the
 //                   update matrix U -= L21 L21^T with k = s at the end.
@@ -182,41 +184,145 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
 
 // ------------------------------------------------------- blocked POTRF+TRSM
 
-constexpr int XLD = PANEL_NB + 1;  // padded row stride of the TRSM slab
 constexpr int DLD = PANEL_NB + 1;  // padded column stride of the diagonal block
+constexpr size_t POTRF_SMEM = (2 * PANEL_NB * DLD + 32 * 33) * sizeof(double);
 
-// step kb, one CTA per front: factor the w x w diagonal block in place
-__global__ void __launch_bounds__(256)
+// Lower Cholesky of an n x n (n <= 32) block held in shared memory (ld `ld`),
+// by one warp: lane i keeps row i in registers and the right-looking updates
+// exchange L[k][j] with shuffles.  Returns the first nonpositive pivot (or -1)
+// in every lane.
+__device__ int warp_potrf32(double* S, int ld, int n) {
+  const int lane = threadIdx.x & 31;
+  double a[32];
+#pragma unroll
+  for (int k = 0; k < 32; k++) a[k] = (lane < n && k <= lane) ? S[lane + k * ld] : 0.0;
+  int bad = -1;
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    if (j < n) {
+      const double d = __shfl_sync(0xffffffffu, a[j], j);
+      if (!(d > 0.0) && bad < 0) bad = j;
+      const double ljj = sqrt(d);
+      if (lane == j) a[j] = ljj;
+      else if (lane > j) a[j] /= ljj;
+#pragma unroll
+      for (int k = j + 1; k < 32; k++) {
+        const double lkj = __shfl_sync(0xffffffffu, a[j], k);
+        if (lane >= k) a[k] -= a[j] * lkj;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 32; k++)
+    if (lane < n && k <= lane) S[lane + k * ld] = a[k];
+  return bad;
+}
+
+// Inverse of an n x n (n <= 32) lower-triangular block by one warp: lane t
+// computes column t by forward substitution (L read as broadcasts).
+__device__ void warp_trinv32(const double* S, int ld, double* X, int ldx, int n) {
+  const int t = threadIdx.x & 31;
+  double x[32];
+#pragma unroll
+  for (int i = 0; i < 32; i++) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; k++) acc += S[i + k * ld] * x[k];
+    x[i] = (i < n) ? (((i == t) ? 1.0 : 0.0) - acc) / S[i + i * ld] : 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < 32; i++) X[i + t * ldx] = (t < n) ? x[i] : 0.0;
+}
+
+// Step kb, one CTA per front: factor the w x w diagonal block in place as a
+// 2 x 2 recursion over 32-blocks (warp-level POTRF of the diagonal blocks,
+// inverse-based TRSM and the SYRK update in between) and store the inverse of
+// the factored block (lower, ld PANEL_NB) for the TRSM of the rows below.
+__global__ void __launch_bounds__(128)
 k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-             const int* __restrict__ rows, double* __restrict__ L, int kb, int* status) {
-  __shared__ double D[PANEL_NB * DLD];
+             const int* __restrict__ rows, double* __restrict__ L, double* __restrict__ Dinv, int kb,
+             int* status) {
+  extern __shared__ double sm[];
+  double* D = sm;                        // the block, col-major, ld DLD
+  double* X = sm + PANEL_NB * DLD;       // its inverse
+  double* T = X + PANEL_NB * DLD;        // 32 x 33 scratch
+  __shared__ int bad;
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   if (kb >= s) return;
   const int w = min(PANEL_NB, s - kb);
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int w1 = min(32, w), w2 = w - w1;
+  const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5;
   double* P = L + F.l_off;
-  for (int k = tid; k < w * w; k += nt) {
-    const int i = k % w, j = k / w;
-    if (i >= j) D[i + j * DLD] = P[(kb + i) + (size_t) (kb + j) * f];
+  for (int k = tid; k < PANEL_NB * PANEL_NB; k += nt) {
+    const int i = k % PANEL_NB, j = k / PANEL_NB;
+    D[i + j * DLD] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : 0.0;
+    X[i + j * DLD] = 0.0;
+  }
+  if (tid == 0) bad = -1;
+  __syncthreads();
+  if (warp == 0) {
+    const int b = warp_potrf32(D, DLD, w1);
+    if (b < 0) warp_trinv32(D, DLD, X, DLD, w1);
+    if ((tid & 31) == 0) bad = b;
   }
   __syncthreads();
-  for (int j = 0; j < w; j++) {
-    const double d = D[j + j * DLD];
-    if (!(d > 0.0)) {
-      if (tid == 0) atomicMin(status, rows[F.rows_off + kb + j]);
-      return;
+  if (bad >= 0) {
+    if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
+    return;
+  }
+  if (w2 > 0) {
+    double* D21 = D + 32;
+    double* D22 = D + 32 + 32 * DLD;
+    const double* X11 = X;
+    // L21 = D21 X11^T
+    for (int e = tid; e < 32 * 32; e += nt) {
+      const int i = e % 32, j = e / 32;
+      double acc = 0.0;
+      for (int k = 0; k <= j; k++) acc += D21[i + k * DLD] * X11[j + k * DLD];
+      T[i + j * 33] = (i < w2) ? acc : 0.0;
     }
     __syncthreads();
-    const double ljj = sqrt(d);
-    for (int i = j + 1 + tid; i < w; i += nt) D[i + j * DLD] /= ljj;
-    if (tid == 0) D[j + j * DLD] = ljj;
+    for (int e = tid; e < 32 * 32; e += nt) {
+      const int i = e % 32, j = e / 32;
+      D21[i + j * DLD] = T[i + j * 33];
+    }
     __syncthreads();
-    const int rem = w - j - 1;
-    for (int k = tid; k < rem * rem; k += nt) {
-      const int i = j + 1 + k % rem, c = j + 1 + k / rem;
-      if (i >= c) D[i + c * DLD] -= D[i + j * DLD] * D[c + j * DLD];
+    // D22 -= L21 L21^T (lower)
+    for (int e = tid; e < 32 * 32; e += nt) {
+      const int i = e % 32, j = e / 32;
+      if (i >= j && i < w2) {
+        double acc = 0.0;
+        for (int k = 0; k < 32; k++) acc += D21[i + k * DLD] * D21[j + k * DLD];
+        D22[i + j * DLD] -= acc;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const int b = warp_potrf32(D22, DLD, w2);
+      if (b < 0) warp_trinv32(D22, DLD, X + 32 + 32 * DLD, DLD, w2);
+      if ((tid & 31) == 0) bad = b < 0 ? -1 : 32 + b;
+    }
+    __syncthreads();
+    if (bad >= 0) {
+      if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
+      return;
+    }
+    // X21 = -X22 (L21 X11)
+    const double* X22 = X + 32 + 32 * DLD;
+    for (int e = tid; e < 32 * 32; e += nt) {
+      const int i = e % 32, j = e / 32;
+      double acc = 0.0;
+      for (int k = j; k < 32; k++) acc += D21[i + k * DLD] * X11[k + j * DLD];
+      T[i + j * 33] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < 32 * 32; e += nt) {
+      const int i = e % 32, j = e / 32;
+      double acc = 0.0;
+      for (int k = 0; k <= i; k++) acc += X22[i + k * DLD] * T[k + j * 33];
+      X[32 + i + j * DLD] = -acc;
     }
     __syncthreads();
   }
@@ -224,43 +330,11 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
     const int i = k % w, j = k / w;
     if (i >= j) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * DLD];
   }
-}
-
-// step kb: rows below the (already factored) diagonal block, X := X L_kk^-T
-__global__ void __launch_bounds__(TRSM_ROWS)
-k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-       double* __restrict__ L, int kb, const int* status) {
-  extern __shared__ double sm[];
-  double* D = sm;                          // PANEL_NB x PANEL_NB, col-major
-  double* X = sm + PANEL_NB * PANEL_NB;    // TRSM_ROWS x XLD, row-major
-  if (failed(status)) return;
-  const FrontDesc F = fronts[list[blockIdx.y]];
-  const int f = F.f, s = F.s;
-  if (kb >= s) return;
-  const int w = min(PANEL_NB, s - kb);
-  const int r_begin = kb + w + blockIdx.x * TRSM_ROWS;
-  if (r_begin >= f) return;
-  const int nrows = min(TRSM_ROWS, f - r_begin);
-  const int tid = threadIdx.x, nt = blockDim.x;
-  double* P = L + F.l_off;
-  for (int k = tid; k < w * w; k += nt) {
-    const int i = k % w, j = k / w;
-    D[i + j * PANEL_NB] = (i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : 0.0;
+  double* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
+  for (int k = tid; k < PANEL_NB * PANEL_NB; k += nt) {
+    const int i = k % PANEL_NB, j = k / PANEL_NB;
+    Di[k] = X[i + j * DLD];
   }
-  for (int j = 0; j < w; j++)
-    for (int r = tid; r < nrows; r += nt) X[r * XLD + j] = P[(r_begin + r) + (size_t) (kb + j) * f];
-  __syncthreads();
-  if (tid < nrows) {
-    double* x = X + tid * XLD;
-    for (int j = 0; j < w; j++) {
-      const double xj = x[j] / D[j + j * PANEL_NB];
-      x[j] = xj;
-      for (int k = j + 1; k < w; k++) x[k] -= xj * D[k + j * PANEL_NB];
-    }
-  }
-  __syncthreads();
-  for (int j = 0; j < w; j++)
-    for (int r = tid; r < nrows; r += nt) P[(r_begin + r) + (size_t) (kb + j) * f] = X[r * XLD + j];
 }
 
 // ------------------------------------------------------------- DMMA GEMM
@@ -279,6 +353,74 @@ __device__ __forceinline__ void dmma16888(double (&c)[4], const double (&a)[4], 
       "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+constexpr int TLD = PANEL_NB + 8;  // padded k-row stride of the TRSM operands
+
+// Step kb: rows below the diagonal block, X := X L_kk^-T = X * Dinv^T, one
+// CTA per 64-row slab, DMMA m16n8k8; in place (the slab is staged first).
+__global__ void __launch_bounds__(128)
+k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
+       double* __restrict__ L, const double* __restrict__ Dinv, int kb, const int* status) {
+  extern __shared__ double sm[];
+  double* As = sm;                        // [k][r]: slab, k-major
+  double* Bs = sm + PANEL_NB * TLD;       // [k][c]: Dinv[c][k]
+  if (failed(status)) return;
+  const FrontDesc F = fronts[list[blockIdx.y]];
+  const int f = F.f, s = F.s;
+  if (kb >= s) return;
+  const int w = min(PANEL_NB, s - kb);
+  const int r0 = kb + w + blockIdx.x * TRSM_ROWS;
+  if (r0 >= f) return;
+  const int nr = min(TRSM_ROWS, f - r0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* P = L + F.l_off;
+  const double* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
+  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
+    const int r = e % PANEL_NB, k = e / PANEL_NB;
+    As[k * TLD + r] = (r < nr && k < w) ? P[(r0 + r) + (size_t) (kb + k) * f] : 0.0;
+    Bs[k * TLD + r] = Di[r + k * PANEL_NB];
+  }
+  __syncthreads();
+  const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
+  double acc[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
+  for (int kk = 0; kk < PANEL_NB; kk += 8) {
+    double a[2][4], b[4][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++) {
+      const int r = wm * 32 + mi * 16 + g;
+      a[mi][0] = As[(kk + t) * TLD + r];
+      a[mi][1] = As[(kk + t) * TLD + r + 8];
+      a[mi][2] = As[(kk + t + 4) * TLD + r];
+      a[mi][3] = As[(kk + t + 4) * TLD + r + 8];
+    }
+#pragma unroll
+    for (int ni = 0; ni < 4; ni++) {
+      const int c = wn * 32 + ni * 8 + g;
+      b[ni][0] = Bs[(kk + t) * TLD + c];
+      b[ni][1] = Bs[(kk + t + 4) * TLD + c];
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+      for (int ni = 0; ni < 4; ni++) dmma16888(acc[mi][ni], a[mi], b[ni]);
+  }
+#pragma unroll
+  for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+    for (int ni = 0; ni < 4; ni++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = wm * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+        const int c = wn * 32 + ni * 8 + 2 * t + (q & 1);
+        if (r < nr && c < w) P[(r0 + r) + (size_t) (kb + c) * f] = acc[mi][ni][q];
+      }
 }
 
 constexpr int GLD = GEMM_BM + 8;  // padded k-row stride of the staged tiles
@@ -406,18 +548,45 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
 
 }  // namespace
 
+// algorithmic work of a whole front (the reference's flop count,
+// src/taucs_sn_llt.c:3957-3965) and of its assembly / extend-add traffic
+static double front_flops(const FrontDesc& F) {
+  double fl = 0.0;
+  for (int k = 0, c = F.f; k < F.s; k++, c--) fl += 1.0 + (double) c * (double) c;
+  return fl;
+}
+
+static double build_bytes(const Plan& P, const FrontDesc& F) {
+  double by = 0.0;
+  for (int ci = F.child_begin; ci < F.child_end; ci++) {
+    const FrontDesc& C = P.fronts[P.children[ci]];
+    const double mc = C.f - C.s;
+    by += 8.0 * mc * (mc + 1.0) / 2.0 + 4.0 * mc;
+  }
+  const double m = F.f - F.s;
+  by += 8.0 * ((double) F.f * F.s - (double) F.s * (F.s - 1) / 2.0) + 8.0 * m * (m + 1.0) / 2.0;
+  by += 12.0 * (P.acol_ptr[F.acol_off + F.s] - P.acol_ptr[F.acol_off]);
+  return by;
+}
+
+// small fronts: read children's U and A once, write panel and U once
+static double front_bytes(const Plan& P, const FrontDesc& F) {
+  return build_bytes(P, F);
+}
+
 static void set_smem_attrs() {
   static bool done = false;
   if (done) return;
   cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(double));
+  cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) POTRF_SMEM);
   cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (PANEL_NB * PANEL_NB + TRSM_ROWS * XLD) * (int) sizeof(double));
+                       2 * PANEL_NB * TLD * (int) sizeof(double));
   done = true;
 }
 
 int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L, double* U,
-                        int* status, cudaStream_t st) {
+                        double* Dinv, int* status, cudaStream_t st) {
   set_smem_attrs();
   k_init_status<<<1, 1, 0, st>>>(status);
   count_launch();
@@ -434,8 +603,17 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
         while (e < ns && P.fronts[LP.small_fronts[e]].f <= classes[cl]) e++;
         if (e > b) {
           const size_t smem = (size_t) classes[cl] * classes[cl] * sizeof(double);
+          double fl = 0.0, by = 0.0;
+          if (prof_enabled())
+            for (int q = b; q < e; q++) {
+              const FrontDesc& F = P.fronts[LP.small_fronts[q]];
+              fl += front_flops(F);
+              by += front_bytes(P, F);
+            }
+          prof_begin(KC_SMALL, st);
           k_small_front<<<e - b, 128, smem, st>>>(lst + b, D.fronts, D.children, D.maps, D.rows,
                                                    D.acol_ptr, D.a_rows, D.a_idx, vals, L, U, status);
+          prof_end(KC_SMALL, st, fl, by);
           count_launch();
         }
         b = e;
@@ -445,10 +623,17 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
     if (nb == 0) continue;
     const int* blst = D.big_list + D.big_off[h];
     const int ntiles = (int) LP.build_tiles.size();
-    k_build<<<ntiles, 256, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
-                                    D.a_rows, D.a_idx, vals, L, U, status);
-    count_launch();
-    const size_t trsm_smem = (PANEL_NB * PANEL_NB + TRSM_ROWS * XLD) * sizeof(double);
+    {
+      double by = 0.0;
+      if (prof_enabled())
+        for (int fi : LP.big_fronts) by += build_bytes(P, P.fronts[fi]);
+      prof_begin(KC_BUILD, st);
+      k_build<<<ntiles, 256, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
+                                      D.a_rows, D.a_idx, vals, L, U, status);
+      prof_end(KC_BUILD, st, 0.0, by);
+      count_launch();
+    }
+    const size_t trsm_smem = 2 * PANEL_NB * TLD * sizeof(double);
     for (int kb = 0; kb < LP.max_s_big; kb += PANEL_NB) {
       int gx_t = 0, gx_g = 0;
       for (int fi : LP.big_fronts) {
@@ -459,14 +644,35 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
         const int cb = kb + w;
         if (cb < F.s) gx_g = std::max(gx_g, trap_tiles(F.f - cb, F.s - cb));
       }
-      k_potrf_diag<<<nb, 256, 0, st>>>(blst, D.fronts, D.rows, L, kb, status);
+      double fp = 0.0, ft = 0.0, fg = 0.0, bp = 0.0, bt = 0.0, bg = 0.0;
+      if (prof_enabled())
+        for (int fi : LP.big_fronts) {
+          const FrontDesc& F = P.fronts[fi];
+          if (kb >= F.s) continue;
+          const double w = std::min(PANEL_NB, F.s - kb);
+          const double below = F.f - kb - w;              // rows under the diagonal block
+          const double sq = F.s - kb - w;                 // trailing columns of the panel
+          fp += w * w * w / 3.0;
+          bp += 8.0 * w * w;
+          ft += below * w * w;
+          bt += 16.0 * below * w + 8.0 * w * w / 2.0;
+          fg += 2.0 * w * (sq * (sq + 1.0) / 2.0 + (F.f - F.s) * sq);
+          bg += 16.0 * (sq * (sq + 1.0) / 2.0 + (F.f - F.s) * sq) + 8.0 * below * w;
+        }
+      prof_begin(KC_POTRF, st);
+      k_potrf_diag<<<nb, 128, POTRF_SMEM, st>>>(blst, D.fronts, D.rows, L, Dinv, kb, status);
+      prof_end(KC_POTRF, st, fp, bp);
       count_launch();
       if (gx_t > 0) {
-        k_trsm<<<dim3(gx_t, nb), TRSM_ROWS, trsm_smem, st>>>(blst, D.fronts, L, kb, status);
+        prof_begin(KC_TRSM, st);
+        k_trsm<<<dim3(gx_t, nb), 128, trsm_smem, st>>>(blst, D.fronts, L, Dinv, kb, status);
+        prof_end(KC_TRSM, st, ft, bt);
         count_launch();
       }
       if (gx_g > 0) {
+        prof_begin(KC_GEMM_PANEL, st);
         k_gemm<<<dim3(gx_g, nb), 128, 0, st>>>(blst, D.fronts, L, U, kb, 0, status);
+        prof_end(KC_GEMM_PANEL, st, fg, bg);
         count_launch();
       }
     }
@@ -477,7 +683,17 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
       if (m > 0) gx_u = std::max(gx_u, trap_tiles(m, m));
     }
     if (gx_u > 0) {
+      double fu = 0.0, bu = 0.0;
+      if (prof_enabled())
+        for (int fi : LP.big_fronts) {
+          const FrontDesc& F = P.fronts[fi];
+          const double m = F.f - F.s;
+          fu += 2.0 * F.s * m * (m + 1.0) / 2.0;
+          bu += 16.0 * m * (m + 1.0) / 2.0 + 8.0 * m * F.s;
+        }
+      prof_begin(KC_GEMM_U, st);
       k_gemm<<<dim3(gx_u, nb), 128, 0, st>>>(blst, D.fronts, L, U, 0, 1, status);
+      prof_end(KC_GEMM_U, st, fu, bu);
       count_launch();
     }
   }

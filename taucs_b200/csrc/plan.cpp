@@ -302,6 +302,28 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
     }
   }
 
+  // inverses of the diagonal blocks and solve flags for the big fronts
+  {
+    int64_t doff = 0;
+    int boff = 0;
+    for (int i = 0; i < nf; i++) {
+      FrontDesc& F = P.fronts[i];
+      if (F.f > SMALL_F_MAX) {
+        const int nbs = (F.s + PANEL_NB - 1) / PANEL_NB;
+        F.dinv_off = doff;
+        doff += (int64_t) nbs * PANEL_NB * PANEL_NB;
+        F.blk_off = boff;
+        boff += nbs;
+      } else {
+        F.dinv_off = -1;
+        F.blk_off = -1;
+      }
+      F.pad_ = 0;
+    }
+    P.dinv_len = std::max<int64_t>(doff, 32);
+    P.n_blk = std::max(boff, 1);
+  }
+
   // levels, front classes, build tiles
   P.levels.resize(H);
   {
@@ -327,6 +349,9 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
           for (int c0 = 0; c0 < m; c0 += BUILD_TC)
             for (int r0 = (c0 / BUILD_TR) * BUILD_TR; r0 < m; r0 += BUILD_TR)
               LP.build_tiles.push_back(Tile{i, r0, -1 - c0});
+          const int nrb = (F.f + PANEL_NB - 1) / PANEL_NB, nbs = (F.s + PANEL_NB - 1) / PANEL_NB;
+          for (int r = 0; r < nrb; r++) LP.solve_fwd_blocks.push_back(int2_{i, r});
+          for (int k = nbs - 1; k >= 0; k--) LP.solve_bwd_blocks.push_back(int2_{i, k});
         }
       }
       // the fused small-front kernel is launched per size class

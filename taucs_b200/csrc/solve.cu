@@ -24,11 +24,11 @@ namespace {
 constexpr int SB = 32;   // substitution block (one warp)
 
 __global__ void __launch_bounds__(256)
-k_fwd(int fbegin, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
       const int* __restrict__ maps, const int* __restrict__ rows, const double* __restrict__ L,
       const double* __restrict__ B, int ldb, double* __restrict__ W, int nrhs) {
   __shared__ double xs[SB][SOLVE_NRHS];
-  const FrontDesc F = fronts[fbegin + blockIdx.x];
+  const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
   double* Wf = W + F.v_off * SOLVE_NRHS;
@@ -85,11 +85,11 @@ k_fwd(int fbegin, const FrontDesc* __restrict__ fronts, const int* __restrict__ 
 }
 
 __global__ void __launch_bounds__(256)
-k_bwd(int fbegin, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
+k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
       const double* __restrict__ L, double* __restrict__ X, int ldx, double* __restrict__ W,
       int nrhs) {
   __shared__ double xs[SB][SOLVE_NRHS];
-  const FrontDesc F = fronts[fbegin + blockIdx.x];
+  const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   double* Wf = W + F.v_off * SOLVE_NRHS;
@@ -176,28 +176,344 @@ k_bwd(int fbegin, const FrontDesc* __restrict__ fronts, const int* __restrict__ 
   }
 }
 
+
+// ---------------------------------------------------------------- big fronts
+// One CTA per 64-row block.  Forward: block r waits for the solved blocks
+// k < r of L11 (flags, release/acquire), accumulates L[r,k] y_k, then solves
+// its own diagonal block and publishes y_r.  Backward: blocks run from the
+// last one; block k waits for x_j, j > k.  Waits are bounded: on timeout the
+// CTA records SOLVE_TIMEOUT in the status word and carries on, so no launch
+// can hang.
+
+constexpr int BR = PANEL_NB;   // rows per block
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ void wait_epoch(const int* flag, int epoch, int* status) {
+  if (threadIdx.x == 0) {
+    int it = 0;
+    while (ld_acquire(flag) != epoch) {
+      if (++it > (1 << 22)) {
+        atomicExch(status, SOLVE_TIMEOUT);
+        break;
+      }
+      __nanosleep(128);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int lb_dev(const int* a, int n, int key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(128)
+k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
+          const int* __restrict__ children, const int* __restrict__ maps, const int* __restrict__ rows,
+          const double* __restrict__ L, const double* __restrict__ B, int ldb, double* __restrict__ W,
+          int nrhs, int* __restrict__ flags, int epoch, int* status) {
+  __shared__ double wv[BR][SOLVE_NRHS];
+  __shared__ double yk[BR][SOLVE_NRHS];
+  __shared__ double part[BR][SOLVE_NRHS];
+  __shared__ double dg[BR][BR + 1];   // diagonal block, column-major: dg[col][row]
+  const int2_ bk = blocks[blockIdx.x];
+  const FrontDesc F = fronts[bk.a];
+  const int r = bk.b, f = F.f, s = F.s;
+  const int nbs = (s + BR - 1) / BR;
+  const int r0 = r * BR, nr = min(BR, f - r0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* Wf = W + F.v_off * SOLVE_NRHS;
+  const int* rw = rows + F.rows_off;
+  const double* P = L + F.l_off;
+
+  for (int k = tid; k < BR * SOLVE_NRHS; k += 128) {
+    const int i = k % BR, q = k / BR;
+    wv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : 0.0;
+  }
+  __syncthreads();
+  for (int ci = F.child_begin; ci < F.child_end; ci++) {
+    const FrontDesc C = fronts[children[ci]];
+    const int mc = C.f - C.s;
+    const int* mp = maps + C.map_off;
+    const int ia = lb_dev(mp, mc, r0), ib = lb_dev(mp, mc, r0 + nr);
+    if (ia >= ib) continue;
+    const double* Wc = W + C.v_off * SOLVE_NRHS;
+    for (int k = tid; k < (ib - ia) * nrhs; k += 128) {
+      const int i = ia + k % (ib - ia), q = k / (ib - ia);
+      wv[mp[i] - r0][q] += Wc[C.s + i + q * C.f];
+    }
+    __syncthreads();
+  }
+  // contributions of the solved blocks to the left
+  const int row = tid % BR, half = tid / BR;
+  double acc[SOLVE_NRHS];
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
+  const int kend = r < nbs ? r : nbs;
+  for (int k = 0; k < kend; k++) {
+    wait_epoch(flags + F.blk_off + k, epoch, status);
+    const int bwk = min(BR, s - k * BR);
+    for (int e = tid; e < BR * SOLVE_NRHS; e += 128) {
+      const int j = e % BR, q = e / BR;
+      yk[j][q] = (j < bwk && q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : 0.0;
+    }
+    __syncthreads();
+    if (row < nr) {
+      const double* pc = P + (r0 + row) + (size_t) (k * BR) * f;
+      const int jb = half * (BR / 2), je = min(bwk, jb + BR / 2);
+      for (int j = jb; j < je; j++) {
+        const double l = pc[(size_t) j * f];
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++) acc[q] += l * yk[j][q];
+      }
+    }
+    __syncthreads();
+  }
+  if (half == 1)
+    for (int q = 0; q < SOLVE_NRHS; q++) part[row][q] = acc[q];
+  __syncthreads();
+  if (half == 0)
+    for (int q = 0; q < SOLVE_NRHS; q++) wv[row][q] -= acc[q] + part[row][q];
+  __syncthreads();
+  if (r < nbs) {
+    // diagonal block (rows r0.., columns r0..r0+bw) staged in shared memory,
+    // then one warp substitutes: lanes own rows lane and lane+32
+    const int bw = min(BR, s - r0);
+    for (int e = tid; e < BR * BR; e += 128) {
+      const int i = e % BR, j = e / BR;
+      dg[j][i] = (i < nr && j < bw) ? P[(r0 + i) + (size_t) (r0 + j) * f] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int q = 0; q < nrhs; q++) {
+        double v0 = wv[lane][q], v1 = wv[lane + 32][q];
+        for (int j = 0; j < bw; j++) {
+          const double src = (j < 32) ? __shfl_sync(0xffffffffu, v0, j) : __shfl_sync(0xffffffffu, v1, j - 32);
+          const double xj = src / dg[j][j];
+          if (lane == j) v0 = xj;
+          else if (lane > j) v0 -= dg[j][lane] * xj;
+          if (lane + 32 == j) v1 = xj;
+          else if (lane + 32 > j) v1 -= dg[j][lane + 32] * xj;
+        }
+        wv[lane][q] = v0;
+        wv[lane + 32][q] = v1;
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = tid; k < nr * nrhs; k += 128) {
+    const int i = k % nr, q = k / nr;
+    Wf[r0 + i + (size_t) q * f] = wv[i][q];
+  }
+  __syncthreads();
+  if (r < nbs && tid == 0) {
+    __threadfence();
+    st_release(flags + F.blk_off + r, epoch);
+  }
+}
+
+// x at the update rows of every big front of a level, gathered once into the
+// front's work vector (rows s..f-1) so the backward blocks read it coalesced
+__global__ void __launch_bounds__(128)
+k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
+             const int* __restrict__ rows, const double* __restrict__ X, int ldx, double* __restrict__ W,
+             int nrhs) {
+  const int2_ bk = blocks[blockIdx.x];
+  const FrontDesc F = fronts[bk.a];
+  const int r0 = max(bk.b * BR, F.s), r1 = min(bk.b * BR + BR, F.f);
+  if (r0 >= r1) return;
+  double* Wf = W + F.v_off * SOLVE_NRHS;
+  const int* rw = rows + F.rows_off;
+  const int nr = r1 - r0;
+  for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
+    const int i = r0 + e % nr, q = e / nr;
+    Wf[i + (size_t) q * F.f] = X[rw[i] + (size_t) q * ldx];
+  }
+}
+
+__global__ void __launch_bounds__(128)
+k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
+          const int* __restrict__ rows, const double* __restrict__ L, double* __restrict__ X, int ldx,
+          double* __restrict__ W, int nrhs, int* __restrict__ flags, int epoch, int* status) {
+  __shared__ double xv[BR][SOLVE_NRHS];
+  __shared__ double xj[BR][SOLVE_NRHS];
+  __shared__ double dg[BR][BR + 1];   // diagonal block, dg[row][col]
+  const int2_ bk = blocks[blockIdx.x];
+  const FrontDesc F = fronts[bk.a];
+  const int k = bk.b, f = F.f, s = F.s, m = f - s;
+  const int nbs = (s + BR - 1) / BR;
+  const int c0 = k * BR, bw = min(BR, s - c0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* Wf = W + F.v_off * SOLVE_NRHS;
+  const int* rw = rows + F.rows_off;
+  const double* P = L + F.l_off;
+
+  for (int e = tid; e < BR * SOLVE_NRHS; e += 128) {
+    const int c = e % BR, q = e / BR;
+    xv[c][q] = (c < bw && q < nrhs) ? Wf[c0 + c + (size_t) q * f] : 0.0;
+  }
+  __syncthreads();
+  // y - L21^T x2 for my columns: warp per column, lanes over the update rows
+  for (int c = warp; c < bw; c += 4) {
+    double acc[SOLVE_NRHS];
+#pragma unroll
+    for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
+    const double* pc = P + (size_t) (c0 + c) * f + s;
+    const double* z = Wf + s;
+    for (int i = lane; i < m; i += 32) {
+      const double l = pc[i];
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++)
+        if (q < nrhs) acc[q] += l * __ldcg(z + i + (size_t) q * f);
+    }
+#pragma unroll
+    for (int q = 0; q < SOLVE_NRHS; q++) {
+      double v = acc[q];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      acc[q] = v;
+    }
+    if (lane == 0)
+      for (int q = 0; q < nrhs; q++) xv[c][q] -= acc[q];
+  }
+  __syncthreads();
+  // solved blocks below, last first
+  for (int j = nbs - 1; j > k; j--) {
+    wait_epoch(flags + F.blk_off + j, epoch, status);
+    const int bwj = min(BR, s - j * BR);
+    for (int e = tid; e < BR * SOLVE_NRHS; e += 128) {
+      const int i = e % BR, q = e / BR;
+      xj[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : 0.0;
+    }
+    __syncthreads();
+    for (int c = warp; c < bw; c += 4) {
+      const double* pc = P + (size_t) (c0 + c) * f + j * BR;
+      double acc[SOLVE_NRHS];
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
+      for (int i = lane; i < bwj; i += 32) {
+        const double l = pc[i];
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++) acc[q] += l * xj[i][q];
+      }
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[q] = v;
+      }
+      if (lane == 0)
+        for (int q = 0; q < nrhs; q++) xv[c][q] -= acc[q];
+    }
+    __syncthreads();
+  }
+  // L_kk^T substitution from the staged diagonal block, one warp, columns
+  // lane and lane+32
+  for (int e = tid; e < BR * BR; e += 128) {
+    const int i = e % BR, j = e / BR;
+    dg[i][j] = (i < bw && j < bw) ? P[(c0 + i) + (size_t) (c0 + j) * f] : 0.0;   // dg[row][col]
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int q = 0; q < nrhs; q++) {
+      double v0 = xv[lane][q], v1 = xv[lane + 32][q];
+      for (int c = bw - 1; c >= 0; c--) {
+        const double src = (c < 32) ? __shfl_sync(0xffffffffu, v0, c) : __shfl_sync(0xffffffffu, v1, c - 32);
+        const double x = src / dg[c][c];
+        if (lane == c) v0 = x;
+        else if (lane < c) v0 -= dg[c][lane] * x;
+        if (lane + 32 == c) v1 = x;
+        else if (lane + 32 < c) v1 -= dg[c][lane + 32] * x;
+      }
+      xv[lane][q] = v0;
+      xv[lane + 32][q] = v1;
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < bw * nrhs; e += 128) {
+    const int c = e % bw, q = e / bw;
+    Wf[c0 + c + (size_t) q * f] = xv[c][q];
+    X[rw[c0 + c] + (size_t) q * ldx] = xv[c][q];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    st_release(flags + F.blk_off + k, epoch);
+  }
+}
+
 }  // namespace
 
+// algorithmic bytes of one pass over a front: the lower panel once, its
+// row indices, and the gather/scatter of nrhs vector entries per row
+static double solve_pass_bytes(const FrontDesc& F, int nrhs) {
+  const double s = F.s, m = F.f - F.s;
+  return 8.0 * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * 8.0 * nrhs * F.f;
+}
+
 int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
-                      const double* B, int ld, double* W, double* Y, cudaStream_t st) {
-  (void) Y;
+                      const double* B, int ld, double* W, int* flags, int* epoch, int* status,
+                      cudaStream_t st) {
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
     const double* Bq = B + (size_t) q0 * ld;
     double* Xq = X + (size_t) q0 * ld;
+    const int ef = ++*epoch;
     for (int h = 0; h < P.n_levels; h++) {
       const LevelPlan& LP = P.levels[h];
-      const int cnt = LP.front_end - LP.front_begin;
-      if (cnt <= 0) continue;
-      k_fwd<<<cnt, 256, 0, st>>>(LP.front_begin, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq);
-      count_launch();
+      double by = 0.0;
+      if (prof_enabled())
+        for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq);
+      prof_begin(KC_SOLVE_FWD, st);
+      const int ns = (int) LP.small_fronts.size();
+      if (ns > 0) {
+        k_fwd<<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L,
+                                  Bq, ld, W, nq);
+        count_launch();
+      }
+      const int nb = (int) LP.solve_fwd_blocks.size();
+      if (nb > 0) {
+        k_fwd_big<<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, Bq,
+                                      ld, W, nq, flags, ef, status);
+        count_launch();
+      }
+      prof_end(KC_SOLVE_FWD, st, 0.0, by);
     }
+    const int eb = ++*epoch;
     for (int h = P.n_levels - 1; h >= 0; h--) {
       const LevelPlan& LP = P.levels[h];
-      const int cnt = LP.front_end - LP.front_begin;
-      if (cnt <= 0) continue;
-      k_bwd<<<cnt, 256, 0, st>>>(LP.front_begin, D.fronts, D.rows, L, Xq, ld, W, nq);
-      count_launch();
+      double by = 0.0;
+      if (prof_enabled())
+        for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq);
+      prof_begin(KC_SOLVE_BWD, st);
+      const int nb = (int) LP.solve_bwd_blocks.size();
+      if (nb > 0) {
+        k_gather_upd<<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
+                                                                        Xq, ld, W, nq);
+        count_launch();
+        k_bwd_big<<<nb, 128, 0, st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb,
+                                      status);
+        count_launch();
+      }
+      const int ns = (int) LP.small_fronts.size();
+      if (ns > 0) {
+        k_bwd<<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, Xq, ld, W, nq);
+        count_launch();
+      }
+      prof_end(KC_SOLVE_BWD, st, 0.0, by);
     }
   }
   return (int) cudaGetLastError();
