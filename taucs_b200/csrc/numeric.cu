@@ -21,8 +21,9 @@
 //   k_trsm          then one CTA per 64-row slab below it computes
 //                   X L_kk^-T = X Dinv^T on DMMA;
 //   k_gemm          C -= A B^T on DMMA (mma.sync m16n8k8 f64) tiles: the
-//                   trailing update of the panel after each step, and the
-//                   update matrix U -= L21 L21^T with k = s at the end.
+//                   panel updates of a recursive (left half, GEMM, right
+//                   half) panel factorization, and the update matrix
+//                   U -= L21 L21^T with k = s at the end.
 //
 // Every kernel first reads the status word and returns when an earlier front
 // hit a nonpositive pivot; the smallest failing global column is recorded
@@ -92,9 +93,9 @@ k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts
       return;
     }
     __syncthreads();
-    const double ljj = sqrt(d);
-    for (int i = j + 1 + tid; i < f; i += nt) W[i + j * f] /= ljj;
-    if (tid == 0) W[j + j * f] = ljj;
+    const double rj = rsqrt(d);
+    for (int i = j + 1 + tid; i < f; i += nt) W[i + j * f] *= rj;
+    if (tid == 0) W[j + j * f] = d * rj;
     __syncthreads();
     for (int k = j + 1 + warp; k < f; k += nw) {
       const double lkj = W[k + j * f];
@@ -185,12 +186,14 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
 // ------------------------------------------------------- blocked POTRF+TRSM
 
 constexpr int DLD = PANEL_NB + 1;  // padded column stride of the diagonal block
-constexpr size_t POTRF_SMEM = (2 * PANEL_NB * DLD + 32 * 33) * sizeof(double);
+constexpr size_t POTRF_SMEM = (2 * PANEL_NB * DLD + 32 * DLD) * sizeof(double);
 
 // Lower Cholesky of an n x n (n <= 32) block held in shared memory (ld `ld`),
 // by one warp: lane i keeps row i in registers and the right-looking updates
-// exchange L[k][j] with shuffles.  Returns the first nonpositive pivot (or -1)
-// in every lane.
+// exchange L[k][j] with shuffles.  The critical path per column is one
+// shuffle, one reciprocal square root and one multiply; every division of
+// the textbook loop is replaced by a multiply with rsqrt(pivot).  Returns the
+// first nonpositive pivot (or -1) in every lane.
 __device__ int warp_potrf32(double* S, int ld, int n) {
   const int lane = threadIdx.x & 31;
   double a[32];
@@ -202,9 +205,8 @@ __device__ int warp_potrf32(double* S, int ld, int n) {
     if (j < n) {
       const double d = __shfl_sync(0xffffffffu, a[j], j);
       if (!(d > 0.0) && bad < 0) bad = j;
-      const double ljj = sqrt(d);
-      if (lane == j) a[j] = ljj;
-      else if (lane > j) a[j] /= ljj;
+      const double r = rsqrt(d);
+      a[j] = (lane == j) ? d * r : a[j] * r;
 #pragma unroll
       for (int k = j + 1; k < 32; k++) {
         const double lkj = __shfl_sync(0xffffffffu, a[j], k);
@@ -219,25 +221,54 @@ __device__ int warp_potrf32(double* S, int ld, int n) {
 }
 
 // Inverse of an n x n (n <= 32) lower-triangular block by one warp: lane t
-// computes column t by forward substitution (L read as broadcasts).
+// computes column t by forward substitution; L is read as broadcasts, the
+// reciprocal diagonal is formed once in parallel, and each dot product is
+// split over four accumulators to shorten the dependent FMA chain.
 __device__ void warp_trinv32(const double* S, int ld, double* X, int ldx, int n) {
   const int t = threadIdx.x & 31;
+  const double rd_own = (t < n) ? 1.0 / S[t + t * ld] : 0.0;
   double x[32];
 #pragma unroll
   for (int i = 0; i < 32; i++) {
-    double acc = 0.0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
-    for (int k = 0; k < i; k++) acc += S[i + k * ld] * x[k];
-    x[i] = (i < n) ? (((i == t) ? 1.0 : 0.0) - acc) / S[i + i * ld] : 0.0;
+    for (int k = 0; k < i; k++) {
+      const double p = S[i + k * ld] * x[k];
+      if ((k & 3) == 0) a0 += p;
+      else if ((k & 3) == 1) a1 += p;
+      else if ((k & 3) == 2) a2 += p;
+      else a3 += p;
+    }
+    const double rdi = __shfl_sync(0xffffffffu, rd_own, i);
+    x[i] = (i < n) ? (((i == t) ? 1.0 : 0.0) - ((a0 + a1) + (a2 + a3))) * rdi : 0.0;
   }
 #pragma unroll
   for (int i = 0; i < 32; i++) X[i + t * ldx] = (t < n) ? x[i] : 0.0;
 }
 
-// Step kb, one CTA per front: factor the w x w diagonal block in place as a
-// 2 x 2 recursion over 32-blocks (warp-level POTRF of the diagonal blocks,
-// inverse-based TRSM and the SYRK update in between) and store the inverse of
-// the factored block (lower, ld PANEL_NB) for the TRSM of the rows below.
+// C (32x32, ld DLD) = A (32x32, ld lda) * op(B) for the 2x2 recursion of the
+// diagonal block.  Thread (i = tid % 32, warp w) owns C[i][8w .. 8w+7]: eight
+// independent accumulation chains, A read with unit stride across lanes and
+// B read as warp-wide broadcasts.  TRANSB selects B^T.
+template <bool TRANSB>
+__device__ __forceinline__ void prod32(const double* A, int lda, const double* B, int ldb, double (&c)[8]) {
+  const int i = threadIdx.x & 31, j0 = (threadIdx.x >> 5) * 8;
+#pragma unroll
+  for (int q = 0; q < 8; q++) c[q] = 0.0;
+#pragma unroll 8
+  for (int k = 0; k < 32; k++) {
+    const double a = A[i + k * lda];
+#pragma unroll
+    for (int q = 0; q < 8; q++) c[q] += a * (TRANSB ? B[(j0 + q) + k * ldb] : B[k + (j0 + q) * ldb]);
+  }
+}
+
+// Step kb, one CTA (4 warps) per front: factor the w x w diagonal block in
+// place as a 2 x 2 recursion over 32-blocks -- warp-level POTRF of the
+// diagonal blocks, L21 = D21 L11^-T, D22 -= L21 L21^T -- and store the inverse
+// of the factored block (lower, ld PANEL_NB) for the TRSM of the rows below.
+// The block is padded with the identity to 64 x 64 so that the warp routines
+// always run at their compile-time size.
 __global__ void __launch_bounds__(128)
 k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
              const int* __restrict__ rows, double* __restrict__ L, double* __restrict__ Dinv, int kb,
@@ -245,26 +276,39 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
   extern __shared__ double sm[];
   double* D = sm;                        // the block, col-major, ld DLD
   double* X = sm + PANEL_NB * DLD;       // its inverse
-  double* T = X + PANEL_NB * DLD;        // 32 x 33 scratch
+  double* T = X + PANEL_NB * DLD;        // 32 x DLD scratch
   __shared__ int bad;
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   if (kb >= s) return;
   const int w = min(PANEL_NB, s - kb);
-  const int w1 = min(32, w), w2 = w - w1;
-  const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5;
   double* P = L + F.l_off;
-  for (int k = tid; k < PANEL_NB * PANEL_NB; k += nt) {
-    const int i = k % PANEL_NB, j = k / PANEL_NB;
-    D[i + j * DLD] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : 0.0;
-    X[i + j * DLD] = 0.0;
+  {
+    double v[PANEL_NB * PANEL_NB / 128];
+#pragma unroll
+    for (int q = 0; q < PANEL_NB * PANEL_NB / 128; q++) {
+      const int k = tid + q * 128, i = k % PANEL_NB, j = k / PANEL_NB;
+      v[q] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? 1.0 : 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < PANEL_NB * PANEL_NB / 128; q++) {
+      const int k = tid + q * 128, i = k % PANEL_NB, j = k / PANEL_NB;
+      D[i + j * DLD] = v[q];
+      X[i + j * DLD] = 0.0;
+    }
   }
   if (tid == 0) bad = -1;
   __syncthreads();
+  double c[8];
+  const int ci = tid & 31, cj = (tid >> 5) * 8;
+  double* D21 = D + 32;
+  double* D22 = D + 32 + 32 * DLD;
+  double* X22 = X + 32 + 32 * DLD;
   if (warp == 0) {
-    const int b = warp_potrf32(D, DLD, w1);
-    if (b < 0) warp_trinv32(D, DLD, X, DLD, w1);
+    const int b = warp_potrf32(D, DLD, 32);
+    if (b < 0) warp_trinv32(D, DLD, X, DLD, 32);
     if ((tid & 31) == 0) bad = b;
   }
   __syncthreads();
@@ -272,68 +316,45 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
     if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
     return;
   }
-  if (w2 > 0) {
-    double* D21 = D + 32;
-    double* D22 = D + 32 + 32 * DLD;
-    const double* X11 = X;
-    // L21 = D21 X11^T
-    for (int e = tid; e < 32 * 32; e += nt) {
-      const int i = e % 32, j = e / 32;
-      double acc = 0.0;
-      for (int k = 0; k <= j; k++) acc += D21[i + k * DLD] * X11[j + k * DLD];
-      T[i + j * 33] = (i < w2) ? acc : 0.0;
-    }
-    __syncthreads();
-    for (int e = tid; e < 32 * 32; e += nt) {
-      const int i = e % 32, j = e / 32;
-      D21[i + j * DLD] = T[i + j * 33];
-    }
-    __syncthreads();
-    // D22 -= L21 L21^T (lower)
-    for (int e = tid; e < 32 * 32; e += nt) {
-      const int i = e % 32, j = e / 32;
-      if (i >= j && i < w2) {
-        double acc = 0.0;
-        for (int k = 0; k < 32; k++) acc += D21[i + k * DLD] * D21[j + k * DLD];
-        D22[i + j * DLD] -= acc;
-      }
-    }
-    __syncthreads();
-    if (warp == 0) {
-      const int b = warp_potrf32(D22, DLD, w2);
-      if (b < 0) warp_trinv32(D22, DLD, X + 32 + 32 * DLD, DLD, w2);
-      if ((tid & 31) == 0) bad = b < 0 ? -1 : 32 + b;
-    }
-    __syncthreads();
-    if (bad >= 0) {
-      if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
-      return;
-    }
-    // X21 = -X22 (L21 X11)
-    const double* X22 = X + 32 + 32 * DLD;
-    for (int e = tid; e < 32 * 32; e += nt) {
-      const int i = e % 32, j = e / 32;
-      double acc = 0.0;
-      for (int k = j; k < 32; k++) acc += D21[i + k * DLD] * X11[k + j * DLD];
-      T[i + j * 33] = acc;
-    }
-    __syncthreads();
-    for (int e = tid; e < 32 * 32; e += nt) {
-      const int i = e % 32, j = e / 32;
-      double acc = 0.0;
-      for (int k = 0; k <= i; k++) acc += X22[i + k * DLD] * T[k + j * 33];
-      X[32 + i + j * DLD] = -acc;
-    }
-    __syncthreads();
+  // L21 = D21 X11^T
+  prod32<true>(D21, DLD, X, DLD, c);
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 8; q++) D21[ci + (cj + q) * DLD] = c[q];
+  __syncthreads();
+  // D22 -= L21 L21^T (lower part)
+  prod32<true>(D21, DLD, D21, DLD, c);
+#pragma unroll
+  for (int q = 0; q < 8; q++)
+    if (ci >= cj + q) D22[ci + (cj + q) * DLD] -= c[q];
+  __syncthreads();
+  if (warp == 0) {
+    const int b = warp_potrf32(D22, DLD, 32);
+    if (b < 0) warp_trinv32(D22, DLD, X22, DLD, 32);
+    if ((tid & 31) == 0) bad = b < 0 ? -1 : 32 + b;
   }
-  for (int k = tid; k < w * w; k += nt) {
+  __syncthreads();
+  if (bad >= 0) {
+    if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
+    return;
+  }
+  // X21 = -X22 (L21 X11)
+  prod32<false>(D21, DLD, X, DLD, c);
+#pragma unroll
+  for (int q = 0; q < 8; q++) T[ci + (cj + q) * DLD] = c[q];
+  __syncthreads();
+  prod32<false>(X22, DLD, T, DLD, c);
+#pragma unroll
+  for (int q = 0; q < 8; q++) X[32 + ci + (cj + q) * DLD] = -c[q];
+  __syncthreads();
+  for (int k = tid; k < w * w; k += 128) {
     const int i = k % w, j = k / w;
     if (i >= j) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * DLD];
   }
   double* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
-  for (int k = tid; k < PANEL_NB * PANEL_NB; k += nt) {
+  for (int k = tid; k < PANEL_NB * PANEL_NB; k += 128) {
     const int i = k % PANEL_NB, j = k / PANEL_NB;
-    Di[k] = X[i + j * DLD];
+    Di[k] = (i < w && j < w) ? X[i + j * DLD] : 0.0;
   }
 }
 
@@ -423,23 +444,40 @@ k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
       }
 }
 
-constexpr int GLD = GEMM_BM + 8;  // padded k-row stride of the staged tiles
+constexpr int GEMM_STAGES = 3;
 
 // number of lower-trapezoid tiles of a region with `rows` rows and `cols`
 // columns whose column tile c covers rows [c*BN, rows)
-__host__ __device__ inline int trap_tiles(int rows, int cols) {
+__host__ __device__ inline int trap_tiles(int rows, int cols, int bm, int bn) {
   int t = 0;
-  for (int c0 = 0; c0 < cols; c0 += GEMM_BN) t += (rows - c0 + GEMM_BM - 1) / GEMM_BM;
+  for (int c0 = 0; c0 < cols; c0 += bn) t += (rows - c0 + bm - 1) / bm;
   return t;
 }
 
-// mode 0: trailing update of the panel after step kb (K = [kb, kb+w));
+template <int BM, int BN>
+struct GemmCfg {
+  static constexpr int WM = 2;                     // warps along M
+  static constexpr int WN = BN / 32;               // warps along N (32 columns each)
+  static constexpr int THREADS = 32 * WM * WN;
+  static constexpr int MI = BM / WM / 16;          // m16 tiles per warp
+  static constexpr int NI = 4;                     // n8 tiles per warp
+  static constexpr int LD = BM + 8;                // padded k-row stride (BM >= BN)
+  static constexpr size_t SMEM = (size_t) GEMM_STAGES * 2 * GEMM_BK * LD * sizeof(double);
+};
+
+// C -= A B^T on DMMA m16n8k8 tiles of BM x BN (64x64: 4 warps, 128x128: 8
+// warps), GEMM_STAGES-deep cp.async pipeline, accumulators preloaded with -C.
+// mode 0: panel update of columns [c_lo, min(c_hi, s)) and all rows below
+//         c_lo by the panel columns [k_lo, k_hi) (one node of the recursive
+//         panel factorization);
 // mode 1: U -= L21 L21^T (K = [0, s))
-__global__ void __launch_bounds__(128)
+template <int BM, int BN>
+__global__ void __launch_bounds__(GemmCfg<BM, BN>::THREADS)
 k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, double* __restrict__ L,
-       double* __restrict__ U, int kb, int mode, const int* status) {
-  __shared__ __align__(16) double As[2][GEMM_BK][GLD];
-  __shared__ __align__(16) double Bs[2][GEMM_BK][GLD];
+       double* __restrict__ U, int c_lo, int c_hi, int k_lo, int k_hi, int mode, const int* status) {
+  using Cfg = GemmCfg<BM, BN>;
+  constexpr int MI = Cfg::MI, NI = Cfg::NI, LD = Cfg::LD, NT = Cfg::THREADS;
+  extern __shared__ __align__(16) double gsm[];   // GEMM_STAGES x {A, B} x GEMM_BK x LD
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.y]];
   const int f = F.f, s = F.s, m = f - s;
@@ -447,12 +485,10 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
   const double* P = L + F.l_off;
   double* Cbase;
   if (mode == 0) {
-    if (kb >= s) return;
-    const int w = min(PANEL_NB, s - kb);
-    const int cb = kb + w;
-    if (cb >= s) return;
-    rows = f - cb; cols = s - cb; roff = cb;
-    kbeg = kb; kend = kb + w;
+    const int cb = c_lo, ce = min(c_hi, s);
+    if (cb >= ce) return;
+    rows = f - cb; cols = ce - cb; roff = cb;
+    kbeg = k_lo; kend = k_hi;
     Cbase = L + F.l_off + cb + (size_t) cb * f;
     ldc = f;
   } else {
@@ -466,83 +502,103 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
   int idx = blockIdx.x, c0 = 0;
   for (;;) {
     if (c0 >= cols) return;
-    const int nt_c = (rows - c0 + GEMM_BM - 1) / GEMM_BM;
+    const int nt_c = (rows - c0 + BM - 1) / BM;
     if (idx < nt_c) break;
     idx -= nt_c;
-    c0 += GEMM_BN;
+    c0 += BN;
   }
-  const int r0 = c0 + idx * GEMM_BM;
-  const int nr = min(GEMM_BM, rows - r0), nc = min(GEMM_BN, cols - c0);
+  const int r0 = c0 + idx * BM;
+  const int nr = min(BM, rows - r0), nc = min(BN, cols - c0);
   const double* Ag = P + (roff + r0);
   const double* Bg = P + (roff + c0);
+  double* C = Cbase + r0 + (size_t) c0 * ldc;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
-  double acc[2][4][4];
+  const int wm = warp % Cfg::WM, wn = warp / Cfg::WM, g = lane >> 2, t = lane & 3;
+  const int wrow = wm * (BM / Cfg::WM), wcol = wn * 32;
+  // accumulators start at -C, so acc = A B^T - C and the result is -acc
+  double acc[MI][NI][4];
 #pragma unroll
-  for (int a = 0; a < 2; a++)
+  for (int mi = 0; mi < MI; mi++)
 #pragma unroll
-    for (int b = 0; b < 4; b++)
-#pragma unroll
-      for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
-
-  auto load = [&](int stage, int k0) {
-#pragma unroll
-    for (int q = 0; q < (GEMM_BM * GEMM_BK) / 128; q++) {
-      const int e = tid + q * 128;
-      const int r = e % GEMM_BM, k = e / GEMM_BM;
-      const bool kv = (k0 + k) < kend;
-      const bool pa = kv && r < nr, pb = kv && r < nc;
-      const size_t col = (size_t) (kv ? k0 + k : kbeg) * f;
-      cp_async8(&As[stage][k][r], Ag + (pa ? r : 0) + col, pa);
-      cp_async8(&Bs[stage][k][r], Bg + (pb ? r : 0) + col, pb);
-    }
-    cp_async_commit();
-  };
-
-  int stage = 0;
-  load(0, kbeg);
-  for (int k0 = kbeg; k0 < kend; k0 += GEMM_BK) {
-    const bool more = k0 + GEMM_BK < kend;
-    if (more) load(stage ^ 1, k0 + GEMM_BK);
-    if (more) cp_async_wait<1>();
-    else cp_async_wait<0>();
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < GEMM_BK; kk += 8) {
-      double a[2][4], b[4][2];
-#pragma unroll
-      for (int mi = 0; mi < 2; mi++) {
-        const int r = wm * 32 + mi * 16 + g;
-        a[mi][0] = As[stage][kk + t][r];
-        a[mi][1] = As[stage][kk + t][r + 8];
-        a[mi][2] = As[stage][kk + t + 4][r];
-        a[mi][3] = As[stage][kk + t + 4][r + 8];
-      }
-#pragma unroll
-      for (int ni = 0; ni < 4; ni++) {
-        const int c = wn * 32 + ni * 8 + g;
-        b[ni][0] = Bs[stage][kk + t][c];
-        b[ni][1] = Bs[stage][kk + t + 4][c];
-      }
-#pragma unroll
-      for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-        for (int ni = 0; ni < 4; ni++) dmma16888(acc[mi][ni], a[mi], b[ni]);
-    }
-    __syncthreads();
-    stage ^= 1;
-  }
-  double* C = Cbase + r0 + (size_t) c0 * ldc;
-#pragma unroll
-  for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-    for (int ni = 0; ni < 4; ni++)
+    for (int ni = 0; ni < NI; ni++)
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        const int r = wm * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
-        const int c = wn * 32 + ni * 8 + 2 * t + (q & 1);
-        if (r < nr && c < nc && r0 + r >= c0 + c) C[r + (size_t) c * ldc] -= acc[mi][ni][q];
+        const int r = wrow + mi * 16 + g + ((q & 2) ? 8 : 0);
+        const int c = wcol + ni * 8 + 2 * t + (q & 1);
+        acc[mi][ni][q] = (r < nr && c < nc && r0 + r >= c0 + c) ? -C[r + (size_t) c * ldc] : 0.0;
+      }
+
+  auto load = [&](int st, int k0) {
+    double* As = gsm + (size_t) (st * 2) * GEMM_BK * LD;
+    double* Bs = As + GEMM_BK * LD;
+#pragma unroll
+    for (int q = 0; q < (BM * GEMM_BK) / NT; q++) {
+      const int e = tid + q * NT;
+      const int r = e % BM, k = e / BM;
+      const bool kv = (k0 + k) < kend;
+      const bool pa = kv && r < nr;
+      const size_t col = (size_t) (kv ? k0 + k : kbeg) * f;
+      cp_async8(As + k * LD + r, Ag + (pa ? r : 0) + col, pa);
+    }
+#pragma unroll
+    for (int q = 0; q < (BN * GEMM_BK) / NT; q++) {
+      const int e = tid + q * NT;
+      const int r = e % BN, k = e / BN;
+      const bool kv = (k0 + k) < kend;
+      const bool pb = kv && r < nc;
+      const size_t col = (size_t) (kv ? k0 + k : kbeg) * f;
+      cp_async8(Bs + k * LD + r, Bg + (pb ? r : 0) + col, pb);
+    }
+  };
+
+  const int nk = (kend - kbeg + GEMM_BK - 1) / GEMM_BK;
+#pragma unroll
+  for (int st = 0; st < GEMM_STAGES - 1; st++) {
+    if (st < nk) load(st, kbeg + st * GEMM_BK);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; kt++) {
+    cp_async_wait<GEMM_STAGES - 2>();
+    __syncthreads();
+    const int kn = kt + GEMM_STAGES - 1;
+    if (kn < nk) load(kn % GEMM_STAGES, kbeg + kn * GEMM_BK);
+    cp_async_commit();
+    const double* As = gsm + (size_t) ((kt % GEMM_STAGES) * 2) * GEMM_BK * LD;
+    const double* Bs = As + GEMM_BK * LD;
+#pragma unroll
+    for (int kk = 0; kk < GEMM_BK; kk += 8) {
+      double a[MI][4], b[NI][2];
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++) {
+        const int r = wrow + mi * 16 + g;
+        a[mi][0] = As[(kk + t) * LD + r];
+        a[mi][1] = As[(kk + t) * LD + r + 8];
+        a[mi][2] = As[(kk + t + 4) * LD + r];
+        a[mi][3] = As[(kk + t + 4) * LD + r + 8];
+      }
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++) {
+        const int c = wcol + ni * 8 + g;
+        b[ni][0] = Bs[(kk + t) * LD + c];
+        b[ni][1] = Bs[(kk + t + 4) * LD + c];
+      }
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++) dmma16888(acc[mi][ni], a[mi], b[ni]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+    for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = wrow + mi * 16 + g + ((q & 2) ? 8 : 0);
+        const int c = wcol + ni * 8 + 2 * t + (q & 1);
+        if (r < nr && c < nc && r0 + r >= c0 + c) C[r + (size_t) c * ldc] = -acc[mi][ni][q];
       }
 }
 
@@ -574,12 +630,34 @@ static double front_bytes(const Plan& P, const FrontDesc& F) {
   return build_bytes(P, F);
 }
 
+// Tile shape per launch.  Measured on the 64^3 benchmark: the 64x64 tiles
+// (4 warps, 164 registers, 3 CTAs per SM) reach 24 TF/s on the update
+// matrices; 128x128 tiles (8 warps, 228 registers) fit one CTA per SM and
+// reach 19 TF/s, so they are not selected.
+static bool big_tiles(int maxr, int maxc, int tiles64) {
+  (void) maxr; (void) maxc; (void) tiles64;
+  return false;
+}
+
+static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, double* L,
+                        double* U, int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
+  if (big)
+    k_gemm<128, 128><<<dim3(gx128, nb), GemmCfg<128, 128>::THREADS, GemmCfg<128, 128>::SMEM, st>>>(
+        blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
+  else
+    k_gemm<64, 64><<<dim3(gx64, nb), GemmCfg<64, 64>::THREADS, GemmCfg<64, 64>::SMEM, st>>>(
+        blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
+}
+
 static void set_smem_attrs() {
   static bool done = false;
   if (done) return;
   cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(double));
   cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) POTRF_SMEM);
+  cudaFuncSetAttribute(k_gemm<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) GemmCfg<64, 64>::SMEM);
+  cudaFuncSetAttribute(k_gemm<128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) GemmCfg<128, 128>::SMEM);
   cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        2 * PANEL_NB * TLD * (int) sizeof(double));
   done = true;
@@ -634,31 +712,28 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
       count_launch();
     }
     const size_t trsm_smem = 2 * PANEL_NB * TLD * sizeof(double);
-    for (int kb = 0; kb < LP.max_s_big; kb += PANEL_NB) {
-      int gx_t = 0, gx_g = 0;
+    // recursive panel factorization over aligned column intervals: factor
+    // the left half, update the right half with one GEMM (K = half width),
+    // factor the right half; leaves are 64-column POTRF + TRSM steps
+    const int S = LP.max_s_big;
+    int span = PANEL_NB;
+    while (span < S) span *= 2;
+    auto leaf = [&](int kb) {
+      int gx_t = 0;
+      double fp = 0.0, ft = 0.0, bp = 0.0, bt = 0.0;
       for (int fi : LP.big_fronts) {
         const FrontDesc& F = P.fronts[fi];
         if (kb >= F.s) continue;
         const int w = std::min(PANEL_NB, F.s - kb);
         gx_t = std::max(gx_t, (F.f - kb - w + TRSM_ROWS - 1) / TRSM_ROWS);
-        const int cb = kb + w;
-        if (cb < F.s) gx_g = std::max(gx_g, trap_tiles(F.f - cb, F.s - cb));
-      }
-      double fp = 0.0, ft = 0.0, fg = 0.0, bp = 0.0, bt = 0.0, bg = 0.0;
-      if (prof_enabled())
-        for (int fi : LP.big_fronts) {
-          const FrontDesc& F = P.fronts[fi];
-          if (kb >= F.s) continue;
-          const double w = std::min(PANEL_NB, F.s - kb);
-          const double below = F.f - kb - w;              // rows under the diagonal block
-          const double sq = F.s - kb - w;                 // trailing columns of the panel
-          fp += w * w * w / 3.0;
-          bp += 8.0 * w * w;
-          ft += below * w * w;
-          bt += 16.0 * below * w + 8.0 * w * w / 2.0;
-          fg += 2.0 * w * (sq * (sq + 1.0) / 2.0 + (F.f - F.s) * sq);
-          bg += 16.0 * (sq * (sq + 1.0) / 2.0 + (F.f - F.s) * sq) + 8.0 * below * w;
+        if (prof_enabled()) {
+          const double ww = w, below = F.f - kb - w;
+          fp += ww * ww * ww / 3.0;
+          bp += 8.0 * ww * ww;
+          ft += 2.0 * below * ww * ww;
+          bt += 16.0 * below * ww + 8.0 * ww * ww;
         }
+      }
       prof_begin(KC_POTRF, st);
       k_potrf_diag<<<nb, 128, POTRF_SMEM, st>>>(blst, D.fronts, D.rows, L, Dinv, kb, status);
       prof_end(KC_POTRF, st, fp, bp);
@@ -669,20 +744,53 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
         prof_end(KC_TRSM, st, ft, bt);
         count_launch();
       }
-      if (gx_g > 0) {
-        prof_begin(KC_GEMM_PANEL, st);
-        k_gemm<<<dim3(gx_g, nb), 128, 0, st>>>(blst, D.fronts, L, U, kb, 0, status);
-        prof_end(KC_GEMM_PANEL, st, fg, bg);
-        count_launch();
+    };
+    auto update = [&](int c_lo, int c_hi, int k_lo, int k_hi) {
+      int gx = 0, gx64 = 0, maxc = 0, maxr = 0;
+      double fg = 0.0, bg = 0.0;
+      for (int fi : LP.big_fronts) {
+        const FrontDesc& F = P.fronts[fi];
+        const int ce = std::min(c_hi, F.s);
+        if (c_lo >= ce) continue;
+        gx = std::max(gx, trap_tiles(F.f - c_lo, ce - c_lo, 128, 128));
+        gx64 = std::max(gx64, trap_tiles(F.f - c_lo, ce - c_lo, 64, 64));
+        maxc = std::max(maxc, ce - c_lo);
+        maxr = std::max(maxr, F.f - c_lo);
+        if (prof_enabled()) {
+          const double c = ce - c_lo, below = F.f - ce, k = k_hi - k_lo;
+          const double entries = c * (c + 1.0) / 2.0 + below * c;
+          fg += 2.0 * k * entries;
+          bg += 16.0 * entries + 8.0 * k * (F.f - c_lo);
+        }
       }
-    }
-    int gx_u = 0;
+      if (gx64 == 0) return;
+      prof_begin(KC_GEMM_PANEL, st);
+      launch_gemm(big_tiles(maxr, maxc, gx64 * nb), gx, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, 0, status, st);
+      prof_end(KC_GEMM_PANEL, st, fg, bg);
+      count_launch();
+    };
+    struct Rec {
+      static void run(int a, int b, int S_, const decltype(leaf)& lf, const decltype(update)& up) {
+        if (a >= S_) return;
+        if (b - a <= PANEL_NB) { lf(a); return; }
+        const int mid = (a + b) / 2;
+        run(a, mid, S_, lf, up);
+        if (mid < S_) up(mid, b, a, mid);
+        run(mid, b, S_, lf, up);
+      }
+    };
+    Rec::run(0, span, S, leaf, update);
+    int gx_u = 0, gx_u64 = 0, maxm = 0;
     for (int fi : LP.big_fronts) {
       const FrontDesc& F = P.fronts[fi];
       const int m = F.f - F.s;
-      if (m > 0) gx_u = std::max(gx_u, trap_tiles(m, m));
+      if (m > 0) {
+        gx_u = std::max(gx_u, trap_tiles(m, m, 128, 128));
+        gx_u64 = std::max(gx_u64, trap_tiles(m, m, 64, 64));
+        maxm = std::max(maxm, m);
+      }
     }
-    if (gx_u > 0) {
+    if (gx_u64 > 0) {
       double fu = 0.0, bu = 0.0;
       if (prof_enabled())
         for (int fi : LP.big_fronts) {
@@ -692,7 +800,7 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
           bu += 16.0 * m * (m + 1.0) / 2.0 + 8.0 * m * F.s;
         }
       prof_begin(KC_GEMM_U, st);
-      k_gemm<<<dim3(gx_u, nb), 128, 0, st>>>(blst, D.fronts, L, U, 0, 1, status);
+      launch_gemm(big_tiles(maxm, maxm, gx_u64 * nb), gx_u, gx_u64, nb, blst, D, L, U, 0, 0, 0, 0, 1, status, st);
       prof_end(KC_GEMM_U, st, fu, bu);
       count_launch();
     }

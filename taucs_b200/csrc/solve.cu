@@ -221,14 +221,15 @@ __device__ __forceinline__ int lb_dev(const int* a, int n, int key) {
   return lo;
 }
 
+template <int NQ>
 __global__ void __launch_bounds__(128)
 k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ children, const int* __restrict__ maps, const int* __restrict__ rows,
           const double* __restrict__ L, const double* __restrict__ B, int ldb, double* __restrict__ W,
           int nrhs, int* __restrict__ flags, int epoch, int* status) {
-  __shared__ double wv[BR][SOLVE_NRHS];
-  __shared__ double yk[BR][SOLVE_NRHS];
-  __shared__ double part[BR][SOLVE_NRHS];
+  __shared__ double wv[BR][NQ];
+  __shared__ double yk[BR][NQ];
+  __shared__ double part[BR][NQ];
   __shared__ double dg[BR][BR + 1];   // diagonal block, column-major: dg[col][row]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
@@ -240,7 +241,7 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
-  for (int k = tid; k < BR * SOLVE_NRHS; k += 128) {
+  for (int k = tid; k < BR * NQ; k += 128) {
     const int i = k % BR, q = k / BR;
     wv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : 0.0;
   }
@@ -258,40 +259,43 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     }
     __syncthreads();
   }
-  // contributions of the solved blocks to the left
+  // contributions of the solved blocks to the left; this thread's 32
+  // entries of L[r, k] are loaded before waiting for y_k
   const int row = tid % BR, half = tid / BR;
-  double acc[SOLVE_NRHS];
+  double acc[NQ];
 #pragma unroll
-  for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
+  for (int q = 0; q < NQ; q++) acc[q] = 0.0;
   const int kend = r < nbs ? r : nbs;
   for (int k = 0; k < kend; k++) {
-    wait_epoch(flags + F.blk_off + k, epoch, status);
     const int bwk = min(BR, s - k * BR);
-    for (int e = tid; e < BR * SOLVE_NRHS; e += 128) {
+    double lv[BR / 2];
+    const double* pc = P + (r0 + row) + (size_t) (k * BR + half * (BR / 2)) * f;
+#pragma unroll
+    for (int j = 0; j < BR / 2; j++)
+      lv[j] = (row < nr && half * (BR / 2) + j < bwk) ? pc[(size_t) j * f] : 0.0;
+    wait_epoch(flags + F.blk_off + k, epoch, status);
+    for (int e = tid; e < BR * NQ; e += 128) {
       const int j = e % BR, q = e / BR;
       yk[j][q] = (j < bwk && q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : 0.0;
     }
     __syncthreads();
-    if (row < nr) {
-      const double* pc = P + (r0 + row) + (size_t) (k * BR) * f;
-      const int jb = half * (BR / 2), je = min(bwk, jb + BR / 2);
-      for (int j = jb; j < je; j++) {
-        const double l = pc[(size_t) j * f];
 #pragma unroll
-        for (int q = 0; q < SOLVE_NRHS; q++) acc[q] += l * yk[j][q];
-      }
-    }
+    for (int j = 0; j < BR / 2; j++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) acc[q] += lv[j] * yk[half * (BR / 2) + j][q];
     __syncthreads();
   }
   if (half == 1)
-    for (int q = 0; q < SOLVE_NRHS; q++) part[row][q] = acc[q];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) part[row][q] = acc[q];
   __syncthreads();
   if (half == 0)
-    for (int q = 0; q < SOLVE_NRHS; q++) wv[row][q] -= acc[q] + part[row][q];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) wv[row][q] -= acc[q] + part[row][q];
   __syncthreads();
   if (r < nbs) {
-    // diagonal block (rows r0.., columns r0..r0+bw) staged in shared memory,
-    // then one warp substitutes: lanes own rows lane and lane+32
+    // diagonal block staged in shared memory, then one warp substitutes:
+    // lanes own rows lane and lane+32
     const int bw = min(BR, s - r0);
     for (int e = tid; e < BR * BR; e += 128) {
       const int i = e % BR, j = e / BR;
@@ -345,13 +349,16 @@ k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fro
   }
 }
 
+template <int NQ>
 __global__ void __launch_bounds__(128)
 k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ rows, const double* __restrict__ L, double* __restrict__ X, int ldx,
           double* __restrict__ W, int nrhs, int* __restrict__ flags, int epoch, int* status) {
-  __shared__ double xv[BR][SOLVE_NRHS];
-  __shared__ double xj[BR][SOLVE_NRHS];
-  __shared__ double dg[BR][BR + 1];   // diagonal block, dg[row][col]
+  constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;   // columns per pass of the L21 product
+  __shared__ double xv[BR][NQ];
+  __shared__ double xj[BR][NQ];
+  __shared__ double red[BR][NQ];
+  __shared__ double tile[BR][BR + 1];   // a 64x64 block of L11, tile[col][row]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int k = bk.b, f = F.f, s = F.s, m = f - s;
@@ -362,69 +369,79 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
-  for (int e = tid; e < BR * SOLVE_NRHS; e += 128) {
+  for (int e = tid; e < BR * NQ; e += 128) {
     const int c = e % BR, q = e / BR;
     xv[c][q] = (c < bw && q < nrhs) ? Wf[c0 + c + (size_t) q * f] : 0.0;
   }
   __syncthreads();
-  // y - L21^T x2 for my columns: warp per column, lanes over the update rows
-  for (int c = warp; c < bw; c += 4) {
-    double acc[SOLVE_NRHS];
+  // y - L21^T x2: warp w owns columns 16w..16w+15, G at a time; lanes run
+  // down the update rows with one coalesced load per column per step
+  const double* z = Wf + s;
+  for (int cg = warp * 16; cg < warp * 16 + 16; cg += G) {
+    double acc[G][NQ];
 #pragma unroll
-    for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
-    const double* pc = P + (size_t) (c0 + c) * f + s;
-    const double* z = Wf + s;
+    for (int a_ = 0; a_ < G; a_++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) acc[a_][q] = 0.0;
     for (int i = lane; i < m; i += 32) {
-      const double l = pc[i];
+      double zi[NQ];
 #pragma unroll
-      for (int q = 0; q < SOLVE_NRHS; q++)
-        if (q < nrhs) acc[q] += l * __ldcg(z + i + (size_t) q * f);
+      for (int q = 0; q < NQ; q++) zi[q] = (q < nrhs) ? __ldcg(z + i + (size_t) q * f) : 0.0;
+#pragma unroll
+      for (int a_ = 0; a_ < G; a_++) {
+        const double l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) acc[a_][q] += l * zi[q];
+      }
     }
 #pragma unroll
-    for (int q = 0; q < SOLVE_NRHS; q++) {
-      double v = acc[q];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      acc[q] = v;
-    }
-    if (lane == 0)
-      for (int q = 0; q < nrhs; q++) xv[c][q] -= acc[q];
+    for (int a_ = 0; a_ < G; a_++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        double v = acc[a_][q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && cg + a_ < bw) xv[cg + a_][q] -= v;
+      }
   }
   __syncthreads();
-  // solved blocks below, last first
+  // solved blocks below, last first: the block of L11 is staged before the
+  // wait for x_j
+  const int col = tid % BR, half = tid / BR;
   for (int j = nbs - 1; j > k; j--) {
-    wait_epoch(flags + F.blk_off + j, epoch, status);
     const int bwj = min(BR, s - j * BR);
-    for (int e = tid; e < BR * SOLVE_NRHS; e += 128) {
+    for (int e = tid; e < BR * BR; e += 128) {
+      const int i = e % BR, c = e / BR;
+      tile[c][i] = (i < bwj && c < bw) ? P[(j * BR + i) + (size_t) (c0 + c) * f] : 0.0;
+    }
+    wait_epoch(flags + F.blk_off + j, epoch, status);
+    for (int e = tid; e < BR * NQ; e += 128) {
       const int i = e % BR, q = e / BR;
       xj[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : 0.0;
     }
     __syncthreads();
-    for (int c = warp; c < bw; c += 4) {
-      const double* pc = P + (size_t) (c0 + c) * f + j * BR;
-      double acc[SOLVE_NRHS];
+    double acc[NQ];
 #pragma unroll
-      for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
-      for (int i = lane; i < bwj; i += 32) {
-        const double l = pc[i];
+    for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+#pragma unroll 8
+    for (int i = half * (BR / 2); i < half * (BR / 2) + BR / 2; i++) {
+      const double l = tile[col][i];
 #pragma unroll
-        for (int q = 0; q < SOLVE_NRHS; q++) acc[q] += l * xj[i][q];
-      }
-#pragma unroll
-      for (int q = 0; q < SOLVE_NRHS; q++) {
-        double v = acc[q];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[q] = v;
-      }
-      if (lane == 0)
-        for (int q = 0; q < nrhs; q++) xv[c][q] -= acc[q];
+      for (int q = 0; q < NQ; q++) acc[q] += l * xj[i][q];
     }
+    if (half == 1)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) red[col][q] = acc[q];
+    __syncthreads();
+    if (half == 0)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) xv[col][q] -= acc[q] + red[col][q];
     __syncthreads();
   }
   // L_kk^T substitution from the staged diagonal block, one warp, columns
   // lane and lane+32
   for (int e = tid; e < BR * BR; e += 128) {
-    const int i = e % BR, j = e / BR;
-    dg[i][j] = (i < bw && j < bw) ? P[(c0 + i) + (size_t) (c0 + j) * f] : 0.0;   // dg[row][col]
+    const int i = e % BR, c = e / BR;
+    tile[i][c] = (i < bw && c < bw) ? P[(c0 + i) + (size_t) (c0 + c) * f] : 0.0;   // tile[row][col]
   }
   __syncthreads();
   if (warp == 0) {
@@ -432,11 +449,11 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
       double v0 = xv[lane][q], v1 = xv[lane + 32][q];
       for (int c = bw - 1; c >= 0; c--) {
         const double src = (c < 32) ? __shfl_sync(0xffffffffu, v0, c) : __shfl_sync(0xffffffffu, v1, c - 32);
-        const double x = src / dg[c][c];
+        const double x = src / tile[c][c];
         if (lane == c) v0 = x;
-        else if (lane < c) v0 -= dg[c][lane] * x;
+        else if (lane < c) v0 -= tile[c][lane] * x;
         if (lane + 32 == c) v1 = x;
-        else if (lane + 32 < c) v1 -= dg[c][lane + 32] * x;
+        else if (lane + 32 < c) v1 -= tile[c][lane + 32] * x;
       }
       xv[lane][q] = v0;
       xv[lane + 32][q] = v1;
@@ -486,8 +503,15 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       }
       const int nb = (int) LP.solve_fwd_blocks.size();
       if (nb > 0) {
-        k_fwd_big<<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, Bq,
-                                      ld, W, nq, flags, ef, status);
+        const int2_* bl = D.sfwd + D.sfwd_off[h];
+        if (nq == 1)
+          k_fwd_big<1><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+        else if (nq == 2)
+          k_fwd_big<2><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+        else if (nq <= 4)
+          k_fwd_big<4><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+        else
+          k_fwd_big<8><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         count_launch();
       }
       prof_end(KC_SOLVE_FWD, st, 0.0, by);
@@ -504,8 +528,15 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
         k_gather_upd<<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                         Xq, ld, W, nq);
         count_launch();
-        k_bwd_big<<<nb, 128, 0, st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb,
-                                      status);
+        const int2_* bl = D.sbwd + D.sbwd_off[h];
+        if (nq == 1)
+          k_bwd_big<1><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+        else if (nq == 2)
+          k_bwd_big<2><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+        else if (nq <= 4)
+          k_bwd_big<4><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+        else
+          k_bwd_big<8><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
         count_launch();
       }
       const int ns = (int) LP.small_fronts.size();
