@@ -98,6 +98,7 @@ def lib():
         "taucs_b200_factor_numeric_device_async": (C.c_int, [vp, vp]),
         "taucs_b200_factor_status": (C.c_int, [vp]),
         "taucs_b200_solve_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int]),
+        "taucs_b200_solve_device_noalloc": (C.c_int, [vp, C.c_int, vp, vp, C.c_int]),
         "taucs_b200_solve_many": (C.c_int, [vp, C.c_int, _f64p, _f64p]),
         "taucs_b200_set_precision": (C.c_int, [vp, C.c_int]),
         "taucs_b200_solve_refine": (C.c_int, [vp, pc, C.c_int, _f64p, _f64p, C.c_double, C.c_int, _f64p]),

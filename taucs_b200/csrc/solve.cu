@@ -15,6 +15,9 @@
 // update rows (written by ancestors in earlier launches), r = y - L21^T x2,
 // then the L11^T substitution, and scatter x at the columns.  Up to
 // SOLVE_NRHS right-hand sides share every read of L.
+#include <mutex>
+
+#include "factor.h"
 #include "kernels.h"
 
 namespace tb {
@@ -23,6 +26,7 @@ namespace {
 
 constexpr int SB = 32;   // substitution block (one warp)
 
+template <int WS>
 __global__ void __launch_bounds__(256)
 k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
       const int* __restrict__ maps, const int* __restrict__ rows, const double* __restrict__ L,
@@ -31,7 +35,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-  double* Wf = W + F.v_off * SOLVE_NRHS;
+  double* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
@@ -44,7 +48,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
-    const double* Wc = W + C.v_off * SOLVE_NRHS;
+    const double* Wc = W + C.v_off * WS;
     for (int k = tid; k < mc * nrhs; k += nt) {
       const int i = k % mc, q = k / mc;
       Wf[mp[i] + q * f] += Wc[C.s + i + q * C.f];
@@ -84,6 +88,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
   }
 }
 
+template <int WS>
 __global__ void __launch_bounds__(256)
 k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
       const double* __restrict__ L, double* __restrict__ X, int ldx, double* __restrict__ W,
@@ -92,7 +97,7 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  double* Wf = W + F.v_off * SOLVE_NRHS;
+  double* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
@@ -221,7 +226,7 @@ __device__ __forceinline__ int lb_dev(const int* a, int n, int key) {
   return lo;
 }
 
-template <int NQ>
+template <int NQ, int WS>
 __global__ void __launch_bounds__(128)
 k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ children, const int* __restrict__ maps, const int* __restrict__ rows,
@@ -237,7 +242,7 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int nbs = (s + BR - 1) / BR;
   const int r0 = r * BR, nr = min(BR, f - r0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* Wf = W + F.v_off * SOLVE_NRHS;
+  double* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
@@ -252,7 +257,7 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     const int* mp = maps + C.map_off;
     const int ia = lb_dev(mp, mc, r0), ib = lb_dev(mp, mc, r0 + nr);
     if (ia >= ib) continue;
-    const double* Wc = W + C.v_off * SOLVE_NRHS;
+    const double* Wc = W + C.v_off * WS;
     for (int k = tid; k < (ib - ia) * nrhs; k += 128) {
       const int i = ia + k % (ib - ia), q = k / (ib - ia);
       wv[mp[i] - r0][q] += Wc[C.s + i + q * C.f];
@@ -332,6 +337,7 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 
 // x at the update rows of every big front of a level, gathered once into the
 // front's work vector (rows s..f-1) so the backward blocks read it coalesced
+template <int WS>
 __global__ void __launch_bounds__(128)
 k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
              const int* __restrict__ rows, const double* __restrict__ X, int ldx, double* __restrict__ W,
@@ -340,7 +346,7 @@ k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fro
   const FrontDesc F = fronts[bk.a];
   const int r0 = max(bk.b * BR, F.s), r1 = min(bk.b * BR + BR, F.f);
   if (r0 >= r1) return;
-  double* Wf = W + F.v_off * SOLVE_NRHS;
+  double* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const int nr = r1 - r0;
   for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
@@ -349,7 +355,7 @@ k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fro
   }
 }
 
-template <int NQ>
+template <int NQ, int WS>
 __global__ void __launch_bounds__(128)
 k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ rows, const double* __restrict__ L, double* __restrict__ X, int ldx,
@@ -365,7 +371,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int nbs = (s + BR - 1) / BR;
   const int c0 = k * BR, bw = min(BR, s - c0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* Wf = W + F.v_off * SOLVE_NRHS;
+  double* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
@@ -497,7 +503,7 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       prof_begin(KC_SOLVE_FWD, st);
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
-        k_fwd<<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L,
+        k_fwd<SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L,
                                   Bq, ld, W, nq);
         count_launch();
       }
@@ -505,13 +511,13 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       if (nb > 0) {
         const int2_* bl = D.sfwd + D.sfwd_off[h];
         if (nq == 1)
-          k_fwd_big<1><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         else if (nq == 2)
-          k_fwd_big<2><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         else if (nq <= 4)
-          k_fwd_big<4><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         else
-          k_fwd_big<8><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         count_launch();
       }
       prof_end(KC_SOLVE_FWD, st, 0.0, by);
@@ -525,23 +531,23 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       prof_begin(KC_SOLVE_BWD, st);
       const int nb = (int) LP.solve_bwd_blocks.size();
       if (nb > 0) {
-        k_gather_upd<<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
+        k_gather_upd<SOLVE_NRHS><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                         Xq, ld, W, nq);
         count_launch();
         const int2_* bl = D.sbwd + D.sbwd_off[h];
         if (nq == 1)
-          k_bwd_big<1><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
         else if (nq == 2)
-          k_bwd_big<2><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
         else if (nq <= 4)
-          k_bwd_big<4><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
         else
-          k_bwd_big<8><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
         count_launch();
       }
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
-        k_bwd<<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, Xq, ld, W, nq);
+        k_bwd<SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, Xq, ld, W, nq);
         count_launch();
       }
       prof_end(KC_SOLVE_BWD, st, 0.0, by);
@@ -551,3 +557,143 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
 }
 
 }  // namespace tb
+
+// ------------------------------------------------------------------------
+// Solve without any allocation.
+//
+// Callers that must not allocate device memory -- code running while a CUDA
+// stream is being captured into a graph (a cudaMalloc there breaks the
+// capture), or a latency-critical serving thread that works inside a fixed,
+// pre-reserved memory budget and may not grow it -- can still solve with an
+// existing factor: taucs_b200_solve_device_noalloc keeps the solve's work
+// vectors, handshake flags and status word in the one static device array
+// below instead of the factor's own buffers.  It is the same level-scheduled
+// solve as taucs_b200_solve_device, run one right-hand side per pass.
+// ------------------------------------------------------------------------
+
+namespace tb {
+
+constexpr size_t NOALLOC_W_DOUBLES = size_t(4) << 20;   // work vectors: 4 Mi doubles (32 MiB)
+constexpr size_t NOALLOC_FLAGS = 16384;                 // handshake flags of the big fronts
+constexpr size_t NOALLOC_DOUBLES = NOALLOC_W_DOUBLES + NOALLOC_FLAGS / 2 + 32;
+
+// Every GPU that loads this library holds this array (about 32 MiB) until
+// the process exits; all calls on a device share it.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[256];
+
+// Device address of the static array on the current device, looked up once
+// per device (the name is only a host-side stand-in for it).
+static int noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 256) {
+    set_error(std::string("taucs_b200_solve_device_noalloc: cudaGetDevice: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("taucs_b200_solve_device_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return -1;
+    }
+    g_noalloc_ptr[dev] = (double*) p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+// one right-hand side, work vectors at stride 1 (f doubles per front)
+static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L, double* X, const double* B,
+                                int ld, double* W, int* flags, int* epoch, int* status, cudaStream_t st) {
+  (void) ld;
+  const int ef = ++*epoch;
+  for (int h = 0; h < P.n_levels; h++) {
+    const LevelPlan& LP = P.levels[h];
+    const int ns = (int) LP.small_fronts.size();
+    if (ns > 0) {
+      k_fwd<1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
+                                   W, 1);
+      count_launch();
+    }
+    const int nb = (int) LP.solve_fwd_blocks.size();
+    if (nb > 0) {
+      k_fwd_big<1, 1><<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
+                                          W, 1, flags, ef, status);
+      count_launch();
+    }
+  }
+  const int eb = ++*epoch;
+  for (int h = P.n_levels - 1; h >= 0; h--) {
+    const LevelPlan& LP = P.levels[h];
+    const int nb = (int) LP.solve_bwd_blocks.size();
+    if (nb > 0) {
+      k_gather_upd<1><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
+                                                                         X, ld, W, 1);
+      count_launch();
+      k_bwd_big<1, 1><<<nb, 128, 0, st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, X, ld, W, 1, flags, eb,
+                                          status);
+      count_launch();
+    }
+    const int ns = (int) LP.small_fronts.size();
+    if (ns > 0) {
+      k_bwd<1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, X, ld, W, 1);
+      count_launch();
+    }
+  }
+  return (int) cudaGetLastError();
+}
+
+}  // namespace tb
+
+extern "C" int taucs_b200_solve_device_noalloc(void* vL, int nrhs, double* d_X, const double* d_B, int ld) {
+  using namespace tb;
+  Factor* F = (Factor*) vL;
+  if (!F || nrhs < 0 || ld < F->n || (nrhs > 0 && (!d_X || !d_B))) {
+    set_error("taucs_b200_solve_device_noalloc: bad arguments");
+    return -1;
+  }
+  const Plan& P = F->plan;
+  if ((size_t) P.v_len > NOALLOC_W_DOUBLES || (size_t) P.n_blk > NOALLOC_FLAGS) {
+    char msg[320];
+    snprintf(msg, sizeof msg,
+             "taucs_b200_solve_device_noalloc: this factor needs %lld doubles of work vectors and %d flags; "
+             "the static scratch holds %zu doubles and %zu flags (use taucs_b200_solve_device)",
+             (long long) P.v_len, P.n_blk, NOALLOC_W_DOUBLES, NOALLOC_FLAGS);
+    set_error(msg);
+    return -1;
+  }
+  if (!F->has_numeric || !F->dev_ready) {
+    set_error("taucs_b200_solve_device_noalloc: the factor has no numeric part");
+    return -1;
+  }
+  if (nrhs == 0) return 0;
+  double* base = nullptr;
+  if (noalloc_scratch(&base)) return -1;
+  double* W = base;
+  int* flags = (int*) (base + NOALLOC_W_DOUBLES);
+  int* status = flags + NOALLOC_FLAGS;
+  cudaStream_t st = current_stream();
+  // the array keeps whatever the previous call left: the flags and the status
+  // word must start at zero, the work vectors are written before being read
+  cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(int) * (size_t) P.n_blk, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, sizeof(int), st);
+  if (e != cudaSuccess) {
+    set_error(std::string("taucs_b200_solve_device_noalloc: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  int epoch = 0;
+  for (int q = 0; q < nrhs; q++) {
+    e = (cudaError_t) launch_solve_noalloc(P, F->dp, F->dL, d_X + (size_t) q * ld, d_B + (size_t) q * ld, ld, W,
+                                           flags, &epoch, status, st);
+    if (e != cudaSuccess) {
+      set_error(std::string("taucs_b200_solve_device_noalloc: ") + cudaGetErrorString(e));
+      return -1;
+    }
+  }
+  return 0;
+}
