@@ -259,6 +259,9 @@ taucs_ccs_matrix* taucs_b200_generate_lognormal(int X, int Y, int Z, double sigm
 #define TAUCS_B200_KC_OTHER       8
 int taucs_b200_profile(int enable);
 int taucs_b200_profile_read(int kernel_class, double* ms, long* launches, double* flops, double* bytes);
+/* every profiled launch in issue order: its class and device time (ms);
+ * copies at most cap entries and returns the number recorded */
+long taucs_b200_profile_log(int* kernel_class, float* ms, long cap);
 
 /* CUDA kernel launches issued by this library on the calling thread since
  * the last reset (for launch accounting in benchmarks). */

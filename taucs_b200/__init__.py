@@ -110,6 +110,7 @@ def lib():
         "taucs_b200_profile": (C.c_int, [C.c_int]),
         "taucs_b200_profile_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "taucs_b200_profile_log": (C.c_long, [vp, vp, C.c_long]),
         "taucs_b200_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():

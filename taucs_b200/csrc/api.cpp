@@ -40,19 +40,22 @@ static bool dev_upload(T** dst, const T* src, size_t n, cudaStream_t st) {
 int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
   std::vector<int> small, big;
   std::vector<Tile> tiles;
-  std::vector<int2_> sf, sb;
+  std::vector<int2_> sf, sb, sl;
   D->small_off.clear(); D->big_off.clear(); D->tile_off.clear(); D->sfwd_off.clear(); D->sbwd_off.clear();
+  D->sl21_off.clear();
   for (const LevelPlan& LP : P.levels) {
     D->small_off.push_back((int) small.size());
     D->big_off.push_back((int) big.size());
     D->tile_off.push_back((int) tiles.size());
     D->sfwd_off.push_back((int) sf.size());
     D->sbwd_off.push_back((int) sb.size());
+    D->sl21_off.push_back((int) sl.size());
     small.insert(small.end(), LP.small_fronts.begin(), LP.small_fronts.end());
     big.insert(big.end(), LP.big_fronts.begin(), LP.big_fronts.end());
     tiles.insert(tiles.end(), LP.build_tiles.begin(), LP.build_tiles.end());
     sf.insert(sf.end(), LP.solve_fwd_blocks.begin(), LP.solve_fwd_blocks.end());
     sb.insert(sb.end(), LP.solve_bwd_blocks.begin(), LP.solve_bwd_blocks.end());
+    sl.insert(sl.end(), LP.solve_l21_tasks.begin(), LP.solve_l21_tasks.end());
   }
   bool ok = dev_upload(&D->fronts, P.fronts.data(), P.fronts.size(), st)
          && dev_upload(&D->children, P.children.data(), P.children.size(), st)
@@ -65,7 +68,8 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
          && dev_upload(&D->big_list, big.data(), big.size(), st)
          && dev_upload(&D->tiles, tiles.data(), tiles.size(), st)
          && dev_upload(&D->sfwd, sf.data(), sf.size(), st)
-         && dev_upload(&D->sbwd, sb.data(), sb.size(), st);
+         && dev_upload(&D->sbwd, sb.data(), sb.size(), st)
+         && dev_upload(&D->sl21, sl.data(), sl.size(), st);
   if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "plan upload");
   return ok ? 0 : -1;
 }
@@ -74,7 +78,7 @@ void devplan_free(DevPlan* D) {
   cudaFree(D->fronts); cudaFree(D->children); cudaFree(D->rows); cudaFree(D->maps);
   cudaFree(D->acol_ptr); cudaFree(D->a_rows); cudaFree(D->a_idx);
   cudaFree(D->small_list); cudaFree(D->big_list); cudaFree(D->tiles);
-  cudaFree(D->sfwd); cudaFree(D->sbwd);
+  cudaFree(D->sfwd); cudaFree(D->sbwd); cudaFree(D->sl21);
   *D = DevPlan();
 }
 
@@ -93,6 +97,7 @@ static void free_device(Factor* F) {
   cudaFree(F->dA); F->dA = nullptr;
   cudaFree(F->dstatus); F->dstatus = nullptr;
   cudaFree(F->dW); F->dW = nullptr;
+  cudaFree(F->dpart); F->dpart = nullptr;
   cudaFree(F->dX); F->dX = nullptr;
   cudaFree(F->dscale); F->dscale = nullptr;
   cudaFree(F->dcolptr); F->dcolptr = nullptr;
@@ -124,6 +129,7 @@ static int ensure_device(Factor* F) {
          && dev_upload(&F->dflags, (const int*) nullptr, (size_t) P.n_blk, st)
          && cuda_ok(cudaMemsetAsync(F->dflags, 0, sizeof(int) * (size_t) P.n_blk, st), "flags")
          && dev_upload(&F->dW, (const double*) nullptr, (size_t) P.v_len * SOLVE_NRHS, st)
+         && dev_upload(&F->dpart, (const double*) nullptr, (size_t) P.part_len, st)
          && dev_upload(&F->dX, (const double*) nullptr, (size_t) F->n * SOLVE_NRHS, st)
          && dev_upload(&F->dcolptr, F->colptr.data(), F->colptr.size(), st)
          && dev_upload(&F->drowind, F->rowind.data(), F->rowind.size(), st)
@@ -217,7 +223,7 @@ int solve_device(Factor* F, int nrhs, double* dX, const double* dB, int ld) {
   if (!F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
   cudaStream_t st = current_stream();
   if (!cuda_ok(cudaMemsetAsync(F->dstatus + 1, 0, sizeof(int), st), "solve status")) return -1;
-  int e = launch_solve_fp64(F->plan, F->dp, F->dL, nrhs, dX, dB, ld, F->dW, F->dflags, &F->epoch,
+  int e = launch_solve_fp64(F->plan, F->dp, F->dL, nrhs, dX, dB, ld, F->dW, F->dpart, F->dflags, &F->epoch,
                             F->dstatus + 1, st);
   return cuda_ok((cudaError_t) e, "solve launch") ? 0 : -1;
 }

@@ -24,6 +24,7 @@ struct Factor {
   double* dA = nullptr;        // A values
   int* dstatus = nullptr;
   double* dW = nullptr;        // solve work vectors (v_len * SOLVE_NRHS)
+  double* dpart = nullptr;     // backward-solve partial sums (plan.part_len)
   double* dX = nullptr;        // solve staging (n * SOLVE_NRHS)
   int* hstatus = nullptr;      // pinned status readback (2 ints: factor, solve)
   double* dDinv = nullptr;     // inverses of the big fronts' 64x64 diagonal blocks

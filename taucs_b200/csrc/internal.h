@@ -67,7 +67,8 @@ struct FrontDesc {
   int64_t v_off;      // solve work-vector offset (f entries per right-hand side)
   int64_t dinv_off;   // inverses of the 64x64 diagonal blocks (big fronts), -1 otherwise
   int blk_off;        // solve flags: first of ceil(s/64) per big front, -1 otherwise
-  int pad_;
+  int nchunk;         // solve: row chunks of L21 for the backward partial products
+  int64_t part_off;   // solve: partial sums (nchunk x s x SOLVE_NRHS doubles), -1 if none
   int s, f;           // columns, front order (m = f - s)
   int child_begin;    // range in child list
   int child_end;
@@ -84,6 +85,7 @@ struct LevelPlan {
   // solve: big fronts are split into 64-row blocks, one CTA each
   std::vector<int2_> solve_fwd_blocks;   // (front, row block)
   std::vector<int2_> solve_bwd_blocks;   // (front, column block), last block first
+  std::vector<int2_> solve_l21_tasks;    // (front, column block << 16 | row chunk)
   // small fronts, fused kernel
   std::vector<int> small_fronts;
   // medium/large fronts
@@ -102,6 +104,7 @@ struct Plan {
   int64_t v_len = 0;               // doubles of per-front work vectors (1 rhs)
   int64_t dinv_len = 0;            // doubles of diagonal-block inverses
   int n_blk = 0;                   // solve flags
+  int64_t part_len = 0;            // doubles of backward partial sums
   int64_t nnz = 0;
   std::vector<FrontDesc> fronts;
   std::vector<int> children;       // device-order child indices

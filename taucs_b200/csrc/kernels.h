@@ -25,6 +25,8 @@ constexpr int GEMM_BN = 64;
 constexpr int GEMM_BK = 16;
 // right-hand sides handled per solve pass
 constexpr int SOLVE_NRHS = 8;
+// rows of L21 per CTA in the backward solve's partial products
+constexpr int SOLVE_RCH = 512;
 
 // Device copies of the plan arrays.
 struct DevPlan {
@@ -40,7 +42,8 @@ struct DevPlan {
   Tile* tiles = nullptr;
   int2_* sfwd = nullptr;       // solve blocks, all levels concatenated
   int2_* sbwd = nullptr;
-  std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off;  // per level (host)
+  int2_* sl21 = nullptr;
+  std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off, sl21_off;  // per level (host)
   std::vector<int> lvl_max_f_small;               // per level (host)
 };
 
@@ -61,7 +64,7 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
 // SOLVE_TIMEOUT if a bounded wait gave up
 constexpr int SOLVE_TIMEOUT = -2;
 int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
-                      const double* B, int ld, double* W, int* flags, int* epoch, int* status,
+                      const double* B, int ld, double* W, double* part, int* flags, int* epoch, int* status,
                       cudaStream_t st);
 
 // launch accounting

@@ -318,10 +318,23 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
         F.dinv_off = -1;
         F.blk_off = -1;
       }
-      F.pad_ = 0;
     }
     P.dinv_len = std::max<int64_t>(doff, 32);
     P.n_blk = std::max(boff, 1);
+    int64_t poff = 0;
+    for (int i = 0; i < nf; i++) {
+      FrontDesc& F = P.fronts[i];
+      const int m = F.f - F.s;
+      if (F.f > SMALL_F_MAX && m > 0) {
+        F.nchunk = (m + SOLVE_RCH - 1) / SOLVE_RCH;
+        F.part_off = poff;
+        poff += (int64_t) F.nchunk * F.s * SOLVE_NRHS;
+      } else {
+        F.nchunk = 0;
+        F.part_off = -1;
+      }
+    }
+    P.part_len = std::max<int64_t>(poff, 32);
   }
 
   // levels, front classes, build tiles
@@ -352,6 +365,9 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
           const int nrb = (F.f + PANEL_NB - 1) / PANEL_NB, nbs = (F.s + PANEL_NB - 1) / PANEL_NB;
           for (int r = 0; r < nrb; r++) LP.solve_fwd_blocks.push_back(int2_{i, r});
           for (int k = nbs - 1; k >= 0; k--) LP.solve_bwd_blocks.push_back(int2_{i, k});
+          const int nch = (m + SOLVE_RCH - 1) / SOLVE_RCH;
+          for (int k = 0; k < nbs; k++)
+            for (int c = 0; c < nch; c++) LP.solve_l21_tasks.push_back(int2_{i, (k << 16) | c});
         }
       }
       // the fused small-front kernel is launched per size class

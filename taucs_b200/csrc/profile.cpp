@@ -23,6 +23,7 @@ std::vector<cudaEvent_t> g_pool;
 cudaEvent_t g_open = nullptr;
 double g_ms[KC_COUNT], g_flops[KC_COUNT], g_bytes[KC_COUNT];
 long g_n[KC_COUNT];
+std::vector<std::pair<int, float>> g_log;   // (class, ms) of every launch, in order
 
 cudaEvent_t get_event() {
   if (!g_pool.empty()) {
@@ -41,6 +42,7 @@ void drain() {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, r.a, r.b);
     g_ms[r.kc] += ms;
+    if (g_log.size() < (size_t) 1 << 20) g_log.emplace_back(r.kc, ms);
     g_flops[r.kc] += r.flops;
     g_bytes[r.kc] += r.bytes;
     g_n[r.kc] += 1;
@@ -82,7 +84,19 @@ int taucs_b200_profile(int enable) {
   drain();
   g_on = enable != 0;
   for (int k = 0; k < KC_COUNT; k++) { g_ms[k] = g_flops[k] = g_bytes[k] = 0.0; g_n[k] = 0; }
+  g_log.clear();
   return 0;
+}
+
+long taucs_b200_profile_log(int* kernel_class, float* ms, long cap) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  drain();
+  const long n = (long) g_log.size();
+  for (long i = 0; i < n && i < cap; i++) {
+    if (kernel_class) kernel_class[i] = g_log[i].first;
+    if (ms) ms[i] = g_log[i].second;
+  }
+  return n;
 }
 
 int taucs_b200_profile_read(int kernel_class, double* ms, long* launches, double* flops, double* bytes) {

@@ -191,6 +191,7 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
 // can hang.
 
 constexpr int BR = PANEL_NB;   // rows per block
+constexpr size_t BWD_SMEM = 2 * BR * (BR + 1) * sizeof(double);
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -246,6 +247,14 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
+  if (r < nbs) {
+    // stage the diagonal block now, off the chain's critical path
+    const int bw = min(BR, s - r0);
+    for (int e = tid; e < BR * BR; e += 128) {
+      const int i = e % BR, j = e / BR;
+      dg[j][i] = (i < nr && j < bw) ? P[(r0 + i) + (size_t) (r0 + j) * f] : 0.0;
+    }
+  }
   for (int k = tid; k < BR * NQ; k += 128) {
     const int i = k % BR, q = k / BR;
     wv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : 0.0;
@@ -299,20 +308,19 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     for (int q = 0; q < NQ; q++) wv[row][q] -= acc[q] + part[row][q];
   __syncthreads();
   if (r < nbs) {
-    // diagonal block staged in shared memory, then one warp substitutes:
+    // the diagonal block was staged at kernel start; one warp substitutes:
     // lanes own rows lane and lane+32
     const int bw = min(BR, s - r0);
-    for (int e = tid; e < BR * BR; e += 128) {
-      const int i = e % BR, j = e / BR;
-      dg[j][i] = (i < nr && j < bw) ? P[(r0 + i) + (size_t) (r0 + j) * f] : 0.0;
-    }
-    __syncthreads();
     if (warp == 0) {
+      // reciprocal diagonal formed in parallel, off the substitution's critical path
+      const double rd0 = (lane < bw) ? 1.0 / dg[lane][lane] : 0.0;
+      const double rd1 = (lane + 32 < bw) ? 1.0 / dg[lane + 32][lane + 32] : 0.0;
       for (int q = 0; q < nrhs; q++) {
         double v0 = wv[lane][q], v1 = wv[lane + 32][q];
         for (int j = 0; j < bw; j++) {
           const double src = (j < 32) ? __shfl_sync(0xffffffffu, v0, j) : __shfl_sync(0xffffffffu, v1, j - 32);
-          const double xj = src / dg[j][j];
+          const double rj = (j < 32) ? __shfl_sync(0xffffffffu, rd0, j) : __shfl_sync(0xffffffffu, rd1, j - 32);
+          const double xj = src * rj;
           if (lane == j) v0 = xj;
           else if (lane > j) v0 -= dg[j][lane] * xj;
           if (lane + 32 == j) v1 = xj;
@@ -329,10 +337,8 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     Wf[r0 + i + (size_t) q * f] = wv[i][q];
   }
   __syncthreads();
-  if (r < nbs && tid == 0) {
-    __threadfence();
-    st_release(flags + F.blk_off + r, epoch);
-  }
+  // the barrier orders every thread's writes before thread 0's release store
+  if (r < nbs && tid == 0) st_release(flags + F.blk_off + r, epoch);
 }
 
 // x at the update rows of every big front of a level, gathered once into the
@@ -355,16 +361,65 @@ k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fro
   }
 }
 
+// Backward solve, L21^T x2 split over (column block, 512-row chunk) CTAs so
+// that the whole GPU streams L21; each CTA stores its partial sums, which the
+// chain kernel adds in chunk order.
 template <int NQ, int WS>
+__global__ void __launch_bounds__(128)
+k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts, const double* __restrict__ L,
+          const double* __restrict__ W, double* __restrict__ part, int nrhs) {
+  constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;
+  const int2_ tk = tasks[blockIdx.x];
+  const FrontDesc F = fronts[tk.a];
+  const int k = tk.b >> 16, ch = tk.b & 0xffff;
+  const int f = F.f, s = F.s, m = f - s;
+  const int c0 = k * BR, bw = min(BR, s - c0);
+  const int i0 = ch * SOLVE_RCH, i1 = min(m, i0 + SOLVE_RCH);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double* z = W + F.v_off * WS + s;
+  const double* P = L + F.l_off;
+  for (int cg = warp * 16; cg < warp * 16 + 16; cg += G) {
+    double acc[G][NQ];
+#pragma unroll
+    for (int a_ = 0; a_ < G; a_++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) acc[a_][q] = 0.0;
+    for (int i = i0 + lane; i < i1; i += 32) {
+      double zi[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) zi[q] = (q < nrhs) ? __ldcg(z + i + (size_t) q * f) : 0.0;
+#pragma unroll
+      for (int a_ = 0; a_ < G; a_++) {
+        const double l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) acc[a_][q] += l * zi[q];
+      }
+    }
+#pragma unroll
+    for (int a_ = 0; a_ < G; a_++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        double v = acc[a_][q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && cg + a_ < bw && q < nrhs)
+          part[F.part_off + ((size_t) ch * s + c0 + cg + a_) * SOLVE_NRHS + q] = v;
+      }
+  }
+}
+
+template <int NQ, int WS, bool PARTS>
 __global__ void __launch_bounds__(128)
 k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ rows, const double* __restrict__ L, double* __restrict__ X, int ldx,
-          double* __restrict__ W, int nrhs, int* __restrict__ flags, int epoch, int* status) {
+          double* __restrict__ W, const double* __restrict__ part, int nrhs, int* __restrict__ flags, int epoch,
+          int* status) {
   constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;   // columns per pass of the L21 product
   __shared__ double xv[BR][NQ];
   __shared__ double xj[BR][NQ];
   __shared__ double red[BR][NQ];
-  __shared__ double tile[BR][BR + 1];   // a 64x64 block of L11, tile[col][row]
+  extern __shared__ double bsm[];
+  double (*tile)[BR + 1] = reinterpret_cast<double (*)[BR + 1]>(bsm);             // block of L11, [col][row]
+  double (*dgb)[BR + 1] = reinterpret_cast<double (*)[BR + 1]>(bsm + BR * (BR + 1));  // diagonal block, [row][col]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int k = bk.b, f = F.f, s = F.s, m = f - s;
@@ -375,15 +430,32 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int* rw = rows + F.rows_off;
   const double* P = L + F.l_off;
 
+  // stage the diagonal block now, off the chain's critical path
+  for (int e = tid; e < BR * BR; e += 128) {
+    const int i = e % BR, c = e / BR;
+    dgb[i][c] = (i < bw && c < bw) ? P[(c0 + i) + (size_t) (c0 + c) * f] : 0.0;
+  }
   for (int e = tid; e < BR * NQ; e += 128) {
     const int c = e % BR, q = e / BR;
     xv[c][q] = (c < bw && q < nrhs) ? Wf[c0 + c + (size_t) q * f] : 0.0;
   }
   __syncthreads();
+  if (PARTS) {
+    // y - L21^T x2 from the per-chunk partial sums, added in chunk order
+    for (int e = tid; e < bw * NQ; e += 128) {
+      const int c = e % bw, q = e / bw;
+      if (q < nrhs) {
+        double acc = 0.0;
+        for (int ch = 0; ch < F.nchunk; ch++)
+          acc += __ldcg(part + F.part_off + ((size_t) ch * s + c0 + c) * SOLVE_NRHS + q);
+        xv[c][q] -= acc;
+      }
+    }
+  }
   // y - L21^T x2: warp w owns columns 16w..16w+15, G at a time; lanes run
   // down the update rows with one coalesced load per column per step
   const double* z = Wf + s;
-  for (int cg = warp * 16; cg < warp * 16 + 16; cg += G) {
+  for (int cg = warp * 16; !PARTS && cg < warp * 16 + 16; cg += G) {
     double acc[G][NQ];
 #pragma unroll
     for (int a_ = 0; a_ < G; a_++)
@@ -445,21 +517,19 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   }
   // L_kk^T substitution from the staged diagonal block, one warp, columns
   // lane and lane+32
-  for (int e = tid; e < BR * BR; e += 128) {
-    const int i = e % BR, c = e / BR;
-    tile[i][c] = (i < bw && c < bw) ? P[(c0 + i) + (size_t) (c0 + c) * f] : 0.0;   // tile[row][col]
-  }
-  __syncthreads();
   if (warp == 0) {
+    const double rd0 = (lane < bw) ? 1.0 / dgb[lane][lane] : 0.0;
+    const double rd1 = (lane + 32 < bw) ? 1.0 / dgb[lane + 32][lane + 32] : 0.0;
     for (int q = 0; q < nrhs; q++) {
       double v0 = xv[lane][q], v1 = xv[lane + 32][q];
       for (int c = bw - 1; c >= 0; c--) {
         const double src = (c < 32) ? __shfl_sync(0xffffffffu, v0, c) : __shfl_sync(0xffffffffu, v1, c - 32);
-        const double x = src / tile[c][c];
+        const double rc = (c < 32) ? __shfl_sync(0xffffffffu, rd0, c) : __shfl_sync(0xffffffffu, rd1, c - 32);
+        const double x = src * rc;
         if (lane == c) v0 = x;
-        else if (lane < c) v0 -= tile[c][lane] * x;
+        else if (lane < c) v0 -= dgb[c][lane] * x;
         if (lane + 32 == c) v1 = x;
-        else if (lane + 32 < c) v1 -= tile[c][lane + 32] * x;
+        else if (lane + 32 < c) v1 -= dgb[c][lane + 32] * x;
       }
       xv[lane][q] = v0;
       xv[lane + 32][q] = v1;
@@ -472,10 +542,8 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     X[rw[c0 + c] + (size_t) q * ldx] = xv[c][q];
   }
   __syncthreads();
-  if (tid == 0) {
-    __threadfence();
-    st_release(flags + F.blk_off + k, epoch);
-  }
+  // the barrier orders every thread's writes before thread 0's release store
+  if (tid == 0) st_release(flags + F.blk_off + k, epoch);
 }
 
 }  // namespace
@@ -487,9 +555,21 @@ static double solve_pass_bytes(const FrontDesc& F, int nrhs) {
   return 8.0 * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * 8.0 * nrhs * F.f;
 }
 
+static void solve_attrs() {
+  static bool done = false;
+  if (done) return;
+  cudaFuncSetAttribute(k_bwd_big<1, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
+  cudaFuncSetAttribute(k_bwd_big<2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
+  cudaFuncSetAttribute(k_bwd_big<4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
+  cudaFuncSetAttribute(k_bwd_big<8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
+  cudaFuncSetAttribute(k_bwd_big<1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
+  done = true;
+}
+
 int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
-                      const double* B, int ld, double* W, int* flags, int* epoch, int* status,
+                      const double* B, int ld, double* W, double* part, int* flags, int* epoch, int* status,
                       cudaStream_t st) {
+  solve_attrs();
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
     const double* Bq = B + (size_t) q0 * ld;
@@ -534,15 +614,24 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
         k_gather_upd<SOLVE_NRHS><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                         Xq, ld, W, nq);
         count_launch();
+        const int nt = (int) LP.solve_l21_tasks.size();
+        const int2_* tl = D.sl21 + D.sl21_off[h];
+        if (nt > 0) {
+          if (nq == 1) k_bwd_l21<1, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          else if (nq == 2) k_bwd_l21<2, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          else if (nq <= 4) k_bwd_l21<4, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          else k_bwd_l21<8, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          count_launch();
+        }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
         if (nq == 1)
-          k_bwd_big<1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<1, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq == 2)
-          k_bwd_big<2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<2, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
-          k_bwd_big<4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<4, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         else
-          k_bwd_big<8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, nq, flags, eb, status);
+          k_bwd_big<8, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         count_launch();
       }
       const int ns = (int) LP.small_fronts.size();
@@ -610,7 +699,7 @@ static int noalloc_scratch(double** out) {
 // one right-hand side, work vectors at stride 1 (f doubles per front)
 static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L, double* X, const double* B,
                                 int ld, double* W, int* flags, int* epoch, int* status, cudaStream_t st) {
-  (void) ld;
+  solve_attrs();
   const int ef = ++*epoch;
   for (int h = 0; h < P.n_levels; h++) {
     const LevelPlan& LP = P.levels[h];
@@ -635,8 +724,8 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
       k_gather_upd<1><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                          X, ld, W, 1);
       count_launch();
-      k_bwd_big<1, 1><<<nb, 128, 0, st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, X, ld, W, 1, flags, eb,
-                                          status);
+      k_bwd_big<1, 1, false><<<nb, 128, BWD_SMEM, st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, X, ld, W, nullptr, 1,
+                                                 flags, eb, status);
       count_launch();
     }
     const int ns = (int) LP.small_fronts.size();
