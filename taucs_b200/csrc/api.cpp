@@ -23,7 +23,7 @@ cudaStream_t current_stream() { return g_stream; }
 static std::atomic<long> g_launches{0};
 void count_launch(long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
-static bool cuda_ok(cudaError_t e, const char* what) {
+bool cuda_ok(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return true;
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
   return false;
@@ -82,13 +82,15 @@ void devplan_free(DevPlan* D) {
   *D = DevPlan();
 }
 
-static void free_numeric(Factor* F) {
+void free_numeric(Factor* F) {
   cudaFree(F->dL); F->dL = nullptr;
   cudaFree(F->dU); F->dU = nullptr;
   cudaFree(F->dDinv); F->dDinv = nullptr;
   cudaFree(F->dL32); F->dL32 = nullptr;
   cudaFree(F->dU32); F->dU32 = nullptr;
+  cudaFree(F->dDinv32); F->dDinv32 = nullptr;
   F->has_numeric = false;
+  F->has_numeric32 = false;
 }
 
 static void free_device(Factor* F) {
@@ -102,6 +104,22 @@ static void free_device(Factor* F) {
   cudaFree(F->dscale); F->dscale = nullptr;
   cudaFree(F->dcolptr); F->dcolptr = nullptr;
   cudaFree(F->drowind); F->drowind = nullptr;
+  cudaFree(F->dA32); F->dA32 = nullptr;
+  cudaFree(F->dW32); F->dW32 = nullptr;
+  cudaFree(F->dpart32); F->dpart32 = nullptr;
+  cudaFree(F->dV32); F->dV32 = nullptr;
+  cudaFree(F->dcolidx); F->dcolidx = nullptr;
+  cudaFree(F->ddiagpos); F->ddiagpos = nullptr;
+  cudaFree(F->dcsr_ptr); F->dcsr_ptr = nullptr;
+  cudaFree(F->dcsr_col); F->dcsr_col = nullptr;
+  cudaFree(F->dcsr_val); F->dcsr_val = nullptr;
+  cudaFree(F->dR); F->dR = nullptr;
+  cudaFree(F->dXr); F->dXr = nullptr;
+  cudaFree(F->dBr); F->dBr = nullptr;
+  cudaFree(F->dnorm); F->dnorm = nullptr;
+  if (F->hnorm) cudaFreeHost(F->hnorm);
+  F->hnorm = nullptr;
+  F->refine_ready = false;
   cudaFree(F->dflags); F->dflags = nullptr;
   if (F->hstatus) cudaFreeHost(F->hstatus);
   F->hstatus = nullptr;
@@ -109,7 +127,7 @@ static void free_device(Factor* F) {
 }
 
 // device plan and per-handle buffers, allocated on the first numeric call
-static int ensure_device(Factor* F) {
+int ensure_device(Factor* F) {
   if (F->dev_ready) return 0;
   int dev = 0;
   if (!cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) return -1;
@@ -173,9 +191,7 @@ Factor* symbolic(taucs_ccs_matrix* A, int max_depth) {
   return F;
 }
 
-int numeric_device(Factor* F, const double* d_vals, bool wait);
-
-int numeric_device(Factor* F, const double* d_vals, bool wait) {
+int numeric_fp64_device(Factor* F, const double* d_vals, bool wait) {
   if (ensure_device(F)) return -1;
   cudaStream_t st = current_stream();
   const Plan& P = F->plan;
@@ -188,6 +204,7 @@ int numeric_device(Factor* F, const double* d_vals, bool wait) {
     free_numeric(F);
     return -1;
   }
+  F->dvals_cur = d_vals;
   int e = launch_numeric_fp64(P, F->dp, d_vals, F->dL, F->dU, F->dDinv, F->dstatus, st);
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   if (!cuda_ok(cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st), "status")) return -1;
@@ -201,6 +218,19 @@ int numeric_device(Factor* F, const double* d_vals, bool wait) {
     return -1;
   }
   return 0;
+}
+
+int numeric_fp32_device(Factor* F, const double* d_vals);
+
+int numeric_device(Factor* F, const double* d_vals, bool wait) {
+  if (F->precision == 1) {
+    // FP32 fronts; a nonpositive FP32 pivot falls back to the FP64 factor
+    free_numeric(F);
+    if (numeric_fp32_device(F, d_vals) == 0) return 0;
+    tprintf("\t\tFP32 factorization failed; refactoring in FP64\n");
+    return numeric_fp64_device(F, d_vals, true);
+  }
+  return numeric_fp64_device(F, d_vals, wait);
 }
 
 int numeric_host(Factor* F, taucs_ccs_matrix* A) {
@@ -240,7 +270,12 @@ static int solve_status(Factor* F, cudaStream_t st) {
   return 0;
 }
 
+int solve_refine_host(Factor* F, taucs_ccs_matrix* A, int nrhs, double* X, const double* B, double tol, int maxits,
+                      double* res);
+
 int solve_host(Factor* F, int nrhs, double* X, const double* B) {
+  if (F && !F->has_numeric && F->has_numeric32)   // FP32 factor: refined to a 1e-12 scaled residual
+    return solve_refine_host(F, nullptr, nrhs, X, B, 1e-12, 10, nullptr) < 0 ? -1 : 0;
   if (!F || !F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
   cudaStream_t st = current_stream();
   const int n = F->n;
@@ -360,7 +395,8 @@ int taucs_b200_factor_numeric_device_async(void* L, const double* d_values) {
 
 int taucs_b200_factor_status(void* vL) {
   Factor* F = (Factor*) vL;
-  if (!F || !F->has_numeric) return -1;
+  if (!F || (!F->has_numeric && !F->has_numeric32)) return -1;
+  if (!F->has_numeric) return 0;
   if (!cuda_ok(cudaStreamSynchronize(current_stream()), "status")) return -1;
   if (*F->hstatus != INT_MAX) { free_numeric(F); return -1; }
   return 0;

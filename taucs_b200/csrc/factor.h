@@ -33,14 +33,36 @@ struct Factor {
   bool has_numeric = false;
   int precision = 0;           // 0 FP64, 1 FP32 fronts
 
-  // FP32 path
+  // FP32 fronts (precision 1) and iterative refinement
   float* dL32 = nullptr;
   float* dU32 = nullptr;
-  double* dscale = nullptr;    // diagonal scaling (n)
-  int* dcolptr = nullptr;      // device copy of the permuted pattern (for SpMV)
+  float* dDinv32 = nullptr;
+  float* dA32 = nullptr;       // scaled values D A D in FP32
+  float* dW32 = nullptr;       // solve work vectors (FP32)
+  float* dpart32 = nullptr;
+  float* dV32 = nullptr;       // FP32 right-hand sides / corrections (n x SOLVE_NRHS)
+  double* dscale = nullptr;    // D = diag(A)^-1/2 (n)
+  bool has_numeric32 = false;
+  int* dcolptr = nullptr;      // device copy of the permuted pattern
   int* drowind = nullptr;
+  int* dcolidx = nullptr;      // column of every entry (nnz)
+  int* ddiagpos = nullptr;     // position of each column's diagonal entry (n)
+  int* dcsr_ptr = nullptr;     // full symmetric CSR of the pattern, for the FP64 residual
+  int* dcsr_col = nullptr;
+  int* dcsr_val = nullptr;     // index of each CSR entry in A's value array
+  double* dR = nullptr;        // residual (n x SOLVE_NRHS)
+  double* dXr = nullptr;       // refined solution (n x SOLVE_NRHS)
+  double* dBr = nullptr;       // right-hand sides (n x SOLVE_NRHS)
+  unsigned long long* dnorm = nullptr;  // 2 x SOLVE_NRHS inf-norm bit patterns
+  unsigned long long* hnorm = nullptr;  // pinned readback
+  bool refine_ready = false;
+  const double* dvals_cur = nullptr;   // values of the last numeric factorization (device)
 };
 
 cudaStream_t current_stream();
+bool cuda_ok(cudaError_t e, const char* what);
+int ensure_device(Factor* F);
+void free_numeric(Factor* F);
+int numeric_fp64_device(Factor* F, const double* d_vals, bool wait);
 
 }  // namespace tb

@@ -55,6 +55,9 @@ void devplan_free(DevPlan* D);
 // INT_MAX; returns a cudaError_t code
 int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L,
                         double* U, double* Dinv, int* status, cudaStream_t st);
+// the same factorization with FP32 fronts (TF32x3 tensor products)
+int launch_numeric_fp32(const Plan& P, const DevPlan& D, const float* vals, float* L,
+                        float* U, float* Dinv, int* status, cudaStream_t st);
 
 // multi-RHS solve, device vectors in permuted order: X (n x nrhs, ld) from
 // B (n x nrhs, ld); W scratch of P.v_len * SOLVE_NRHS doubles, Y n *
@@ -65,6 +68,10 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
 constexpr int SOLVE_TIMEOUT = -2;
 int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
                       const double* B, int ld, double* W, double* part, int* flags, int* epoch, int* status,
+                      cudaStream_t st);
+// the same solve on an FP32 factor with FP32 vectors
+int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, int nrhs, float* X,
+                      const float* B, int ld, float* W, float* part, int* flags, int* epoch, int* status,
                       cudaStream_t st);
 
 // launch accounting

@@ -47,6 +47,9 @@ __device__ __forceinline__ int lower_bound_dev(const int* a, int n, int key) {
   return lo;
 }
 
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+
 __device__ __forceinline__ bool failed(const int* status) {
   return *(volatile const int*) status != INT_MAX;
 }
@@ -55,14 +58,16 @@ __global__ void k_init_status(int* status) { *status = INT_MAX; }
 
 // ------------------------------------------------------------ small fronts
 
+template <typename T>
 __global__ void __launch_bounds__(128)
 k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
               const int* __restrict__ children, const int* __restrict__ maps,
               const int* __restrict__ rows, const int* __restrict__ acol_ptr,
               const int* __restrict__ a_rows, const int* __restrict__ a_idx,
-              const double* __restrict__ vals, double* __restrict__ L, double* __restrict__ U,
+              const T* __restrict__ vals, T* __restrict__ L, T* __restrict__ U,
               int* status) {
-  extern __shared__ double W[];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* W = reinterpret_cast<T*>(smraw);
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s, m = f - s;
@@ -79,7 +84,7 @@ k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
-    const double* Uc = U + C.u_off;
+    const T* Uc = U + C.u_off;
     for (int j = warp; j < mc; j += nw) {
       const int pj = mp[j] * f;
       for (int i = j + lane; i < mc; i += 32) W[mp[i] + pj] += Uc[i + (size_t) j * mc];
@@ -87,28 +92,28 @@ k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts
     __syncthreads();
   }
   for (int j = 0; j < s; j++) {
-    const double d = W[j + j * f];
+    const T d = W[j + j * f];
     if (!(d > 0.0)) {
       if (tid == 0) atomicMin(status, rows[F.rows_off + j]);
       return;
     }
     __syncthreads();
-    const double rj = rsqrt(d);
+    const T rj = rsqrt_t(d);
     for (int i = j + 1 + tid; i < f; i += nt) W[i + j * f] *= rj;
     if (tid == 0) W[j + j * f] = d * rj;
     __syncthreads();
     for (int k = j + 1 + warp; k < f; k += nw) {
-      const double lkj = W[k + j * f];
-      double* wk = W + k * f;
-      const double* wj = W + j * f;
+      const T lkj = W[k + j * f];
+      T* wk = W + k * f;
+      const T* wj = W + j * f;
       for (int i = k + lane; i < f; i += 32) wk[i] -= wj[i] * lkj;
     }
     __syncthreads();
   }
-  double* Lp = L + F.l_off;
+  T* Lp = L + F.l_off;
   for (int k = tid; k < f * s; k += nt) Lp[k] = W[k];
   if (m > 0) {
-    double* Up = U + F.u_off;
+    T* Up = U + F.u_off;
     for (int k = tid; k < m * m; k += nt) {
       const int i = k % m, c = k / m;
       Up[k] = W[(s + i) + (s + c) * f];
@@ -118,27 +123,28 @@ k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts
 
 // --------------------------------------------------------------- front build
 
+template <typename T>
 __global__ void __launch_bounds__(256)
 k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
         const int* __restrict__ children, const int* __restrict__ maps,
         const int* __restrict__ acol_ptr, const int* __restrict__ a_rows,
-        const int* __restrict__ a_idx, const double* __restrict__ vals,
-        double* __restrict__ L, double* __restrict__ U, const int* status) {
-  __shared__ double W[BUILD_TR * BUILD_TC];
+        const int* __restrict__ a_idx, const T* __restrict__ vals,
+        T* __restrict__ L, T* __restrict__ U, const int* status) {
+  __shared__ T W[BUILD_TR * BUILD_TC];
   if (failed(status)) return;
-  const Tile T = tiles[blockIdx.x];
-  const FrontDesc F = fronts[T.front];
+  const Tile tl = tiles[blockIdx.x];
+  const FrontDesc F = fronts[tl.front];
   const int f = F.f, s = F.s, m = f - s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  const bool panel = T.c0 >= 0;
+  const bool panel = tl.c0 >= 0;
   int R0, C0, nr, nc;
   if (panel) {
-    R0 = T.r0; C0 = T.c0;
+    R0 = tl.r0; C0 = tl.c0;
     nr = min(BUILD_TR, f - R0); nc = min(BUILD_TC, s - C0);
   } else {
-    const int uc0 = -1 - T.c0;
-    R0 = s + T.r0; C0 = s + uc0;
-    nr = min(BUILD_TR, m - T.r0); nc = min(BUILD_TC, m - uc0);
+    const int uc0 = -1 - tl.c0;
+    R0 = s + tl.r0; C0 = s + uc0;
+    nr = min(BUILD_TR, m - tl.r0); nc = min(BUILD_TC, m - uc0);
   }
   for (int k = tid; k < BUILD_TR * BUILD_TC; k += nt) W[k] = 0.0;
   __syncthreads();
@@ -160,22 +166,22 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     if (ja >= jb) continue;
     const int ia = lower_bound_dev(mp, mc, R0), ib = lower_bound_dev(mp, mc, R0 + nr);
     if (ia >= ib) continue;
-    const double* Uc = U + C.u_off;
+    const T* Uc = U + C.u_off;
     for (int j = ja + warp; j < jb; j += nw) {
       const int pj = (mp[j] - C0) * BUILD_TR;
-      const double* uj = Uc + (size_t) j * mc;
+      const T* uj = Uc + (size_t) j * mc;
       for (int i = max(ia, j) + lane; i < ib; i += 32) W[(mp[i] - R0) + pj] += uj[i];
     }
     __syncthreads();
   }
   if (panel) {
-    double* dst = L + F.l_off;
+    T* dst = L + F.l_off;
     for (int k = tid; k < BUILD_TR * BUILD_TC; k += nt) {
       const int r = k % BUILD_TR, c = k / BUILD_TR;
       if (r < nr && c < nc) dst[(R0 + r) + (size_t) (C0 + c) * f] = W[k];
     }
   } else {
-    double* dst = U + F.u_off;
+    T* dst = U + F.u_off;
     for (int k = tid; k < BUILD_TR * BUILD_TC; k += nt) {
       const int r = k % BUILD_TR, c = k / BUILD_TR;
       if (r < nr && c < nc) dst[(R0 - s + r) + (size_t) (C0 - s + c) * m] = W[k];
@@ -186,7 +192,6 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
 // ------------------------------------------------------- blocked POTRF+TRSM
 
 constexpr int DLD = PANEL_NB + 1;  // padded column stride of the diagonal block
-constexpr size_t POTRF_SMEM = (2 * PANEL_NB * DLD + 32 * DLD) * sizeof(double);
 
 // Lower Cholesky of an n x n (n <= 32) block held in shared memory (ld `ld`),
 // by one warp: lane i keeps row i in registers and the right-looking updates
@@ -194,22 +199,23 @@ constexpr size_t POTRF_SMEM = (2 * PANEL_NB * DLD + 32 * DLD) * sizeof(double);
 // shuffle, one reciprocal square root and one multiply; every division of
 // the textbook loop is replaced by a multiply with rsqrt(pivot).  Returns the
 // first nonpositive pivot (or -1) in every lane.
-__device__ int warp_potrf32(double* S, int ld, int n) {
+template <typename T>
+__device__ int warp_potrf32(T* S, int ld, int n) {
   const int lane = threadIdx.x & 31;
-  double a[32];
+  T a[32];
 #pragma unroll
   for (int k = 0; k < 32; k++) a[k] = (lane < n && k <= lane) ? S[lane + k * ld] : 0.0;
   int bad = -1;
 #pragma unroll
   for (int j = 0; j < 32; j++) {
     if (j < n) {
-      const double d = __shfl_sync(0xffffffffu, a[j], j);
+      const T d = __shfl_sync(0xffffffffu, a[j], j);
       if (!(d > 0.0) && bad < 0) bad = j;
-      const double r = rsqrt(d);
+      const T r = rsqrt_t(d);
       a[j] = (lane == j) ? d * r : a[j] * r;
 #pragma unroll
       for (int k = j + 1; k < 32; k++) {
-        const double lkj = __shfl_sync(0xffffffffu, a[j], k);
+        const T lkj = __shfl_sync(0xffffffffu, a[j], k);
         if (lane >= k) a[k] -= a[j] * lkj;
       }
     }
@@ -224,23 +230,24 @@ __device__ int warp_potrf32(double* S, int ld, int n) {
 // computes column t by forward substitution; L is read as broadcasts, the
 // reciprocal diagonal is formed once in parallel, and each dot product is
 // split over four accumulators to shorten the dependent FMA chain.
-__device__ void warp_trinv32(const double* S, int ld, double* X, int ldx, int n) {
+template <typename T>
+__device__ void warp_trinv32(const T* S, int ld, T* X, int ldx, int n) {
   const int t = threadIdx.x & 31;
-  const double rd_own = (t < n) ? 1.0 / S[t + t * ld] : 0.0;
-  double x[32];
+  const T rd_own = (t < n) ? T(1) / S[t + t * ld] : T(0);
+  T x[32];
 #pragma unroll
   for (int i = 0; i < 32; i++) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    T a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
 #pragma unroll
     for (int k = 0; k < i; k++) {
-      const double p = S[i + k * ld] * x[k];
+      const T p = S[i + k * ld] * x[k];
       if ((k & 3) == 0) a0 += p;
       else if ((k & 3) == 1) a1 += p;
       else if ((k & 3) == 2) a2 += p;
       else a3 += p;
     }
-    const double rdi = __shfl_sync(0xffffffffu, rd_own, i);
-    x[i] = (i < n) ? (((i == t) ? 1.0 : 0.0) - ((a0 + a1) + (a2 + a3))) * rdi : 0.0;
+    const T rdi = __shfl_sync(0xffffffffu, rd_own, i);
+    x[i] = (i < n) ? (((i == t) ? T(1) : T(0)) - ((a0 + a1) + (a2 + a3))) * rdi : 0.0;
   }
 #pragma unroll
   for (int i = 0; i < 32; i++) X[i + t * ldx] = (t < n) ? x[i] : 0.0;
@@ -250,14 +257,14 @@ __device__ void warp_trinv32(const double* S, int ld, double* X, int ldx, int n)
 // diagonal block.  Thread (i = tid % 32, warp w) owns C[i][8w .. 8w+7]: eight
 // independent accumulation chains, A read with unit stride across lanes and
 // B read as warp-wide broadcasts.  TRANSB selects B^T.
-template <bool TRANSB>
-__device__ __forceinline__ void prod32(const double* A, int lda, const double* B, int ldb, double (&c)[8]) {
+template <bool TRANSB, typename T>
+__device__ __forceinline__ void prod32(const T* A, int lda, const T* B, int ldb, T (&c)[8]) {
   const int i = threadIdx.x & 31, j0 = (threadIdx.x >> 5) * 8;
 #pragma unroll
   for (int q = 0; q < 8; q++) c[q] = 0.0;
 #pragma unroll 8
   for (int k = 0; k < 32; k++) {
-    const double a = A[i + k * lda];
+    const T a = A[i + k * lda];
 #pragma unroll
     for (int q = 0; q < 8; q++) c[q] += a * (TRANSB ? B[(j0 + q) + k * ldb] : B[k + (j0 + q) * ldb]);
   }
@@ -269,14 +276,16 @@ __device__ __forceinline__ void prod32(const double* A, int lda, const double* B
 // of the factored block (lower, ld PANEL_NB) for the TRSM of the rows below.
 // The block is padded with the identity to 64 x 64 so that the warp routines
 // always run at their compile-time size.
+template <typename T>
 __global__ void __launch_bounds__(128)
 k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-             const int* __restrict__ rows, double* __restrict__ L, double* __restrict__ Dinv, int kb,
+             const int* __restrict__ rows, T* __restrict__ L, T* __restrict__ Dinv, int kb,
              int* status) {
-  extern __shared__ double sm[];
-  double* D = sm;                        // the block, col-major, ld DLD
-  double* X = sm + PANEL_NB * DLD;       // its inverse
-  double* T = X + PANEL_NB * DLD;        // 32 x DLD scratch
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  T* D = sm;                        // the block, col-major, ld DLD
+  T* X = sm + PANEL_NB * DLD;       // its inverse
+  T* Ts = X + PANEL_NB * DLD;       // 32 x DLD scratch
   __shared__ int bad;
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.x]];
@@ -284,13 +293,13 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
   if (kb >= s) return;
   const int w = min(PANEL_NB, s - kb);
   const int tid = threadIdx.x, warp = tid >> 5;
-  double* P = L + F.l_off;
+  T* P = L + F.l_off;
   {
-    double v[PANEL_NB * PANEL_NB / 128];
+    T v[PANEL_NB * PANEL_NB / 128];
 #pragma unroll
     for (int q = 0; q < PANEL_NB * PANEL_NB / 128; q++) {
       const int k = tid + q * 128, i = k % PANEL_NB, j = k / PANEL_NB;
-      v[q] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? 1.0 : 0.0);
+      v[q] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
     }
 #pragma unroll
     for (int q = 0; q < PANEL_NB * PANEL_NB / 128; q++) {
@@ -301,11 +310,11 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
   }
   if (tid == 0) bad = -1;
   __syncthreads();
-  double c[8];
+  T c[8];
   const int ci = tid & 31, cj = (tid >> 5) * 8;
-  double* D21 = D + 32;
-  double* D22 = D + 32 + 32 * DLD;
-  double* X22 = X + 32 + 32 * DLD;
+  T* D21 = D + 32;
+  T* D22 = D + 32 + 32 * DLD;
+  T* X22 = X + 32 + 32 * DLD;
   if (warp == 0) {
     const int b = warp_potrf32(D, DLD, 32);
     if (b < 0) warp_trinv32(D, DLD, X, DLD, 32);
@@ -341,9 +350,9 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
   // X21 = -X22 (L21 X11)
   prod32<false>(D21, DLD, X, DLD, c);
 #pragma unroll
-  for (int q = 0; q < 8; q++) T[ci + (cj + q) * DLD] = c[q];
+  for (int q = 0; q < 8; q++) Ts[ci + (cj + q) * DLD] = c[q];
   __syncthreads();
-  prod32<false>(X22, DLD, T, DLD, c);
+  prod32<false>(X22, DLD, Ts, DLD, c);
 #pragma unroll
   for (int q = 0; q < 8; q++) X[32 + ci + (cj + q) * DLD] = -c[q];
   __syncthreads();
@@ -351,7 +360,7 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
     const int i = k % w, j = k / w;
     if (i >= j) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * DLD];
   }
-  double* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
+  T* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
   for (int k = tid; k < PANEL_NB * PANEL_NB; k += 128) {
     const int i = k % PANEL_NB, j = k / PANEL_NB;
     Di[k] = (i < w && j < w) ? X[i + j * DLD] : 0.0;
@@ -376,16 +385,58 @@ __device__ __forceinline__ void dmma16888(double (&c)[4], const double (&a)[4], 
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
+__device__ __forceinline__ void cp_async_t(double* smem, const double* gmem, bool pred) { cp_async8(smem, gmem, pred); }
+__device__ __forceinline__ void cp_async_t(float* smem, const float* gmem, bool pred) {
+  const unsigned saddr = (unsigned) __cvta_generic_to_shared(smem);
+  const int sz = pred ? 4 : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(gmem), "r"(sz));
+}
+
+// FP64 fronts: one DMMA per fragment pair
+__device__ __forceinline__ void mma_tile(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  dmma16888(c, a, b);
+}
+
+// FP32 fronts: three TF32 products per fragment pair (hi*hi + hi*lo + lo*hi,
+// the operands split as x = tf32(x) + tf32(x - tf32(x))), which keeps close
+// to FP32 accuracy on the TF32 tensor path (same m16n8k8 fragment layout as
+// the FP64 DMMA)
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+  const float r = x - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ void mma_tile(float (&c)[4], const float (&a)[4], const float (&b)[2]) {
+  unsigned ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+  for (int i = 0; i < 4; i++) split_tf32(a[i], ah[i], al[i]);
+#pragma unroll
+  for (int i = 0; i < 2; i++) split_tf32(b[i], bh[i], bl[i]);
+  mma_tf32(c, al, bh);
+  mma_tf32(c, ah, bl);
+  mma_tf32(c, ah, bh);
+}
+
 constexpr int TLD = PANEL_NB + 8;  // padded k-row stride of the TRSM operands
 
 // Step kb: rows below the diagonal block, X := X L_kk^-T = X * Dinv^T, one
 // CTA per 64-row slab, DMMA m16n8k8; in place (the slab is staged first).
+template <typename T>
 __global__ void __launch_bounds__(128)
 k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-       double* __restrict__ L, const double* __restrict__ Dinv, int kb, const int* status) {
-  extern __shared__ double sm[];
-  double* As = sm;                        // [k][r]: slab, k-major
-  double* Bs = sm + PANEL_NB * TLD;       // [k][c]: Dinv[c][k]
+       T* __restrict__ L, const T* __restrict__ Dinv, int kb, const int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  T* As = sm;                        // [k][r]: slab, k-major
+  T* Bs = sm + PANEL_NB * TLD;       // [k][c]: Dinv[c][k]
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.y]];
   const int f = F.f, s = F.s;
@@ -395,8 +446,8 @@ k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
   if (r0 >= f) return;
   const int nr = min(TRSM_ROWS, f - r0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* P = L + F.l_off;
-  const double* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
+  T* P = L + F.l_off;
+  const T* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
   for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
     const int r = e % PANEL_NB, k = e / PANEL_NB;
     As[k * TLD + r] = (r < nr && k < w) ? P[(r0 + r) + (size_t) (kb + k) * f] : 0.0;
@@ -404,7 +455,7 @@ k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
   }
   __syncthreads();
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
-  double acc[2][4][4];
+  T acc[2][4][4];
 #pragma unroll
   for (int a = 0; a < 2; a++)
 #pragma unroll
@@ -412,7 +463,7 @@ k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
 #pragma unroll
       for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
   for (int kk = 0; kk < PANEL_NB; kk += 8) {
-    double a[2][4], b[4][2];
+    T a[2][4], b[4][2];
 #pragma unroll
     for (int mi = 0; mi < 2; mi++) {
       const int r = wm * 32 + mi * 16 + g;
@@ -430,7 +481,7 @@ k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
 #pragma unroll
     for (int mi = 0; mi < 2; mi++)
 #pragma unroll
-      for (int ni = 0; ni < 4; ni++) dmma16888(acc[mi][ni], a[mi], b[ni]);
+      for (int ni = 0; ni < 4; ni++) mma_tile(acc[mi][ni], a[mi], b[ni]);
   }
 #pragma unroll
   for (int mi = 0; mi < 2; mi++)
@@ -462,7 +513,8 @@ struct GemmCfg {
   static constexpr int MI = BM / WM / 16;          // m16 tiles per warp
   static constexpr int NI = 4;                     // n8 tiles per warp
   static constexpr int LD = BM + 8;                // padded k-row stride (BM >= BN)
-  static constexpr size_t SMEM = (size_t) GEMM_STAGES * 2 * GEMM_BK * LD * sizeof(double);
+  template <typename T>
+  static constexpr size_t smem() { return (size_t) GEMM_STAGES * 2 * GEMM_BK * LD * sizeof(T); }
 };
 
 // C -= A B^T on DMMA m16n8k8 tiles of BM x BN (64x64: 4 warps, 128x128: 8
@@ -471,19 +523,20 @@ struct GemmCfg {
 //         c_lo by the panel columns [k_lo, k_hi) (one node of the recursive
 //         panel factorization);
 // mode 1: U -= L21 L21^T (K = [0, s))
-template <int BM, int BN>
+template <typename T, int BM, int BN>
 __global__ void __launch_bounds__(GemmCfg<BM, BN>::THREADS)
-k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, double* __restrict__ L,
-       double* __restrict__ U, int c_lo, int c_hi, int k_lo, int k_hi, int mode, const int* status) {
+k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, T* __restrict__ L,
+       T* __restrict__ U, int c_lo, int c_hi, int k_lo, int k_hi, int mode, const int* status) {
   using Cfg = GemmCfg<BM, BN>;
   constexpr int MI = Cfg::MI, NI = Cfg::NI, LD = Cfg::LD, NT = Cfg::THREADS;
-  extern __shared__ __align__(16) double gsm[];   // GEMM_STAGES x {A, B} x GEMM_BK x LD
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* gsm = reinterpret_cast<T*>(smraw);   // GEMM_STAGES x {A, B} x GEMM_BK x LD
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.y]];
   const int f = F.f, s = F.s, m = f - s;
   int rows, cols, roff, kbeg, kend, ldc;
-  const double* P = L + F.l_off;
-  double* Cbase;
+  const T* P = L + F.l_off;
+  T* Cbase;
   if (mode == 0) {
     const int cb = c_lo, ce = min(c_hi, s);
     if (cb >= ce) return;
@@ -509,15 +562,15 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
   }
   const int r0 = c0 + idx * BM;
   const int nr = min(BM, rows - r0), nc = min(BN, cols - c0);
-  const double* Ag = P + (roff + r0);
-  const double* Bg = P + (roff + c0);
-  double* C = Cbase + r0 + (size_t) c0 * ldc;
+  const T* Ag = P + (roff + r0);
+  const T* Bg = P + (roff + c0);
+  T* C = Cbase + r0 + (size_t) c0 * ldc;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp % Cfg::WM, wn = warp / Cfg::WM, g = lane >> 2, t = lane & 3;
   const int wrow = wm * (BM / Cfg::WM), wcol = wn * 32;
   // accumulators start at -C, so acc = A B^T - C and the result is -acc
-  double acc[MI][NI][4];
+  T acc[MI][NI][4];
 #pragma unroll
   for (int mi = 0; mi < MI; mi++)
 #pragma unroll
@@ -530,8 +583,8 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
       }
 
   auto load = [&](int st, int k0) {
-    double* As = gsm + (size_t) (st * 2) * GEMM_BK * LD;
-    double* Bs = As + GEMM_BK * LD;
+    T* As = gsm + (size_t) (st * 2) * GEMM_BK * LD;
+    T* Bs = As + GEMM_BK * LD;
 #pragma unroll
     for (int q = 0; q < (BM * GEMM_BK) / NT; q++) {
       const int e = tid + q * NT;
@@ -539,7 +592,7 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
       const bool kv = (k0 + k) < kend;
       const bool pa = kv && r < nr;
       const size_t col = (size_t) (kv ? k0 + k : kbeg) * f;
-      cp_async8(As + k * LD + r, Ag + (pa ? r : 0) + col, pa);
+      cp_async_t(As + k * LD + r, Ag + (pa ? r : 0) + col, pa);
     }
 #pragma unroll
     for (int q = 0; q < (BN * GEMM_BK) / NT; q++) {
@@ -548,7 +601,7 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
       const bool kv = (k0 + k) < kend;
       const bool pb = kv && r < nc;
       const size_t col = (size_t) (kv ? k0 + k : kbeg) * f;
-      cp_async8(Bs + k * LD + r, Bg + (pb ? r : 0) + col, pb);
+      cp_async_t(Bs + k * LD + r, Bg + (pb ? r : 0) + col, pb);
     }
   };
 
@@ -564,11 +617,11 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
     const int kn = kt + GEMM_STAGES - 1;
     if (kn < nk) load(kn % GEMM_STAGES, kbeg + kn * GEMM_BK);
     cp_async_commit();
-    const double* As = gsm + (size_t) ((kt % GEMM_STAGES) * 2) * GEMM_BK * LD;
-    const double* Bs = As + GEMM_BK * LD;
+    const T* As = gsm + (size_t) ((kt % GEMM_STAGES) * 2) * GEMM_BK * LD;
+    const T* Bs = As + GEMM_BK * LD;
 #pragma unroll
     for (int kk = 0; kk < GEMM_BK; kk += 8) {
-      double a[MI][4], b[NI][2];
+      T a[MI][4], b[NI][2];
 #pragma unroll
       for (int mi = 0; mi < MI; mi++) {
         const int r = wrow + mi * 16 + g;
@@ -586,7 +639,7 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, doubl
 #pragma unroll
       for (int mi = 0; mi < MI; mi++)
 #pragma unroll
-        for (int ni = 0; ni < NI; ni++) dmma16888(acc[mi][ni], a[mi], b[ni]);
+        for (int ni = 0; ni < NI; ni++) mma_tile(acc[mi][ni], a[mi], b[ni]);
     }
   }
   cp_async_wait<0>();
@@ -639,33 +692,40 @@ static bool big_tiles(int maxr, int maxc, int tiles64) {
   return false;
 }
 
-static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, double* L,
-                        double* U, int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
+template <typename T>
+static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, T* L, T* U,
+                        int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
   if (big)
-    k_gemm<128, 128><<<dim3(gx128, nb), GemmCfg<128, 128>::THREADS, GemmCfg<128, 128>::SMEM, st>>>(
+    k_gemm<T, 128, 128><<<dim3(gx128, nb), GemmCfg<128, 128>::THREADS, GemmCfg<128, 128>::smem<T>(), st>>>(
         blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
   else
-    k_gemm<64, 64><<<dim3(gx64, nb), GemmCfg<64, 64>::THREADS, GemmCfg<64, 64>::SMEM, st>>>(
+    k_gemm<T, 64, 64><<<dim3(gx64, nb), GemmCfg<64, 64>::THREADS, GemmCfg<64, 64>::smem<T>(), st>>>(
         blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
 }
 
+template <typename T>
+static constexpr size_t potrf_smem() { return (2 * PANEL_NB * DLD + 32 * DLD) * sizeof(T); }
+
+template <typename T>
 static void set_smem_attrs() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_small_front, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(double));
-  cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) POTRF_SMEM);
-  cudaFuncSetAttribute(k_gemm<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) GemmCfg<64, 64>::SMEM);
-  cudaFuncSetAttribute(k_gemm<128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) GemmCfg<128, 128>::SMEM);
-  cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       2 * PANEL_NB * TLD * (int) sizeof(double));
+  cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
+  cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) potrf_smem<T>());
+  cudaFuncSetAttribute(k_gemm<T, 64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) GemmCfg<64, 64>::smem<T>());
+  cudaFuncSetAttribute(k_gemm<T, 128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int) GemmCfg<128, 128>::smem<T>());
+  cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       2 * PANEL_NB * TLD * (int) sizeof(T));
   done = true;
 }
 
-int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L, double* U,
-                        double* Dinv, int* status, cudaStream_t st) {
-  set_smem_attrs();
+template <typename T>
+static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, T* U, T* Dinv, int* status,
+                          cudaStream_t st) {
+  set_smem_attrs<T>();
   k_init_status<<<1, 1, 0, st>>>(status);
   count_launch();
   for (int h = 0; h < P.n_levels; h++) {
@@ -680,7 +740,7 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
         int e = b;
         while (e < ns && P.fronts[LP.small_fronts[e]].f <= classes[cl]) e++;
         if (e > b) {
-          const size_t smem = (size_t) classes[cl] * classes[cl] * sizeof(double);
+          const size_t smem = (size_t) classes[cl] * classes[cl] * sizeof(T);
           double fl = 0.0, by = 0.0;
           if (prof_enabled())
             for (int q = b; q < e; q++) {
@@ -689,7 +749,7 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
               by += front_bytes(P, F);
             }
           prof_begin(KC_SMALL, st);
-          k_small_front<<<e - b, 128, smem, st>>>(lst + b, D.fronts, D.children, D.maps, D.rows,
+          k_small_front<T><<<e - b, 128, smem, st>>>(lst + b, D.fronts, D.children, D.maps, D.rows,
                                                    D.acol_ptr, D.a_rows, D.a_idx, vals, L, U, status);
           prof_end(KC_SMALL, st, fl, by);
           count_launch();
@@ -706,12 +766,12 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
       if (prof_enabled())
         for (int fi : LP.big_fronts) by += build_bytes(P, P.fronts[fi]);
       prof_begin(KC_BUILD, st);
-      k_build<<<ntiles, 256, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
+      k_build<T><<<ntiles, 256, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
                                       D.a_rows, D.a_idx, vals, L, U, status);
       prof_end(KC_BUILD, st, 0.0, by);
       count_launch();
     }
-    const size_t trsm_smem = 2 * PANEL_NB * TLD * sizeof(double);
+    const size_t trsm_smem = 2 * PANEL_NB * TLD * sizeof(T);
     // recursive panel factorization over aligned column intervals: factor
     // the left half, update the right half with one GEMM (K = half width),
     // factor the right half; leaves are 64-column POTRF + TRSM steps
@@ -735,12 +795,12 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
         }
       }
       prof_begin(KC_POTRF, st);
-      k_potrf_diag<<<nb, 128, POTRF_SMEM, st>>>(blst, D.fronts, D.rows, L, Dinv, kb, status);
+      k_potrf_diag<T><<<nb, 128, potrf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, Dinv, kb, status);
       prof_end(KC_POTRF, st, fp, bp);
       count_launch();
       if (gx_t > 0) {
         prof_begin(KC_TRSM, st);
-        k_trsm<<<dim3(gx_t, nb), 128, trsm_smem, st>>>(blst, D.fronts, L, Dinv, kb, status);
+        k_trsm<T><<<dim3(gx_t, nb), 128, trsm_smem, st>>>(blst, D.fronts, L, Dinv, kb, status);
         prof_end(KC_TRSM, st, ft, bt);
         count_launch();
       }
@@ -806,6 +866,16 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
     }
   }
   return (int) cudaGetLastError();
+}
+
+int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L, double* U, double* Dinv,
+                        int* status, cudaStream_t st) {
+  return launch_numeric<double>(P, D, vals, L, U, Dinv, status, st);
+}
+
+int launch_numeric_fp32(const Plan& P, const DevPlan& D, const float* vals, float* L, float* U, float* Dinv,
+                        int* status, cudaStream_t st) {
+  return launch_numeric<float>(P, D, vals, L, U, Dinv, status, st);
 }
 
 }  // namespace tb

@@ -1,16 +1,325 @@
-// Mixed precision and iterative refinement (placeholder).
+// Mixed precision: FP32 fronts with FP64 iterative refinement.
+//
+// The reference's precedent (progs/direct.c:656-663) is one refinement step
+// with everything in FP32 and an FP64-accumulated SpMV
+// (taucs_sccs_times_vec_dacc, src/taucs_ccs_ops.c:348-386).  Here:
+//   * the matrix is scaled symmetrically, A_s = D A D with D = diag(A)^-1/2,
+//     and A_s is factored with FP32 fronts (TF32x3 tensor products, FP32
+//     POTRF); a nonpositive FP32 pivot refactors in FP64;
+//   * refinement keeps x, b and the residual r = b - A x in FP64 on the device
+//     (symmetric CSR SpMV over the lower-triangle values, each row summed by
+//     one thread in a fixed order), solves L_s L_s^T d_s = D r in FP32 and
+//     updates x += D d_s, until the scaled residual
+//     ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) reaches the target; when a
+//     step fails to halve the residual twice in a row, or the step limit is
+//     reached, it refactors in FP64 and finishes with the FP64 factor.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "factor.h"
+
+namespace tb {
+
+namespace {
+
+__global__ void k_diag_scale(int n, const int* __restrict__ diagpos, const double* __restrict__ vals,
+                             double* __restrict__ scale, int* status) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double d = diagpos[j] >= 0 ? vals[diagpos[j]] : 0.0;
+  if (!(d > 0.0)) {
+    atomicMin(status, j);
+    scale[j] = 1.0;
+  } else {
+    scale[j] = rsqrt(d);
+  }
+}
+
+__global__ void k_scaled_f32(long nnz, const int* __restrict__ rowind, const int* __restrict__ colidx,
+                             const double* __restrict__ vals, const double* __restrict__ scale,
+                             float* __restrict__ out) {
+  const long k = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  out[k] = (float) (vals[k] * scale[rowind[k]] * scale[colidx[k]]);
+}
+
+// non-negative doubles order like their bit patterns
+__device__ __forceinline__ void max_abs(unsigned long long* slot, double v) {
+  atomicMax(slot, (unsigned long long) __double_as_longlong(fabs(v)));
+}
+
+// R = B - A X (FP64), inf-norms of R and X per column
+__global__ void k_residual(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                           const int* __restrict__ vi, const double* __restrict__ vals,
+                           const double* __restrict__ X, const double* __restrict__ B, double* __restrict__ R,
+                           int ld, int nrhs, unsigned long long* norms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  for (int q = 0; q < nrhs; q++) {
+    double r = 0.0, x = 0.0;
+    if (i < n) {
+      double acc = B[i + (size_t) q * ld];
+      for (int e = rp[i]; e < rp[i + 1]; e++) acc -= vals[vi[e]] * X[ci[e] + (size_t) q * ld];
+      R[i + (size_t) q * ld] = acc;
+      r = fabs(acc);
+      x = fabs(X[i + (size_t) q * ld]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+      x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    }
+    if (lane == 0) {
+      max_abs(norms + q, r);
+      max_abs(norms + SOLVE_NRHS + q, x);
+    }
+  }
+}
+
+__global__ void k_scale_down(int n, const double* __restrict__ R, const double* __restrict__ scale,
+                             float* __restrict__ out, int ld, int nrhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < nrhs; q++) out[i + (size_t) q * n] = (float) (R[i + (size_t) q * ld] * scale[i]);
+}
+
+__global__ void k_update32(int n, double* __restrict__ X, const float* __restrict__ D, const double* __restrict__ scale,
+                           int ld, int nrhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < nrhs; q++) X[i + (size_t) q * ld] += scale[i] * (double) D[i + (size_t) q * n];
+}
+
+__global__ void k_update64(int n, double* __restrict__ X, const double* __restrict__ D, int ld, int nrhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < nrhs; q++) X[i + (size_t) q * ld] += D[i + (size_t) q * ld];
+}
+
+__global__ void k_init_status2(int* s) { *s = INT_MAX; }
+
+// ||A||_inf of the full symmetric matrix from the CSR of both triangles
+__global__ void k_anorm(int n, const int* __restrict__ rp, const int* __restrict__ vi, const double* __restrict__ vals,
+                        unsigned long long* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double a = 0.0;
+  if (i < n)
+    for (int e = rp[i]; e < rp[i + 1]; e++) a += fabs(vals[vi[e]]);
+  for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+  if ((threadIdx.x & 31) == 0) max_abs(out, a);
+}
+
+inline int nblk(long n, int b) { return (int) ((n + b - 1) / b); }
+
+}  // namespace
+
+// pattern-derived arrays for scaling and the FP64 residual
+static int ensure_refine(Factor* F) {
+  if (F->refine_ready) return 0;
+  if (ensure_device(F)) return -1;
+  const int n = F->n;
+  const long nnz = F->colptr[n];
+  std::vector<int> colidx(std::max(nnz, 1L)), diagpos(std::max(n, 1), -1), cnt(n + 1, 0);
+  for (int j = 0; j < n; j++)
+    for (int ip = F->colptr[j]; ip < F->colptr[j + 1]; ip++) {
+      const int i = F->rowind[ip];
+      colidx[ip] = j;
+      if (i == j && diagpos[j] < 0) diagpos[j] = ip;
+      cnt[i + 1]++;
+      if (i != j) cnt[j + 1]++;
+    }
+  for (int i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+  const long ne = cnt[n];
+  std::vector<int> ccol(std::max(ne, 1L)), cval(std::max(ne, 1L)), fill(cnt.begin(), cnt.end() - 1);
+  for (int j = 0; j < n; j++)
+    for (int ip = F->colptr[j]; ip < F->colptr[j + 1]; ip++) {
+      const int i = F->rowind[ip];
+      ccol[fill[i]] = j; cval[fill[i]] = ip; fill[i]++;
+      if (i != j) { ccol[fill[j]] = i; cval[fill[j]] = ip; fill[j]++; }
+    }
+  cudaStream_t st = current_stream();
+  auto up = [&](int** d, const std::vector<int>& h) {
+    return cuda_ok(cudaMalloc(d, sizeof(int) * h.size()), "cudaMalloc") &&
+           cuda_ok(cudaMemcpyAsync(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st), "copy");
+  };
+  const size_t nv = (size_t) n * SOLVE_NRHS;
+  bool ok = up(&F->dcolidx, colidx) && up(&F->ddiagpos, diagpos) && up(&F->dcsr_ptr, cnt) && up(&F->dcsr_col, ccol) &&
+            up(&F->dcsr_val, cval) &&
+            cuda_ok(cudaMalloc(&F->dscale, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
+            cuda_ok(cudaMalloc(&F->dR, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(cudaMalloc(&F->dXr, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(cudaMalloc(&F->dBr, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(cudaMalloc(&F->dV32, sizeof(float) * nv), "cudaMalloc") &&
+            cuda_ok(cudaMalloc(&F->dnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS), "cudaMalloc") &&
+            cuda_ok(cudaMallocHost(&F->hnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS), "cudaMallocHost") &&
+            cuda_ok(cudaStreamSynchronize(st), "refine setup");
+  if (!ok) return -1;
+  F->refine_ready = true;
+  return 0;
+}
+
+int numeric_fp32_device(Factor* F, const double* d_vals) {
+  if (ensure_device(F) || ensure_refine(F)) return -1;
+  const Plan& P = F->plan;
+  cudaStream_t st = current_stream();
+  auto al = [&](float** d, size_t n, const char* w) { return *d || cuda_ok(cudaMalloc(d, sizeof(float) * std::max<size_t>(n, 1)), w); };
+  if (!al(&F->dL32, P.l_len, "cudaMalloc(L32)") || !al(&F->dU32, P.u_len, "cudaMalloc(U32)") ||
+      !al(&F->dDinv32, P.dinv_len, "cudaMalloc(Dinv32)") || !al(&F->dA32, P.nnz, "cudaMalloc(A32)") ||
+      !al(&F->dW32, (size_t) P.v_len * SOLVE_NRHS, "cudaMalloc(W32)") || !al(&F->dpart32, P.part_len, "cudaMalloc(part32)")) {
+    free_numeric(F);
+    return -1;
+  }
+  F->dvals_cur = d_vals;
+  k_init_status2<<<1, 1, 0, st>>>(F->dstatus);
+  k_diag_scale<<<nblk(F->n, 256), 256, 0, st>>>(F->n, F->ddiagpos, d_vals, F->dscale, F->dstatus);
+  k_scaled_f32<<<nblk(P.nnz, 256), 256, 0, st>>>(P.nnz, F->drowind, F->dcolidx, d_vals, F->dscale, F->dA32);
+  count_launch(3);
+  cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!cuda_ok(cudaStreamSynchronize(st), "scaling")) return -1;
+  if (*F->hstatus != INT_MAX) {
+    tprintf("\t\tscaling: nonpositive diagonal in column %d\n", *F->hstatus);
+    return -1;
+  }
+  int e = launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dstatus, st);
+  if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
+  cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!cuda_ok(cudaStreamSynchronize(st), "numeric factorization (FP32)")) return -1;
+  if (*F->hstatus != INT_MAX) {
+    tprintf("\t\tFP32 fronts: nonpositive pivot in column %d\n", *F->hstatus);
+    return -1;
+  }
+  F->has_numeric32 = true;
+  return 0;
+}
+
+// Refines X (device, n x nrhs, ld) for B; returns the number of correction
+// steps or -1; res (host, nrhs) gets the final scaled residuals.
+static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int ld, double tol, int maxits,
+                         double anorm, double* res) {
+  const Plan& P = F->plan;
+  const int n = F->n;
+  cudaStream_t st = current_stream();
+  int total = 0;
+  for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
+    const int nq = std::min(SOLVE_NRHS, nrhs - q0);
+    double* X = dX + (size_t) q0 * ld;
+    const double* B = dB + (size_t) q0 * ld;
+    std::vector<double> bnorm(nq, 0.0);
+    // ||b||_inf per column, from a residual pass with X = 0
+    cudaMemsetAsync(X, 0, sizeof(double) * ((size_t) ld * (nq - 1) + n), st);
+    bool use64 = !F->has_numeric32;
+    double prev_worst = INFINITY;
+    int slow = 0, steps = 0;
+    bool done = false;
+    for (int it = 0; !done; it++) {
+      cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long) * 2 * SOLVE_NRHS, st);
+      k_residual<<<nblk(n, 256), 256, 0, st>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, F->dR,
+                                               ld, nq, F->dnorm);
+      count_launch();
+      cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS, cudaMemcpyDeviceToHost, st);
+      if (!cuda_ok(cudaStreamSynchronize(st), "refinement")) return -1;
+      double worst = 0.0;
+      for (int q = 0; q < nq; q++) {
+        double rn, xn;
+        memcpy(&rn, &F->hnorm[q], 8);
+        memcpy(&xn, &F->hnorm[SOLVE_NRHS + q], 8);
+        if (it == 0) bnorm[q] = rn;   // X = 0: r = b
+        const double den = anorm * xn + bnorm[q];
+        const double rq = den > 0 ? rn / den : 0.0;
+        if (res) res[q0 + q] = rq;
+        worst = std::max(worst, rq);
+      }
+      if (it > 0 && worst <= tol) break;
+      if (it > 0) {
+        if (worst > 0.5 * prev_worst) slow++;
+        else slow = 0;
+        if (!use64 && (slow >= 2 || steps >= maxits)) {
+          // refinement stalled with the FP32 factor: finish in FP64
+          tprintf("\t\trefinement stalled at %.3e after %d steps; refactoring in FP64\n", worst, steps);
+          if (!F->has_numeric && numeric_fp64_device(F, F->dvals_cur, true)) return -1;
+          use64 = true;
+          slow = 0;
+        } else if (use64 && (slow >= 2 || steps >= maxits + 5)) {
+          done = true;
+          total = -1;
+          continue;
+        }
+      }
+      prev_worst = worst;
+      // one correction step
+      if (use64) {
+        if (launch_solve_fp64(P, F->dp, F->dL, nq, F->dR, F->dR, ld, F->dW, F->dpart, F->dflags, &F->epoch,
+                              F->dstatus + 1, st)) return -1;
+        k_update64<<<nblk(n, 256), 256, 0, st>>>(n, X, F->dR, ld, nq);
+      } else {
+        k_scale_down<<<nblk(n, 256), 256, 0, st>>>(n, F->dR, F->dscale, F->dV32, ld, nq);
+        if (launch_solve_fp32(P, F->dp, F->dL32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32, F->dflags, &F->epoch,
+                              F->dstatus + 1, st)) return -1;
+        k_update32<<<nblk(n, 256), 256, 0, st>>>(n, X, F->dV32, F->dscale, ld, nq);
+      }
+      count_launch(2);
+      steps++;
+    }
+    if (total >= 0) total = std::max(total, steps);
+  }
+  return total;
+}
+
+int solve_refine_host(Factor* F, taucs_ccs_matrix* A, int nrhs, double* X, const double* B, double tol, int maxits,
+                      double* res) {
+  if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
+  if (ensure_refine(F)) return -1;
+  const int n = F->n;
+  double anorm = 0.0;
+  if (A) {
+    std::vector<double> rs(n, 0.0);
+    for (int j = 0; j < n; j++)
+      for (int ip = A->colptr[j]; ip < A->colptr[j + 1]; ip++) {
+        const int i = A->rowind[ip];
+        rs[i] += fabs(A->values.d[ip]);
+        if (i != j) rs[j] += fabs(A->values.d[ip]);
+      }
+    for (double v : rs) anorm = std::max(anorm, v);
+  }
+  cudaStream_t st = current_stream();
+  if (!A) {
+    cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long), st);
+    k_anorm<<<nblk(n, 256), 256, 0, st>>>(n, F->dcsr_ptr, F->dcsr_val, F->dvals_cur, F->dnorm);
+    count_launch();
+    cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (!cuda_ok(cudaStreamSynchronize(st), "norm")) return -1;
+    memcpy(&anorm, &F->hnorm[0], 8);
+  }
+  int worst_steps = 0;
+  for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
+    const int nq = std::min(SOLVE_NRHS, nrhs - q0);
+    if (!cuda_ok(cudaMemcpyAsync(F->dBr, B + (size_t) q0 * n, sizeof(double) * (size_t) n * nq, cudaMemcpyHostToDevice, st), "rhs"))
+      return -1;
+    const int s = refine_device(F, nq, F->dXr, F->dBr, n, tol, maxits, anorm, res ? res + q0 : nullptr);
+    if (!cuda_ok(cudaMemcpyAsync(X + (size_t) q0 * n, F->dXr, sizeof(double) * (size_t) n * nq, cudaMemcpyDeviceToHost, st), "x"))
+      return -1;
+    if (!cuda_ok(cudaStreamSynchronize(st), "solve_refine")) return -1;
+    if (s < 0) worst_steps = -1;
+    else if (worst_steps >= 0) worst_steps = std::max(worst_steps, s);
+  }
+  return worst_steps;
+}
+
+}  // namespace tb
 
 using namespace tb;
 
 extern "C" int taucs_b200_set_precision(void* L, int precision) {
-  if (!L || precision != 0) return -1;
-  ((Factor*) L)->precision = 0;
+  if (!L || (precision != 0 && precision != 1)) return -1;
+  ((Factor*) L)->precision = precision;
   return 0;
 }
 
 extern "C" int taucs_b200_solve_refine(void* L, taucs_ccs_matrix* A, int nrhs, double* X, const double* B,
                                        double tol, int maxits, double* res_out) {
-  (void) L; (void) A; (void) nrhs; (void) X; (void) B; (void) tol; (void) maxits; (void) res_out;
-  return -1;
+  if (!L || nrhs < 0 || (nrhs > 0 && (!X || !B))) return -1;
+  if (nrhs == 0) return 0;
+  return solve_refine_host((Factor*) L, A, nrhs, X, B, tol, maxits < 0 ? 0 : maxits, res_out);
 }

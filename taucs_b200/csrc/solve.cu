@@ -26,18 +26,18 @@ namespace {
 
 constexpr int SB = 32;   // substitution block (one warp)
 
-template <int WS>
+template <typename T, int WS>
 __global__ void __launch_bounds__(256)
 k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
-      const int* __restrict__ maps, const int* __restrict__ rows, const double* __restrict__ L,
-      const double* __restrict__ B, int ldb, double* __restrict__ W, int nrhs) {
-  __shared__ double xs[SB][SOLVE_NRHS];
+      const int* __restrict__ maps, const int* __restrict__ rows, const T* __restrict__ L,
+      const T* __restrict__ B, int ldb, T* __restrict__ W, int nrhs) {
+  __shared__ T xs[SB][SOLVE_NRHS];
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-  double* Wf = W + F.v_off * WS;
+  T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
-  const double* P = L + F.l_off;
+  const T* P = L + F.l_off;
 
   for (int k = tid; k < f * nrhs; k += nt) {
     const int r = k % f, q = k / f;
@@ -48,7 +48,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
-    const double* Wc = W + C.v_off * WS;
+    const T* Wc = W + C.v_off * WS;
     for (int k = tid; k < mc * nrhs; k += nt) {
       const int i = k % mc, q = k / mc;
       Wf[mp[i] + q * f] += Wc[C.s + i + q * C.f];
@@ -59,9 +59,9 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     const int bw = min(SB, s - jb);
     if (warp == 0) {
       for (int q = 0; q < nrhs; q++) {
-        double v = (lane < bw) ? Wf[jb + lane + q * f] : 0.0;
+        T v = (lane < bw) ? Wf[jb + lane + q * f] : 0.0;
         for (int j = 0; j < bw; j++) {
-          const double xj = __shfl_sync(0xffffffffu, v, j) / P[(jb + j) + (size_t) (jb + j) * f];
+          const T xj = __shfl_sync(0xffffffffu, v, j) / P[(jb + j) + (size_t) (jb + j) * f];
           if (lane == j) v = xj;
           if (lane > j && lane < bw) v -= P[(jb + lane) + (size_t) (jb + j) * f] * xj;
         }
@@ -73,11 +73,11 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     }
     __syncthreads();
     for (int r = jb + bw + tid; r < f; r += nt) {
-      double acc[SOLVE_NRHS];
+      T acc[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
       for (int j = 0; j < bw; j++) {
-        const double l = P[r + (size_t) (jb + j) * f];
+        const T l = P[r + (size_t) (jb + j) * f];
 #pragma unroll
         for (int q = 0; q < SOLVE_NRHS; q++)
           if (q < nrhs) acc[q] += l * xs[j][q];
@@ -88,18 +88,18 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
   }
 }
 
-template <int WS>
+template <typename T, int WS>
 __global__ void __launch_bounds__(256)
 k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
-      const double* __restrict__ L, double* __restrict__ X, int ldx, double* __restrict__ W,
+      const T* __restrict__ L, T* __restrict__ X, int ldx, T* __restrict__ W,
       int nrhs) {
-  __shared__ double xs[SB][SOLVE_NRHS];
+  __shared__ T xs[SB][SOLVE_NRHS];
   const FrontDesc F = fronts[list[blockIdx.x]];
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-  double* Wf = W + F.v_off * WS;
+  T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
-  const double* P = L + F.l_off;
+  const T* P = L + F.l_off;
 
   // x at the update rows (final: written by ancestors)
   for (int k = tid; k < (f - s) * nrhs; k += nt) {
@@ -109,19 +109,19 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
   __syncthreads();
   // r_j = y_j - sum_{i >= s} L[i,j] x_i
   for (int j = warp; j < s; j += nw) {
-    double acc[SOLVE_NRHS];
+    T acc[SOLVE_NRHS];
 #pragma unroll
     for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
-    const double* pj = P + (size_t) j * f;
+    const T* pj = P + (size_t) j * f;
     for (int i = s + lane; i < f; i += 32) {
-      const double l = pj[i];
+      const T l = pj[i];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++)
         if (q < nrhs) acc[q] += l * Wf[i + q * f];
     }
 #pragma unroll
     for (int q = 0; q < SOLVE_NRHS; q++) {
-      double v = acc[q];
+      T v = acc[q];
       for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
       acc[q] = v;
     }
@@ -136,19 +136,19 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     // contributions of the already solved x in rows [je, s)
     if (je < s) {
       for (int j = jb + warp; j < je; j += nw) {
-        double acc[SOLVE_NRHS];
+        T acc[SOLVE_NRHS];
 #pragma unroll
         for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
-        const double* pj = P + (size_t) j * f;
+        const T* pj = P + (size_t) j * f;
         for (int i = je + lane; i < s; i += 32) {
-          const double l = pj[i];
+          const T l = pj[i];
 #pragma unroll
           for (int q = 0; q < SOLVE_NRHS; q++)
             if (q < nrhs) acc[q] += l * Wf[i + q * f];
         }
 #pragma unroll
         for (int q = 0; q < SOLVE_NRHS; q++) {
-          double v = acc[q];
+          T v = acc[q];
           for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
           acc[q] = v;
         }
@@ -159,9 +159,9 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     }
     if (warp == 0) {
       for (int q = 0; q < nrhs; q++) {
-        double v = (lane < bw) ? Wf[jb + lane + q * f] : 0.0;
+        T v = (lane < bw) ? Wf[jb + lane + q * f] : 0.0;
         for (int j = bw - 1; j >= 0; j--) {
-          const double xj = __shfl_sync(0xffffffffu, v, j) / P[(jb + j) + (size_t) (jb + j) * f];
+          const T xj = __shfl_sync(0xffffffffu, v, j) / P[(jb + j) + (size_t) (jb + j) * f];
           if (lane == j) v = xj;
           if (lane < j) v -= P[(jb + j) + (size_t) (jb + lane) * f] * xj;
         }
@@ -191,7 +191,8 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
 // can hang.
 
 constexpr int BR = PANEL_NB;   // rows per block
-constexpr size_t BWD_SMEM = 2 * BR * (BR + 1) * sizeof(double);
+template <typename T>
+constexpr size_t bwd_smem() { return 2 * BR * (BR + 1) * sizeof(T); }
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -227,25 +228,25 @@ __device__ __forceinline__ int lb_dev(const int* a, int n, int key) {
   return lo;
 }
 
-template <int NQ, int WS>
+template <typename T, int NQ, int WS>
 __global__ void __launch_bounds__(128)
 k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ children, const int* __restrict__ maps, const int* __restrict__ rows,
-          const double* __restrict__ L, const double* __restrict__ B, int ldb, double* __restrict__ W,
+          const T* __restrict__ L, const T* __restrict__ B, int ldb, T* __restrict__ W,
           int nrhs, int* __restrict__ flags, int epoch, int* status) {
-  __shared__ double wv[BR][NQ];
-  __shared__ double yk[BR][NQ];
-  __shared__ double part[BR][NQ];
-  __shared__ double dg[BR][BR + 1];   // diagonal block, column-major: dg[col][row]
+  __shared__ T wv[BR][NQ];
+  __shared__ T yk[BR][NQ];
+  __shared__ T part[BR][NQ];
+  __shared__ T dg[BR][BR + 1];   // diagonal block, column-major: dg[col][row]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int r = bk.b, f = F.f, s = F.s;
   const int nbs = (s + BR - 1) / BR;
   const int r0 = r * BR, nr = min(BR, f - r0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* Wf = W + F.v_off * WS;
+  T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
-  const double* P = L + F.l_off;
+  const T* P = L + F.l_off;
 
   if (r < nbs) {
     // stage the diagonal block now, off the chain's critical path
@@ -266,7 +267,7 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     const int* mp = maps + C.map_off;
     const int ia = lb_dev(mp, mc, r0), ib = lb_dev(mp, mc, r0 + nr);
     if (ia >= ib) continue;
-    const double* Wc = W + C.v_off * WS;
+    const T* Wc = W + C.v_off * WS;
     for (int k = tid; k < (ib - ia) * nrhs; k += 128) {
       const int i = ia + k % (ib - ia), q = k / (ib - ia);
       wv[mp[i] - r0][q] += Wc[C.s + i + q * C.f];
@@ -276,14 +277,14 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   // contributions of the solved blocks to the left; this thread's 32
   // entries of L[r, k] are loaded before waiting for y_k
   const int row = tid % BR, half = tid / BR;
-  double acc[NQ];
+  T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
   const int kend = r < nbs ? r : nbs;
   for (int k = 0; k < kend; k++) {
     const int bwk = min(BR, s - k * BR);
-    double lv[BR / 2];
-    const double* pc = P + (r0 + row) + (size_t) (k * BR + half * (BR / 2)) * f;
+    T lv[BR / 2];
+    const T* pc = P + (r0 + row) + (size_t) (k * BR + half * (BR / 2)) * f;
 #pragma unroll
     for (int j = 0; j < BR / 2; j++)
       lv[j] = (row < nr && half * (BR / 2) + j < bwk) ? pc[(size_t) j * f] : 0.0;
@@ -313,14 +314,14 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     const int bw = min(BR, s - r0);
     if (warp == 0) {
       // reciprocal diagonal formed in parallel, off the substitution's critical path
-      const double rd0 = (lane < bw) ? 1.0 / dg[lane][lane] : 0.0;
-      const double rd1 = (lane + 32 < bw) ? 1.0 / dg[lane + 32][lane + 32] : 0.0;
+      const T rd0 = (lane < bw) ? T(1) / dg[lane][lane] : T(0);
+      const T rd1 = (lane + 32 < bw) ? T(1) / dg[lane + 32][lane + 32] : T(0);
       for (int q = 0; q < nrhs; q++) {
-        double v0 = wv[lane][q], v1 = wv[lane + 32][q];
+        T v0 = wv[lane][q], v1 = wv[lane + 32][q];
         for (int j = 0; j < bw; j++) {
-          const double src = (j < 32) ? __shfl_sync(0xffffffffu, v0, j) : __shfl_sync(0xffffffffu, v1, j - 32);
-          const double rj = (j < 32) ? __shfl_sync(0xffffffffu, rd0, j) : __shfl_sync(0xffffffffu, rd1, j - 32);
-          const double xj = src * rj;
+          const T src = (j < 32) ? __shfl_sync(0xffffffffu, v0, j) : __shfl_sync(0xffffffffu, v1, j - 32);
+          const T rj = (j < 32) ? __shfl_sync(0xffffffffu, rd0, j) : __shfl_sync(0xffffffffu, rd1, j - 32);
+          const T xj = src * rj;
           if (lane == j) v0 = xj;
           else if (lane > j) v0 -= dg[j][lane] * xj;
           if (lane + 32 == j) v1 = xj;
@@ -343,16 +344,16 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 
 // x at the update rows of every big front of a level, gathered once into the
 // front's work vector (rows s..f-1) so the backward blocks read it coalesced
-template <int WS>
+template <typename T, int WS>
 __global__ void __launch_bounds__(128)
 k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
-             const int* __restrict__ rows, const double* __restrict__ X, int ldx, double* __restrict__ W,
+             const int* __restrict__ rows, const T* __restrict__ X, int ldx, T* __restrict__ W,
              int nrhs) {
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int r0 = max(bk.b * BR, F.s), r1 = min(bk.b * BR + BR, F.f);
   if (r0 >= r1) return;
-  double* Wf = W + F.v_off * WS;
+  T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const int nr = r1 - r0;
   for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x) {
@@ -364,10 +365,10 @@ k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fro
 // Backward solve, L21^T x2 split over (column block, 512-row chunk) CTAs so
 // that the whole GPU streams L21; each CTA stores its partial sums, which the
 // chain kernel adds in chunk order.
-template <int NQ, int WS>
+template <typename T, int NQ, int WS>
 __global__ void __launch_bounds__(128)
-k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts, const double* __restrict__ L,
-          const double* __restrict__ W, double* __restrict__ part, int nrhs) {
+k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts, const T* __restrict__ L,
+          const T* __restrict__ W, T* __restrict__ part, int nrhs) {
   constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;
   const int2_ tk = tasks[blockIdx.x];
   const FrontDesc F = fronts[tk.a];
@@ -376,21 +377,21 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
   const int c0 = k * BR, bw = min(BR, s - c0);
   const int i0 = ch * SOLVE_RCH, i1 = min(m, i0 + SOLVE_RCH);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const double* z = W + F.v_off * WS + s;
-  const double* P = L + F.l_off;
+  const T* z = W + F.v_off * WS + s;
+  const T* P = L + F.l_off;
   for (int cg = warp * 16; cg < warp * 16 + 16; cg += G) {
-    double acc[G][NQ];
+    T acc[G][NQ];
 #pragma unroll
     for (int a_ = 0; a_ < G; a_++)
 #pragma unroll
       for (int q = 0; q < NQ; q++) acc[a_][q] = 0.0;
     for (int i = i0 + lane; i < i1; i += 32) {
-      double zi[NQ];
+      T zi[NQ];
 #pragma unroll
       for (int q = 0; q < NQ; q++) zi[q] = (q < nrhs) ? __ldcg(z + i + (size_t) q * f) : 0.0;
 #pragma unroll
       for (int a_ = 0; a_ < G; a_++) {
-        const double l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
+        const T l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
 #pragma unroll
         for (int q = 0; q < NQ; q++) acc[a_][q] += l * zi[q];
       }
@@ -399,7 +400,7 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
     for (int a_ = 0; a_ < G; a_++)
 #pragma unroll
       for (int q = 0; q < NQ; q++) {
-        double v = acc[a_][q];
+        T v = acc[a_][q];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if (lane == 0 && cg + a_ < bw && q < nrhs)
           part[F.part_off + ((size_t) ch * s + c0 + cg + a_) * SOLVE_NRHS + q] = v;
@@ -407,28 +408,29 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
   }
 }
 
-template <int NQ, int WS, bool PARTS>
+template <typename T, int NQ, int WS, bool PARTS>
 __global__ void __launch_bounds__(128)
 k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
-          const int* __restrict__ rows, const double* __restrict__ L, double* __restrict__ X, int ldx,
-          double* __restrict__ W, const double* __restrict__ part, int nrhs, int* __restrict__ flags, int epoch,
+          const int* __restrict__ rows, const T* __restrict__ L, T* __restrict__ X, int ldx,
+          T* __restrict__ W, const T* __restrict__ part, int nrhs, int* __restrict__ flags, int epoch,
           int* status) {
   constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;   // columns per pass of the L21 product
-  __shared__ double xv[BR][NQ];
-  __shared__ double xj[BR][NQ];
-  __shared__ double red[BR][NQ];
-  extern __shared__ double bsm[];
-  double (*tile)[BR + 1] = reinterpret_cast<double (*)[BR + 1]>(bsm);             // block of L11, [col][row]
-  double (*dgb)[BR + 1] = reinterpret_cast<double (*)[BR + 1]>(bsm + BR * (BR + 1));  // diagonal block, [row][col]
+  __shared__ T xv[BR][NQ];
+  __shared__ T xj[BR][NQ];
+  __shared__ T red[BR][NQ];
+  extern __shared__ __align__(16) unsigned char bsmraw[];
+  T* bsm = reinterpret_cast<T*>(bsmraw);
+  T (*tile)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm);             // block of L11, [col][row]
+  T (*dgb)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm + BR * (BR + 1));  // diagonal block, [row][col]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int k = bk.b, f = F.f, s = F.s, m = f - s;
   const int nbs = (s + BR - 1) / BR;
   const int c0 = k * BR, bw = min(BR, s - c0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* Wf = W + F.v_off * WS;
+  T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
-  const double* P = L + F.l_off;
+  const T* P = L + F.l_off;
 
   // stage the diagonal block now, off the chain's critical path
   for (int e = tid; e < BR * BR; e += 128) {
@@ -445,7 +447,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     for (int e = tid; e < bw * NQ; e += 128) {
       const int c = e % bw, q = e / bw;
       if (q < nrhs) {
-        double acc = 0.0;
+        T acc = 0.0;
         for (int ch = 0; ch < F.nchunk; ch++)
           acc += __ldcg(part + F.part_off + ((size_t) ch * s + c0 + c) * SOLVE_NRHS + q);
         xv[c][q] -= acc;
@@ -454,20 +456,20 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   }
   // y - L21^T x2: warp w owns columns 16w..16w+15, G at a time; lanes run
   // down the update rows with one coalesced load per column per step
-  const double* z = Wf + s;
+  const T* z = Wf + s;
   for (int cg = warp * 16; !PARTS && cg < warp * 16 + 16; cg += G) {
-    double acc[G][NQ];
+    T acc[G][NQ];
 #pragma unroll
     for (int a_ = 0; a_ < G; a_++)
 #pragma unroll
       for (int q = 0; q < NQ; q++) acc[a_][q] = 0.0;
     for (int i = lane; i < m; i += 32) {
-      double zi[NQ];
+      T zi[NQ];
 #pragma unroll
       for (int q = 0; q < NQ; q++) zi[q] = (q < nrhs) ? __ldcg(z + i + (size_t) q * f) : 0.0;
 #pragma unroll
       for (int a_ = 0; a_ < G; a_++) {
-        const double l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
+        const T l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
 #pragma unroll
         for (int q = 0; q < NQ; q++) acc[a_][q] += l * zi[q];
       }
@@ -476,7 +478,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     for (int a_ = 0; a_ < G; a_++)
 #pragma unroll
       for (int q = 0; q < NQ; q++) {
-        double v = acc[a_][q];
+        T v = acc[a_][q];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         if (lane == 0 && cg + a_ < bw) xv[cg + a_][q] -= v;
       }
@@ -497,12 +499,12 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
       xj[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : 0.0;
     }
     __syncthreads();
-    double acc[NQ];
+    T acc[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) acc[q] = 0.0;
 #pragma unroll 8
     for (int i = half * (BR / 2); i < half * (BR / 2) + BR / 2; i++) {
-      const double l = tile[col][i];
+      const T l = tile[col][i];
 #pragma unroll
       for (int q = 0; q < NQ; q++) acc[q] += l * xj[i][q];
     }
@@ -518,14 +520,14 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   // L_kk^T substitution from the staged diagonal block, one warp, columns
   // lane and lane+32
   if (warp == 0) {
-    const double rd0 = (lane < bw) ? 1.0 / dgb[lane][lane] : 0.0;
-    const double rd1 = (lane + 32 < bw) ? 1.0 / dgb[lane + 32][lane + 32] : 0.0;
+    const T rd0 = (lane < bw) ? T(1) / dgb[lane][lane] : T(0);
+    const T rd1 = (lane + 32 < bw) ? T(1) / dgb[lane + 32][lane + 32] : T(0);
     for (int q = 0; q < nrhs; q++) {
-      double v0 = xv[lane][q], v1 = xv[lane + 32][q];
+      T v0 = xv[lane][q], v1 = xv[lane + 32][q];
       for (int c = bw - 1; c >= 0; c--) {
-        const double src = (c < 32) ? __shfl_sync(0xffffffffu, v0, c) : __shfl_sync(0xffffffffu, v1, c - 32);
-        const double rc = (c < 32) ? __shfl_sync(0xffffffffu, rd0, c) : __shfl_sync(0xffffffffu, rd1, c - 32);
-        const double x = src * rc;
+        const T src = (c < 32) ? __shfl_sync(0xffffffffu, v0, c) : __shfl_sync(0xffffffffu, v1, c - 32);
+        const T rc = (c < 32) ? __shfl_sync(0xffffffffu, rd0, c) : __shfl_sync(0xffffffffu, rd1, c - 32);
+        const T x = src * rc;
         if (lane == c) v0 = x;
         else if (lane < c) v0 -= dgb[c][lane] * x;
         if (lane + 32 == c) v1 = x;
@@ -555,25 +557,26 @@ static double solve_pass_bytes(const FrontDesc& F, int nrhs) {
   return 8.0 * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * 8.0 * nrhs * F.f;
 }
 
+template <typename T>
 static void solve_attrs() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_bwd_big<1, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
-  cudaFuncSetAttribute(k_bwd_big<2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
-  cudaFuncSetAttribute(k_bwd_big<4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
-  cudaFuncSetAttribute(k_bwd_big<8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
-  cudaFuncSetAttribute(k_bwd_big<1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) BWD_SMEM);
+  cudaFuncSetAttribute(k_bwd_big<T, 1, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
+  cudaFuncSetAttribute(k_bwd_big<T, 2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
+  cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
+  cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
+  cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
   done = true;
 }
 
-int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
-                      const double* B, int ld, double* W, double* part, int* flags, int* epoch, int* status,
-                      cudaStream_t st) {
-  solve_attrs();
+template <typename T>
+static int launch_solve(const Plan& P, const DevPlan& D, const T* L, int nrhs, T* X, const T* B, int ld, T* W,
+                        T* part, int* flags, int* epoch, int* status, cudaStream_t st) {
+  solve_attrs<T>();
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
-    const double* Bq = B + (size_t) q0 * ld;
-    double* Xq = X + (size_t) q0 * ld;
+    const T* Bq = B + (size_t) q0 * ld;
+    T* Xq = X + (size_t) q0 * ld;
     const int ef = ++*epoch;
     for (int h = 0; h < P.n_levels; h++) {
       const LevelPlan& LP = P.levels[h];
@@ -583,7 +586,7 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       prof_begin(KC_SOLVE_FWD, st);
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
-        k_fwd<SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L,
+        k_fwd<T, SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L,
                                   Bq, ld, W, nq);
         count_launch();
       }
@@ -591,13 +594,13 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       if (nb > 0) {
         const int2_* bl = D.sfwd + D.sfwd_off[h];
         if (nq == 1)
-          k_fwd_big<1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         else if (nq == 2)
-          k_fwd_big<2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         else if (nq <= 4)
-          k_fwd_big<4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         else
-          k_fwd_big<8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
         count_launch();
       }
       prof_end(KC_SOLVE_FWD, st, 0.0, by);
@@ -611,38 +614,48 @@ int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs
       prof_begin(KC_SOLVE_BWD, st);
       const int nb = (int) LP.solve_bwd_blocks.size();
       if (nb > 0) {
-        k_gather_upd<SOLVE_NRHS><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
+        k_gather_upd<T, SOLVE_NRHS><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                         Xq, ld, W, nq);
         count_launch();
         const int nt = (int) LP.solve_l21_tasks.size();
         const int2_* tl = D.sl21 + D.sl21_off[h];
         if (nt > 0) {
-          if (nq == 1) k_bwd_l21<1, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
-          else if (nq == 2) k_bwd_l21<2, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
-          else if (nq <= 4) k_bwd_l21<4, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
-          else k_bwd_l21<8, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          if (nq == 1) k_bwd_l21<T, 1, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          else if (nq == 2) k_bwd_l21<T, 2, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          else if (nq <= 4) k_bwd_l21<T, 4, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          else k_bwd_l21<T, 8, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
           count_launch();
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
         if (nq == 1)
-          k_bwd_big<1, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 1, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq == 2)
-          k_bwd_big<2, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
-          k_bwd_big<4, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         else
-          k_bwd_big<8, SOLVE_NRHS, true><<<nb, 128, BWD_SMEM, st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
         count_launch();
       }
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
-        k_bwd<SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, Xq, ld, W, nq);
+        k_bwd<T, SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, Xq, ld, W, nq);
         count_launch();
       }
       prof_end(KC_SOLVE_BWD, st, 0.0, by);
     }
   }
   return (int) cudaGetLastError();
+}
+
+int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X, const double* B, int ld,
+                      double* W, double* part, int* flags, int* epoch, int* status, cudaStream_t st) {
+  return launch_solve<double>(P, D, L, nrhs, X, B, ld, W, part, flags, epoch, status, st);
+}
+
+int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, int nrhs, float* X, const float* B, int ld,
+                      float* W, float* part, int* flags, int* epoch, int* status, cudaStream_t st) {
+  return launch_solve<float>(P, D, L, nrhs, X, B, ld, W, part, flags, epoch, status, st);
 }
 
 }  // namespace tb
@@ -699,19 +712,19 @@ static int noalloc_scratch(double** out) {
 // one right-hand side, work vectors at stride 1 (f doubles per front)
 static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L, double* X, const double* B,
                                 int ld, double* W, int* flags, int* epoch, int* status, cudaStream_t st) {
-  solve_attrs();
+  solve_attrs<double>();
   const int ef = ++*epoch;
   for (int h = 0; h < P.n_levels; h++) {
     const LevelPlan& LP = P.levels[h];
     const int ns = (int) LP.small_fronts.size();
     if (ns > 0) {
-      k_fwd<1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
+      k_fwd<double, 1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
                                    W, 1);
       count_launch();
     }
     const int nb = (int) LP.solve_fwd_blocks.size();
     if (nb > 0) {
-      k_fwd_big<1, 1><<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
+      k_fwd_big<double, 1, 1><<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
                                           W, 1, flags, ef, status);
       count_launch();
     }
@@ -721,16 +734,16 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
     const LevelPlan& LP = P.levels[h];
     const int nb = (int) LP.solve_bwd_blocks.size();
     if (nb > 0) {
-      k_gather_upd<1><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
+      k_gather_upd<double, 1><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                          X, ld, W, 1);
       count_launch();
-      k_bwd_big<1, 1, false><<<nb, 128, BWD_SMEM, st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, X, ld, W, nullptr, 1,
+      k_bwd_big<double, 1, 1, false><<<nb, 128, bwd_smem<double>(), st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, X, ld, W, nullptr, 1,
                                                  flags, eb, status);
       count_launch();
     }
     const int ns = (int) LP.small_fronts.size();
     if (ns > 0) {
-      k_bwd<1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, X, ld, W, 1);
+      k_bwd<double, 1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, X, ld, W, 1);
       count_launch();
     }
   }
