@@ -253,7 +253,7 @@ int solve_device(Factor* F, int nrhs, double* dX, const double* dB, int ld) {
   if (!F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
   cudaStream_t st = current_stream();
   if (!cuda_ok(cudaMemsetAsync(F->dstatus + 1, 0, sizeof(int), st), "solve status")) return -1;
-  int e = launch_solve_fp64(F->plan, F->dp, F->dL, nrhs, dX, dB, ld, F->dW, F->dpart, F->dflags, &F->epoch,
+  int e = launch_solve_fp64(F->plan, F->dp, F->dL, F->dDinv, nrhs, dX, dB, ld, F->dW, F->dpart, F->dflags, &F->epoch,
                             F->dstatus + 1, st);
   return cuda_ok((cudaError_t) e, "solve launch") ? 0 : -1;
 }

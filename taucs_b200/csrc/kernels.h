@@ -66,11 +66,12 @@ int launch_numeric_fp32(const Plan& P, const DevPlan& D, const float* vals, floa
 // a big front; epoch must differ from every value they hold; status gets
 // SOLVE_TIMEOUT if a bounded wait gave up
 constexpr int SOLVE_TIMEOUT = -2;
-int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X,
+// Dinv: the factor's 64x64 diagonal-block inverses (FrontDesc::dinv_off)
+int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, const double* Dinv, int nrhs, double* X,
                       const double* B, int ld, double* W, double* part, int* flags, int* epoch, int* status,
                       cudaStream_t st);
 // the same solve on an FP32 factor with FP32 vectors
-int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, int nrhs, float* X,
+int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, const float* Dinv, int nrhs, float* X,
                       const float* B, int ld, float* W, float* part, int* flags, int* epoch, int* status,
                       cudaStream_t st);
 

@@ -425,6 +425,37 @@ __device__ __forceinline__ void mma_tile(float (&c)[4], const float (&a)[4], con
   mma_tf32(c, ah, bh);
 }
 
+// MI x NI fragment products of one k8 step.  FP32: every A and B fragment is
+// split into TF32 hi/lo parts once, then three products per pair.
+template <int MI, int NI>
+__device__ __forceinline__ void mma_block(double (&acc)[MI][NI][4], const double (&a)[MI][4], const double (&b)[NI][2]) {
+#pragma unroll
+  for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+    for (int ni = 0; ni < NI; ni++) dmma16888(acc[mi][ni], a[mi], b[ni]);
+}
+
+template <int MI, int NI>
+__device__ __forceinline__ void mma_block(float (&acc)[MI][NI][4], const float (&a)[MI][4], const float (&b)[NI][2]) {
+  unsigned ah[MI][4], al[MI][4], bh[NI][2], bl[NI][2];
+#pragma unroll
+  for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) split_tf32(a[mi][i], ah[mi][i], al[mi][i]);
+#pragma unroll
+  for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+    for (int i = 0; i < 2; i++) split_tf32(b[ni][i], bh[ni][i], bl[ni][i]);
+#pragma unroll
+  for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+    for (int ni = 0; ni < NI; ni++) {
+      mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+      mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+      mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
+    }
+}
+
 constexpr int TLD = PANEL_NB + 8;  // padded k-row stride of the TRSM operands
 
 // Step kb: rows below the diagonal block, X := X L_kk^-T = X * Dinv^T, one
@@ -478,10 +509,7 @@ k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
       b[ni][0] = Bs[(kk + t) * TLD + c];
       b[ni][1] = Bs[(kk + t + 4) * TLD + c];
     }
-#pragma unroll
-    for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-      for (int ni = 0; ni < 4; ni++) mma_tile(acc[mi][ni], a[mi], b[ni]);
+    mma_block<2, 4>(acc, a, b);
   }
 #pragma unroll
   for (int mi = 0; mi < 2; mi++)
@@ -636,10 +664,7 @@ k_gemm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, T* __
         b[ni][0] = Bs[(kk + t) * LD + c];
         b[ni][1] = Bs[(kk + t + 4) * LD + c];
       }
-#pragma unroll
-      for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-        for (int ni = 0; ni < NI; ni++) mma_tile(acc[mi][ni], a[mi], b[ni]);
+      mma_block<MI, NI>(acc, a, b);
     }
   }
   cp_async_wait<0>();

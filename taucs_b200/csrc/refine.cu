@@ -250,12 +250,12 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
       prev_worst = worst;
       // one correction step
       if (use64) {
-        if (launch_solve_fp64(P, F->dp, F->dL, nq, F->dR, F->dR, ld, F->dW, F->dpart, F->dflags, &F->epoch,
+        if (launch_solve_fp64(P, F->dp, F->dL, F->dDinv, nq, F->dR, F->dR, ld, F->dW, F->dpart, F->dflags, &F->epoch,
                               F->dstatus + 1, st)) return -1;
         k_update64<<<nblk(n, 256), 256, 0, st>>>(n, X, F->dR, ld, nq);
       } else {
         k_scale_down<<<nblk(n, 256), 256, 0, st>>>(n, F->dR, F->dscale, F->dV32, ld, nq);
-        if (launch_solve_fp32(P, F->dp, F->dL32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32, F->dflags, &F->epoch,
+        if (launch_solve_fp32(P, F->dp, F->dL32, F->dDinv32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32, F->dflags, &F->epoch,
                               F->dstatus + 1, st)) return -1;
         k_update32<<<nblk(n, 256), 256, 0, st>>>(n, X, F->dV32, F->dscale, ld, nq);
       }

@@ -58,17 +58,30 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
   for (int jb = 0; jb < s; jb += SB) {
     const int bw = min(SB, s - jb);
     if (warp == 0) {
-      for (int q = 0; q < nrhs; q++) {
-        T v = (lane < bw) ? Wf[jb + lane + q * f] : 0.0;
-        for (int j = 0; j < bw; j++) {
-          const T xj = __shfl_sync(0xffffffffu, v, j) / P[(jb + j) + (size_t) (jb + j) * f];
-          if (lane == j) v = xj;
-          if (lane > j && lane < bw) v -= P[(jb + lane) + (size_t) (jb + j) * f] * xj;
+      // all right-hand sides advance together through one substitution chain
+      const T rd = (lane < bw) ? T(1) / P[(jb + lane) + (size_t) (jb + lane) * f] : T(0);
+      T v[SOLVE_NRHS];
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && lane < bw) ? Wf[jb + lane + q * f] : T(0);
+      for (int j = 0; j < bw; j++) {
+        const T rj = __shfl_sync(0xffffffffu, rd, j);
+        const T l = (lane > j && lane < bw) ? P[(jb + lane) + (size_t) (jb + j) * f] : T(0);
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++) {
+          if (q < nrhs) {
+            const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
+            if (lane == j) v[q] = xj;
+            else v[q] -= l * xj;
+          }
         }
-        if (lane < bw) {
-          Wf[jb + lane + q * f] = v;
-          xs[lane][q] = v;
-        }
+      }
+      if (lane < bw) {
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++)
+          if (q < nrhs) {
+            Wf[jb + lane + q * f] = v[q];
+            xs[lane][q] = v[q];
+          }
       }
     }
     __syncthreads();
@@ -82,7 +95,9 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
         for (int q = 0; q < SOLVE_NRHS; q++)
           if (q < nrhs) acc[q] += l * xs[j][q];
       }
-      for (int q = 0; q < nrhs; q++) Wf[r + q * f] -= acc[q];
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++)
+        if (q < nrhs) Wf[r + q * f] -= acc[q];
     }
     __syncthreads();
   }
@@ -125,8 +140,11 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
       for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
       acc[q] = v;
     }
-    if (lane == 0)
-      for (int q = 0; q < nrhs; q++) Wf[j + q * f] -= acc[q];
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++)
+        if (q < nrhs) Wf[j + q * f] -= acc[q];
+    }
   }
   __syncthreads();
   // L11^T substitution, blocks from the end
@@ -152,20 +170,35 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
           for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
           acc[q] = v;
         }
-        if (lane == 0)
-          for (int q = 0; q < nrhs; q++) Wf[j + q * f] -= acc[q];
+        if (lane == 0) {
+#pragma unroll
+          for (int q = 0; q < SOLVE_NRHS; q++)
+            if (q < nrhs) Wf[j + q * f] -= acc[q];
+        }
       }
       __syncthreads();
     }
     if (warp == 0) {
-      for (int q = 0; q < nrhs; q++) {
-        T v = (lane < bw) ? Wf[jb + lane + q * f] : 0.0;
-        for (int j = bw - 1; j >= 0; j--) {
-          const T xj = __shfl_sync(0xffffffffu, v, j) / P[(jb + j) + (size_t) (jb + j) * f];
-          if (lane == j) v = xj;
-          if (lane < j) v -= P[(jb + j) + (size_t) (jb + lane) * f] * xj;
+      const T rd = (lane < bw) ? T(1) / P[(jb + lane) + (size_t) (jb + lane) * f] : T(0);
+      T v[SOLVE_NRHS];
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && lane < bw) ? Wf[jb + lane + q * f] : T(0);
+      for (int j = bw - 1; j >= 0; j--) {
+        const T rj = __shfl_sync(0xffffffffu, rd, j);
+        const T l = (lane < j) ? P[(jb + j) + (size_t) (jb + lane) * f] : T(0);
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++) {
+          if (q < nrhs) {
+            const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
+            if (lane == j) v[q] = xj;
+            else v[q] -= l * xj;
+          }
         }
-        if (lane < bw) xs[lane][q] = v;
+      }
+      if (lane < bw) {
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++)
+          if (q < nrhs) xs[lane][q] = v[q];
       }
     }
     __syncthreads();
@@ -212,7 +245,7 @@ __device__ void wait_epoch(const int* flag, int epoch, int* status) {
         atomicExch(status, SOLVE_TIMEOUT);
         break;
       }
-      __nanosleep(128);
+      __nanosleep(32);
     }
   }
   __syncthreads();
@@ -232,12 +265,14 @@ template <typename T, int NQ, int WS>
 __global__ void __launch_bounds__(128)
 k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ children, const int* __restrict__ maps, const int* __restrict__ rows,
-          const T* __restrict__ L, const T* __restrict__ B, int ldb, T* __restrict__ W,
-          int nrhs, int* __restrict__ flags, int epoch, int* status) {
+          const T* __restrict__ L, const T* __restrict__ Dinv, const T* __restrict__ B, int ldb,
+          T* __restrict__ W, int nrhs, int* __restrict__ flags, int epoch, int* status) {
   __shared__ T wv[BR][NQ];
   __shared__ T yk[BR][NQ];
   __shared__ T part[BR][NQ];
-  __shared__ T dg[BR][BR + 1];   // diagonal block, column-major: dg[col][row]
+  // dg[col][row]: rows < bw hold L_rr^-1 (lower), rows >= bw the update
+  // rows of L that share this 64-row block (last diagonal block only)
+  __shared__ T dg[BR][BR + 1];
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int r = bk.b, f = F.f, s = F.s;
@@ -249,11 +284,14 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const T* P = L + F.l_off;
 
   if (r < nbs) {
-    // stage the diagonal block now, off the chain's critical path
+    // stage the block's inverse now, off the chain's critical path
     const int bw = min(BR, s - r0);
+    const T* Di = Dinv + F.dinv_off + (size_t) r * BR * BR;
     for (int e = tid; e < BR * BR; e += 128) {
       const int i = e % BR, j = e / BR;
-      dg[j][i] = (i < nr && j < bw) ? P[(r0 + i) + (size_t) (r0 + j) * f] : 0.0;
+      T v = 0.0;
+      if (j < bw && i < nr) v = (i < bw) ? (i >= j ? Di[i + j * BR] : T(0)) : P[(r0 + i) + (size_t) (r0 + j) * f];
+      dg[j][i] = v;
     }
   }
   for (int k = tid; k < BR * NQ; k += 128) {
@@ -309,28 +347,48 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     for (int q = 0; q < NQ; q++) wv[row][q] -= acc[q] + part[row][q];
   __syncthreads();
   if (r < nbs) {
-    // the diagonal block was staged at kernel start; one warp substitutes:
-    // lanes own rows lane and lane+32
+    // y_r = L_rr^-1 w_r: a 64x64 product split over the two thread halves
+    // instead of a 64-step substitution chain
     const int bw = min(BR, s - r0);
-    if (warp == 0) {
-      // reciprocal diagonal formed in parallel, off the substitution's critical path
-      const T rd0 = (lane < bw) ? T(1) / dg[lane][lane] : T(0);
-      const T rd1 = (lane + 32 < bw) ? T(1) / dg[lane + 32][lane + 32] : T(0);
-      for (int q = 0; q < nrhs; q++) {
-        T v0 = wv[lane][q], v1 = wv[lane + 32][q];
-        for (int j = 0; j < bw; j++) {
-          const T src = (j < 32) ? __shfl_sync(0xffffffffu, v0, j) : __shfl_sync(0xffffffffu, v1, j - 32);
-          const T rj = (j < 32) ? __shfl_sync(0xffffffffu, rd0, j) : __shfl_sync(0xffffffffu, rd1, j - 32);
-          const T xj = src * rj;
-          if (lane == j) v0 = xj;
-          else if (lane > j) v0 -= dg[j][lane] * xj;
-          if (lane + 32 == j) v1 = xj;
-          else if (lane + 32 > j) v1 -= dg[j][lane + 32] * xj;
-        }
-        wv[lane][q] = v0;
-        wv[lane + 32][q] = v1;
-      }
+    T y[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) y[q] = 0.0;
+#pragma unroll 8
+    for (int j = half * (BR / 2); j < half * (BR / 2) + BR / 2; j++) {
+      const T d = (row < bw) ? dg[j][row] : T(0);
+#pragma unroll
+      for (int q = 0; q < NQ; q++) y[q] += d * wv[j][q];
     }
+    if (half == 1)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) part[row][q] = y[q];
+    __syncthreads();
+    if (half == 0 && row < bw)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) yk[row][q] = y[q] + part[row][q];
+    __syncthreads();
+    if (bw < nr) {
+      // update rows inside the last diagonal block: w_i -= L[i, r] y_r
+      T u[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) u[q] = 0.0;
+      if (row >= bw)
+        for (int j = half * (BR / 2); j < min(bw, half * (BR / 2) + BR / 2); j++) {
+          const T l = dg[j][row];
+#pragma unroll
+          for (int q = 0; q < NQ; q++) u[q] += l * yk[j][q];
+        }
+      if (half == 1)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) part[row][q] = u[q];
+      __syncthreads();
+      if (half == 0 && row >= bw)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) wv[row][q] -= u[q] + part[row][q];
+    }
+    if (half == 0 && row < bw)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) wv[row][q] = yk[row][q];
     __syncthreads();
   }
   for (int k = tid; k < nr * nrhs; k += 128) {
@@ -411,7 +469,7 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
 template <typename T, int NQ, int WS, bool PARTS>
 __global__ void __launch_bounds__(128)
 k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
-          const int* __restrict__ rows, const T* __restrict__ L, T* __restrict__ X, int ldx,
+          const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ Dinv, T* __restrict__ X, int ldx,
           T* __restrict__ W, const T* __restrict__ part, int nrhs, int* __restrict__ flags, int epoch,
           int* status) {
   constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;   // columns per pass of the L21 product
@@ -421,7 +479,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   extern __shared__ __align__(16) unsigned char bsmraw[];
   T* bsm = reinterpret_cast<T*>(bsmraw);
   T (*tile)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm);             // block of L11, [col][row]
-  T (*dgb)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm + BR * (BR + 1));  // diagonal block, [row][col]
+  T (*dgb)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm + BR * (BR + 1));  // L_kk^-1, [row][col]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int k = bk.b, f = F.f, s = F.s, m = f - s;
@@ -432,10 +490,11 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   const int* rw = rows + F.rows_off;
   const T* P = L + F.l_off;
 
-  // stage the diagonal block now, off the chain's critical path
+  // stage the block's inverse now, off the chain's critical path
+  const T* Di = Dinv + F.dinv_off + (size_t) k * BR * BR;
   for (int e = tid; e < BR * BR; e += 128) {
     const int i = e % BR, c = e / BR;
-    dgb[i][c] = (i < bw && c < bw) ? P[(c0 + i) + (size_t) (c0 + c) * f] : 0.0;
+    dgb[i][c] = (i < bw && c < bw && i >= c) ? Di[i + c * BR] : T(0);
   }
   for (int e = tid; e < BR * NQ; e += 128) {
     const int c = e % BR, q = e / BR;
@@ -517,31 +576,30 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
       for (int q = 0; q < NQ; q++) xv[col][q] -= acc[q] + red[col][q];
     __syncthreads();
   }
-  // L_kk^T substitution from the staged diagonal block, one warp, columns
-  // lane and lane+32
-  if (warp == 0) {
-    const T rd0 = (lane < bw) ? T(1) / dgb[lane][lane] : T(0);
-    const T rd1 = (lane + 32 < bw) ? T(1) / dgb[lane + 32][lane + 32] : T(0);
-    for (int q = 0; q < nrhs; q++) {
-      T v0 = xv[lane][q], v1 = xv[lane + 32][q];
-      for (int c = bw - 1; c >= 0; c--) {
-        const T src = (c < 32) ? __shfl_sync(0xffffffffu, v0, c) : __shfl_sync(0xffffffffu, v1, c - 32);
-        const T rc = (c < 32) ? __shfl_sync(0xffffffffu, rd0, c) : __shfl_sync(0xffffffffu, rd1, c - 32);
-        const T x = src * rc;
-        if (lane == c) v0 = x;
-        else if (lane < c) v0 -= dgb[c][lane] * x;
-        if (lane + 32 == c) v1 = x;
-        else if (lane + 32 < c) v1 -= dgb[c][lane + 32] * x;
-      }
-      xv[lane][q] = v0;
-      xv[lane + 32][q] = v1;
+  // x_k = L_kk^-T v_k from the staged inverse, split over the two halves
+  {
+    T x[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) x[q] = 0.0;
+#pragma unroll 8
+    for (int i = half * (BR / 2); i < half * (BR / 2) + BR / 2; i++) {
+      const T d = dgb[i][col];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) x[q] += d * xv[i][q];
     }
+    if (half == 1)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) red[col][q] = x[q];
+    __syncthreads();
+    if (half == 0)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) xj[col][q] = x[q] + red[col][q];
+    __syncthreads();
   }
-  __syncthreads();
   for (int e = tid; e < bw * nrhs; e += 128) {
     const int c = e % bw, q = e / bw;
-    Wf[c0 + c + (size_t) q * f] = xv[c][q];
-    X[rw[c0 + c] + (size_t) q * ldx] = xv[c][q];
+    Wf[c0 + c + (size_t) q * f] = xj[c][q];
+    X[rw[c0 + c] + (size_t) q * ldx] = xj[c][q];
   }
   __syncthreads();
   // the barrier orders every thread's writes before thread 0's release store
@@ -570,7 +628,7 @@ static void solve_attrs() {
 }
 
 template <typename T>
-static int launch_solve(const Plan& P, const DevPlan& D, const T* L, int nrhs, T* X, const T* B, int ld, T* W,
+static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Dinv, int nrhs, T* X, const T* B, int ld, T* W,
                         T* part, int* flags, int* epoch, int* status, cudaStream_t st) {
   solve_attrs<T>();
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
@@ -594,13 +652,13 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, int nrhs, T
       if (nb > 0) {
         const int2_* bl = D.sfwd + D.sfwd_off[h];
         if (nq == 1)
-          k_fwd_big<T, 1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
         else if (nq == 2)
-          k_fwd_big<T, 2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
         else if (nq <= 4)
-          k_fwd_big<T, 4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
         else
-          k_fwd_big<T, 8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Bq, ld, W, nq, flags, ef, status);
+          k_fwd_big<T, 8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
         count_launch();
       }
       prof_end(KC_SOLVE_FWD, st, 0.0, by);
@@ -628,13 +686,13 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, int nrhs, T
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
         if (nq == 1)
-          k_bwd_big<T, 1, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 1, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq == 2)
-          k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
-          k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else
-          k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         count_launch();
       }
       const int ns = (int) LP.small_fronts.size();
@@ -648,14 +706,16 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, int nrhs, T
   return (int) cudaGetLastError();
 }
 
-int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, int nrhs, double* X, const double* B, int ld,
-                      double* W, double* part, int* flags, int* epoch, int* status, cudaStream_t st) {
-  return launch_solve<double>(P, D, L, nrhs, X, B, ld, W, part, flags, epoch, status, st);
+int launch_solve_fp64(const Plan& P, const DevPlan& D, const double* L, const double* Dinv, int nrhs, double* X,
+                      const double* B, int ld, double* W, double* part, int* flags, int* epoch, int* status,
+                      cudaStream_t st) {
+  return launch_solve<double>(P, D, L, Dinv, nrhs, X, B, ld, W, part, flags, epoch, status, st);
 }
 
-int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, int nrhs, float* X, const float* B, int ld,
-                      float* W, float* part, int* flags, int* epoch, int* status, cudaStream_t st) {
-  return launch_solve<float>(P, D, L, nrhs, X, B, ld, W, part, flags, epoch, status, st);
+int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, const float* Dinv, int nrhs, float* X,
+                      const float* B, int ld, float* W, float* part, int* flags, int* epoch, int* status,
+                      cudaStream_t st) {
+  return launch_solve<float>(P, D, L, Dinv, nrhs, X, B, ld, W, part, flags, epoch, status, st);
 }
 
 }  // namespace tb
@@ -710,7 +770,8 @@ static int noalloc_scratch(double** out) {
 }
 
 // one right-hand side, work vectors at stride 1 (f doubles per front)
-static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L, double* X, const double* B,
+static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L, const double* Dinv, double* X,
+                                const double* B,
                                 int ld, double* W, int* flags, int* epoch, int* status, cudaStream_t st) {
   solve_attrs<double>();
   const int ef = ++*epoch;
@@ -724,8 +785,8 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
     }
     const int nb = (int) LP.solve_fwd_blocks.size();
     if (nb > 0) {
-      k_fwd_big<double, 1, 1><<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
-                                          W, 1, flags, ef, status);
+      k_fwd_big<double, 1, 1><<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, Dinv, B,
+                                          ld, W, 1, flags, ef, status);
       count_launch();
     }
   }
@@ -737,7 +798,7 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
       k_gather_upd<double, 1><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                          X, ld, W, 1);
       count_launch();
-      k_bwd_big<double, 1, 1, false><<<nb, 128, bwd_smem<double>(), st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, X, ld, W, nullptr, 1,
+      k_bwd_big<double, 1, 1, false><<<nb, 128, bwd_smem<double>(), st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, Dinv, X, ld, W, nullptr, 1,
                                                  flags, eb, status);
       count_launch();
     }
@@ -790,7 +851,7 @@ extern "C" int taucs_b200_solve_device_noalloc(void* vL, int nrhs, double* d_X, 
   }
   int epoch = 0;
   for (int q = 0; q < nrhs; q++) {
-    e = (cudaError_t) launch_solve_noalloc(P, F->dp, F->dL, d_X + (size_t) q * ld, d_B + (size_t) q * ld, ld, W,
+    e = (cudaError_t) launch_solve_noalloc(P, F->dp, F->dL, F->dDinv, d_X + (size_t) q * ld, d_B + (size_t) q * ld, ld, W,
                                            flags, &epoch, status, st);
     if (e != cudaSuccess) {
       set_error(std::string("taucs_b200_solve_device_noalloc: ") + cudaGetErrorString(e));
