@@ -59,6 +59,19 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
 int launch_numeric_fp32(const Plan& P, const DevPlan& D, const float* vals, float* L,
                         float* U, float* Dinv, int* status, cudaStream_t st);
 
+// status value recorded when a bounded device wait of the factorization gave
+// up (never a column index)
+constexpr int NUMERIC_TIMEOUT = -4;
+
+// FP32 fronts: C -= A B^T on tcgen05 (TF32x3, 128x128 tiles, TMEM
+// accumulator); same modes and arguments as the mma.sync GEMM.
+// gemm_tc_init() sets the kernel's shared-memory limit once and reports
+// whether the kernel is usable; gemm_tc_tiles() = CTAs per front.
+bool gemm_tc_init();
+int gemm_tc_tiles(int rows, int cols);
+void launch_gemm_tc(int gx, int nb, const int* list, const FrontDesc* fronts, float* L, float* U, int c_lo, int c_hi,
+                    int k_lo, int k_hi, int mode, int* status, cudaStream_t st);
+
 // multi-RHS solve, device vectors in permuted order: X (n x nrhs, ld) from
 // B (n x nrhs, ld); W scratch of P.v_len * SOLVE_NRHS doubles, Y n *
 // SOLVE_NRHS doubles

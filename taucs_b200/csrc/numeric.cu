@@ -728,6 +728,16 @@ static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, 
         blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
 }
 
+// FP32 fronts take the tcgen05 kernel (gemm_tc.cu) when it is available
+static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, float* L, float* U,
+                        int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
+  if (gemm_tc_init()) {
+    launch_gemm_tc(gx128, nb, blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
+    return;
+  }
+  launch_gemm<float>(big, gx128, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
+}
+
 template <typename T>
 static constexpr size_t potrf_smem() { return (2 * PANEL_NB * DLD + 32 * DLD) * sizeof(T); }
 
