@@ -1,24 +1,33 @@
 #!/usr/bin/env python
-"""Benchmark: FP64 multifrontal numeric factorization + supernodal solve.
+"""Benchmark of the multifrontal Cholesky factor + solve path.
 
-Workload (default): the 64^3 7-point Laplacian generated exactly as the
-reference's taucs_ccs_generate_mesh3d(64,64,64) (n = 262,144), AMD ordering,
-one right-hand side b = A x_true with x_true ~ U(-1,1) (seed 0).  One STEP is
-one numeric factorization on the analysed pattern plus one solve -- the
-reference's taucs_ccs_factor_llt_numeric + taucs_supernodal_solve_llt
-(src/taucs_sn_llt.c:2169-2209, :2844-2885).  Ordering and symbolic analysis
-happen once, before the timed region, as in the reference's pattern-reuse
-path (src/taucs_linsolve.c:433-453).
+Default workload (--workload mixed80): the precision configuration -- a 3D
+7-point operator on an 80^3 grid (n = 512,000) whose edge conductances are
+exp(2 N(0,1)) times an anisotropy of 1:1:100 in x:y:z (seeded generator,
+taucs_b200_generate_lognormal), AMD ordering, 8 right-hand sides ~ U(-1,1)
+(seed 0).  One STEP factors the analysed pattern with FP32 fronts (diagonal
+scaling, tcgen05 TF32x3 products) and refines all 8 solutions in FP64 to a
+scaled residual ||Ax-b||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-12 --
+the FP32+refinement form.  The plain FP64 path (FP64 fronts, one solve of the
+8 right-hand sides) is timed beside it on the same inputs and reported as
+`fp64` with the speed-up.  Ordering and symbolic analysis happen once, before
+the timed region, as in the reference's pattern-reuse path
+(src/taucs_linsolve.c:433-453; numeric = src/taucs_sn_llt.c:2169-2209, solve
+= :2844-2885).
+
+--workload fp64-64: the 64^3 7-point Laplacian of the reference's
+taucs_ccs_generate_mesh3d, AMD, FP64 numeric factor + one 1-RHS solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints ONE JSON line (rank 0).  `value` is whole-job systems/s with the
-matrix values and b resident in device memory; `e2e` is the same metric
-through the C ABI with pinned host buffers (values, b in; x out) copied
+Prints ONE JSON line (rank 0).  `value` is whole-job systems/s with values
+and right-hand sides resident in device memory; `e2e` is the same metric
+through the C ABI with pinned host buffers (values, B in; X out) copied
 inside every step.  Under torchrun every rank factors its own replica (no
 collective on the data path; max over ranks for time).
 """
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -32,8 +41,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "fp64 numeric factor + solve throughput (64^3 7-point Laplacian, AMD)"
 UNIT = "systems/s"
+METRIC_MIXED = ("FP32+refine vs FP64 factor+solve time at 1e-12 residual "
+                "(80^3 lognormal sigma=2, aniso 1:1:100, AMD, 8 RHS): FP32+refine systems/s")
+METRIC_FP64 = "fp64 numeric factor + solve throughput (64^3 7-point Laplacian, AMD)"
+NRHS = 8
+TOL = 1e-12
+SAMPLE_GRID = 56          # bounded CPU sample of the lognormal workload
 
 KC = dict(small_front=0, build=1, potrf=2, trsm=3, gemm_panel=4, gemm_u=5, solve_fwd=6, solve_bwd=7)
 TENSOR_KC = {"gemm_panel", "gemm_u", "trsm", "potrf"}
@@ -42,10 +56,11 @@ TENSOR_KC = {"gemm_panel", "gemm_u", "trsm", "potrf"}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--grid", type=int, default=64, help="mesh side (64 = the benchmark configuration)")
+    ap.add_argument("--workload", default="mixed80", choices=["mixed80", "fp64-64"])
+    ap.add_argument("--grid", type=int, default=None, help="grid side (default 80 / 64 per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -57,6 +72,25 @@ def dist_env():
 def scaled_residual(A, x, b):
     r = A.matvec(x) - b
     return float(np.max(np.abs(r)) / (A.inf_norm() * np.max(np.abs(x)) + np.max(np.abs(b))))
+
+
+def make_system(workload, g):
+    """(A unpermuted, perm, iperm, PAP^T, B) of the workload."""
+    import taucs_b200 as tb
+    if workload == "mixed80":
+        A = tb.lognormal(g, g, g, 2.0, (1.0, 1.0, 100.0), 0)
+        nrhs = NRHS
+    else:
+        A = tb.mesh3d(g)
+        nrhs = 1
+    perm, iperm = tb.order(A, "amd")
+    P = A.permute(perm, iperm)
+    rng = np.random.default_rng(0)
+    if workload == "mixed80":
+        B = rng.uniform(-1, 1, (A.n, nrhs))
+    else:
+        B = P.matvec(rng.uniform(-1, 1, A.n)).reshape(-1, 1)
+    return A, perm, iperm, P, B
 
 
 class ClockSampler:
@@ -139,102 +173,167 @@ def measured_peaks():
         return {}
 
 
-def cpu_baseline(grid, n_threads):
-    """The reference's own CPU multifrontal path (oracle/_ref), one numeric
-    factorization + one solve of the same system, on this host's cores."""
-    from oracle.bindings import Port, Ref, ref_available
-    if ref_available():
-        R = Ref(threads=n_threads)
-        R.set_threads(n_threads)
-        n, cp, ri, va = R.mesh3d(grid, grid, grid)
-        perm, iperm = R.order(n, cp, ri, va, "amd")
-        _, pc, pr, pv = R.permute(n, cp, ri, va, perm, iperm)
-        L = R.symbolic(n, pc, pr, pv)
-        xt = np.random.default_rng(0).uniform(-1, 1, n)
-        b = Port().spmv(n, pc, pr, pv, xt)
-        t0 = time.perf_counter()
-        assert R.numeric(L, n, pc, pr, pv) == 0
-        x = R.solve(L, b)
-        dt = time.perf_counter() - t0
-        R.free(L)
-        return {"value": 1.0 / dt, "unit": UNIT, "cores": n_threads, "kind": "reference",
-                "seconds_per_system": dt,
-                "sample": f"one taucs_ccs_factor_llt_numeric + one taucs_supernodal_solve_llt of the same "
-                          f"{grid}^3 system (reference sources + OpenBLAS 0.3.15, {n_threads} threads)",
-                "max_abs_err": float(np.max(np.abs(x - xt)))}
-    # fallback: the plain-C restatement on a smaller sample, scaled by flops
+def tf32_gemm_peak():
+    """cuBLAS TF32 GEMM (FP32 inputs on the tensor cores) 8192^3, best of 5."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    best = 0.0
+    for _ in range(6):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+# ---------------------------------------------------------------- CPU (reference)
+
+def ref_system(workload, g):
+    """The workload's PAP^T in the reference library (oracle/_ref): the matrix
+    comes from the same generator, the ordering from the reference's AMD."""
     import taucs_b200 as tb
-    P = Port()
-    g = max(8, grid // 2)
-    A = tb.mesh3d(g)
-    perm, iperm = tb.order(A, "amd")
-    Pm = A.permute(perm, iperm)
-    h = P.analyze(*Pm.arrays()[:3])
-    t0 = time.perf_counter()
-    P.numeric(h, Pm.colptr, Pm.rowind, Pm.values)
-    P.solve(h, Pm.matvec(np.ones(A.n)))
-    dt = time.perf_counter() - t0
-    flops_s = tb.factor_symbolic(Pm).info().flops
-    Af = tb.mesh3d(grid)
-    pf, ipf = tb.order(Af, "amd")
-    flops_f = tb.factor_symbolic(Af.permute(pf, ipf)).info().flops
-    P.free(h)
-    dt_full = dt * flops_f / flops_s
-    return {"value": 1.0 / dt_full, "unit": UNIT, "cores": 1, "kind": "port", "seconds_per_system": dt_full,
-            "sample": f"oracle restatement on {g}^3, time scaled by the flop ratio to {grid}^3"}
+    from oracle.bindings import Ref
+    R = Ref()
+    if workload == "mixed80":
+        A = tb.lognormal(g, g, g, 2.0, (1.0, 1.0, 100.0), 0)
+        n, cp, ri, va = A.n, A.colptr, A.rowind, A.values
+    else:
+        n, cp, ri, va = R.mesh3d(g, g, g)
+    perm, iperm = R.order(n, cp, ri, va, "amd")
+    _, pc, pr, pv = R.permute(n, cp, ri, va, perm, iperm)
+    return R, n, pc, pr, pv
+
+
+def ref_step(R, L, n, pc, pr, pv, B):
+    assert R.numeric(L, n, pc, pr, pv) == 0
+    X = np.empty_like(B)
+    for q in range(B.shape[1]):       # the reference solves one right-hand side per call
+        X[:, q] = R.solve(L, np.ascontiguousarray(B[:, q]))
+    return X
+
+
+def cpu_reference(workload, g, n_threads, steps=1, warmup=0):
+    """The reference's CPU multifrontal path (sources + OpenBLAS) on this
+    host's cores.  mixed80: a bounded sample -- the same generator at
+    SAMPLE_GRID^3 -- whose time is scaled by the reference's flop count to the
+    full grid; fp64-64: the full system.  Returns (seconds per full system,
+    description, kind, cores)."""
+    from oracle.bindings import Port, Ref, ref_available
+    os.environ["OPENBLAS_NUM_THREADS"] = str(n_threads)
+    if not ref_available():
+        raise RuntimeError("oracle/_ref/libtaucs_ref.so was not built")
+    gs = SAMPLE_GRID if workload == "mixed80" else g
+    R, n, pc, pr, pv = ref_system(workload, gs)
+    R.set_threads(n_threads)
+    L = R.symbolic(n, pc, pr, pv)
+    flops_s = R.dump_symbolic(L).flops()
+    rng = np.random.default_rng(0)
+    B = rng.uniform(-1, 1, (n, NRHS)) if workload == "mixed80" else \
+        Port().spmv(n, pc, pr, pv, rng.uniform(-1, 1, n)).reshape(-1, 1)
+    for _ in range(warmup):
+        ref_step(R, L, n, pc, pr, pv, B)
+        R.free_numeric(L)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref_step(R, L, n, pc, pr, pv, B)
+        times.append(time.perf_counter() - t0)
+        R.free_numeric(L)
+    R.free(L)
+    dt = sum(times) / len(times)
+    if workload == "mixed80":
+        import taucs_b200 as tb
+        A, _, _, P, _ = make_system(workload, g)
+        flops_f = tb.factor_symbolic(P).info().flops
+        scale = flops_f / flops_s
+        desc = (f"reference FP64 factor + {NRHS} one-RHS solves of the {gs}^3 lognormal system "
+                f"(same generator, sigma=2, aniso 1:1:100, AMD), {dt:.2f} s, scaled by the reference's "
+                f"flop count x{scale:.2f} to {g}^3; sources + OpenBLAS 0.3.15, {n_threads} threads")
+        return dt * scale, desc, "reference", n_threads
+    desc = (f"reference FP64 numeric factor + 1-RHS solve of the full {g}^3 system "
+            f"(sources + OpenBLAS 0.3.15, {n_threads} threads)")
+    return dt, desc, "reference", n_threads
 
 
 def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
+    g = args.grid or (80 if args.workload == "mixed80" else 64)
     n_threads = os.cpu_count() or 1
-    os.environ["OPENBLAS_NUM_THREADS"] = str(n_threads)
-    from oracle.bindings import Port, Ref, ref_available
-    if not ref_available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtaucs_ref.so was not built"}))
+    try:
+        # bounded: one warm-up and at most 3 timed steps of the bounded sample
+        warm = min(args.warmup, 1)
+        steps = max(1, min(args.steps, 3))
+        sec, desc, kind, cores = cpu_reference(args.workload, g, n_threads, steps=steps, warmup=warm)
+    except Exception as exc:  # one line, never a traceback
+        print(json.dumps({"impl": "reference", "unavailable": repr(exc)}))
         return
-    R = Ref(threads=n_threads)
-    R.set_threads(n_threads)
-    g = args.grid
-    n, cp, ri, va = R.mesh3d(g, g, g)
-    perm, iperm = R.order(n, cp, ri, va, "amd")
-    _, pc, pr, pv = R.permute(n, cp, ri, va, perm, iperm)
-    L = R.symbolic(n, pc, pr, pv)
-    xt = np.random.default_rng(0).uniform(-1, 1, n)
-    b = Port().spmv(n, pc, pr, pv, xt)
-    sym = R.dump_symbolic(L)
-    # each step is one full system: about 15-25 s of CPU work at 64^3, so the
-    # run is bounded to 1 warm-up step and at most 3 timed steps
-    warm = min(args.warmup, 1)
-    steps = max(1, min(args.steps, 3))
-    x = None
-    for _ in range(warm):
-        R.numeric(L, n, pc, pr, pv)
-        x = R.solve(L, b)
-        R.free_numeric(L)
-    times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        assert R.numeric(L, n, pc, pr, pv) == 0
-        x = R.solve(L, b)
-        times.append(time.perf_counter() - t0)
-        R.free_numeric(L)
-    R.free(L)
-    tot = sum(times)
-    val = steps / tot
-    out = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world,
-           "steps": steps, "warmup": warm, "ms_per_step": 1e3 * tot / steps, "higher_is_better": True,
+    val = 1.0 / sec
+    metric = METRIC_MIXED if args.workload == "mixed80" else METRIC_FP64
+    out = {"impl": "reference", "metric": metric, "value": val, "unit": UNIT, "n_gpus": world,
+           "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sec, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": f"mesh3d {g}^3 7-point Laplacian (reference generator), AMD, "
-                                  f"numeric factor + 1-RHS solve", "n": n, "nnz_lower": int(cp[-1]),
-                      "flops": sym.flops()},
+           "config": {"workload": workload_name(args.workload, g)},
            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-           "cpu_baseline": {"value": val, "unit": UNIT, "cores": n_threads, "kind": "reference",
-                            "sample": f"{steps} timed steps of the full {g}^3 system after {warm} warm-up "
-                                      f"(reference sources + OpenBLAS 0.3.15, {n_threads} threads)"},
-           "max_abs_err": float(np.max(np.abs(x - xt)))}
+           "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}}
     print(json.dumps(out))
+
+
+def workload_name(workload, g):
+    if workload == "mixed80":
+        return (f"lognormal {g}^3 7-point (sigma=2, aniso 1:1:100, seed 0), AMD, {NRHS} RHS; "
+                f"numeric factor + solve to scaled residual <= {TOL:g}")
+    return f"mesh3d {g}^3 7-point Laplacian (reference generator), AMD, FP64 numeric factor + 1-RHS solve"
+
+
+# ---------------------------------------------------------------- GPU
+
+def read_profile(tb, nsteps):
+    kern = {}
+    rd = tb.lib().taucs_b200_profile_read
+    for name, kc in KC.items():
+        t, nl, fl, by = C.c_double(), C.c_long(), C.c_double(), C.c_double()
+        rd(kc, C.byref(t), C.byref(nl), C.byref(fl), C.byref(by))
+        if nl.value:
+            kern[name] = {"ms_per_step": t.value / nsteps, "launches_per_step": nl.value // nsteps,
+                          "gflop_per_step": fl.value / nsteps / 1e9, "gb_per_step": by.value / nsteps / 1e9}
+    for v in kern.values():
+        if v["gflop_per_step"] > 0:
+            v["tflop_s"] = v["gflop_per_step"] / v["ms_per_step"]
+        if v["gb_per_step"] > 0:
+            v["gb_s"] = v["gb_per_step"] / v["ms_per_step"] * 1e3
+    return kern
+
+
+def roofline(kern, tensor_peak, tensor_src, hbm_peak):
+    if not kern:
+        return None
+    dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])[0]
+    d = kern[dom]
+    per_launch_ms = d["ms_per_step"] / max(d["launches_per_step"], 1)
+    if dom in TENSOR_KC:
+        ach = d["gflop_per_step"] / d["ms_per_step"]  # GFLOP/ms = TFLOP/s
+        return {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": tensor_peak, "unit": "TFLOP/s",
+                "frac": ach / tensor_peak, "peak_source": tensor_src,
+                "algorithmic_per_launch": d["gflop_per_step"] / max(d["launches_per_step"], 1) * 1e9,
+                "avg_launch_ms": per_launch_ms, "traffic": None}
+    ach = d["gb_per_step"] / d["ms_per_step"] * 1e3
+    return {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+            "frac": ach / hbm_peak if hbm_peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "algorithmic_per_launch": d["gb_per_step"] / max(d["launches_per_step"], 1) * 1e9,
+            "avg_launch_ms": per_launch_ms, "traffic": None}
 
 
 def run_ours(args):
@@ -250,39 +349,65 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     stream = torch.cuda.current_stream()
     tb.set_stream(stream.cuda_stream)
-    g = args.grid
+    mixed = args.workload == "mixed80"
+    g = args.grid or (80 if mixed else 64)
 
     # ---- setup (untimed): generator, AMD, permutation, symbolic analysis
-    A = tb.mesh3d(g)
-    perm, iperm = tb.order(A, "amd")
-    P = A.permute(perm, iperm)
+    A, perm, iperm, P, B = make_system(args.workload, g)
     F = tb.factor_symbolic(P)
     info = F.info()
-    n, nnz = A.n, P.nnz
-    xt = np.random.default_rng(0).uniform(-1, 1, n)
-    b = P.matvec(xt)
+    n, nnz, nrhs = A.n, P.nnz, B.shape[1]
+    Bf = np.asfortranarray(B)
     d_vals = torch.from_numpy(P.values).cuda()
-    d_b = torch.from_numpy(b).cuda()
+    d_b = torch.from_numpy(Bf.T.copy()).cuda()        # column-major n x nrhs
     d_x = torch.empty_like(d_b)
     # pinned host buffers for the end-to-end path
     h_vals = torch.empty(nnz, dtype=torch.float64, pin_memory=True).numpy()
     h_vals[:] = P.values
     Ph = tb.Matrix(n, P.colptr, P.rowind, h_vals)
-    h_b = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    h_b[:] = b
-    h_x = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    h_b = torch.empty(nrhs * n, dtype=torch.float64, pin_memory=True).numpy()
+    h_b[:] = Bf.T.reshape(-1)
+    h_x = torch.empty(nrhs * n, dtype=torch.float64, pin_memory=True).numpy()
+    res_buf = np.empty(nrhs, np.float64)
+    lib = tb.lib()
 
-    def step_device():
-        if tb.lib().taucs_b200_factor_numeric_device_async(F.h, d_vals.data_ptr()) != 0:
+    def numeric_device(prec):
+        F.set_precision(prec)
+        if lib.taucs_b200_factor_numeric_device(F.h, d_vals.data_ptr()) != 0:
+            raise RuntimeError("numeric failed: " + tb.last_error())
+
+    def step_mixed():
+        numeric_device(1)
+        its = lib.taucs_b200_solve_refine_device(F.h, nrhs, C.c_void_p(d_x.data_ptr()), C.c_void_p(d_b.data_ptr()),
+                                                  n, TOL, 10, res_buf)
+        if its < 0:
+            raise RuntimeError("refinement did not reach the target: " + tb.last_error())
+        return its
+
+    def step_fp64():
+        F.set_precision(0)
+        if lib.taucs_b200_factor_numeric_device_async(F.h, d_vals.data_ptr()) != 0:
             raise RuntimeError("numeric launch failed: " + tb.last_error())
-        if F.solve_device(1, d_x.data_ptr(), d_b.data_ptr(), n) != 0:
+        if F.solve_device(nrhs, d_x.data_ptr(), d_b.data_ptr(), n) != 0:
             raise RuntimeError("solve launch failed: " + tb.last_error())
 
-    def step_e2e():
+    def step_e2e_mixed():
+        F.set_precision(1)
         if F.numeric(Ph) != 0:
             raise RuntimeError("numeric failed: " + tb.last_error())
-        if tb.lib().taucs_supernodal_solve_llt(F.h, h_x, h_b) != 0:
+        its = lib.taucs_b200_solve_refine(F.h, None, nrhs, h_x, h_b, TOL, 10, res_buf)
+        if its < 0:
+            raise RuntimeError("refinement did not reach the target: " + tb.last_error())
+
+    def step_e2e_fp64():
+        F.set_precision(0)
+        if F.numeric(Ph) != 0:
+            raise RuntimeError("numeric failed: " + tb.last_error())
+        if lib.taucs_supernodal_solve_llt(F.h, h_x, h_b) != 0:
             raise RuntimeError("solve failed: " + tb.last_error())
+
+    step_main = step_mixed if mixed else step_fp64
+    step_e2e = step_e2e_mixed if mixed else step_e2e_fp64
 
     def barrier():
         torch.cuda.synchronize()
@@ -296,116 +421,112 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident timing
-    for _ in range(max(args.warmup, 3)):
-        step_device()
-    assert tb.lib().taucs_b200_factor_status(F.h) == 0, tb.last_error()
+    def timed(step, k):
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = None
+        for _ in range(k):
+            out = step()
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1)), out
+
+    def x_host():
+        torch.cuda.synchronize()
+        return d_x.cpu().numpy().reshape(nrhs, n).T
+
+    W = max(args.warmup, 3)
+    K = args.steps
+    # ---- the measured form, device-resident
+    for _ in range(W):
+        step_main()
     clocks = ClockSampler(local_rank)
-    barrier()
     clocks.start()
     tb.launch_count(reset=True)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step_device()
-    e1.record(stream)
-    barrier()
+    ms, its = timed(step_main, K)
     clk = clocks.stop()
-    launches = tb.launch_count(reset=True) // max(args.steps, 1)
-    ms = max_over_ranks(e0.elapsed_time(e1))
-    ok = tb.lib().taucs_b200_factor_status(F.h) == 0
-    x_dev = d_x.cpu().numpy()
-    res_dev = scaled_residual(P, x_dev, b)
+    launches = tb.launch_count(reset=True) // max(K, 1)
+    X = x_host()
+    res_main = max(scaled_residual(P, X[:, q], B[:, q]) for q in range(nrhs))
+    steps_main = its if mixed else None
+
+    # ---- the plain FP64 path on the same inputs (mixed80 only)
+    fp64 = None
+    if mixed:
+        for _ in range(W):
+            step_fp64()
+        ms64, _ = timed(step_fp64, K)
+        X64 = x_host()
+        res64 = max(scaled_residual(P, X64[:, q], B[:, q]) for q in range(nrhs))
+        fp64 = {"value": world * K / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64 / K,
+                "scaled_residual": res64, "speedup_of_fp32_refine": ms64 / ms,
+                "max_rel_diff_x": float(np.max(np.abs(X - X64)) / np.max(np.abs(X64)))}
 
     # ---- end-to-end through the C ABI with pinned host buffers
     for _ in range(2):
         step_e2e()
-    barrier()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
-        step_e2e()
-    f1.record(stream)
-    barrier()
-    ms_e2e = max_over_ranks(f0.elapsed_time(f1))
-    res_e2e = scaled_residual(P, h_x, b)
+    ms_e2e, _ = timed(step_e2e, K)
+    Xe = h_x.reshape(nrhs, n).T
+    res_e2e = max(scaled_residual(P, Xe[:, q], B[:, q]) for q in range(nrhs))
 
     # ---- roofline: CUDA events around every launch, separate profiled steps
-    tb.lib().taucs_b200_profile(1)
-    nprof = max(2, min(args.steps, 5))
+    lib.taucs_b200_profile(1)
+    nprof = max(2, min(K, 3))
     for _ in range(nprof):
-        step_device()
+        step_main()
     torch.cuda.synchronize()
-    import ctypes as C
-    kern = {}
-    rd = tb.lib().taucs_b200_profile_read
-    for name, kc in KC.items():
-        t, nl, fl, by = C.c_double(), C.c_long(), C.c_double(), C.c_double()
-        rd(kc, C.byref(t), C.byref(nl), C.byref(fl), C.byref(by))
-        if nl.value:
-            kern[name] = {"ms_per_step": t.value / nprof, "launches_per_step": nl.value // nprof,
-                          "gflop_per_step": fl.value / nprof / 1e9, "gb_per_step": by.value / nprof / 1e9}
-    tb.lib().taucs_b200_profile(0)
+    kern = read_profile(tb, nprof)
+    lib.taucs_b200_profile(0)
 
     peaks = measured_peaks()
-    fp64_peak = fp64_gemm_peak()
     hbm_peak = peaks.get("hbm_gbs")
-    dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])[0] if kern else None
-    roof = None
-    if dom:
-        d = kern[dom]
-        per_launch_ms = d["ms_per_step"] / max(d["launches_per_step"], 1)
-        if dom in TENSOR_KC:
-            ach = d["gflop_per_step"] / d["ms_per_step"]  # GFLOP/ms = TFLOP/s
-            roof = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
-                    "frac": ach / fp64_peak,
-                    "peak_source": "FP64: cuBLAS DGEMM 8192^3 measured in this run (of measured)",
-                    "algorithmic_per_launch": d["gflop_per_step"] / max(d["launches_per_step"], 1) * 1e9,
-                    "avg_launch_ms": per_launch_ms, "traffic": None}
-        else:
-            ach = d["gb_per_step"] / d["ms_per_step"] * 1e3
-            roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": ach / hbm_peak if hbm_peak else None,
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                    "algorithmic_per_launch": d["gb_per_step"] / max(d["launches_per_step"], 1) * 1e9,
-                    "avg_launch_ms": per_launch_ms, "traffic": None}
-    for v in kern.values():
-        if v["gflop_per_step"] > 0:
-            v["tflop_s"] = v["gflop_per_step"] / v["ms_per_step"]
-        if v["gb_per_step"] > 0:
-            v["gb_s"] = v["gb_per_step"] / v["ms_per_step"] * 1e3
+    if mixed:
+        tf32 = tf32_gemm_peak()
+        tensor_peak = tf32 / 3.0
+        tensor_src = (f"cuBLAS TF32 GEMM 8192^3 measured in this run ({tf32:.0f} TF/s) / 3: the TF32x3 "
+                      f"products do 3 tensor-core MMAs per FP32-accurate product (of measured)")
+    else:
+        tensor_peak = fp64_gemm_peak()
+        tensor_src = "FP64: cuBLAS DGEMM 8192^3 measured in this run (of measured)"
+    roof = roofline(kern, tensor_peak, tensor_src, hbm_peak)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(g, os.cpu_count() or 1)
+            nth = os.cpu_count() or 1
+            sec, desc, kind, cores = cpu_reference(args.workload, g, nth)
+            cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
         except Exception as exc:  # report, never hide
             cpu = {"error": repr(exc)}
 
-    steps = args.steps
+    h2d = 8 * nnz + 8 * n * nrhs
+    d2h = 8 * n * nrhs + (8 * nrhs if mixed else 4)
     out = {
-        "metric": METRIC, "value": world * steps / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
-        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"mesh3d {g}^3 7-point Laplacian (reference generator), AMD, "
-                               f"FP64 numeric factor + 1-RHS solve", "n": n, "nnz_lower": nnz,
+        "metric": METRIC_MIXED if mixed else METRIC_FP64, "value": world * K / (ms * 1e-3), "unit": UNIT,
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args.workload, g), "n": n, "nnz_lower": nnz, "nrhs": nrhs,
                    "flops": info.flops, "supernodes": info.n_live, "levels": info.n_levels,
-                   "max_front": info.max_front, "l_gb": info.l_bytes / 1e9, "u_arena_gb": info.u_bytes / 1e9,
-                   "l2_policy": "inputs larger than L2 (L and update arena > 4 GB touched per step)",
+                   "max_front": info.max_front, "l_gb_fp64": info.l_bytes / 1e9,
+                   "u_arena_gb_fp64": info.u_bytes / 1e9,
+                   "l2_policy": "inputs larger than L2 (several GB of L and update arena touched per step)",
                    "parallelism": f"replicas x{world}"},
         "clocks": clk,
-        "e2e": {"value": world * steps / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e / steps,
-                "h2d_bytes_per_step": 8 * nnz + 8 * n, "d2h_bytes_per_step": 8 * n + 4},
+        "e2e": {"value": world * K / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e / K,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": roof,
         "kernels": kern,
         "cpu_baseline": cpu,
-        "factor_tflop_s": info.flops / (ms / steps * 1e-3) / 1e12,
-        "scaled_residual": {"device": res_dev, "e2e": res_e2e},
-        "status_ok": bool(ok),
+        "scaled_residual": {"device": res_main, "e2e": res_e2e},
     }
+    if mixed:
+        out["refinement_steps"] = steps_main
+        out["fp64"] = fp64
+    else:
+        out["factor_tflop_s"] = info.flops / (ms / K * 1e-3) / 1e12
     if rank == 0:
         print(json.dumps(out))
     if dist is not None:

@@ -207,6 +207,11 @@ int taucs_b200_set_precision(void* L, int precision);
 int taucs_b200_solve_refine(void* L, taucs_ccs_matrix* A, int nrhs, double* X,
                             const double* B, double tol, int maxits, double* res_out);
 
+/* The same refinement on device vectors: d_X (written) and d_B are
+ * n x nrhs, column-major with leading dimension ld >= n, permuted order. */
+int taucs_b200_solve_refine_device(void* L, int nrhs, double* d_X, const double* d_B,
+                                   int ld, double tol, int maxits, double* res_out);
+
 /* Inspection of the symbolic factor, in the reference's own arrays (slots
  * 0..n_sn-1, virtual root n_sn) -- used by the parity tests. */
 typedef struct {

@@ -102,6 +102,7 @@ def lib():
         "taucs_b200_solve_many": (C.c_int, [vp, C.c_int, _f64p, _f64p]),
         "taucs_b200_set_precision": (C.c_int, [vp, C.c_int]),
         "taucs_b200_solve_refine": (C.c_int, [vp, pc, C.c_int, _f64p, _f64p, C.c_double, C.c_int, _f64p]),
+        "taucs_b200_solve_refine_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_int, _f64p]),
         "taucs_b200_factor_info": (C.c_int, [vp, C.POINTER(Info)]),
         "taucs_b200_export_symbolic": (C.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i64p, _i32p]),
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
@@ -318,6 +319,14 @@ class Factor:
         its = lib().taucs_b200_solve_refine(self.h, A.ptr, nrhs, xc, bc, tol, maxits, res)
         x = xc.T.copy()
         return (x[:, 0] if one else x), its, res
+
+    def solve_refine_device(self, nrhs, d_x, d_b, ld, tol=1e-12, maxits=10):
+        """Refinement on device vectors (column-major, leading dimension ld);
+        returns (steps, final scaled residuals)."""
+        res = np.empty(max(nrhs, 1), np.float64)
+        its = lib().taucs_b200_solve_refine_device(self.h, nrhs, C.c_void_p(d_x), C.c_void_p(d_b), ld, tol,
+                                                   maxits, res)
+        return its, res[:nrhs]
 
 
 def factor_mf(A, max_depth=0):

@@ -82,7 +82,64 @@ void devplan_free(DevPlan* D) {
   *D = DevPlan();
 }
 
+static bool graphs_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("TAUCS_B200_NO_GRAPHS");
+    return !(e && *e && strcmp(e, "0") != 0);
+  }();
+  return on;
+}
+
+void drop_graphs(Factor* F) {
+  for (auto& kv : F->graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  F->graphs.clear();
+}
+
+int run_graphed(Factor* F, const GraphKey& key, cudaStream_t st, const std::function<int(cudaStream_t)>& record) {
+  if (!graphs_enabled() || prof_enabled()) return record(st);
+  Factor::Graph& g = F->graphs[key];
+  if (!g.seen) {
+    g.seen = true;
+    return record(st);
+  }
+  if (!g.exec) {
+    if (!F->cap_stream && cudaStreamCreateWithFlags(&F->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      F->cap_stream = nullptr;
+      return record(st);
+    }
+    // recorded on a private stream (the legacy default stream cannot be
+    // captured); replays are ordered on st
+    cudaGraph_t graph = nullptr;
+    const long l0 = g_launches.load();
+    int rc = (int) cudaStreamBeginCapture(F->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (rc == 0) {
+      rc = record(F->cap_stream);
+      const cudaError_t ec = cudaStreamEndCapture(F->cap_stream, &graph);
+      if (rc == 0) rc = (int) ec;
+    }
+    const long nl = g_launches.load() - l0;
+    count_launch(-nl);   // recorded, not run
+    if (rc == 0 && graph) rc = (int) cudaGraphInstantiate(&g.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != 0 || !g.exec) {
+      g.exec = nullptr;
+      cudaGetLastError();
+      return record(st);
+    }
+    g.launches = nl;
+  }
+  count_launch(g.launches);
+  return (int) cudaGraphLaunch(g.exec, st);
+}
+
+void invalidate_numeric(Factor* F) {
+  F->has_numeric = false;
+  F->has_numeric32 = false;
+}
+
 void free_numeric(Factor* F) {
+  drop_graphs(F);
   cudaFree(F->dL); F->dL = nullptr;
   cudaFree(F->dU); F->dU = nullptr;
   cudaFree(F->dDinv); F->dDinv = nullptr;
@@ -95,6 +152,8 @@ void free_numeric(Factor* F) {
 
 static void free_device(Factor* F) {
   free_numeric(F);
+  if (F->cap_stream) cudaStreamDestroy(F->cap_stream);
+  F->cap_stream = nullptr;
   if (F->dev_ready) devplan_free(&F->dp);
   cudaFree(F->dA); F->dA = nullptr;
   cudaFree(F->dstatus); F->dstatus = nullptr;
@@ -205,7 +264,9 @@ int numeric_fp64_device(Factor* F, const double* d_vals, bool wait) {
     return -1;
   }
   F->dvals_cur = d_vals;
-  int e = launch_numeric_fp64(P, F->dp, d_vals, F->dL, F->dU, F->dDinv, F->dstatus, st);
+  int e = run_graphed(F, GraphKey{1, (uint64_t) d_vals, 0, 0, 0, 0}, st, [&](cudaStream_t s) {
+    return launch_numeric_fp64(P, F->dp, d_vals, F->dL, F->dU, F->dDinv, F->dstatus, s);
+  });
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   if (!cuda_ok(cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st), "status")) return -1;
   F->has_numeric = true;
@@ -225,7 +286,7 @@ int numeric_fp32_device(Factor* F, const double* d_vals);
 int numeric_device(Factor* F, const double* d_vals, bool wait) {
   if (F->precision == 1) {
     // FP32 fronts; a nonpositive FP32 pivot falls back to the FP64 factor
-    free_numeric(F);
+    invalidate_numeric(F);
     if (numeric_fp32_device(F, d_vals) == 0) return 0;
     tprintf("\t\tFP32 factorization failed; refactoring in FP64\n");
     return numeric_fp64_device(F, d_vals, true);
@@ -253,8 +314,11 @@ int solve_device(Factor* F, int nrhs, double* dX, const double* dB, int ld) {
   if (!F->has_numeric) { set_error("solve: the factor has no numeric part"); return -1; }
   cudaStream_t st = current_stream();
   if (!cuda_ok(cudaMemsetAsync(F->dstatus + 1, 0, sizeof(int), st), "solve status")) return -1;
-  int e = launch_solve_fp64(F->plan, F->dp, F->dL, F->dDinv, nrhs, dX, dB, ld, F->dW, F->dpart, F->dflags, &F->epoch,
-                            F->dstatus + 1, st);
+  int e = run_graphed(F, GraphKey{3, (uint64_t) nrhs, (uint64_t) dX, (uint64_t) dB, (uint64_t) ld, 0}, st,
+                      [&](cudaStream_t s) {
+                        return launch_solve_fp64(F->plan, F->dp, F->dL, F->dDinv, nrhs, dX, dB, ld, F->dW, F->dpart,
+                                                 F->dflags, &F->epoch, F->dstatus + 1, s);
+                      });
   return cuda_ok((cudaError_t) e, "solve launch") ? 0 : -1;
 }
 

@@ -1,6 +1,10 @@
 // The factor handle returned through the C ABI.
 #pragma once
 
+#include <array>
+#include <cstdint>
+#include <functional>
+#include <map>
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -57,12 +61,32 @@ struct Factor {
   unsigned long long* hnorm = nullptr;  // pinned readback
   bool refine_ready = false;
   const double* dvals_cur = nullptr;   // values of the last numeric factorization (device)
+
+  // recorded launch sequences (numeric factorization, solves, refinement
+  // steps), keyed by what they were recorded for; replayed as CUDA graphs
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    long launches = 0;    // kernel launches inside the graph
+    bool seen = false;    // the first run of a key is eager (one-time setup)
+  };
+  std::map<std::array<uint64_t, 6>, Graph> graphs;
+  cudaStream_t cap_stream = nullptr;
 };
+
+using GraphKey = std::array<uint64_t, 6>;
+// Enqueues record(stream) on st: the first time for a key eagerly, then
+// recorded once into a CUDA graph and replayed.  Eager whenever per-launch
+// profiling is on or TAUCS_B200_NO_GRAPHS is set.  Returns record's result
+// (0 or a cudaError_t).
+int run_graphed(Factor* F, const GraphKey& key, cudaStream_t st, const std::function<int(cudaStream_t)>& record);
+void drop_graphs(Factor* F);
 
 cudaStream_t current_stream();
 bool cuda_ok(cudaError_t e, const char* what);
 int ensure_device(Factor* F);
 void free_numeric(Factor* F);
+// marks the numeric factors stale without freeing their buffers
+void invalidate_numeric(Factor* F);
 int numeric_fp64_device(Factor* F, const double* d_vals, bool wait);
 
 }  // namespace tb

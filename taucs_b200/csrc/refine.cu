@@ -182,7 +182,9 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
     tprintf("\t\tscaling: nonpositive diagonal in column %d\n", *F->hstatus);
     return -1;
   }
-  int e = launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dstatus, st);
+  int e = run_graphed(F, GraphKey{2, (uint64_t) F->dA32, 0, 0, 0, 0}, st, [&](cudaStream_t s) {
+    return launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dstatus, s);
+  });
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (!cuda_ok(cudaStreamSynchronize(st), "numeric factorization (FP32)")) return -1;
@@ -207,18 +209,40 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     double* X = dX + (size_t) q0 * ld;
     const double* B = dB + (size_t) q0 * ld;
     std::vector<double> bnorm(nq, 0.0);
+    // r = b - A x and the inf-norms of r and x, read back to the host
+    auto residual = [&](cudaStream_t s) {
+      cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long) * 2 * SOLVE_NRHS, s);
+      k_residual<<<nblk(n, 256), 256, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, F->dR,
+                                              ld, nq, F->dnorm);
+      count_launch();
+      cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS, cudaMemcpyDeviceToHost, s);
+      return (int) cudaGetLastError();
+    };
+    // one correction step x += A~^-1 r, then the next residual
+    auto correction = [&](cudaStream_t s, bool u64) {
+      int e;
+      if (u64) {
+        e = launch_solve_fp64(P, F->dp, F->dL, F->dDinv, nq, F->dR, F->dR, ld, F->dW, F->dpart, F->dflags, &F->epoch,
+                              F->dstatus + 1, s);
+        k_update64<<<nblk(n, 256), 256, 0, s>>>(n, X, F->dR, ld, nq);
+      } else {
+        k_scale_down<<<nblk(n, 256), 256, 0, s>>>(n, F->dR, F->dscale, F->dV32, ld, nq);
+        e = launch_solve_fp32(P, F->dp, F->dL32, F->dDinv32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32,
+                              F->dflags, &F->epoch, F->dstatus + 1, s);
+        k_update32<<<nblk(n, 256), 256, 0, s>>>(n, X, F->dV32, F->dscale, ld, nq);
+      }
+      count_launch(2);
+      return e ? e : residual(s);
+    };
     // ||b||_inf per column, from a residual pass with X = 0
     cudaMemsetAsync(X, 0, sizeof(double) * ((size_t) ld * (nq - 1) + n), st);
+    if (run_graphed(F, GraphKey{6, (uint64_t) nq, (uint64_t) X, (uint64_t) B, (uint64_t) ld, 0}, st, residual))
+      return -1;
     bool use64 = !F->has_numeric32;
     double prev_worst = INFINITY;
     int slow = 0, steps = 0;
     bool done = false;
     for (int it = 0; !done; it++) {
-      cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long) * 2 * SOLVE_NRHS, st);
-      k_residual<<<nblk(n, 256), 256, 0, st>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, F->dR,
-                                               ld, nq, F->dnorm);
-      count_launch();
-      cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS, cudaMemcpyDeviceToHost, st);
       if (!cuda_ok(cudaStreamSynchronize(st), "refinement")) return -1;
       double worst = 0.0;
       for (int q = 0; q < nq; q++) {
@@ -248,18 +272,10 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
         }
       }
       prev_worst = worst;
-      // one correction step
-      if (use64) {
-        if (launch_solve_fp64(P, F->dp, F->dL, F->dDinv, nq, F->dR, F->dR, ld, F->dW, F->dpart, F->dflags, &F->epoch,
-                              F->dstatus + 1, st)) return -1;
-        k_update64<<<nblk(n, 256), 256, 0, st>>>(n, X, F->dR, ld, nq);
-      } else {
-        k_scale_down<<<nblk(n, 256), 256, 0, st>>>(n, F->dR, F->dscale, F->dV32, ld, nq);
-        if (launch_solve_fp32(P, F->dp, F->dL32, F->dDinv32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32, F->dflags, &F->epoch,
-                              F->dstatus + 1, st)) return -1;
-        k_update32<<<nblk(n, 256), 256, 0, st>>>(n, X, F->dV32, F->dscale, ld, nq);
-      }
-      count_launch(2);
+      const bool u64 = use64;
+      if (run_graphed(F, GraphKey{u64 ? 5u : 4u, (uint64_t) nq, (uint64_t) X, (uint64_t) B, (uint64_t) ld, 0}, st,
+                      [&](cudaStream_t s) { return correction(s, u64); }))
+        return -1;
       steps++;
     }
     if (total >= 0) total = std::max(total, steps);
@@ -267,31 +283,38 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
   return total;
 }
 
+// ||A||_inf of the factored values, computed on the device
+static int device_anorm(Factor* F, double* anorm) {
+  cudaStream_t st = current_stream();
+  cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long), st);
+  k_anorm<<<nblk(F->n, 256), 256, 0, st>>>(F->n, F->dcsr_ptr, F->dcsr_val, F->dvals_cur, F->dnorm);
+  count_launch();
+  cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  if (!cuda_ok(cudaStreamSynchronize(st), "norm")) return -1;
+  memcpy(anorm, &F->hnorm[0], 8);
+  return 0;
+}
+
+int solve_refine_device(Factor* F, int nrhs, double* dX, const double* dB, int ld, double tol, int maxits,
+                        double* res) {
+  if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
+  if (ensure_refine(F)) return -1;
+  double anorm = 0.0;
+  if (device_anorm(F, &anorm)) return -1;
+  return refine_device(F, nrhs, dX, dB, ld, tol, maxits, anorm, res);
+}
+
 int solve_refine_host(Factor* F, taucs_ccs_matrix* A, int nrhs, double* X, const double* B, double tol, int maxits,
                       double* res) {
   if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
   if (ensure_refine(F)) return -1;
   const int n = F->n;
+  // A, when given, has the factored pattern and values; the norm comes from
+  // the device copy
+  (void) A;
   double anorm = 0.0;
-  if (A) {
-    std::vector<double> rs(n, 0.0);
-    for (int j = 0; j < n; j++)
-      for (int ip = A->colptr[j]; ip < A->colptr[j + 1]; ip++) {
-        const int i = A->rowind[ip];
-        rs[i] += fabs(A->values.d[ip]);
-        if (i != j) rs[j] += fabs(A->values.d[ip]);
-      }
-    for (double v : rs) anorm = std::max(anorm, v);
-  }
+  if (device_anorm(F, &anorm)) return -1;
   cudaStream_t st = current_stream();
-  if (!A) {
-    cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long), st);
-    k_anorm<<<nblk(n, 256), 256, 0, st>>>(n, F->dcsr_ptr, F->dcsr_val, F->dvals_cur, F->dnorm);
-    count_launch();
-    cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if (!cuda_ok(cudaStreamSynchronize(st), "norm")) return -1;
-    memcpy(&anorm, &F->hnorm[0], 8);
-  }
   int worst_steps = 0;
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
@@ -315,6 +338,15 @@ extern "C" int taucs_b200_set_precision(void* L, int precision) {
   if (!L || (precision != 0 && precision != 1)) return -1;
   ((Factor*) L)->precision = precision;
   return 0;
+}
+
+extern "C" int taucs_b200_solve_refine_device(void* L, int nrhs, double* d_X, const double* d_B, int ld, double tol,
+                                              int maxits, double* res_out) {
+  if (!L || nrhs < 0 || (nrhs > 0 && (!d_X || !d_B))) return -1;
+  if (nrhs == 0) return 0;
+  Factor* F = (Factor*) L;
+  if (ld < F->n) { set_error("taucs_b200_solve_refine_device: ld < n"); return -1; }
+  return solve_refine_device(F, nrhs, d_X, d_B, ld, tol, maxits < 0 ? 0 : maxits, res_out);
 }
 
 extern "C" int taucs_b200_solve_refine(void* L, taucs_ccs_matrix* A, int nrhs, double* X, const double* B,

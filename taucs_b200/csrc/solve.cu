@@ -631,11 +631,15 @@ template <typename T>
 static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Dinv, int nrhs, T* X, const T* B, int ld, T* W,
                         T* part, int* flags, int* epoch, int* status, cudaStream_t st) {
   solve_attrs<T>();
+  // the handshake flags restart from zero on every call, so the epochs of a
+  // call are always 1, 2, ... and a recorded launch sequence stays valid
+  cudaMemsetAsync(flags, 0, sizeof(int) * (size_t) P.n_blk, st);
+  int ep = 0;
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
     const T* Bq = B + (size_t) q0 * ld;
     T* Xq = X + (size_t) q0 * ld;
-    const int ef = ++*epoch;
+    const int ef = ++ep;
     for (int h = 0; h < P.n_levels; h++) {
       const LevelPlan& LP = P.levels[h];
       double by = 0.0;
@@ -663,7 +667,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       }
       prof_end(KC_SOLVE_FWD, st, 0.0, by);
     }
-    const int eb = ++*epoch;
+    const int eb = ++ep;
     for (int h = P.n_levels - 1; h >= 0; h--) {
       const LevelPlan& LP = P.levels[h];
       double by = 0.0;
@@ -703,6 +707,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       prof_end(KC_SOLVE_BWD, st, 0.0, by);
     }
   }
+  (void) epoch;
   return (int) cudaGetLastError();
 }
 
