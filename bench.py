@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--workload", default="mixed80", choices=["mixed80", "fp64-64"])
     ap.add_argument("--grid", type=int, default=None, help="grid side (default 80 / 64 per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="duration of the Poisson request stream at 2000 req/s (60 = the full configuration)")
     return ap.parse_args()
 
 
@@ -297,6 +300,162 @@ def workload_name(workload, g):
     return f"mesh3d {g}^3 7-point Laplacian (reference generator), AMD, FP64 numeric factor + 1-RHS solve"
 
 
+# ---------------------------------------------------------------- serving
+
+class ServeStream:
+    """Seeded request stream of the serving configuration: Poisson arrivals;
+    70% 2D 5-point lognormal grids with n ~ U[1000, 20000] (side = floor(sqrt n)),
+    25% 3D 7-point grids with side ~ U{16..40}, 5% 3D 64^3; sigma = 1; of all
+    requests 50% bring new coefficients on a pattern already seen, 20% new
+    right-hand sides (1-32 columns) for a matrix already seen, the rest a
+    freshly drawn size with new coefficients.  The 64^3 requests take their
+    coefficients from 8 generated sets, each scaled by a distinct factor per
+    request (a new SPD matrix every time, without 16 MB of generation per
+    request).  Right-hand sides are views of one seeded U(-1,1) pool."""
+
+    def __init__(self, tb, seed=0):
+        self.tb = tb
+        self.rng = np.random.default_rng(seed)
+        self.base = {}          # pattern -> Matrix (colptr/rowind shared by all its requests)
+        self.big_sets = []
+        self.seen_pat, self.seen_mat = [], []
+        self.pool = self.rng.uniform(-1, 1, 64 ** 3 * 32 + 1)
+
+    def _pattern(self):
+        v = self.rng.random()
+        if v < 0.70:
+            s = int(np.sqrt(self.rng.integers(1000, 20001)))
+            return (s, s, 0)
+        if v < 0.95:
+            s = int(self.rng.integers(16, 41))
+            return (s, s, s)
+        return (64, 64, 64)
+
+    def _new_matrix(self, pk):
+        tb = self.tb
+        if pk == (64, 64, 64):
+            if not self.big_sets:
+                self.big_sets = [tb.lognormal(64, 64, 64, 1.0, (1, 1, 1), 1000 + i) for i in range(8)]
+            M = self.big_sets[int(self.rng.integers(8))]
+            c = 1.0 + float(self.rng.random())
+            return tb.Matrix(M.n, M.colptr, M.rowind, M.values * c)
+        return tb.lognormal(pk[0], pk[1], pk[2], 1.0, (1, 1, 1), int(self.rng.integers(1 << 30)))
+
+    def draw(self, n_req):
+        out = []
+        for _ in range(n_req):
+            u = self.rng.random()
+            nrhs = 1
+            if u < 0.20 and self.seen_mat:
+                A, pk = self.seen_mat[int(self.rng.integers(len(self.seen_mat)))]
+                nrhs = int(self.rng.integers(1, 33))
+            elif u < 0.70 and self.seen_pat:
+                pk = self.seen_pat[int(self.rng.integers(len(self.seen_pat)))]
+                A = self._new_matrix(pk)
+            else:
+                pk = self._pattern()
+                if pk not in self.seen_pat:
+                    self.seen_pat.append(pk)
+                A = self._new_matrix(pk)
+            self.seen_mat.append((A, pk))
+            off = int(self.rng.integers(0, len(self.pool) - A.n * nrhs))
+            B = self.pool[off:off + A.n * nrhs].reshape(nrhs, A.n).T     # column-major view
+            out.append((A, B, pk))
+        return out
+
+
+def serve_stream(tb, S, reqs, rate, rng):
+    """Submits reqs at Poisson arrival times (rate req/s) and waits for all;
+    returns per-request results, the span first submit -> last completion,
+    and the client's worst lag behind the arrival schedule."""
+    gaps = rng.exponential(1.0 / rate, len(reqs))
+    t_arr = np.cumsum(gaps)
+    ids, lag = [], 0.0
+    t0 = time.perf_counter()
+    for (A, B, _), ta in zip(reqs, t_arr):
+        now = time.perf_counter() - t0
+        if ta > now:
+            time.sleep(ta - now)
+        else:
+            lag = max(lag, now - ta)
+        ids.append(S.submit(A, B, TOL))
+    res = [S.wait(i) for i in ids]
+    span = time.perf_counter() - t0
+    return res, span, lag
+
+
+def fp64_one_at_a_time(tb, reqs):
+    """The same requests solved one after another through the FP64 C API
+    (patterns analysed beforehand, as the server caches them): permute,
+    factor, solve, un-permute per request."""
+    cache = {}
+    for A, _, pk in reqs:
+        if pk not in cache:
+            p, ip = tb.order(A, "amd")
+            F = tb.factor_symbolic(A.permute(p, ip))
+            F.set_precision(0)
+            cache[pk] = (p, ip, F)
+    t0 = time.perf_counter()
+    for A, B, pk in reqs:
+        p, ip, F = cache[pk]
+        if F.numeric(A.permute(p, ip)) != 0:
+            raise RuntimeError("FP64 factor failed")
+        X = np.empty_like(B)
+        X[p, :] = F.solve(np.ascontiguousarray(B[p, :]))
+    dt = time.perf_counter() - t0
+    for _, _, F in cache.values():
+        F.free()
+    return len(reqs) / dt
+
+
+def run_serving(tb, seconds=2.0, rate=2000.0, sustain_rate=250.0, sustain_seconds=4.0, workers=16,
+                budget=120e9, fp64_sample=200):
+    rng = np.random.default_rng(1)
+    gen = ServeStream(tb, seed=0)
+    n_main = int(seconds * rate)
+    n_sus = int(sustain_seconds * sustain_rate)
+    main = gen.draw(n_main)
+    sus = gen.draw(n_sus)
+    S = tb.Server(workers=workers, budget_bytes=budget)
+    # warm-up, untimed: analyse every pattern of the streams once
+    seen = {}
+    for A, _, pk in main + sus:
+        if pk not in seen:
+            seen[pk] = A
+    for A in seen.values():
+        S.wait(S.submit(A, np.ones(A.n), TOL))
+    st0 = S.stats()
+    res, span, lag = serve_stream(tb, S, main, rate, rng)
+    st1 = S.stats()
+    res_s, span_s, lag_s = serve_stream(tb, S, sus, sustain_rate, rng)
+    S.close()
+    lat = np.array([r[2] for r in res]) * 1e3
+    lat_s = np.array([r[2] for r in res_s]) * 1e3
+    cols = sum(B.shape[1] for _, B, _ in main)
+    fails = sum(1 for r in res + res_s if r[0] != 0)
+    worst = max(r[4] for r in res + res_s)
+    served = len(main) / span
+    fp64 = fp64_one_at_a_time(tb, main[:fp64_sample])
+    return {
+        "workload": (f"Poisson {rate:g} req/s for {seconds:g} s ({n_main} requests): 70% 2D n in [1k,20k], "
+                     f"25% 3D side 16-40, 5% 64^3, sigma=1; 50% new coefficients on a seen pattern, 20% new RHS "
+                     f"(1-32) on a seen matrix; FP32 fronts + FP64 refinement to {TOL:g}"),
+        "workers": workers, "budget_gb": budget / 1e9, "patterns": len(seen),
+        "requests_per_s": served, "rhs_columns_per_s": cols / span,
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "note": "offered rate above capacity: latencies include queueing of the backlog",
+        "client_max_lag_ms": lag * 1e3,
+        "sustained": {"rate": sustain_rate, "requests": n_sus, "requests_per_s": n_sus / span_s,
+                      "p50_ms": float(np.percentile(lat_s, 50)), "p99_ms": float(np.percentile(lat_s, 99)),
+                      "client_max_lag_ms": lag_s * 1e3},
+        "fp64_one_at_a_time_requests_per_s": fp64, "speedup_vs_fp64_one_at_a_time": served / fp64,
+        "factorizations": st1["factorizations"] - st0["factorizations"],
+        "resident_solves": st1["resident_solves"] - st0["resident_solves"],
+        "evictions": st1["evictions"], "failed": fails, "worst_scaled_residual": worst,
+    }
+
+
+
 # ---------------------------------------------------------------- GPU
 
 def read_profile(tb, nsteps):
@@ -501,6 +660,15 @@ def run_ours(args):
         except Exception as exc:  # report, never hide
             cpu = {"error": repr(exc)}
 
+    serving = None
+    if mixed and world == 1 and not args.no_serving:
+        F.free()
+        torch.cuda.empty_cache()
+        try:
+            serving = run_serving(tb, seconds=args.serve_seconds)
+        except Exception as exc:  # report, never hide
+            serving = {"error": repr(exc)}
+
     h2d = 8 * nnz + 8 * n * nrhs
     d2h = 8 * n * nrhs + (8 * nrhs if mixed else 4)
     out = {
@@ -525,6 +693,7 @@ def run_ours(args):
     if mixed:
         out["refinement_steps"] = steps_main
         out["fp64"] = fp64
+        out["serving"] = serving
     else:
         out["factor_tflop_s"] = info.flops / (ms / K * 1e-3) / 1e12
     if rank == 0:

@@ -275,6 +275,50 @@ long taucs_b200_launch_count(int reset);
 /* last CUDA or internal error message of the calling thread ("" if none) */
 const char* taucs_b200_last_error(void);
 
+/* ---- Request server (no counterpart in the reference, which solves one
+ * system per taucs_linsolve call on the calling thread,
+ * src/taucs_linsolve.c:433-583).  A server owns `workers` threads, each with
+ * its own CUDA stream on the device that is current at creation.  Submitted
+ * requests are taken from one FIFO queue by the first free worker, so the
+ * work of several requests overlaps on the GPU.  Per sparsity pattern the
+ * AMD ordering and the symbolic factor are computed once; factor instances
+ * of a pattern are reused and keep their last numeric factor, so a request
+ * for a matrix already factored only solves.  Each system is factored with
+ * FP32 fronts and refined in FP64 to the request's scaled residual `tol`.
+ * Device memory held by factor instances stays under hbm_budget_bytes:
+ * idle instances are evicted least recently used first, and a request whose
+ * instance does not fit waits until running requests finish. */
+typedef struct {
+  int    patterns;          /* sparsity patterns analysed             */
+  int    instances;         /* factor instances held on the device    */
+  double bytes_in_use;      /* predicted device bytes of the instances */
+  double budget_bytes;
+  long   factorizations;    /* requests that ran a numeric factorization */
+  long   resident_solves;   /* requests solved on a resident factor    */
+  long   evictions;
+  long   waits_for_memory;  /* requests that waited for device memory  */
+  long   failed;
+  long   queued;            /* requests not yet taken by a worker      */
+} taucs_b200_server_info;
+
+void* taucs_b200_server_create(int workers, double hbm_budget_bytes);
+/* A: unpermuted lower triangle (TAUCS_DOUBLE | TAUCS_SYMMETRIC | TAUCS_LOWER);
+ * B, X: n x nrhs column-major host arrays.  A's arrays, B and X must stay
+ * valid until taucs_b200_server_wait returns for the request.  Returns the
+ * request id (> 0) or -1. */
+long taucs_b200_server_submit(void* server, const taucs_ccs_matrix* A, int nrhs, const double* B,
+                              double* X, double tol);
+/* Blocks until the request is done: 0 on success, -1 on failure, -2 for an
+ * unknown id.  latency_s = completion time - submission time; steps =
+ * refinement steps; residual = worst scaled residual of the request's
+ * columns; factored = 1 if a numeric factorization ran, 0 if it was solved on
+ * a resident factor.  Any output pointer may be NULL. */
+int taucs_b200_server_wait(void* server, long id, double* latency_s, int* steps, double* residual,
+                           int* factored);
+int taucs_b200_server_stats(void* server, taucs_b200_server_info* out);
+/* waits for the workers to finish the queued requests, then frees everything */
+void taucs_b200_server_destroy(void* server);
+
 #ifdef __cplusplus
 }
 #endif

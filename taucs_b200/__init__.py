@@ -52,6 +52,12 @@ class Info(C.Structure):
                 ("solve_bytes", C.c_double), ("max_front", C.c_int), ("max_sn_size", C.c_int)]
 
 
+class ServerInfo(C.Structure):
+    _fields_ = [("patterns", C.c_int), ("instances", C.c_int), ("bytes_in_use", C.c_double),
+                ("budget_bytes", C.c_double), ("factorizations", C.c_long), ("resident_solves", C.c_long),
+                ("evictions", C.c_long), ("waits_for_memory", C.c_long), ("failed", C.c_long), ("queued", C.c_long)]
+
+
 def build(quiet=True):
     """Compiles libtaucs_b200.so in place for sm_100a."""
     kw = dict(stdout=subprocess.DEVNULL, stderr=subprocess.STDOUT) if quiet else {}
@@ -103,6 +109,12 @@ def lib():
         "taucs_b200_set_precision": (C.c_int, [vp, C.c_int]),
         "taucs_b200_solve_refine": (C.c_int, [vp, pc, C.c_int, _f64p, _f64p, C.c_double, C.c_int, _f64p]),
         "taucs_b200_solve_refine_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_int, _f64p]),
+        "taucs_b200_server_create": (vp, [C.c_int, C.c_double]),
+        "taucs_b200_server_submit": (C.c_long, [vp, pc, C.c_int, vp, vp, C.c_double]),
+        "taucs_b200_server_wait": (C.c_int, [vp, C.c_long, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+        "taucs_b200_server_stats": (C.c_int, [vp, C.POINTER(ServerInfo)]),
+        "taucs_b200_server_destroy": (None, [vp]),
         "taucs_b200_factor_info": (C.c_int, [vp, C.POINTER(Info)]),
         "taucs_b200_export_symbolic": (C.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i64p, _i32p]),
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
@@ -344,6 +356,55 @@ def etree(A):
     par = np.empty(A.n, np.int32)
     lib().taucs_b200_etree(A.ptr, par)
     return par
+
+
+class Server:
+    """Request server (taucs_b200_server_*): worker threads with their own CUDA
+    streams take factor/solve requests from one queue, so requests overlap on
+    the GPU; patterns, orderings and factors are cached; device memory held by
+    factor instances stays under `budget_bytes`."""
+
+    def __init__(self, workers=8, budget_bytes=64e9):
+        self.h = lib().taucs_b200_server_create(int(workers), float(budget_bytes))
+        if not self.h:
+            raise RuntimeError("server_create failed: " + last_error())
+        self._live = {}
+
+    def submit(self, A, B, tol=1e-12):
+        """A: unpermuted lower-triangle Matrix; B: (n,) or (n, nrhs).  Returns a
+        request id; the solution is returned by wait()."""
+        B = np.asarray(B, dtype=np.float64)
+        Bc = np.ascontiguousarray((B.reshape(-1, 1) if B.ndim == 1 else B).T)   # nrhs x n = column-major n x nrhs
+        Xc = np.empty_like(Bc)
+        rid = lib().taucs_b200_server_submit(self.h, A.ptr, Bc.shape[0], Bc.ctypes.data, Xc.ctypes.data, float(tol))
+        if rid <= 0:
+            raise RuntimeError("server_submit failed")
+        self._live[rid] = (A, Bc, Xc, B.ndim == 1)
+        return rid
+
+    def wait(self, rid):
+        """(status, X, latency_s, refinement steps, worst scaled residual, factored)"""
+        lat, st, res, fac = C.c_double(), C.c_int(), C.c_double(), C.c_int()
+        rc = lib().taucs_b200_server_wait(self.h, rid, C.byref(lat), C.byref(st), C.byref(res), C.byref(fac))
+        A, Bc, Xc, one = self._live.pop(rid)
+        X = Xc.T.copy()
+        return rc, (X[:, 0] if one else X), lat.value, st.value, res.value, bool(fac.value)
+
+    def stats(self):
+        inf = ServerInfo()
+        lib().taucs_b200_server_stats(self.h, C.byref(inf))
+        return {k: getattr(inf, k) for k, _ in ServerInfo._fields_}
+
+    def close(self):
+        if self.h:
+            lib().taucs_b200_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def set_stream(stream_handle):
