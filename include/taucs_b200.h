@@ -275,6 +275,35 @@ long taucs_b200_launch_count(int reset);
 /* last CUDA or internal error message of the calling thread ("" if none) */
 const char* taucs_b200_last_error(void);
 
+/* ---- Batches (no counterpart in the reference, which factors one system
+ * per call, src/taucs_sn_llt.c:2894-3006).  `count` independent SPD systems
+ * (unpermuted lower triangles) are ordered by AMD one by one and analysed
+ * as the diagonal blocks of one matrix, so every system keeps its own
+ * supernodes and one level-scheduled launch sequence factors (and one
+ * solves) all of them.  The handle is a factor handle: taucs_b200_set_precision,
+ * taucs_b200_factor_numeric_device (values in the combined order of
+ * taucs_b200_batch_values), taucs_b200_solve_device and
+ * taucs_b200_solve_refine_device (right-hand sides in the combined order of
+ * taucs_b200_batch_rhs; res_out then holds one scaled residual per system
+ * and right-hand side, system-major) and taucs_supernodal_factor_free apply;
+ * refinement meets the target for every system on its own. */
+void* taucs_b200_batch_analyze(int count, taucs_ccs_matrix* const* A);
+/* the systems' values (same patterns) gathered into the combined order */
+int taucs_b200_batch_values(void* L, taucs_ccs_matrix* const* A, double* combined);
+/* right-hand sides of the systems (B[s] of length n_s) into the combined
+ * order, and combined solutions back to the systems' own order */
+int taucs_b200_batch_rhs(void* L, const double* const* B, double* combined);
+int taucs_b200_batch_split(void* L, const double* combined, double* const* X);
+/* numeric factorization of all systems from host values, in the precision
+ * set by taucs_b200_set_precision */
+int taucs_b200_batch_factor(void* L, taucs_ccs_matrix* const* A);
+/* one right-hand side per system, host arrays; every system is refined to
+ * scaled residual <= tol (res: one value per system, may be NULL); returns
+ * the refinement steps, -1 on failure */
+int taucs_b200_batch_solve(void* L, double* const* X, const double* const* B, double tol, int maxits,
+                           double* res);
+int taucs_b200_batch_info(void* L, int* count, int* rows, long* nnz);
+
 /* ---- Request server (no counterpart in the reference, which solves one
  * system per taucs_linsolve call on the calling thread,
  * src/taucs_linsolve.c:433-583).  A server owns `workers` threads, each with

@@ -109,6 +109,14 @@ def lib():
         "taucs_b200_set_precision": (C.c_int, [vp, C.c_int]),
         "taucs_b200_solve_refine": (C.c_int, [vp, pc, C.c_int, _f64p, _f64p, C.c_double, C.c_int, _f64p]),
         "taucs_b200_solve_refine_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_int, _f64p]),
+        "taucs_b200_batch_analyze": (vp, [C.c_int, C.POINTER(pc)]),
+        "taucs_b200_batch_values": (C.c_int, [vp, C.POINTER(pc), _f64p]),
+        "taucs_b200_batch_rhs": (C.c_int, [vp, C.POINTER(C.c_void_p), _f64p]),
+        "taucs_b200_batch_split": (C.c_int, [vp, _f64p, C.POINTER(C.c_void_p)]),
+        "taucs_b200_batch_factor": (C.c_int, [vp, C.POINTER(pc)]),
+        "taucs_b200_batch_solve": (C.c_int, [vp, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_double,
+                                             C.c_int, _f64p]),
+        "taucs_b200_batch_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_long)]),
         "taucs_b200_server_create": (vp, [C.c_int, C.c_double]),
         "taucs_b200_server_submit": (C.c_long, [vp, pc, C.c_int, vp, vp, C.c_double]),
         "taucs_b200_server_wait": (C.c_int, [vp, C.c_long, C.POINTER(C.c_double), C.POINTER(C.c_int),
@@ -335,10 +343,11 @@ class Factor:
     def solve_refine_device(self, nrhs, d_x, d_b, ld, tol=1e-12, maxits=10):
         """Refinement on device vectors (column-major, leading dimension ld);
         returns (steps, final scaled residuals)."""
-        res = np.empty(max(nrhs, 1), np.float64)
+        nseg = getattr(self, "count", 1)          # batches: one residual per system and column
+        res = np.empty(max(nrhs, 1) * nseg, np.float64)
         its = lib().taucs_b200_solve_refine_device(self.h, nrhs, C.c_void_p(d_x), C.c_void_p(d_b), ld, tol,
                                                    maxits, res)
-        return its, res[:nrhs]
+        return its, res[:nrhs * nseg]
 
 
 def factor_mf(A, max_depth=0):
@@ -356,6 +365,57 @@ def etree(A):
     par = np.empty(A.n, np.int32)
     lib().taucs_b200_etree(A.ptr, par)
     return par
+
+
+class Batch(Factor):
+    """Many independent SPD systems (unpermuted lower triangles) analysed,
+    factored and solved as one (taucs_b200_batch_*).  Inherits the factor
+    methods (set_precision, numeric_device, solve_device,
+    solve_refine_device) for device-resident use in the combined order."""
+
+    def __init__(self, systems):
+        self.systems = list(systems)
+        arr = (C.POINTER(CCSStruct) * len(self.systems))(*[C.pointer(A.s) for A in self.systems])
+        h = lib().taucs_b200_batch_analyze(len(self.systems), arr)
+        if not h:
+            raise RuntimeError("batch_analyze failed: " + last_error())
+        self.h = C.c_void_p(h)
+        cnt, rows, nnz = C.c_int(), C.c_int(), C.c_long()
+        lib().taucs_b200_batch_info(self.h, C.byref(cnt), C.byref(rows), C.byref(nnz))
+        self.count, self.n, self.nnz = cnt.value, rows.value, nnz.value
+
+    def _ptrs(self, systems):
+        return (C.POINTER(CCSStruct) * len(systems))(*[C.pointer(A.s) for A in systems])
+
+    def combined_values(self, systems=None):
+        v = np.empty(self.nnz, np.float64)
+        if lib().taucs_b200_batch_values(self.h, self._ptrs(systems or self.systems), v) != 0:
+            raise RuntimeError(last_error())
+        return v
+
+    def combined_rhs(self, bs):
+        bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+        v = np.empty(self.n, np.float64)
+        lib().taucs_b200_batch_rhs(self.h, (C.c_void_p * len(bs))(*[b.ctypes.data for b in bs]), v)
+        return v
+
+    def split(self, combined):
+        xs = [np.empty(A.n, np.float64) for A in self.systems]
+        lib().taucs_b200_batch_split(self.h, np.ascontiguousarray(combined, dtype=np.float64),
+                                     (C.c_void_p * len(xs))(*[x.ctypes.data for x in xs]))
+        return xs
+
+    def factor(self, systems=None):
+        return lib().taucs_b200_batch_factor(self.h, self._ptrs(systems or self.systems))
+
+    def solve_all(self, bs, tol=1e-12, maxits=10):
+        """(steps, [x_s], per-system scaled residuals)"""
+        bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+        xs = [np.empty_like(b) for b in bs]
+        res = np.empty(len(bs), np.float64)
+        steps = lib().taucs_b200_batch_solve(self.h, (C.c_void_p * len(xs))(*[x.ctypes.data for x in xs]),
+                                             (C.c_void_p * len(bs))(*[b.ctypes.data for b in bs]), tol, maxits, res)
+        return steps, xs, res
 
 
 class Server:

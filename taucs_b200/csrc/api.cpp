@@ -173,6 +173,7 @@ static void free_device(Factor* F) {
   cudaFree(F->dcsr_col); F->dcsr_col = nullptr;
   cudaFree(F->dcsr_val); F->dcsr_val = nullptr;
   cudaFree(F->dR); F->dR = nullptr;
+  cudaFree(F->dseg); F->dseg = nullptr;
   cudaFree(F->dXr); F->dXr = nullptr;
   cudaFree(F->dBr); F->dBr = nullptr;
   cudaFree(F->dnorm); F->dnorm = nullptr;

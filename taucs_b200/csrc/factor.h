@@ -61,6 +61,19 @@ struct Factor {
   unsigned long long* hnorm = nullptr;  // pinned readback
   bool refine_ready = false;
   const double* dvals_cur = nullptr;   // values of the last numeric factorization (device)
+  // independent systems held in one factor (a batch): row ranges seg_ptr[s]
+  // .. seg_ptr[s+1]; refinement measures every segment's scaled residual on
+  // its own.  Empty: one segment (the whole matrix).
+  std::vector<int> seg_ptr;
+  int* dseg = nullptr;                 // row -> segment (batches only)
+  int nseg() const { return seg_ptr.empty() ? 1 : (int) seg_ptr.size() - 1; }
+  // batch of systems: combined value k comes from value vmap[k] of system
+  // s (nnz_off[s] <= k < nnz_off[s+1]); combined row seg_ptr[s] + i is row
+  // perm[seg_ptr[s] + i] of system s
+  struct BatchMap {
+    std::vector<int64_t> nnz_off;
+    std::vector<int> perm, vmap;
+  } batch;
 
   // recorded launch sequences (numeric factorization, solves, refinement
   // steps), keyed by what they were recorded for; replayed as CUDA graphs

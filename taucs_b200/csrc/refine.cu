@@ -51,13 +51,27 @@ __device__ __forceinline__ void max_abs(unsigned long long* slot, double v) {
   atomicMax(slot, (unsigned long long) __double_as_longlong(fabs(v)));
 }
 
-// R = B - A X (FP64), inf-norms of R and X per column
+// warp-level max into a segment's slot: one atomic per warp when the warp's
+// rows lie in one segment, one per row otherwise
+__device__ __forceinline__ void seg_max(unsigned long long* slots, int sg, int stride, double v) {
+  const int lane = threadIdx.x & 31;
+  const int sg0 = __shfl_sync(0xffffffffu, sg, 0);
+  if (__all_sync(0xffffffffu, sg == sg0)) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) max_abs(slots + (size_t) sg0 * stride, v);
+  } else {
+    max_abs(slots + (size_t) sg * stride, v);
+  }
+}
+
+// R = B - A X (FP64); inf-norms of R and X per column and segment:
+// norms[(s * SOLVE_NRHS + q) * 2] (r) and [.. + 1] (x); seg == NULL: one segment
 __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                            const int* __restrict__ vi, const double* __restrict__ vals,
                            const double* __restrict__ X, const double* __restrict__ B, double* __restrict__ R,
-                           int ld, int nrhs, unsigned long long* norms) {
+                           int ld, int nrhs, const int* __restrict__ seg, unsigned long long* norms) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
+  const int sg = (seg && i < n) ? seg[i] : 0;
   for (int q = 0; q < nrhs; q++) {
     double r = 0.0, x = 0.0;
     if (i < n) {
@@ -67,14 +81,8 @@ __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restr
       r = fabs(acc);
       x = fabs(X[i + (size_t) q * ld]);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
-      x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-    }
-    if (lane == 0) {
-      max_abs(norms + q, r);
-      max_abs(norms + SOLVE_NRHS + q, x);
-    }
+    seg_max(norms + 2 * q, sg, 2 * SOLVE_NRHS, r);
+    seg_max(norms + 2 * q + 1, sg, 2 * SOLVE_NRHS, x);
   }
 }
 
@@ -101,19 +109,25 @@ __global__ void k_update64(int n, double* __restrict__ X, const double* __restri
 __global__ void k_init_status2(int* s) { *s = INT_MAX; }
 
 // ||A||_inf of the full symmetric matrix from the CSR of both triangles
+// ||A||_inf per segment: out[s]
 __global__ void k_anorm(int n, const int* __restrict__ rp, const int* __restrict__ vi, const double* __restrict__ vals,
-                        unsigned long long* out) {
+                        const int* __restrict__ seg, unsigned long long* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sg = (seg && i < n) ? seg[i] : 0;
   double a = 0.0;
   if (i < n)
     for (int e = rp[i]; e < rp[i + 1]; e++) a += fabs(vals[vi[e]]);
-  for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
-  if ((threadIdx.x & 31) == 0) max_abs(out, a);
+  seg_max(out, sg, 1, a);
 }
 
 inline int nblk(long n, int b) { return (int) ((n + b - 1) / b); }
 
 }  // namespace
+
+// norm slots: 2 x SOLVE_NRHS per segment
+static size_t norm_bytes(const Factor* F) {
+  return sizeof(unsigned long long) * 2 * SOLVE_NRHS * (size_t) F->nseg();
+}
 
 // pattern-derived arrays for scaling and the FP64 residual
 static int ensure_refine(Factor* F) {
@@ -145,6 +159,12 @@ static int ensure_refine(Factor* F) {
            cuda_ok(cudaMemcpyAsync(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st), "copy");
   };
   const size_t nv = (size_t) n * SOLVE_NRHS;
+  if (!F->seg_ptr.empty()) {
+    std::vector<int> seg(std::max(n, 1));
+    for (int sg = 0; sg < F->nseg(); sg++)
+      for (int i = F->seg_ptr[sg]; i < F->seg_ptr[sg + 1]; i++) seg[i] = sg;
+    if (!up(&F->dseg, seg)) return -1;
+  }
   bool ok = up(&F->dcolidx, colidx) && up(&F->ddiagpos, diagpos) && up(&F->dcsr_ptr, cnt) && up(&F->dcsr_col, ccol) &&
             up(&F->dcsr_val, cval) &&
             cuda_ok(cudaMalloc(&F->dscale, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
@@ -152,8 +172,8 @@ static int ensure_refine(Factor* F) {
             cuda_ok(cudaMalloc(&F->dXr, sizeof(double) * nv), "cudaMalloc") &&
             cuda_ok(cudaMalloc(&F->dBr, sizeof(double) * nv), "cudaMalloc") &&
             cuda_ok(cudaMalloc(&F->dV32, sizeof(float) * nv), "cudaMalloc") &&
-            cuda_ok(cudaMalloc(&F->dnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS), "cudaMalloc") &&
-            cuda_ok(cudaMallocHost(&F->hnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS), "cudaMallocHost") &&
+            cuda_ok(cudaMalloc(&F->dnorm, norm_bytes(F)), "cudaMalloc") &&
+            cuda_ok(cudaMallocHost(&F->hnorm, norm_bytes(F)), "cudaMallocHost") &&
             cuda_ok(cudaStreamSynchronize(st), "refine setup");
   if (!ok) return -1;
   F->refine_ready = true;
@@ -199,23 +219,23 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
 // Refines X (device, n x nrhs, ld) for B; returns the number of correction
 // steps or -1; res (host, nrhs) gets the final scaled residuals.
 static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int ld, double tol, int maxits,
-                         double anorm, double* res) {
+                         const std::vector<double>& anorm, double* res) {
   const Plan& P = F->plan;
-  const int n = F->n;
+  const int n = F->n, ns = F->nseg();
   cudaStream_t st = current_stream();
   int total = 0;
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
     double* X = dX + (size_t) q0 * ld;
     const double* B = dB + (size_t) q0 * ld;
-    std::vector<double> bnorm(nq, 0.0);
-    // r = b - A x and the inf-norms of r and x, read back to the host
+    std::vector<double> bnorm((size_t) nq * ns, 0.0);
+    // r = b - A x and the inf-norms of r and x per segment, read back
     auto residual = [&](cudaStream_t s) {
-      cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long) * 2 * SOLVE_NRHS, s);
+      cudaMemsetAsync(F->dnorm, 0, norm_bytes(F), s);
       k_residual<<<nblk(n, 256), 256, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, F->dR,
-                                              ld, nq, F->dnorm);
+                                              ld, nq, F->dseg, F->dnorm);
       count_launch();
-      cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long) * 2 * SOLVE_NRHS, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(F->hnorm, F->dnorm, norm_bytes(F), cudaMemcpyDeviceToHost, s);
       return (int) cudaGetLastError();
     };
     // one correction step x += A~^-1 r, then the next residual
@@ -245,16 +265,17 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     for (int it = 0; !done; it++) {
       if (!cuda_ok(cudaStreamSynchronize(st), "refinement")) return -1;
       double worst = 0.0;
-      for (int q = 0; q < nq; q++) {
-        double rn, xn;
-        memcpy(&rn, &F->hnorm[q], 8);
-        memcpy(&xn, &F->hnorm[SOLVE_NRHS + q], 8);
-        if (it == 0) bnorm[q] = rn;   // X = 0: r = b
-        const double den = anorm * xn + bnorm[q];
-        const double rq = den > 0 ? rn / den : 0.0;
-        if (res) res[q0 + q] = rq;
-        worst = std::max(worst, rq);
-      }
+      for (int sg = 0; sg < ns; sg++)
+        for (int q = 0; q < nq; q++) {
+          double rn, xn;
+          memcpy(&rn, &F->hnorm[((size_t) sg * SOLVE_NRHS + q) * 2], 8);
+          memcpy(&xn, &F->hnorm[((size_t) sg * SOLVE_NRHS + q) * 2 + 1], 8);
+          if (it == 0) bnorm[(size_t) sg * nq + q] = rn;   // X = 0: r = b
+          const double den = anorm[sg] * xn + bnorm[(size_t) sg * nq + q];
+          const double rq = den > 0 ? rn / den : 0.0;
+          if (res) res[(size_t) sg * nrhs + q0 + q] = rq;
+          worst = std::max(worst, rq);
+        }
       if (it > 0 && worst <= tol) break;
       if (it > 0) {
         if (worst > 0.5 * prev_worst) slow++;
@@ -283,15 +304,17 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
   return total;
 }
 
-// ||A||_inf of the factored values, computed on the device
-static int device_anorm(Factor* F, double* anorm) {
+// ||A||_inf of the factored values per segment, computed on the device
+static int device_anorm(Factor* F, std::vector<double>* anorm) {
   cudaStream_t st = current_stream();
-  cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long), st);
-  k_anorm<<<nblk(F->n, 256), 256, 0, st>>>(F->n, F->dcsr_ptr, F->dcsr_val, F->dvals_cur, F->dnorm);
+  const int ns = F->nseg();
+  cudaMemsetAsync(F->dnorm, 0, sizeof(unsigned long long) * ns, st);
+  k_anorm<<<nblk(F->n, 256), 256, 0, st>>>(F->n, F->dcsr_ptr, F->dcsr_val, F->dvals_cur, F->dseg, F->dnorm);
   count_launch();
-  cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(F->hnorm, F->dnorm, sizeof(unsigned long long) * ns, cudaMemcpyDeviceToHost, st);
   if (!cuda_ok(cudaStreamSynchronize(st), "norm")) return -1;
-  memcpy(anorm, &F->hnorm[0], 8);
+  anorm->resize(ns);
+  for (int s = 0; s < ns; s++) memcpy(&(*anorm)[s], &F->hnorm[s], 8);
   return 0;
 }
 
@@ -299,7 +322,7 @@ int solve_refine_device(Factor* F, int nrhs, double* dX, const double* dB, int l
                         double* res) {
   if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
   if (ensure_refine(F)) return -1;
-  double anorm = 0.0;
+  std::vector<double> anorm;
   if (device_anorm(F, &anorm)) return -1;
   return refine_device(F, nrhs, dX, dB, ld, tol, maxits, anorm, res);
 }
@@ -307,12 +330,13 @@ int solve_refine_device(Factor* F, int nrhs, double* dX, const double* dB, int l
 int solve_refine_host(Factor* F, taucs_ccs_matrix* A, int nrhs, double* X, const double* B, double tol, int maxits,
                       double* res) {
   if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
+  if (F->nseg() > 1) { set_error("solve_refine: a batch handle solves through taucs_b200_batch_solve"); return -1; }
   if (ensure_refine(F)) return -1;
   const int n = F->n;
   // A, when given, has the factored pattern and values; the norm comes from
   // the device copy
   (void) A;
-  double anorm = 0.0;
+  std::vector<double> anorm;
   if (device_anorm(F, &anorm)) return -1;
   cudaStream_t st = current_stream();
   int worst_steps = 0;
