@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixed80", choices=["mixed80", "fp64-64"])
+    ap.add_argument("--workload", default="mixed80", choices=["mixed80", "fp64-64", "batch4096"])
+    ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--grid", type=int, default=None, help="grid side (default 80 / 64 per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
@@ -274,6 +275,33 @@ def run_reference(args):
         return
     g = args.grid or (80 if args.workload == "mixed80" else 64)
     n_threads = os.cpu_count() or 1
+    if args.workload == "batch4096":
+        try:
+            import taucs_b200 as tb
+            systems, bs = batch_systems(tb, args.batch_count)
+            flops = 0.0
+            for A in systems:
+                p, ip = tb.order(A, "amd")
+                F = tb.factor_symbolic(A.permute(p, ip))
+                flops += F.info().flops
+                F.free()
+            t_s, fl_s, ns = cpu_reference_batch(systems, bs, n_threads)
+            sec = t_s * flops / fl_s
+        except Exception as exc:
+            print(json.dumps({"impl": "reference", "unavailable": repr(exc)}))
+            return
+        val = args.batch_count / sec
+        desc = (f"reference FP64 factor + solve of {ns} evenly spaced systems of the batch one at a time "
+                f"({t_s:.2f} s), scaled by the reference's flop count to all {args.batch_count} systems; "
+                f"sources + OpenBLAS 0.3.15, {n_threads} threads")
+        print(json.dumps({"impl": "reference", "metric": METRIC_BATCH, "value": val, "unit": UNIT, "n_gpus": world,
+                          "steps": 1, "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": f"{args.batch_count} systems"},
+                          "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                          "cpu_baseline": {"value": val, "unit": UNIT, "cores": n_threads, "kind": "reference",
+                                           "sample": desc}}))
+        return
     try:
         # bounded: one warm-up and at most 3 timed steps of the bounded sample
         warm = min(args.warmup, 1)
@@ -453,6 +481,223 @@ def run_serving(tb, seconds=2.0, rate=2000.0, sustain_rate=250.0, sustain_second
         "resident_solves": st1["resident_solves"] - st0["resident_solves"],
         "evictions": st1["evictions"], "failed": fails, "worst_scaled_residual": worst,
     }
+
+
+
+# ---------------------------------------------------------------- batches
+
+BATCH_COUNT = 4096
+METRIC_BATCH = ("batch of 4096 SPD systems (2048 2D 5-point side 8-96, 2048 3D 7-point side 4-24, lognormal "
+                "sigma=1, 1 RHS each): FP32+refine factor+solve systems/s")
+
+
+def batch_systems(tb, count=BATCH_COUNT, seed=0):
+    """The batch configuration: half 2D 5-point grids with side ~ U{8..96},
+    half 3D 7-point grids with side ~ U{4..24}; lognormal(0, 1) edge
+    conductances (system i uses generator seed i); b_i ~ U(-1, 1)."""
+    rng = np.random.default_rng(seed)
+    systems, bs = [], []
+    for i in range(count):
+        if i < count // 2:
+            s = int(rng.integers(8, 97))
+            A = tb.lognormal(s, s, 0, 1.0, (1, 1, 1), i)
+        else:
+            s = int(rng.integers(4, 25))
+            A = tb.lognormal(s, s, s, 1.0, (1, 1, 1), i)
+        systems.append(A)
+    for A in systems:
+        bs.append(rng.uniform(-1, 1, A.n))
+    return systems, bs
+
+
+def cpu_reference_batch(systems, bs, n_threads, sample=96):
+    """The reference's CPU multifrontal path, one system at a time (its only
+    mode), on an evenly spaced sample of the batch; scaled to the batch by
+    the flop ratio."""
+    import taucs_b200 as tb
+    from oracle.bindings import Ref, ref_available
+    os.environ["OPENBLAS_NUM_THREADS"] = str(n_threads)
+    if not ref_available():
+        raise RuntimeError("oracle/_ref/libtaucs_ref.so was not built")
+    R = Ref(threads=n_threads)
+    R.set_threads(n_threads)
+    idx = np.linspace(0, len(systems) - 1, sample).astype(int)
+    t_tot, fl_s = 0.0, 0.0
+    for i in idx:
+        A = systems[i]
+        perm, iperm = R.order(A.n, A.colptr, A.rowind, A.values, "amd")
+        _, pc, pr, pv = R.permute(A.n, A.colptr, A.rowind, A.values, perm, iperm)
+        L = R.symbolic(A.n, pc, pr, pv)
+        fl_s += R.dump_symbolic(L).flops()
+        b = np.ascontiguousarray(bs[i][np.asarray(perm)])
+        t0 = time.perf_counter()
+        assert R.numeric(L, A.n, pc, pr, pv) == 0
+        R.solve(L, b)
+        t_tot += time.perf_counter() - t0
+        R.free(L)
+    return t_tot, fl_s, len(idx)
+
+
+def run_batch(args):
+    import torch
+    import taucs_b200 as tb
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.current_stream()
+    tb.set_stream(stream.cuda_stream)
+    lib = tb.lib()
+    count = args.batch_count
+    t0 = time.perf_counter()
+    systems, bs = batch_systems(tb, count)
+    B = tb.Batch(systems)
+    t_setup = time.perf_counter() - t0
+    info = B.info()
+    n = B.n
+    d_vals = torch.from_numpy(B.combined_values()).cuda()
+    d_b = torch.from_numpy(B.combined_rhs(bs)).cuda()
+    d_x = torch.empty_like(d_b)
+    res = np.empty(count, np.float64)
+
+    def step_mixed():
+        B.set_precision(1)
+        if lib.taucs_b200_factor_numeric_device(B.h, d_vals.data_ptr()) != 0:
+            raise RuntimeError("batch numeric failed: " + tb.last_error())
+        its = lib.taucs_b200_solve_refine_device(B.h, 1, C.c_void_p(d_x.data_ptr()), C.c_void_p(d_b.data_ptr()),
+                                                  n, TOL, 10, res)
+        if its < 0:
+            raise RuntimeError("batch refinement failed: " + tb.last_error())
+        return its
+
+    def step_fp64():
+        B.set_precision(0)
+        if lib.taucs_b200_factor_numeric_device_async(B.h, d_vals.data_ptr()) != 0:
+            raise RuntimeError("batch numeric failed: " + tb.last_error())
+        if B.solve_device(1, d_x.data_ptr(), d_b.data_ptr(), n) != 0:
+            raise RuntimeError("batch solve failed: " + tb.last_error())
+
+    def timed(step, k):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = None
+        for _ in range(k):
+            out = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def worst_residual():
+        torch.cuda.synchronize()
+        xs = B.split(d_x.cpu().numpy())
+        return max(scaled_residual(A, x, b) for A, x, b in zip(systems, xs, bs))
+
+    W, K = max(args.warmup, 3), args.steps
+    for _ in range(W):
+        step_mixed()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    tb.launch_count(reset=True)
+    ms, its = timed(step_mixed, K)
+    clk = clocks.stop()
+    launches = tb.launch_count(reset=True) // max(K, 1)
+    res_mixed = worst_residual()
+    worst_reported = float(res.max())
+    for _ in range(W):
+        step_fp64()
+    ms64, _ = timed(step_fp64, K)
+    res64 = worst_residual()
+
+    # end to end through the C ABI: host values and right-hand sides per system
+    bptr = (C.c_void_p * count)(*[b.ctypes.data for b in bs])
+    xs_h = [np.empty(A.n) for A in systems]
+    xptr = (C.c_void_p * count)(*[x.ctypes.data for x in xs_h])
+    sptr = (C.POINTER(tb.CCSStruct) * count)(*[C.pointer(A.s) for A in systems])
+
+    def step_e2e():
+        B.set_precision(1)
+        if lib.taucs_b200_batch_factor(B.h, sptr) != 0:
+            raise RuntimeError("batch factor failed: " + tb.last_error())
+        if lib.taucs_b200_batch_solve(B.h, xptr, bptr, TOL, 10, res) < 0:
+            raise RuntimeError("batch solve failed: " + tb.last_error())
+    step_e2e()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        step_e2e()
+    ms_e2e = (time.perf_counter() - t0) * 1e3
+
+    # profiled steps for the roofline
+    lib.taucs_b200_profile(1)
+    nprof = 2
+    for _ in range(nprof):
+        step_mixed()
+    torch.cuda.synchronize()
+    kern = read_profile(tb, nprof)
+    lib.taucs_b200_profile(0)
+    tf32 = tf32_gemm_peak()
+    roof = roofline(kern, tf32 / 3.0, f"cuBLAS TF32 GEMM 8192^3 measured in this run ({tf32:.0f} TF/s) / 3 "
+                                      f"(TF32x3 products, of measured)", measured_peaks().get("hbm_gbs"))
+    B.free()
+    torch.cuda.empty_cache()
+
+    # the same systems one at a time on the GPU (FP64, patterns analysed
+    # beforehand), on an evenly spaced sample
+    idx = np.linspace(0, count - 1, 128).astype(int)
+    pre = []
+    for i in idx:
+        A = systems[i]
+        p, ip = tb.order(A, "amd")
+        P = A.permute(p, ip)
+        F = tb.factor_symbolic(P)
+        F.set_precision(0)
+        pre.append((F, P, np.ascontiguousarray(bs[i][p])))
+    for F, P, b in pre[:4]:
+        F.numeric(P)
+        F.solve(b)
+    t0 = time.perf_counter()
+    for F, P, b in pre:
+        F.numeric(P)
+        F.solve(b)
+    t_one = (time.perf_counter() - t0) / len(pre)
+    for F, _, _ in pre:
+        F.free()
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            nth = os.cpu_count() or 1
+            t_s, fl_s, ns = cpu_reference_batch(systems, bs, nth)
+            sec = t_s * info.flops / fl_s
+            cpu = {"value": count / sec, "unit": UNIT, "cores": nth, "kind": "reference",
+                   "sample": f"reference FP64 factor + solve of {ns} evenly spaced systems of the batch one at a "
+                             f"time ({t_s:.2f} s), scaled by the reference's flop count to all {count} systems; "
+                             f"sources + OpenBLAS 0.3.15, {nth} threads"}
+        except Exception as exc:
+            cpu = {"error": repr(exc)}
+    out = {
+        "metric": METRIC_BATCH, "value": K * count / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{count} systems, one block-diagonal level-scheduled factor + solve per step",
+                   "rows": n, "nnz_lower": B.nnz, "flops": info.flops, "supernodes": info.n_live,
+                   "levels": info.n_levels, "l_gb_fp64": info.l_bytes / 1e9, "setup_s": t_setup,
+                   "l2_policy": "inputs larger than L2 (tens of GB of factor and update arena per step)"},
+        "clocks": clk,
+        "e2e": {"value": K * count / (ms_e2e * 1e-3), "unit": UNIT, "ms_per_step": ms_e2e / K,
+                "h2d_bytes_per_step": 8 * B.nnz + 8 * n, "d2h_bytes_per_step": 8 * n + 8 * count},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "kernels": kern,
+        "cpu_baseline": cpu,
+        "refinement_steps": its,
+        "scaled_residual": {"worst_system": res_mixed, "worst_reported_by_refinement": worst_reported},
+        "fp64": {"value": K * count / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64 / K,
+                 "worst_system_scaled_residual": res64},
+        "one_at_a_time_fp64_gpu": {"value": 1.0 / t_one, "unit": UNIT,
+                                   "sample": "128 evenly spaced systems, FP64 factor + solve each, "
+                                             "patterns analysed beforehand"},
+    }
+    print(json.dumps(out))
 
 
 
@@ -708,6 +953,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch4096":
+        run_batch(args)
     else:
         run_ours(args)
 

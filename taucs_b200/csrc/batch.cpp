@@ -16,6 +16,9 @@
 // meets the scaled-residual target of every system on its own.
 
 #include <algorithm>
+#include <atomic>
+#include <string>
+#include <thread>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
@@ -47,29 +50,30 @@ extern "C" void* taucs_b200_batch_analyze(int count, taucs_ccs_matrix* const* A)
   if (N > INT_MAX || NNZ > INT_MAX) { set_error("batch_analyze: the batch exceeds 2^31 rows or entries"); return nullptr; }
   std::vector<int> colptr(N + 1), rowind(NNZ), seg_ptr(count + 1, 0), perm(N), vmap(NNZ);
   std::vector<int64_t> nnz_off(count + 1, 0);
-  std::vector<Symbolic> syms(count);
-  int64_t r0 = 0, e0 = 0;
-  colptr[0] = 0;
   for (int s = 0; s < count; s++) {
+    seg_ptr[s + 1] = seg_ptr[s] + A[s]->n;
+    nnz_off[s + 1] = nnz_off[s] + A[s]->colptr[A[s]->n];
+  }
+  colptr[0] = 0;
+  // per system, independent of the others (host threads): AMD ordering, the
+  // permuted pattern with the value map, the symbolic factor
+  std::vector<Symbolic> syms(count);
+  std::vector<std::string> errs(count);
+  auto analyse = [&](int s) {
     taucs_ccs_matrix As = *A[s];
     const int n = As.n;
     const int64_t nnz = As.colptr[n];
+    const int64_t r0 = seg_ptr[s], e0 = nnz_off[s];
     int *p = nullptr, *ip = nullptr;
     taucs_ccs_order(&As, &p, &ip, (char*) "amd");
-    if (!p) { set_error("batch_analyze: ordering failed for system " + std::to_string(s)); return nullptr; }
+    if (!p) { errs[s] = "ordering failed"; return; }
     // value positions travel through the permutation as values
     std::vector<double> idx((size_t) nnz);
     for (int64_t k = 0; k < nnz; k++) idx[k] = (double) k;
     As.values.d = idx.data();
     taucs_ccs_matrix* PA = taucs_ccs_permute_symmetrically(&As, p, ip);
-    if (!PA) { free(p); free(ip); return nullptr; }
-    if (symbolic_analyze(n, PA->colptr, PA->rowind, 0, &syms[s]) != TAUCS_SUCCESS) {
-      taucs_ccs_free(PA);
-      free(p);
-      free(ip);
-      set_error("batch_analyze: symbolic analysis failed for system " + std::to_string(s));
-      return nullptr;
-    }
+    if (!PA) { free(p); free(ip); errs[s] = "permutation failed"; return; }
+    if (symbolic_analyze(n, PA->colptr, PA->rowind, 0, &syms[s]) != TAUCS_SUCCESS) errs[s] = "symbolic analysis failed";
     for (int j = 0; j < n; j++) {
       for (int k = PA->colptr[j]; k < PA->colptr[j + 1]; k++) {
         rowind[e0 + k] = (int) r0 + PA->rowind[k];
@@ -81,11 +85,22 @@ extern "C" void* taucs_b200_batch_analyze(int count, taucs_ccs_matrix* const* A)
     taucs_ccs_free(PA);
     free(p);
     free(ip);
-    r0 += n;
-    e0 += nnz;
-    seg_ptr[s + 1] = (int) r0;
-    nnz_off[s + 1] = e0;
+  };
+  {
+    const int nth = std::max(1, std::min<int>(count, (int) std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; t++)
+      pool.emplace_back([&] {
+        for (int s; (s = next.fetch_add(1)) < count;) analyse(s);
+      });
+    for (auto& th : pool) th.join();
   }
+  for (int s = 0; s < count; s++)
+    if (!errs[s].empty()) {
+      set_error("batch_analyze: system " + std::to_string(s) + ": " + errs[s]);
+      return nullptr;
+    }
   // the systems' supernodal trees under one virtual root: slots of system s
   // follow those of systems < s, rows are shifted by the system's offset,
   // and the roots of every tree become children of the joint root

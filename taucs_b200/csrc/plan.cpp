@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <map>
+#include <set>
 #include <numeric>
 
 #include "internal.h"
@@ -31,53 +32,63 @@ namespace tb {
 
 namespace {
 
-// first-fit allocator over [0, inf) offsets (in doubles), 256-byte granules
+// best-fit allocator over [0, inf) offsets (in doubles), 256-byte granules:
+// free blocks indexed by offset (for coalescing) and by (length, offset)
+// (for the smallest block that fits, O(log n) per call)
 struct ArenaPlanner {
-  std::map<int64_t, int64_t> free_;  // offset -> length
+  std::map<int64_t, int64_t> free_;              // offset -> length
+  std::set<std::pair<int64_t, int64_t>> by_len_;  // (length, offset)
   int64_t top = 0;
   static int64_t round(int64_t n) { return (n + 31) & ~int64_t(31); }
+  void add(int64_t off, int64_t len) {
+    free_[off] = len;
+    by_len_.emplace(len, off);
+  }
+  void drop(std::map<int64_t, int64_t>::iterator it) {
+    by_len_.erase({it->second, it->first});
+    free_.erase(it);
+  }
   int64_t alloc(int64_t n) {
     n = round(n);
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second >= n) {
-        int64_t off = it->first;
-        int64_t rest = it->second - n;
-        free_.erase(it);
-        if (rest > 0) free_[off + n] = rest;
-        return off;
-      }
+    auto b = by_len_.lower_bound({n, INT64_MIN});
+    if (b != by_len_.end()) {
+      const int64_t off = b->second, len = b->first;
+      drop(free_.find(off));
+      if (len > n) add(off + n, len - n);
+      return off;
     }
     // extend the top (merge with a free block that ends at top)
     if (!free_.empty()) {
       auto last = std::prev(free_.end());
       if (last->first + last->second == top) {
-        int64_t off = last->first;
-        free_.erase(last);
+        const int64_t off = last->first;
+        drop(last);
         top = off + n;
         return off;
       }
     }
-    int64_t off = top;
+    const int64_t off = top;
     top += n;
     return off;
   }
   void release(int64_t off, int64_t n) {
     n = round(n);
-    auto it = free_.emplace(off, n).first;
-    // coalesce with next
-    auto nx = std::next(it);
-    if (nx != free_.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_.erase(nx);
+    // coalesce with the neighbours, then insert once
+    auto nx = free_.lower_bound(off);
+    if (nx != free_.end() && off + n == nx->first) {
+      n += nx->second;
+      drop(nx);
     }
-    // coalesce with previous
-    if (it != free_.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_.erase(it);
+    auto pv = free_.lower_bound(off);
+    if (pv != free_.begin()) {
+      --pv;
+      if (pv->first + pv->second == off) {
+        off = pv->first;
+        n += pv->second;
+        drop(pv);
       }
     }
+    add(off, n);
   }
 };
 
