@@ -78,6 +78,17 @@ def scaled_residual(A, x, b):
     return float(np.max(np.abs(r)) / (A.inf_norm() * np.max(np.abs(x)) + np.max(np.abs(b))))
 
 
+def max_over_ranks_of(dist, v, device):
+    """The slowest rank's value (timings are reported as the max over ranks);
+    dist is torch.distributed or None for one process."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_system(workload, g):
     """(A unpermuted, perm, iperm, PAP^T, B) of the workload."""
     import taucs_b200 as tb
@@ -819,11 +830,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(dist, v, "cuda")
 
     def timed(step, k):
         barrier()
