@@ -86,8 +86,10 @@ struct LevelPlan {
   std::vector<int2_> solve_fwd_blocks;   // (front, row block)
   std::vector<int2_> solve_bwd_blocks;   // (front, column block), last block first
   std::vector<int2_> solve_l21_tasks;    // (front, column block << 16 | row chunk)
-  // small fronts, fused kernel
+  // small fronts, fused kernel (sorted by order f); the first small_warp of
+  // them are small enough for the one-warp-per-front solve kernels
   std::vector<int> small_fronts;
+  int small_warp = 0;
   // medium/large fronts
   std::vector<int> big_fronts;
   std::vector<Tile> build_tiles;

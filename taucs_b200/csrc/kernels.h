@@ -25,6 +25,8 @@ constexpr int GEMM_BN = 64;
 constexpr int GEMM_BK = 16;
 // right-hand sides handled per solve pass
 constexpr int SOLVE_NRHS = 8;
+// small fronts up to this order are solved by one warp each (eight per CTA)
+constexpr int SOLVE_WARP_F = 48;
 // rows of L21 per CTA in the backward solve's partial products
 constexpr int SOLVE_RCH = 512;
 

@@ -384,6 +384,9 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
       // the fused small-front kernel is launched per size class
       std::stable_sort(LP.small_fronts.begin(), LP.small_fronts.end(),
                        [&](int a, int b) { return P.fronts[a].f < P.fronts[b].f; });
+      while (LP.small_warp < (int) LP.small_fronts.size() &&
+             P.fronts[LP.small_fronts[LP.small_warp]].f <= SOLVE_WARP_F)
+        LP.small_warp++;
     }
   }
 

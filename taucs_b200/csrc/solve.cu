@@ -26,15 +26,28 @@ namespace {
 
 constexpr int SB = 32;   // substitution block (one warp)
 
-template <typename T, int WS>
+// Small fronts: G threads per front (256: one CTA; 32: one warp, eight
+// fronts per CTA for the many tiny fronts near the leaves).  The threads of
+// one front synchronise among themselves only.
+template <int G>
+__device__ __forceinline__ void group_sync() {
+  if (G == 32) __syncwarp();
+  else __syncthreads();
+}
+
+template <typename T, int WS, int G>
 __global__ void __launch_bounds__(256)
-k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+k_fwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
       const int* __restrict__ maps, const int* __restrict__ rows, const T* __restrict__ L,
       const T* __restrict__ B, int ldb, T* __restrict__ W, int nrhs) {
-  __shared__ T xs[SB][SOLVE_NRHS];
-  const FrontDesc F = fronts[list[blockIdx.x]];
+  constexpr int GPC = 256 / G;   // fronts per CTA: one per group of G threads
+  __shared__ T xs_all[GPC][SB][SOLVE_NRHS];
+  const int grp = threadIdx.x / G, li = blockIdx.x * GPC + grp;
+  if (li >= count) return;
+  T (&xs)[SB][SOLVE_NRHS] = xs_all[grp];
+  const FrontDesc F = fronts[list[li]];
   const int f = F.f, s = F.s;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x % G, nt = G, lane = tid & 31, warp = tid >> 5;
   T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const T* P = L + F.l_off;
@@ -43,7 +56,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     const int r = k % f, q = k / f;
     Wf[k] = (r < s) ? B[rw[r] + (size_t) q * ldb] : 0.0;
   }
-  __syncthreads();
+  group_sync<G>();
   for (int ci = F.child_begin; ci < F.child_end; ci++) {
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
@@ -53,7 +66,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
       const int i = k % mc, q = k / mc;
       Wf[mp[i] + q * f] += Wc[C.s + i + q * C.f];
     }
-    __syncthreads();
+    group_sync<G>();
   }
   for (int jb = 0; jb < s; jb += SB) {
     const int bw = min(SB, s - jb);
@@ -84,7 +97,7 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
           }
       }
     }
-    __syncthreads();
+    group_sync<G>();
     for (int r = jb + bw + tid; r < f; r += nt) {
       T acc[SOLVE_NRHS];
 #pragma unroll
@@ -99,19 +112,23 @@ k_fwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
       for (int q = 0; q < SOLVE_NRHS; q++)
         if (q < nrhs) Wf[r + q * f] -= acc[q];
     }
-    __syncthreads();
+    group_sync<G>();
   }
 }
 
-template <typename T, int WS>
+template <typename T, int WS, int G>
 __global__ void __launch_bounds__(256)
-k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
+k_bwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
       const T* __restrict__ L, T* __restrict__ X, int ldx, T* __restrict__ W,
       int nrhs) {
-  __shared__ T xs[SB][SOLVE_NRHS];
-  const FrontDesc F = fronts[list[blockIdx.x]];
+  constexpr int GPC = 256 / G;
+  __shared__ T xs_all[GPC][SB][SOLVE_NRHS];
+  const int grp = threadIdx.x / G, li = blockIdx.x * GPC + grp;
+  if (li >= count) return;
+  T (&xs)[SB][SOLVE_NRHS] = xs_all[grp];
+  const FrontDesc F = fronts[list[li]];
   const int f = F.f, s = F.s;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int tid = threadIdx.x % G, nt = G, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const T* P = L + F.l_off;
@@ -121,7 +138,7 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
     const int i = k % (f - s), q = k / (f - s);
     Wf[s + i + q * f] = X[rw[s + i] + (size_t) q * ldx];
   }
-  __syncthreads();
+  group_sync<G>();
   // r_j = y_j - sum_{i >= s} L[i,j] x_i
   for (int j = warp; j < s; j += nw) {
     T acc[SOLVE_NRHS];
@@ -146,7 +163,7 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
         if (q < nrhs) Wf[j + q * f] -= acc[q];
     }
   }
-  __syncthreads();
+  group_sync<G>();
   // L11^T substitution, blocks from the end
   const int nblk = (s + SB - 1) / SB;
   for (int b = nblk - 1; b >= 0; b--) {
@@ -176,7 +193,7 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
             if (q < nrhs) Wf[j + q * f] -= acc[q];
         }
       }
-      __syncthreads();
+      group_sync<G>();
     }
     if (warp == 0) {
       const T rd = (lane < bw) ? T(1) / P[(jb + lane) + (size_t) (jb + lane) * f] : T(0);
@@ -201,12 +218,12 @@ k_bwd(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const 
           if (q < nrhs) xs[lane][q] = v[q];
       }
     }
-    __syncthreads();
+    group_sync<G>();
     for (int k = tid; k < bw * nrhs; k += nt) {
       const int l = k % bw, q = k / bw;
       Wf[jb + l + q * f] = xs[l][q];
     }
-    __syncthreads();
+    group_sync<G>();
   }
   for (int k = tid; k < s * nrhs; k += nt) {
     const int r = k % s, q = k / s;
@@ -648,9 +665,18 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       prof_begin(KC_SOLVE_FWD, st);
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
-        k_fwd<T, SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L,
-                                  Bq, ld, W, nq);
-        count_launch();
+        const int* sl = D.small_list + D.small_off[h];
+        const int nw = LP.small_warp;
+        if (nw > 0) {
+          k_fwd<T, SOLVE_NRHS, 32><<<(nw + 7) / 8, 256, 0, st>>>(sl, nw, D.fronts, D.children, D.maps, D.rows, L,
+                                                                 Bq, ld, W, nq);
+          count_launch();
+        }
+        if (ns > nw) {
+          k_fwd<T, SOLVE_NRHS, 256><<<ns - nw, 256, 0, st>>>(sl + nw, ns - nw, D.fronts, D.children, D.maps, D.rows,
+                                                             L, Bq, ld, W, nq);
+          count_launch();
+        }
       }
       const int nb = (int) LP.solve_fwd_blocks.size();
       if (nb > 0) {
@@ -701,8 +727,16 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       }
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
-        k_bwd<T, SOLVE_NRHS><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, Xq, ld, W, nq);
-        count_launch();
+        const int* sl = D.small_list + D.small_off[h];
+        const int nw = LP.small_warp;
+        if (nw > 0) {
+          k_bwd<T, SOLVE_NRHS, 32><<<(nw + 7) / 8, 256, 0, st>>>(sl, nw, D.fronts, D.rows, L, Xq, ld, W, nq);
+          count_launch();
+        }
+        if (ns > nw) {
+          k_bwd<T, SOLVE_NRHS, 256><<<ns - nw, 256, 0, st>>>(sl + nw, ns - nw, D.fronts, D.rows, L, Xq, ld, W, nq);
+          count_launch();
+        }
       }
       prof_end(KC_SOLVE_BWD, st, 0.0, by);
     }
@@ -784,7 +818,7 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
     const LevelPlan& LP = P.levels[h];
     const int ns = (int) LP.small_fronts.size();
     if (ns > 0) {
-      k_fwd<double, 1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.children, D.maps, D.rows, L, B, ld,
+      k_fwd<double, 1, 256><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], ns, D.fronts, D.children, D.maps, D.rows, L, B, ld,
                                    W, 1);
       count_launch();
     }
@@ -809,7 +843,7 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
     }
     const int ns = (int) LP.small_fronts.size();
     if (ns > 0) {
-      k_bwd<double, 1><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], D.fronts, D.rows, L, X, ld, W, 1);
+      k_bwd<double, 1, 256><<<ns, 256, 0, st>>>(D.small_list + D.small_off[h], ns, D.fronts, D.rows, L, X, ld, W, 1);
       count_launch();
     }
   }
