@@ -30,6 +30,29 @@ constexpr int SOLVE_WARP_F = 48;
 // rows of L21 per CTA in the backward solve's partial products
 constexpr int SOLVE_RCH = 512;
 
+#ifdef __CUDACC__
+// First index of the sorted a[0, n) whose value is >= key, found by one
+// warp: 32 probes per round narrow the range 32-fold, so a search costs
+// ceil(log32 n) dependent loads instead of log2 n.  Every lane returns the
+// result; all 32 lanes must call it.
+__device__ __forceinline__ int warp_lower_bound(const int* a, int n, int key) {
+  const int lane = threadIdx.x & 31;
+  int lo = 0, hi = n;
+  while (hi - lo > 32) {
+    const int step = (hi - lo + 31) / 32;
+    const int p = lo + lane * step;
+    const unsigned less = __ballot_sync(0xffffffffu, p < hi && a[p] < key);
+    const int cnt = __popc(less);   // the probes below key form a prefix
+    if (cnt == 0) return lo;
+    const int nlo = lo + (cnt - 1) * step + 1;
+    hi = min(hi, lo + cnt * step);
+    lo = nlo;
+  }
+  const int p = lo + lane;
+  return lo + __popc(__ballot_sync(0xffffffffu, p < hi && a[p] < key));
+}
+#endif
+
 // Device copies of the plan arrays.
 struct DevPlan {
   FrontDesc* fronts = nullptr;

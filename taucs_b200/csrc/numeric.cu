@@ -37,16 +37,6 @@ namespace tb {
 
 namespace {
 
-__device__ __forceinline__ int lower_bound_dev(const int* a, int n, int key) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (a[mid] < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
 __device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
 
@@ -131,6 +121,7 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
         const int* __restrict__ a_idx, const T* __restrict__ vals,
         T* __restrict__ L, T* __restrict__ U, const int* status) {
   __shared__ T W[BUILD_TR * BUILD_TC];
+  __shared__ int rng[4];
   if (failed(status)) return;
   const Tile tl = tiles[blockIdx.x];
   const FrontDesc F = fronts[tl.front];
@@ -162,10 +153,17 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
-    const int ja = lower_bound_dev(mp, mc, C0), jb = lower_bound_dev(mp, mc, C0 + nc);
-    if (ja >= jb) continue;
-    const int ia = lower_bound_dev(mp, mc, R0), ib = lower_bound_dev(mp, mc, R0 + nr);
-    if (ia >= ib) continue;
+    // the child's columns and rows that land in this tile: four warps search
+    // the four bounds at once
+    if (warp < 4) {
+      const int key = warp == 0 ? C0 : warp == 1 ? C0 + nc : warp == 2 ? R0 : R0 + nr;
+      const int r = warp_lower_bound(mp, mc, key);
+      if (lane == 0) rng[warp] = r;
+    }
+    __syncthreads();
+    const int ja = rng[0], jb = rng[1], ia = rng[2], ib = rng[3];
+    __syncthreads();
+    if (ja >= jb || ia >= ib) continue;
     const T* Uc = U + C.u_off;
     for (int j = ja + warp; j < jb; j += nw) {
       const int pj = (mp[j] - C0) * BUILD_TR;

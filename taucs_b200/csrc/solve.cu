@@ -268,16 +268,6 @@ __device__ void wait_epoch(const int* flag, int epoch, int* status) {
   __syncthreads();
 }
 
-__device__ __forceinline__ int lb_dev(const int* a, int n, int key) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (a[mid] < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
 template <typename T, int NQ, int WS>
 __global__ void __launch_bounds__(128)
 k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
@@ -316,11 +306,18 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     wv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : 0.0;
   }
   __syncthreads();
+  __shared__ int rng[2];
   for (int ci = F.child_begin; ci < F.child_end; ci++) {
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
-    const int ia = lb_dev(mp, mc, r0), ib = lb_dev(mp, mc, r0 + nr);
+    if (warp < 2) {
+      const int r = warp_lower_bound(mp, mc, warp == 0 ? r0 : r0 + nr);
+      if (lane == 0) rng[warp] = r;
+    }
+    __syncthreads();
+    const int ia = rng[0], ib = rng[1];
+    __syncthreads();
     if (ia >= ib) continue;
     const T* Wc = W + C.v_off * WS;
     for (int k = tid; k < (ib - ia) * nrhs; k += 128) {
