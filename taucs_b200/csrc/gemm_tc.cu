@@ -7,7 +7,7 @@
 //     C -= A B^T      (A: rows of the panel, B: columns, K = panel columns)
 //
 // computed as three TF32 products per element pair, lo*hi + hi*lo + hi*hi,
-// accumulated in FP32 in tensor memory, which keeps FP32 accuracy.  One CTA
+// accumulated in FP32 in tensor memory, which keeps FP32-level accuracy.  One CTA
 // owns a 128 x 128 tile of the lower trapezoid of C:
 //
 //   warps 0-3  producers: each thread loads one row of the A and B K-slabs
@@ -97,10 +97,12 @@ __device__ __forceinline__ void tc_commit(unsigned bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+// x = hi + lo with hi = x truncated to TF32 (exact in FP32) and lo = x - hi
+// (exact); the tensor core uses the top 19 bits of lo, so each product
+// keeps about 21 bits, which with FP32 accumulation is FP32-level accuracy.
 __device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
-  const float r = x - __uint_as_float(hi);
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+  hi = __float_as_uint(x) & 0xffffe000u;
+  lo = __float_as_uint(x - __uint_as_float(hi));
 }
 
 __device__ __forceinline__ void st_shared_v4(unsigned addr, unsigned a, unsigned b, unsigned c, unsigned d) {
@@ -219,10 +221,10 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
         b[j] = (rb && kv) ? brow[(size_t) k * f] : 0.0f;
       }
     };
-    load(0, av, bv);
-    for (int kt = 0; kt < nk && ok; kt++) {
+    // one K-slab: wait for its ring slot, split and store, release it to the
+    // MMA thread; the next slab's loads are issued first
+    auto stage = [&](int kt, float (&a)[KT], float (&b)[KT], float (&an)[KT], float (&bn)[KT]) -> bool {
       const int stg = kt % STAGES, use = kt / STAGES;
-      float an[KT], bn[KT];
       if (kt + 1 < nk) load(kt + 1, an, bn);
       if (use > 0) {
         // one lane polls the ring slot; the warp follows it
@@ -230,21 +232,18 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
         if (lane == 0) got = mbar_wait(empty0 + 8 * stg, (use - 1) & 1);
         got = __shfl_sync(0xffffffffu, got, 0);
         __syncwarp();   // orders the lanes' stores after lane 0's acquire
-        if (!got) {
-          ok = false;
-          break;
-        }
+        if (!got) return false;
       }
       const unsigned st = sbase + stg * TC_STAGE + roff_s;
 #pragma unroll
       for (int c = 0; c < KT / 4; c++) {
         unsigned h[4], l[4];
 #pragma unroll
-        for (int e = 0; e < 4; e++) tf32_split(av[4 * c + e], h[e], l[e]);
+        for (int e = 0; e < 4; e++) tf32_split(a[4 * c + e], h[e], l[e]);
         st_shared_v4(st + 0 * TC_PART + c * 128, h[0], h[1], h[2], h[3]);
         st_shared_v4(st + 1 * TC_PART + c * 128, l[0], l[1], l[2], l[3]);
 #pragma unroll
-        for (int e = 0; e < 4; e++) tf32_split(bv[4 * c + e], h[e], l[e]);
+        for (int e = 0; e < 4; e++) tf32_split(b[4 * c + e], h[e], l[e]);
         st_shared_v4(st + 2 * TC_PART + c * 128, h[0], h[1], h[2], h[3]);
         st_shared_v4(st + 3 * TC_PART + c * 128, l[0], l[1], l[2], l[3]);
       }
@@ -253,8 +252,14 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(full0 + 8 * stg);
-#pragma unroll
-      for (int j = 0; j < KT; j++) { av[j] = an[j]; bv[j] = bn[j]; }
+      return true;
+    };
+    // two register sets in alternation, so no slab is copied between them
+    float a2[KT], b2[KT];
+    load(0, av, bv);
+    for (int kt = 0; kt < nk && ok; kt += 2) {
+      ok = stage(kt, av, bv, a2, b2);
+      if (ok && kt + 1 < nk) ok = stage(kt + 1, a2, b2, av, bv);
     }
     if (!ok) {
       record_timeout(status);
