@@ -633,7 +633,6 @@ template <typename T>
 static void solve_attrs() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_bwd_big<T, 1, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
   cudaFuncSetAttribute(k_bwd_big<T, 2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
   cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
   cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
@@ -678,9 +677,9 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       const int nb = (int) LP.solve_fwd_blocks.size();
       if (nb > 0) {
         const int2_* bl = D.sfwd + D.sfwd_off[h];
-        if (nq == 1)
-          k_fwd_big<T, 1, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
-        else if (nq == 2)
+        // one right-hand side runs the two-column variant, measured faster
+        // than a one-column instantiation (columns >= nrhs are skipped)
+        if (nq <= 2)
           k_fwd_big<T, 2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
         else if (nq <= 4)
           k_fwd_big<T, 4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
@@ -705,16 +704,13 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         const int nt = (int) LP.solve_l21_tasks.size();
         const int2_* tl = D.sl21 + D.sl21_off[h];
         if (nt > 0) {
-          if (nq == 1) k_bwd_l21<T, 1, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
-          else if (nq == 2) k_bwd_l21<T, 2, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
+          if (nq <= 2) k_bwd_l21<T, 2, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
           else if (nq <= 4) k_bwd_l21<T, 4, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
           else k_bwd_l21<T, 8, SOLVE_NRHS><<<nt, 128, 0, st>>>(tl, D.fronts, L, W, part, nq);
           count_launch();
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
-        if (nq == 1)
-          k_bwd_big<T, 1, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
-        else if (nq == 2)
+        if (nq <= 2)
           k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
           k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
