@@ -268,6 +268,18 @@ int taucs_b200_profile_read(int kernel_class, double* ms, long* launches, double
  * copies at most cap entries and returns the number recorded */
 long taucs_b200_profile_log(int* kernel_class, float* ms, long cap);
 
+/* Autotuner (no counterpart in the reference): times the numeric
+ * factorization of L's pattern on the device values d_values with each GEMM
+ * variant (FP64 fronts: 64x64 or 128x128 DMMA tiles; FP32 fronts: the two
+ * tcgen05 pipeline shapes) and keeps, per level of the supernodal tree and
+ * per product (panel updates, update matrix), the faster one for every
+ * later factorization of this handle in its current precision.  Runs four
+ * factorizations; uses the library's per-launch profiling, so no other
+ * thread may profile at the same time.  choices (2 x levels, may be NULL)
+ * receives the variant per level: [2h] panel, [2h + 1] update matrix.
+ * Returns 0, or -1 when a factorization failed. */
+int taucs_b200_autotune(void* L, const double* d_values, int* choices);
+
 /* CUDA kernel launches issued by this library on the calling thread since
  * the last reset (for launch accounting in benchmarks). */
 long taucs_b200_launch_count(int reset);

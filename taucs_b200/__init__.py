@@ -128,6 +128,7 @@ def lib():
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
         "taucs_b200_etree": (C.c_int, [pc, _i32p]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
+        "taucs_b200_autotune": (C.c_int, [vp, vp, _i32p]),
         "taucs_b200_profile": (C.c_int, [C.c_int]),
         "taucs_b200_profile_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -324,6 +325,14 @@ class Factor:
         d = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(n,)).copy()
         C.CDLL(None).free(C.c_void_p(p))
         return d
+
+    def autotune(self, d_values_ptr):
+        """Per-level GEMM variants chosen from measured times (see
+        taucs_b200_autotune); returns the choices, 2 per level."""
+        ch = np.zeros(2 * max(self.info().n_levels, 1), np.int32)
+        if lib().taucs_b200_autotune(self.h, C.c_void_p(d_values_ptr), ch) != 0:
+            raise RuntimeError("autotune failed: " + last_error())
+        return ch
 
     def set_precision(self, p):
         return lib().taucs_b200_set_precision(self.h, p)

@@ -405,6 +405,52 @@ int taucs_b200_set_stream(void* s) {
   return 0;
 }
 
+// Autotuner: for the factor's precision, runs the numeric factorization
+// once with every GEMM launch in each variant (after an untimed run), times
+// every launch with CUDA events, and keeps per level and product the variant
+// that took less device time.  The choice lives in the plan and applies to
+// every later numeric factorization of this handle.
+int taucs_b200_autotune(void* L, const double* d_values, int* choices) {
+  Factor* F = (Factor*) L;
+  if (!F || !d_values) return -1;
+  if (ensure_device(F)) return -1;
+  const int H = F->plan.n_levels, pi = F->precision == 1 ? 1 : 0;
+  std::vector<double> t[2];
+  for (int v = 0; v < 2; v++) {
+    t[v].assign(2 * H, 0.0);
+    F->plan.gemm_choice[pi].assign(2 * H, (uint8_t) v);
+    drop_graphs(F);
+    for (int rep = 0; rep < 2; rep++) {
+      taucs_b200_profile(1);
+      const int rc = numeric_device(F, d_values, true);
+      std::vector<ProfEntry> log = prof_take_log();
+      taucs_b200_profile(0);
+      if (rc) {
+        F->plan.gemm_choice[pi].clear();
+        return -1;
+      }
+      if (rep == 0) continue;
+      for (const ProfEntry& e : log) {
+        if (e.tag < 0 || e.tag >= H) continue;
+        if (e.kc == KC_GEMM_PANEL) t[v][2 * e.tag] += e.ms;
+        if (e.kc == KC_GEMM_U) t[v][2 * e.tag + 1] += e.ms;
+      }
+    }
+  }
+  std::vector<uint8_t>& c = F->plan.gemm_choice[pi];
+  double before = 0.0, after = 0.0;
+  for (int i = 0; i < 2 * H; i++) {
+    c[i] = t[1][i] < t[0][i] ? 1 : 0;
+    before += t[0][i];
+    after += t[c[i]][i];
+    if (choices) choices[i] = c[i];
+  }
+  drop_graphs(F);
+  tprintf("\t\tautotune (%s fronts): GEMM time %.2f ms with the default variants, %.2f ms with the chosen ones\n",
+          pi ? "FP32" : "FP64", before, after);
+  return 0;
+}
+
 long taucs_b200_launch_count(int reset) {
   return reset ? g_launches.exchange(0) : g_launches.load();
 }

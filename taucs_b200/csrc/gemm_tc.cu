@@ -10,17 +10,19 @@
 // accumulated in FP32 in tensor memory, which keeps FP32-level accuracy.  One CTA
 // owns a 128 x 128 tile of the lower trapezoid of C:
 //
-//   warps 0-3  producers: each thread loads one row of the A and B K-slabs
-//              (coalesced, 32 threads = 32 consecutive rows), splits every
-//              value into TF32 hi/lo once, and stores the four operand parts
-//              into a 3-stage shared-memory ring in the canonical K-major,
-//              no-swizzle layout (8-row x 16-byte core matrices);
-//   warp 4     allocates 128 TMEM columns; one thread issues
+//   producers  128 or 256 threads (warps 0-3 or 0-7): each loads one row of
+//              the A and B K-slabs, or half of it (coalesced, 32 threads =
+//              32 consecutive rows), splits every value into TF32 hi/lo
+//              once, and stores the four operand parts into a 2- or 3-stage
+//              shared-memory ring in the canonical K-major, no-swizzle
+//              layout (8-row x 16-byte core matrices);
+//   MMA warp   allocates 128 TMEM columns; one thread issues
 //              tcgen05.mma.cta_group::1.kind::tf32 (M = 128, N = the tile's
 //              columns rounded up to 16, K = 8) and frees each ring stage
 //              with tcgen05.commit;
-//   epilogue   warps 0-3 read their 32 TMEM lanes (tcgen05.ld 32x32b) and
-//              subtract the product from C, 32 consecutive rows per store.
+//   epilogue   the producer warps read their 32 TMEM lanes (tcgen05.ld
+//              32x32b) and subtract the product from C, 32 consecutive rows
+//              per store.
 //
 // Every mbarrier wait is bounded; a wait that gives up records
 // NUMERIC_TIMEOUT in the status word and the CTA winds down (no further MMAs,
@@ -345,15 +347,16 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
 
 }  // namespace
 
-// two-stage ring: 65 KB of shared memory, three CTAs per SM
-constexpr int TC_RING = 2, TC_MINB = 3, TC_NPROD = 128;
-
+// variant 0: two-stage ring (65 KB), 128 producers, three CTAs per SM;
+// variant 1: three-stage ring (97 KB), 256 producers, two CTAs per SM
 bool gemm_tc_init() {
   static int state = 0;   // 0 unknown, 1 ready, -1 unavailable
   if (state == 0) {
-    const cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<TC_RING, TC_MINB, TC_NPROD>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int) tc_smem<TC_RING>());
-    state = (e == cudaSuccess) ? 1 : -1;
+    const cudaError_t e0 = cudaFuncSetAttribute(k_gemm_tc<2, 3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int) tc_smem<2>());
+    const cudaError_t e1 = cudaFuncSetAttribute(k_gemm_tc<3, 2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int) tc_smem<3>());
+    state = (e0 == cudaSuccess && e1 == cudaSuccess) ? 1 : -1;
   }
   return state == 1;
 }
@@ -364,9 +367,14 @@ int gemm_tc_tiles(int rows, int cols) {
   return t;
 }
 
-void launch_gemm_tc(int gx, int nb, const int* list, const FrontDesc* fronts, float* L, float* U, int c_lo, int c_hi,
-                    int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
-  k_gemm_tc<TC_RING, TC_MINB, TC_NPROD><<<dim3(gx, nb), TC_NPROD + 32, tc_smem<TC_RING>(), st>>>(list, fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
+void launch_gemm_tc(int variant, int gx, int nb, const int* list, const FrontDesc* fronts, float* L, float* U,
+                    int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
+  if (variant == 1)
+    k_gemm_tc<3, 2, 256><<<dim3(gx, nb), 256 + 32, tc_smem<3>(), st>>>(list, fronts, L, U, c_lo, c_hi, k_lo, k_hi,
+                                                                       mode, status);
+  else
+    k_gemm_tc<2, 3, 128><<<dim3(gx, nb), 128 + 32, tc_smem<2>(), st>>>(list, fronts, L, U, c_lo, c_hi, k_lo, k_hi,
+                                                                       mode, status);
 }
 
 }  // namespace tb

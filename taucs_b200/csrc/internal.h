@@ -120,6 +120,10 @@ struct Plan {
   double ea_bytes = 0.0;
   double solve_bytes = 0.0;
   int max_front = 0, max_s = 0;
+  // GEMM variant per level and product, [2h] panel updates, [2h + 1] the
+  // update matrix; index 0 for FP64 fronts, 1 for FP32 fronts.  Empty or 0:
+  // the default variant; set by the autotuner from measured times.
+  std::vector<uint8_t> gemm_choice[2];
 };
 
 int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, Plan* P);

@@ -92,10 +92,13 @@ constexpr int NUMERIC_TIMEOUT = -4;
 // accumulator); same modes and arguments as the mma.sync GEMM.
 // gemm_tc_init() sets the kernel's shared-memory limit once and reports
 // whether the kernel is usable; gemm_tc_tiles() = CTAs per front.
+// variant 0: 2-stage ring, 128 producer threads, 3 CTAs per SM; variant 1:
+// 3-stage ring, 256 producer threads, 2 CTAs per SM (chosen per level and
+// product by the autotuner)
 bool gemm_tc_init();
 int gemm_tc_tiles(int rows, int cols);
-void launch_gemm_tc(int gx, int nb, const int* list, const FrontDesc* fronts, float* L, float* U, int c_lo, int c_hi,
-                    int k_lo, int k_hi, int mode, int* status, cudaStream_t st);
+void launch_gemm_tc(int variant, int gx, int nb, const int* list, const FrontDesc* fronts, float* L, float* U,
+                    int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st);
 
 // multi-RHS solve, device vectors in permuted order: X (n x nrhs, ld) from
 // B (n x nrhs, ld); W scratch of P.v_len * SOLVE_NRHS doubles, Y n *
@@ -122,6 +125,14 @@ void count_launch(long k = 1);
 enum KernelClass { KC_SMALL = 0, KC_BUILD, KC_POTRF, KC_TRSM, KC_GEMM_PANEL, KC_GEMM_U, KC_SOLVE_FWD,
                    KC_SOLVE_BWD, KC_OTHER, KC_COUNT };
 bool prof_enabled();
+// every profiled launch: its class, the tag set when it was issued (the
+// numeric factorization tags launches with their level) and its device time
+struct ProfEntry {
+  int kc, tag;
+  float ms;
+};
+void prof_tag(int tag);
+std::vector<ProfEntry> prof_take_log();
 void prof_begin(int kc, cudaStream_t st);
 void prof_end(int kc, cudaStream_t st, double flops, double bytes);
 

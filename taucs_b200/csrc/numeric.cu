@@ -706,13 +706,16 @@ static double front_bytes(const Plan& P, const FrontDesc& F) {
   return build_bytes(P, F);
 }
 
-// Tile shape per launch.  Measured on the 64^3 benchmark: the 64x64 tiles
-// (4 warps, 164 registers, 3 CTAs per SM) reach 24 TF/s on the update
-// matrices; 128x128 tiles (8 warps, 228 registers) fit one CTA per SM and
-// reach 19 TF/s, so they are not selected.
-static bool big_tiles(int maxr, int maxc, int tiles64) {
-  (void) maxr; (void) maxc; (void) tiles64;
-  return false;
+// GEMM variant of level h for the panel updates (kind 0) or the update
+// matrix (kind 1): FP64 fronts choose between 64x64 tiles (4 warps, 3 CTAs
+// per SM; the default, 24 TF/s on the 64^3 update matrices) and 128x128
+// tiles (8 warps, one CTA per SM; 19 TF/s there), FP32 fronts between the
+// two tcgen05 variants.  The choice comes from the autotuner's measurements
+// (Plan::gemm_choice), the default variant otherwise.
+template <typename T>
+static bool gemm_alt(const Plan& P, int h, int kind) {
+  const std::vector<uint8_t>& c = P.gemm_choice[sizeof(T) == 4 ? 1 : 0];
+  return (size_t) (2 * h + kind) < c.size() && c[2 * h + kind] != 0;
 }
 
 template <typename T>
@@ -726,14 +729,15 @@ static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, 
         blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
 }
 
-// FP32 fronts take the tcgen05 kernel (gemm_tc.cu) when it is available
-static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, float* L, float* U,
+// FP32 fronts take the tcgen05 kernel (gemm_tc.cu) when it is available;
+// `alt` selects its second variant
+static void launch_gemm(bool alt, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, float* L, float* U,
                         int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
   if (gemm_tc_init()) {
-    launch_gemm_tc(gx128, nb, blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
+    launch_gemm_tc(alt ? 1 : 0, gx128, nb, blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
     return;
   }
-  launch_gemm<float>(big, gx128, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
+  launch_gemm<float>(false, gx128, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
 }
 
 template <typename T>
@@ -763,6 +767,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
   count_launch();
   for (int h = 0; h < P.n_levels; h++) {
     const LevelPlan& LP = P.levels[h];
+    prof_tag(h);
     // small fronts, in size classes so that the shared-memory request fits the class
     const int ns = (int) LP.small_fronts.size();
     if (ns > 0) {
@@ -858,7 +863,8 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
       }
       if (gx64 == 0) return;
       prof_begin(KC_GEMM_PANEL, st);
-      launch_gemm(big_tiles(maxr, maxc, gx64 * nb), gx, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, 0, status, st);
+      (void) maxr; (void) maxc;
+      launch_gemm(gemm_alt<T>(P, h, 0), gx, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, 0, status, st);
       prof_end(KC_GEMM_PANEL, st, fg, bg);
       count_launch();
     };
@@ -893,11 +899,13 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
           bu += 16.0 * m * (m + 1.0) / 2.0 + 8.0 * m * F.s;
         }
       prof_begin(KC_GEMM_U, st);
-      launch_gemm(big_tiles(maxm, maxm, gx_u64 * nb), gx_u, gx_u64, nb, blst, D, L, U, 0, 0, 0, 0, 1, status, st);
+      (void) maxm;
+      launch_gemm(gemm_alt<T>(P, h, 1), gx_u, gx_u64, nb, blst, D, L, U, 0, 0, 0, 0, 1, status, st);
       prof_end(KC_GEMM_U, st, fu, bu);
       count_launch();
     }
   }
+  prof_tag(-1);
   return (int) cudaGetLastError();
 }
 

@@ -12,7 +12,7 @@ namespace {
 
 struct Rec {
   cudaEvent_t a, b;
-  int kc;
+  int kc, tag;
   double flops, bytes;
 };
 
@@ -23,7 +23,8 @@ std::vector<cudaEvent_t> g_pool;
 cudaEvent_t g_open = nullptr;
 double g_ms[KC_COUNT], g_flops[KC_COUNT], g_bytes[KC_COUNT];
 long g_n[KC_COUNT];
-std::vector<std::pair<int, float>> g_log;   // (class, ms) of every launch, in order
+std::vector<ProfEntry> g_log;   // every launch, in order
+int g_tag = -1;
 
 cudaEvent_t get_event() {
   if (!g_pool.empty()) {
@@ -42,7 +43,7 @@ void drain() {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, r.a, r.b);
     g_ms[r.kc] += ms;
-    if (g_log.size() < (size_t) 1 << 20) g_log.emplace_back(r.kc, ms);
+    if (g_log.size() < (size_t) 1 << 20) g_log.push_back(ProfEntry{r.kc, r.tag, ms});
     g_flops[r.kc] += r.flops;
     g_bytes[r.kc] += r.bytes;
     g_n[r.kc] += 1;
@@ -55,6 +56,16 @@ void drain() {
 }  // namespace
 
 bool prof_enabled() { return g_on; }
+
+void prof_tag(int tag) { g_tag = tag; }
+
+std::vector<ProfEntry> prof_take_log() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  drain();
+  std::vector<ProfEntry> out;
+  out.swap(g_log);
+  return out;
+}
 
 void prof_begin(int kc, cudaStream_t st) {
   (void) kc;
@@ -69,7 +80,7 @@ void prof_end(int kc, cudaStream_t st, double flops, double bytes) {
   std::lock_guard<std::mutex> lk(g_mu);
   cudaEvent_t b = get_event();
   cudaEventRecord(b, st);
-  g_recs.push_back(Rec{g_open, b, kc, flops, bytes});
+  g_recs.push_back(Rec{g_open, b, kc, g_tag, flops, bytes});
   if (g_recs.size() > 4096) drain();
 }
 
@@ -93,8 +104,8 @@ long taucs_b200_profile_log(int* kernel_class, float* ms, long cap) {
   drain();
   const long n = (long) g_log.size();
   for (long i = 0; i < n && i < cap; i++) {
-    if (kernel_class) kernel_class[i] = g_log[i].first;
-    if (ms) ms[i] = g_log[i].second;
+    if (kernel_class) kernel_class[i] = g_log[i].kc;
+    if (ms) ms[i] = g_log[i].ms;
   }
   return n;
 }
