@@ -83,7 +83,8 @@ struct FrontDesc {
 struct LevelPlan {
   int front_begin, front_end;      // fronts of this level (device order)
   // solve: big fronts are split into 64-row blocks, one CTA each
-  std::vector<int2_> solve_fwd_blocks;   // (front, row block)
+  std::vector<int2_> solve_fwd_blocks;   // (front, row block): the n_fwd_diag diagonal blocks first
+  int n_fwd_diag = 0;
   std::vector<int2_> solve_bwd_blocks;   // (front, column block), last block first
   std::vector<int2_> solve_l21_tasks;    // (front, column block << 16 | row chunk)
   // small fronts, fused kernel (sorted by order f); the first small_warp of

@@ -357,6 +357,7 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
       LP.front_begin = fi;
       while (fi < nf && P.fronts[fi].level == h) fi++;
       LP.front_end = fi;
+      std::vector<int2_> fwd_upd;   // forward blocks of update rows, after the diagonal ones
       for (int i = LP.front_begin; i < LP.front_end; i++) {
         const FrontDesc& F = P.fronts[i];
         if (F.f <= SMALL_F_MAX) {
@@ -374,13 +375,16 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
             for (int r0 = (c0 / BUILD_TR) * BUILD_TR; r0 < m; r0 += BUILD_TR)
               LP.build_tiles.push_back(Tile{i, r0, -1 - c0});
           const int nrb = (F.f + PANEL_NB - 1) / PANEL_NB, nbs = (F.s + PANEL_NB - 1) / PANEL_NB;
-          for (int r = 0; r < nrb; r++) LP.solve_fwd_blocks.push_back(int2_{i, r});
+          for (int r = 0; r < nbs; r++) LP.solve_fwd_blocks.push_back(int2_{i, r});
+          for (int r = nbs; r < nrb; r++) fwd_upd.push_back(int2_{i, r});
           for (int k = nbs - 1; k >= 0; k--) LP.solve_bwd_blocks.push_back(int2_{i, k});
           const int nch = (m + SOLVE_RCH - 1) / SOLVE_RCH;
           for (int k = 0; k < nbs; k++)
             for (int c = 0; c < nch; c++) LP.solve_l21_tasks.push_back(int2_{i, (k << 16) | c});
         }
       }
+      LP.n_fwd_diag = (int) LP.solve_fwd_blocks.size();
+      LP.solve_fwd_blocks.insert(LP.solve_fwd_blocks.end(), fwd_upd.begin(), fwd_upd.end());
       // the fused small-front kernel is launched per size class
       std::stable_sort(LP.small_fronts.begin(), LP.small_fronts.end(),
                        [&](int a, int b) { return P.fronts[a].f < P.fronts[b].f; });

@@ -16,6 +16,7 @@
 // then the L11^T substitution, and scatter x at the columns.  Up to
 // SOLVE_NRHS right-hand sides share every read of L.
 #include <mutex>
+#include <type_traits>
 
 #include "factor.h"
 #include "kernels.h"
@@ -241,8 +242,10 @@ k_bwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fro
 // can hang.
 
 constexpr int BR = PANEL_NB;   // rows per block
-template <typename T>
-constexpr size_t bwd_smem() { return 2 * BR * (BR + 1) * sizeof(T); }
+// dynamic shared memory: L_kk^-1, plus one staged 64x64 block of L11 for 8
+// columns
+template <typename T, int NQ>
+constexpr size_t bwd_smem() { return (NQ >= 8 ? 2 : 1) * BR * (BR + 1) * sizeof(T); }
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -252,6 +255,21 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// the same wait for one warp: lane 0 polls, the warp follows it
+__device__ void wait_epoch_warp(const int* flag, int epoch, int* status) {
+  if ((threadIdx.x & 31) == 0) {
+    int it = 0;
+    while (ld_acquire(flag) != epoch) {
+      if (++it > (1 << 22)) {
+        atomicExch(status, SOLVE_TIMEOUT);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  __syncwarp();   // orders the lanes' later loads after lane 0's acquire
 }
 
 __device__ void wait_epoch(const int* flag, int epoch, int* status) {
@@ -268,7 +286,30 @@ __device__ void wait_epoch(const int* flag, int epoch, int* status) {
   __syncthreads();
 }
 
-template <typename T, int NQ, int WS>
+// Forward solve of big fronts.  Diagonal block r of L11 gives
+// y_r = L_rr^-1 (w_r - sum_{k<r} L_rk y_k), chained to block r-1 by
+// release/acquire flags; update rows i get w_i - sum_k L_ik y_k.
+//   FWD_ALL   one launch over all blocks of a level: every block waits for
+//             the blocks k it needs, one at a time (short chains);
+//   FWD_CHAIN the diagonal blocks of a level with long chains: everything
+//             but the last term is done before waiting -- M = L_rr^-1
+//             L_{r,r-1} at kernel start, the sum over k < r-1 and
+//             c = L_rr^-1 (w_r - ...) -- so after the flag of block r-1
+//             only y_r = c - M y_{r-1} remains (one 64x64 product);
+//   FWD_UPD   after FWD_CHAIN, the update-row blocks, with every y_k
+//             already published.
+// In the last diagonal block rows >= s are update rows of the same front.
+constexpr int FWD_ALL = 0, FWD_CHAIN = 1, FWD_UPD = 2;
+// levels whose largest big front has at least this many columns use
+// FWD_CHAIN + FWD_UPD (the split pays off on long chains only)
+constexpr int FWD_CHAIN_MIN_S = 2048;
+
+template <typename T, int MODE>
+constexpr size_t fwd_smem() {
+  return MODE == FWD_CHAIN ? 2 * BR * (BR + 1) * sizeof(T) : MODE == FWD_ALL ? BR * (BR + 1) * sizeof(T) : 0;
+}
+
+template <typename T, int NQ, int WS, int MODE>
 __global__ void __launch_bounds__(128)
 k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ children, const int* __restrict__ maps, const int* __restrict__ rows,
@@ -277,43 +318,69 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   __shared__ T wv[BR][NQ];
   __shared__ T yk[BR][NQ];
   __shared__ T part[BR][NQ];
-  // dg[col][row]: rows < bw hold L_rr^-1 (lower), rows >= bw the update
-  // rows of L that share this 64-row block (last diagonal block only)
-  __shared__ T dg[BR][BR + 1];
+  __shared__ T ykw[4][BR / 2][NQ];   // per warp: the entries of y_k it needs
+  __shared__ int rng[2];
+  // CHAIN: dg[col][row] holds L_rr^-1 in rows < bw and the front's own
+  // update rows of L (last diagonal block) in rows >= bw; mx[col][row] holds
+  // L_{r,r-1}, then M = L_rr^-1 L_{r,r-1} in rows < bw
+  extern __shared__ __align__(16) unsigned char fsm[];
+  T (*dg)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(fsm);
+  T (*mx)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(fsm) + BR;
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int r = bk.b, f = F.f, s = F.s;
   const int nbs = (s + BR - 1) / BR;
   const int r0 = r * BR, nr = min(BR, f - r0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int row = tid % BR, half = tid / BR;
   T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   const T* P = L + F.l_off;
+  constexpr bool CHAIN = MODE == FWD_CHAIN;
+  const bool diag = CHAIN || (MODE == FWD_ALL && r < nbs);
+  const int bw = diag ? min(BR, s - r0) : 0;
 
-  if (r < nbs) {
-    // stage the block's inverse now, off the chain's critical path
-    const int bw = min(BR, s - r0);
+  if (diag) {
+    // staged now, off the chain's critical path
     const T* Di = Dinv + F.dinv_off + (size_t) r * BR * BR;
     for (int e = tid; e < BR * BR; e += 128) {
       const int i = e % BR, j = e / BR;
       T v = 0.0;
       if (j < bw && i < nr) v = (i < bw) ? (i >= j ? Di[i + j * BR] : T(0)) : P[(r0 + i) + (size_t) (r0 + j) * f];
       dg[j][i] = v;
+      if (CHAIN && r > 0) mx[j][i] = (i < nr) ? P[(r0 + i) + (size_t) (r0 - BR + j) * f] : T(0);
     }
+  }
+  if (CHAIN && r > 0) {
+    // M = L_rr^-1 L_{r,r-1} in rows < bw (the inverse is lower triangular),
+    // at kernel start, independent of the chain
+    __syncthreads();
+    T m[BR / 2];
+#pragma unroll
+    for (int jj = 0; jj < BR / 2; jj++) m[jj] = 0.0;
+    if (row < bw)
+      for (int t = 0; t <= row; t++) {
+        const T d = dg[t][row];
+#pragma unroll
+        for (int jj = 0; jj < BR / 2; jj++) m[jj] += d * mx[half * (BR / 2) + jj][t];
+      }
+    __syncthreads();
+    if (row < bw)
+#pragma unroll
+      for (int jj = 0; jj < BR / 2; jj++) mx[half * (BR / 2) + jj][row] = m[jj];
   }
   for (int k = tid; k < BR * NQ; k += 128) {
     const int i = k % BR, q = k / BR;
     wv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : 0.0;
   }
   __syncthreads();
-  __shared__ int rng[2];
   for (int ci = F.child_begin; ci < F.child_end; ci++) {
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
     if (warp < 2) {
-      const int r = warp_lower_bound(mp, mc, warp == 0 ? r0 : r0 + nr);
-      if (lane == 0) rng[warp] = r;
+      const int x = warp_lower_bound(mp, mc, warp == 0 ? r0 : r0 + nr);
+      if (lane == 0) rng[warp] = x;
     }
     __syncthreads();
     const int ia = rng[0], ib = rng[1];
@@ -326,31 +393,58 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     }
     __syncthreads();
   }
-  // contributions of the solved blocks to the left; this thread's 32
-  // entries of L[r, k] are loaded before waiting for y_k
-  const int row = tid % BR, half = tid / BR;
+  // contributions of the solved blocks k < kend; this thread's 32 entries of
+  // L[r, k] are loaded before waiting for y_k
   T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
-  const int kend = r < nbs ? r : nbs;
-  for (int k = 0; k < kend; k++) {
-    const int bwk = min(BR, s - k * BR);
-    T lv[BR / 2];
-    const T* pc = P + (r0 + row) + (size_t) (k * BR + half * (BR / 2)) * f;
+  const int kend = CHAIN ? max(r - 1, 0) : diag ? r : nbs;
+  if constexpr (NQ >= 8) {
+    // 8 columns: y_k staged once for the whole block (measured faster than
+    // the warp-level loop below at 8 columns)
+    for (int k = 0; k < kend; k++) {
+      const int bwk = min(BR, s - k * BR);
+      T lv[BR / 2];
+      const T* pc = P + (r0 + row) + (size_t) (k * BR + half * (BR / 2)) * f;
 #pragma unroll
-    for (int j = 0; j < BR / 2; j++)
-      lv[j] = (row < nr && half * (BR / 2) + j < bwk) ? pc[(size_t) j * f] : 0.0;
-    wait_epoch(flags + F.blk_off + k, epoch, status);
-    for (int e = tid; e < BR * NQ; e += 128) {
-      const int j = e % BR, q = e / BR;
-      yk[j][q] = (j < bwk && q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : 0.0;
+      for (int j = 0; j < BR / 2; j++)
+        lv[j] = (row < nr && half * (BR / 2) + j < bwk) ? pc[(size_t) j * f] : 0.0;
+      wait_epoch(flags + F.blk_off + k, epoch, status);
+      for (int e = tid; e < BR * NQ; e += 128) {
+        const int j = e % BR, q = e / BR;
+        yk[j][q] = (j < bwk && q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : 0.0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < BR / 2; j++)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) acc[q] += lv[j] * yk[half * (BR / 2) + j][q];
+      __syncthreads();
     }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < BR / 2; j++)
-#pragma unroll
-      for (int q = 0; q < NQ; q++) acc[q] += lv[j] * yk[half * (BR / 2) + j][q];
-    __syncthreads();
+  } else {
+    // without block-wide barriers: each warp polls the flags itself and
+    // stages the 32 entries of y_k its rows need
+    T (*yw)[NQ] = ykw[warp];
+    for (int k = 0; k < kend; k++) {
+      const int bwk = min(BR, s - k * BR);
+      T lv[BR / 2];
+      const T* pc = P + (r0 + row) + (size_t) (k * BR + half * (BR / 2)) * f;
+  #pragma unroll
+      for (int j = 0; j < BR / 2; j++)
+        lv[j] = (row < nr && half * (BR / 2) + j < bwk) ? pc[(size_t) j * f] : 0.0;
+      wait_epoch_warp(flags + F.blk_off + k, epoch, status);
+  #pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int j = half * (BR / 2) + lane;
+        yw[lane][q] = (j < bwk && q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : T(0);
+      }
+      __syncwarp();
+  #pragma unroll
+      for (int j = 0; j < BR / 2; j++)
+  #pragma unroll
+        for (int q = 0; q < NQ; q++) acc[q] += lv[j] * yw[j][q];
+      __syncwarp();
+    }
   }
   if (half == 1)
 #pragma unroll
@@ -360,10 +454,15 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 #pragma unroll
     for (int q = 0; q < NQ; q++) wv[row][q] -= acc[q] + part[row][q];
   __syncthreads();
-  if (r < nbs) {
-    // y_r = L_rr^-1 w_r: a 64x64 product split over the two thread halves
-    // instead of a 64-step substitution chain
-    const int bw = min(BR, s - r0);
+  if (!diag) {
+    for (int k = tid; k < nr * nrhs; k += 128) {
+      const int i = k % nr, q = k / nr;
+      Wf[r0 + i + (size_t) q * f] = wv[i][q];
+    }
+    return;
+  }
+  // c = L_rr^-1 w in rows < bw (into yk); update rows keep w
+  {
     T y[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) y[q] = 0.0;
@@ -377,41 +476,64 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 #pragma unroll
       for (int q = 0; q < NQ; q++) part[row][q] = y[q];
     __syncthreads();
-    if (half == 0 && row < bw)
+    if (half == 0)
 #pragma unroll
-      for (int q = 0; q < NQ; q++) yk[row][q] = y[q] + part[row][q];
+      for (int q = 0; q < NQ; q++) yk[row][q] = (row < bw) ? y[q] + part[row][q] : wv[row][q];
     __syncthreads();
-    if (bw < nr) {
-      // update rows inside the last diagonal block: w_i -= L[i, r] y_r
-      T u[NQ];
-#pragma unroll
-      for (int q = 0; q < NQ; q++) u[q] = 0.0;
-      if (row >= bw)
-        for (int j = half * (BR / 2); j < min(bw, half * (BR / 2) + BR / 2); j++) {
-          const T l = dg[j][row];
-#pragma unroll
-          for (int q = 0; q < NQ; q++) u[q] += l * yk[j][q];
-        }
-      if (half == 1)
-#pragma unroll
-        for (int q = 0; q < NQ; q++) part[row][q] = u[q];
-      __syncthreads();
-      if (half == 0 && row >= bw)
-#pragma unroll
-        for (int q = 0; q < NQ; q++) wv[row][q] -= u[q] + part[row][q];
+  }
+  // the critical step: y_r = c - M y_{r-1} (update rows: w - L_{i,r-1} y_{r-1})
+  if (CHAIN && r > 0) {
+    wait_epoch(flags + F.blk_off + r - 1, epoch, status);
+    for (int e = tid; e < BR * NQ; e += 128) {
+      const int j = e % BR, q = e / BR;
+      wv[j][q] = (q < nrhs) ? __ldcg(Wf + (r - 1) * BR + j + (size_t) q * f) : T(0);
     }
-    if (half == 0 && row < bw)
+    __syncthreads();
+    T u[NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) wv[row][q] = yk[row][q];
+    for (int q = 0; q < NQ; q++) u[q] = 0.0;
+#pragma unroll 8
+    for (int j = half * (BR / 2); j < half * (BR / 2) + BR / 2; j++) {
+      const T mv = mx[j][row];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) u[q] += mv * wv[j][q];
+    }
+    if (half == 1)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) part[row][q] = u[q];
+    __syncthreads();
+    if (half == 0)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) yk[row][q] -= u[q] + part[row][q];
+    __syncthreads();
+  }
+  if (bw < nr) {
+    // update rows inside the last diagonal block: w_i -= L[i, r] y_r
+    T u[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) u[q] = 0.0;
+    if (row >= bw)
+      for (int j = half * (BR / 2); j < min(bw, half * (BR / 2) + BR / 2); j++) {
+        const T l = dg[j][row];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) u[q] += l * yk[j][q];
+      }
+    if (half == 1)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) part[row][q] = u[q];
+    __syncthreads();
+    if (half == 0 && row >= bw)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) yk[row][q] -= u[q] + part[row][q];
     __syncthreads();
   }
   for (int k = tid; k < nr * nrhs; k += 128) {
     const int i = k % nr, q = k / nr;
-    Wf[r0 + i + (size_t) q * f] = wv[i][q];
+    Wf[r0 + i + (size_t) q * f] = yk[i][q];
   }
   __syncthreads();
   // the barrier orders every thread's writes before thread 0's release store
-  if (r < nbs && tid == 0) st_release(flags + F.blk_off + r, epoch);
+  if (tid == 0) st_release(flags + F.blk_off + r, epoch);
 }
 
 // x at the update rows of every big front of a level, gathered once into the
@@ -490,10 +612,10 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   __shared__ T xv[BR][NQ];
   __shared__ T xj[BR][NQ];
   __shared__ T red[BR][NQ];
+  __shared__ T xjw[4][BR / 2][NQ];   // per warp: the rows of x_j it needs
   extern __shared__ __align__(16) unsigned char bsmraw[];
-  T* bsm = reinterpret_cast<T*>(bsmraw);
-  T (*tile)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm);             // block of L11, [col][row]
-  T (*dgb)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsm + BR * (BR + 1));  // L_kk^-1, [row][col]
+  T (*dgb)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsmraw);                              // L_kk^-1, [row][col]
+  T (*tile)[BR + 1] = reinterpret_cast<T (*)[BR + 1]>(bsmraw) + BR;   // NQ >= 8: block of L11, [col][row]
   const int2_ bk = blocks[blockIdx.x];
   const FrontDesc F = fronts[bk.a];
   const int k = bk.b, f = F.f, s = F.s, m = f - s;
@@ -557,29 +679,70 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
       }
   }
   __syncthreads();
-  // solved blocks below, last first: the block of L11 is staged before the
-  // wait for x_j
   const int col = tid % BR, half = tid / BR;
-  for (int j = nbs - 1; j > k; j--) {
-    const int bwj = min(BR, s - j * BR);
-    for (int e = tid; e < BR * BR; e += 128) {
-      const int i = e % BR, c = e / BR;
-      tile[c][i] = (i < bwj && c < bw) ? P[(j * BR + i) + (size_t) (c0 + c) * f] : 0.0;
+  if constexpr (NQ >= 8) {
+    // 8 columns: the block of L11 is staged in shared memory before the wait
+    // for x_j (measured faster than the warp-level loop below at 8 columns)
+    for (int j = nbs - 1; j > k; j--) {
+      const int bwj = min(BR, s - j * BR);
+      for (int e = tid; e < BR * BR; e += 128) {
+        const int i = e % BR, c = e / BR;
+        tile[c][i] = (i < bwj && c < bw) ? P[(j * BR + i) + (size_t) (c0 + c) * f] : 0.0;
+      }
+      wait_epoch(flags + F.blk_off + j, epoch, status);
+      for (int e = tid; e < BR * NQ; e += 128) {
+        const int i = e % BR, q = e / BR;
+        xj[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : 0.0;
+      }
+      __syncthreads();
+      T acc[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+#pragma unroll 8
+      for (int i = half * (BR / 2); i < half * (BR / 2) + BR / 2; i++) {
+        const T l = tile[col][i];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) acc[q] += l * xj[i][q];
+      }
+      if (half == 1)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) red[col][q] = acc[q];
+      __syncthreads();
+      if (half == 0)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) xv[col][q] -= acc[q] + red[col][q];
+      __syncthreads();
     }
-    wait_epoch(flags + F.blk_off + j, epoch, status);
-    for (int e = tid; e < BR * NQ; e += 128) {
-      const int i = e % BR, q = e / BR;
-      xj[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : 0.0;
-    }
-    __syncthreads();
+  } else {
+  // solved blocks below, last first, without block-wide barriers: thread
+  // (col, half) keeps its partial sum over the rows of its half across all
+  // tiles (the 32 entries of L it needs are loaded before the wait); each
+  // warp polls the flags itself and stages the 32 rows of x_j it needs; the
+  // two halves are combined once at the end
+  {
     T acc[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) acc[q] = 0.0;
-#pragma unroll 8
-    for (int i = half * (BR / 2); i < half * (BR / 2) + BR / 2; i++) {
-      const T l = tile[col][i];
+    const T* pcol = P + (size_t) (c0 + col) * f + half * (BR / 2);
+    T (*xw)[NQ] = xjw[warp];
+    for (int j = nbs - 1; j > k; j--) {
+      const int bwj = min(BR, s - j * BR);
+      T lv[BR / 2];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) acc[q] += l * xj[i][q];
+      for (int t = 0; t < BR / 2; t++)
+        lv[t] = (col < bw && half * (BR / 2) + t < bwj) ? __ldg(pcol + (size_t) j * BR + t) : T(0);
+      wait_epoch_warp(flags + F.blk_off + j, epoch, status);
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int i = half * (BR / 2) + lane;
+        xw[lane][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + (size_t) j * BR + i + (size_t) q * f) : T(0);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < BR / 2; t++)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) acc[q] += lv[t] * xw[t][q];
+      __syncwarp();
     }
     if (half == 1)
 #pragma unroll
@@ -589,6 +752,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 #pragma unroll
       for (int q = 0; q < NQ; q++) xv[col][q] -= acc[q] + red[col][q];
     __syncthreads();
+  }
   }
   // x_k = L_kk^-T v_k from the staged inverse, split over the two halves
   {
@@ -633,10 +797,19 @@ template <typename T>
 static void solve_attrs() {
   static bool done = false;
   if (done) return;
-  cudaFuncSetAttribute(k_bwd_big<T, 2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
-  cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
-  cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
-  cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T>());
+  // static + dynamic shared memory of these kernels can exceed the default
+  // 48 KB (8 columns in FP64)
+  cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+  cudaFuncSetAttribute(k_fwd_big<T, 4, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+  cudaFuncSetAttribute(k_fwd_big<T, 8, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+  cudaFuncSetAttribute(k_fwd_big<T, 1, 1, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+  cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
+  cudaFuncSetAttribute(k_fwd_big<T, 4, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
+  cudaFuncSetAttribute(k_fwd_big<T, 8, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
+  cudaFuncSetAttribute(k_bwd_big<T, 2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 2>());
+  cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 4>());
+  cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
+  cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
   done = true;
 }
 
@@ -677,15 +850,27 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       const int nb = (int) LP.solve_fwd_blocks.size();
       if (nb > 0) {
         const int2_* bl = D.sfwd + D.sfwd_off[h];
+        const int nd = LP.n_fwd_diag, nu = nb - nd;
         // one right-hand side runs the two-column variant, measured faster
         // than a one-column instantiation (columns >= nrhs are skipped)
-        if (nq <= 2)
-          k_fwd_big<T, 2, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
-        else if (nq <= 4)
-          k_fwd_big<T, 4, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
-        else
-          k_fwd_big<T, 8, SOLVE_NRHS><<<nb, 128, 0, st>>>(bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
-        count_launch();
+        auto run = [&](auto nqc) {
+          constexpr int Q = decltype(nqc)::value;
+          if (LP.max_s_big >= FWD_CHAIN_MIN_S) {
+            k_fwd_big<T, Q, SOLVE_NRHS, FWD_CHAIN><<<nd, 128, fwd_smem<T, FWD_CHAIN>(), st>>>(
+                bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
+            if (nu)
+              k_fwd_big<T, Q, SOLVE_NRHS, FWD_UPD><<<nu, 128, 0, st>>>(bl + nd, D.fronts, D.children, D.maps, D.rows,
+                                                                      L, Dinv, Bq, ld, W, nq, flags, ef, status);
+            count_launch(nu ? 2 : 1);
+          } else {
+            k_fwd_big<T, Q, SOLVE_NRHS, FWD_ALL><<<nb, 128, fwd_smem<T, FWD_ALL>(), st>>>(
+                bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
+            count_launch();
+          }
+        };
+        if (nq <= 2) run(std::integral_constant<int, 2>());
+        else if (nq <= 4) run(std::integral_constant<int, 4>());
+        else run(std::integral_constant<int, 8>());
       }
       prof_end(KC_SOLVE_FWD, st, 0.0, by);
     }
@@ -711,11 +896,11 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
         if (nq <= 2)
-          k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 2>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
-          k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 4>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else
-          k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
+          k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 8>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         count_launch();
       }
       const int ns = (int) LP.small_fronts.size();
@@ -817,8 +1002,8 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
     }
     const int nb = (int) LP.solve_fwd_blocks.size();
     if (nb > 0) {
-      k_fwd_big<double, 1, 1><<<nb, 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, Dinv, B,
-                                          ld, W, 1, flags, ef, status);
+      k_fwd_big<double, 1, 1, FWD_ALL><<<nb, 128, fwd_smem<double, FWD_ALL>(), st>>>(
+          D.sfwd + D.sfwd_off[h], D.fronts, D.children, D.maps, D.rows, L, Dinv, B, ld, W, 1, flags, ef, status);
       count_launch();
     }
   }
@@ -830,7 +1015,7 @@ static int launch_solve_noalloc(const Plan& P, const DevPlan& D, const double* L
       k_gather_upd<double, 1><<<(int) LP.solve_fwd_blocks.size(), 128, 0, st>>>(D.sfwd + D.sfwd_off[h], D.fronts, D.rows,
                                                                          X, ld, W, 1);
       count_launch();
-      k_bwd_big<double, 1, 1, false><<<nb, 128, bwd_smem<double>(), st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, Dinv, X, ld, W, nullptr, 1,
+      k_bwd_big<double, 1, 1, false><<<nb, 128, bwd_smem<double, 1>(), st>>>(D.sbwd + D.sbwd_off[h], D.fronts, D.rows, L, Dinv, X, ld, W, nullptr, 1,
                                                  flags, eb, status);
       count_launch();
     }
