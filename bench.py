@@ -426,7 +426,10 @@ def serve_stream(tb, S, reqs, rate, rng):
 def fp64_one_at_a_time(tb, reqs):
     """The same requests solved one after another through the FP64 C API
     (patterns analysed beforehand, as the server caches them): permute,
-    factor, solve, un-permute per request."""
+    factor, solve, un-permute per request.  Two untimed passes over the
+    sample first, so that every factor replays its recorded launch sequences
+    in the timed pass (the steady state of a long-running caller, as for the
+    server)."""
     cache = {}
     for A, _, pk in reqs:
         if pk not in cache:
@@ -434,13 +437,19 @@ def fp64_one_at_a_time(tb, reqs):
             F = tb.factor_symbolic(A.permute(p, ip))
             F.set_precision(0)
             cache[pk] = (p, ip, F)
+
+    def one_pass():
+        for A, B, pk in reqs:
+            p, ip, F = cache[pk]
+            if F.numeric(A.permute(p, ip)) != 0:
+                raise RuntimeError("FP64 factor failed")
+            X = np.empty_like(B)
+            X[p, :] = F.solve(np.ascontiguousarray(B[p, :]))
+
+    one_pass()
+    one_pass()
     t0 = time.perf_counter()
-    for A, B, pk in reqs:
-        p, ip, F = cache[pk]
-        if F.numeric(A.permute(p, ip)) != 0:
-            raise RuntimeError("FP64 factor failed")
-        X = np.empty_like(B)
-        X[p, :] = F.solve(np.ascontiguousarray(B[p, :]))
+    one_pass()
     dt = time.perf_counter() - t0
     for _, _, F in cache.values():
         F.free()

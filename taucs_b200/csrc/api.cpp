@@ -101,7 +101,7 @@ int run_graphed(Factor* F, const GraphKey& key, cudaStream_t st, const std::func
   Factor::Graph& g = F->graphs[key];
   if (!g.seen) {
     g.seen = true;
-    return record(st);
+    if (!F->graph_first_use) return record(st);
   }
   if (!g.exec) {
     if (!F->cap_stream && cudaStreamCreateWithFlags(&F->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {

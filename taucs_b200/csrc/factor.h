@@ -84,11 +84,15 @@ struct Factor {
   };
   std::map<std::array<uint64_t, 6>, Graph> graphs;
   cudaStream_t cap_stream = nullptr;
+  // record a key's graph on its first run instead of its second: for factors
+  // whose buffers are reused by construction (request server instances), so
+  // the one eager pass buys nothing
+  bool graph_first_use = false;
 };
 
 using GraphKey = std::array<uint64_t, 6>;
-// Enqueues record(stream) on st: the first time for a key eagerly, then
-// recorded once into a CUDA graph and replayed.  Eager whenever per-launch
+// Enqueues record(stream) on st: the first time for a key eagerly (unless
+// F->graph_first_use), then recorded once into a CUDA graph and replayed.  Eager whenever per-launch
 // profiling is on or TAUCS_B200_NO_GRAPHS is set.  Returns record's result
 // (0 or a cudaError_t).
 int run_graphed(Factor* F, const GraphKey& key, cudaStream_t st, const std::function<int(cudaStream_t)>& record);

@@ -98,6 +98,7 @@ struct Pattern {
   Factor* proto = nullptr;    // symbolic factor + plan (host only)
   size_t inst_bytes = 0;
   int state = 0;              // 0 being built, 1 ready, -1 failed
+  int n_created = 0;          // instances made so far
 };
 
 struct Instance {
@@ -366,9 +367,9 @@ class Server {
 
   // An instance for one request, in this order of preference: the idle
   // instance that holds exactly these values (solve only); an idle instance
-  // of the pattern without values; a new instance while the pattern has
-  // fewer than MAX_INSTANCES_PER_PATTERN and the budget allows; the least
-  // recently used idle instance of the pattern; after evicting idle
+  // of the pattern without values; the least recently used idle instance of
+  // the pattern; a new instance while the pattern has fewer than
+  // MAX_INSTANCES_PER_PATTERN and the budget allows; after evicting idle
   // instances of other patterns, least recently used first, a new instance;
   // otherwise wait for a running request to finish.
   Instance* acquire(Pattern* P, uint64_t vkey, bool* hit) {
@@ -395,10 +396,12 @@ class Server {
         if (!I->has_values && !empty) empty = I.get();
         if (I->has_values && (!lru || I->last_use < lru->last_use)) lru = I.get();
       }
-      Instance* take = empty;
+      // an idle instance of the pattern is reused before a new one is made:
+      // a new instance starts cold (device buffers, launch graphs), so
+      // instances are only added while all of the pattern's are busy
+      Instance* take = empty ? empty : lru;
       if (!take && count < MAX_INSTANCES_PER_PATTERN && in_use_ + P->inst_bytes <= budget_)
         return create(P, lk, hit);
-      if (!take) take = lru;
       if (take) {
         take->busy = true;
         take->has_values = false;
@@ -442,6 +445,10 @@ class Server {
     I->last_use = ++tick_;
     Instance* raw = I.get();
     instances_.push_back(std::move(I));
+    // the pattern's first instance runs every launch sequence once eagerly
+    // (module loading and kernel attributes happen outside any capture); the
+    // later ones record their graphs on first use
+    const bool first = P->n_created++ == 0;
     lk.unlock();
     Factor* F = new Factor();
     F->n = P->proto->n;
@@ -450,6 +457,7 @@ class Server {
     F->colptr = P->proto->colptr;
     F->rowind = P->proto->rowind;
     F->precision = 1;
+    F->graph_first_use = !first;
     lk.lock();
     raw->F = F;
     *hit = false;
