@@ -85,6 +85,17 @@ taucs_ccs_matrix* taucs_dccs_permute_symmetrically(taucs_ccs_matrix* A, int* per
 void              taucs_ccs_times_vec(taucs_ccs_matrix* A, void* X, void* B);
 void              taucs_dccs_times_vec(taucs_ccs_matrix* A, double* X, double* B);
 
+/* binary files (src/taucs_ccs_io.c:31-113, :966-1052; matrix writer after
+ * matlab/taucs_ccs_write_binary.m): int nrows, ncols, flags; int
+ * colptr[ncols+1]; int rowind[nnz]; values[nnz], native byte order; vectors
+ * are n raw values.  Double and single values.  Unlike the reference, the
+ * readers return NULL on a missing, short or malformed file (decreasing
+ * colptr, row index out of range) instead of asserting or reading garbage. */
+taucs_ccs_matrix* taucs_ccs_read_binary(char* filename);
+int               taucs_b200_ccs_write_binary(taucs_ccs_matrix* A, char* filename);
+void*             taucs_vec_read_binary(int n, int flags, char* filename);
+int               taucs_vec_write_binary(int n, int flags, void* v, char* filename);
+
 /* vector permutes (src/taucs_vec_base.c:194-206): pv[i] = v[p[i]];
  * v[invp[i]] = pv[i] */
 void taucs_vec_permute(int n, int flags, void* v, void* pv, int p[]);

@@ -133,6 +133,12 @@ class Ref:
         L.ref_factor_symbolic.argtypes = [C.c_void_p, _i32p, _i32p, _i32p, _i32p, _i64p, _i32p]
         L.ref_factor_values.argtypes = [C.c_void_p, _i64p, _f64p]
         L.taucs_logfile.argtypes = [C.c_char_p]
+        L.taucs_ccs_read_binary.restype = C.c_void_p
+        L.taucs_ccs_read_binary.argtypes = [C.c_char_p]
+        L.taucs_vec_read_binary.restype = C.c_void_p
+        L.taucs_vec_read_binary.argtypes = [C.c_int, C.c_int, C.c_char_p]
+        L.taucs_vec_write_binary.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_char_p]
+        L.ref_free.argtypes = [C.c_void_p]
         try:
             self._set_threads = self.lib.openblas_set_num_threads
         except AttributeError:
@@ -163,6 +169,28 @@ class Ref:
         out = self._copy_out(p)
         self.lib.taucs_ccs_free(p)
         return out
+
+    def read_binary(self, path):
+        """the reference's taucs_ccs_read_binary: (n, colptr, rowind, values, flags)"""
+        p = self.lib.taucs_ccs_read_binary(os.fsencode(path))
+        n, nnz, fl = C.c_int(), C.c_int(), C.c_int()
+        self.lib.ref_ccs_dims(p, C.byref(n), C.byref(nnz), C.byref(fl))
+        cp = np.empty(n.value + 1, np.int32)
+        ri = np.empty(nnz.value, np.int32)
+        va = np.empty(nnz.value, np.float64)
+        self.lib.ref_ccs_copy(p, cp, ri, va)
+        self.lib.taucs_ccs_free(p)
+        return n.value, cp, ri, va, fl.value
+
+    def vec_read_binary(self, n, path):
+        p = self.lib.taucs_vec_read_binary(n, 2048, os.fsencode(path))
+        v = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(n,)).copy()
+        self.lib.ref_free(p)
+        return v
+
+    def vec_write_binary(self, v, path):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        return self.lib.taucs_vec_write_binary(v.size, 2048, v.ctypes.data, os.fsencode(path))
 
     def wrap(self, n, cp, ri, va):
         return self.lib.ref_ccs_wrap(n, SPD_FLAGS, cp, ri, va)

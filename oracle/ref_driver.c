@@ -175,3 +175,15 @@ int ref_order(taucs_ccs_matrix* A, const char* which, int* perm, int* invperm)
   free(p); free(ip);
   return 0;
 }
+
+/* src/taucs_ccs_io.c's Harwell-Boeing reader calls the f2c'd readhb routines
+   (external/src/readhb.c), which need libf2c's formatted I/O; the image has
+   no libf2c and the oracle reads no HB files.  These stand-ins let the
+   reference's binary readers (same file) link; they report failure. */
+int ireadhb_(char* f, char* t, int* m, int* n, int* nz) { (void) f; (void) t; (void) m; (void) n; (void) nz; return -1; }
+int dreadhb_(char* f, int* m, int* n, int* nz, int* cp, int* ri, taucs_double* v)
+{ (void) f; (void) m; (void) n; (void) nz; (void) cp; (void) ri; (void) v; return -1; }
+
+/* the reference's vector reader allocates with taucs_malloc (plain malloc in
+   this build) */
+void ref_free(void* p) { free(p); }

@@ -99,6 +99,10 @@ def lib():
         "taucs_supernodal_factor_get_diag": (vp, [vp]),
         "taucs_linsolve": (C.c_int, [pc, C.POINTER(vp), C.c_int, vp, vp, C.POINTER(C.c_char_p), C.POINTER(vp)]),
         "taucs_logfile": (None, [C.c_char_p]),
+        "taucs_ccs_read_binary": (pc, [C.c_char_p]),
+        "taucs_b200_ccs_write_binary": (C.c_int, [pc, C.c_char_p]),
+        "taucs_vec_read_binary": (vp, [C.c_int, C.c_int, C.c_char_p]),
+        "taucs_vec_write_binary": (C.c_int, [C.c_int, C.c_int, vp, C.c_char_p]),
         "taucs_b200_set_stream": (C.c_int, [vp]),
         "taucs_b200_factor_numeric_device": (C.c_int, [vp, vp]),
         "taucs_b200_factor_numeric_device_async": (C.c_int, [vp, vp]),
@@ -209,6 +213,42 @@ class Matrix:
 
 def last_error():
     return (lib().taucs_b200_last_error() or b"").decode()
+
+
+def read_binary(path):
+    """taucs_ccs_read_binary: a square double-valued matrix file as a Matrix
+    (flags as stored in the file)."""
+    p = lib().taucs_ccs_read_binary(os.fsencode(path))
+    if not p:
+        raise RuntimeError("read_binary failed: " + last_error())
+    s = p.contents
+    if s.m != s.n or not s.flags & TAUCS_DOUBLE:
+        lib().taucs_ccs_free(p)
+        raise ValueError("read_binary: only square double-valued matrices map to Matrix")
+    return Matrix._adopt(p)
+
+
+def write_binary(A, path):
+    """taucs_b200_ccs_write_binary: the reference's binary CCS file format."""
+    if lib().taucs_b200_ccs_write_binary(A.ptr, os.fsencode(path)) != 0:
+        raise RuntimeError("write_binary failed: " + last_error())
+
+
+def vec_read_binary(n, path):
+    """taucs_vec_read_binary for n doubles."""
+    p = lib().taucs_vec_read_binary(int(n), TAUCS_DOUBLE, os.fsencode(path))
+    if not p:
+        raise RuntimeError("vec_read_binary failed: " + last_error())
+    v = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(max(int(n), 1),))[:int(n)].copy()
+    C.CDLL(None).free(C.c_void_p(p))
+    return v
+
+
+def vec_write_binary(v, path):
+    """taucs_vec_write_binary for a double vector."""
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    if lib().taucs_vec_write_binary(v.size, TAUCS_DOUBLE, v.ctypes.data, os.fsencode(path)) != 0:
+        raise RuntimeError("vec_write_binary failed: " + last_error())
 
 
 def mesh2d(k, which="dirichlet"):
