@@ -100,6 +100,33 @@ __global__ void k_update32(int n, double* __restrict__ X, const float* __restric
   for (int q = 0; q < nrhs; q++) X[i + (size_t) q * ld] += scale[i] * (double) D[i + (size_t) q * n];
 }
 
+// value k of P A P^T is value vmap[k] of A as given (the value map of
+// taucs_ccs_permute_symmetrically, src/taucs_ccs_ops.c:174-257, precomputed
+// once per pattern)
+__global__ void k_gather_values(long nnz, const int* __restrict__ vmap, const double* __restrict__ raw,
+                                double* __restrict__ out) {
+  for (long k = (long) blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (long) gridDim.x * blockDim.x)
+    out[k] = raw[vmap[k]];
+}
+
+// P b and its inverse (src/taucs_vec_base.c:194-206): dst[i] = src[perm[i]]
+// and dst[perm[i]] = src[i], nq columns, original-order vectors with ld n
+__global__ void k_perm_gather(int n, int nq, const int* __restrict__ perm, const double* __restrict__ src,
+                              double* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int pi = perm[i];
+  for (int q = 0; q < nq; q++) dst[i + (size_t) q * n] = src[pi + (size_t) q * n];
+}
+
+__global__ void k_perm_scatter(int n, int nq, const int* __restrict__ perm, const double* __restrict__ src,
+                               double* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int pi = perm[i];
+  for (int q = 0; q < nq; q++) dst[pi + (size_t) q * n] = src[i + (size_t) q * n];
+}
+
 __global__ void k_update64(int n, double* __restrict__ X, const double* __restrict__ D, int ld, int nrhs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -316,6 +343,38 @@ static int device_anorm(Factor* F, std::vector<double>* anorm) {
   anorm->resize(ns);
   for (int s = 0; s < ns; s++) memcpy(&(*anorm)[s], &F->hnorm[s], 8);
   return 0;
+}
+
+int gather_values_device(long nnz, const int* d_vmap, const double* d_raw, double* d_out) {
+  if (nnz <= 0) return 0;
+  const int grid = (int) std::min<long>(nblk(nnz, 256), 148L * 16);
+  k_gather_values<<<grid, 256, 0, current_stream()>>>(nnz, d_vmap, d_raw, d_out);
+  count_launch();
+  return cuda_ok(cudaGetLastError(), "value gather") ? 0 : -1;
+}
+
+int solve_refine_permuted(Factor* F, int nrhs, double* d_x, const double* d_b, const int* d_perm, double tol,
+                          int maxits, double* res) {
+  if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
+  if (F->nseg() > 1) { set_error("solve_refine: a batch handle solves through taucs_b200_batch_solve"); return -1; }
+  if (ensure_refine(F)) return -1;
+  const int n = F->n;
+  std::vector<double> anorm;
+  if (device_anorm(F, &anorm)) return -1;
+  cudaStream_t st = current_stream();
+  int worst_steps = 0;
+  for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
+    const int nq = std::min(SOLVE_NRHS, nrhs - q0);
+    k_perm_gather<<<nblk(n, 256), 256, 0, st>>>(n, nq, d_perm, d_b + (size_t) q0 * n, F->dBr);
+    count_launch();
+    const int s = refine_device(F, nq, F->dXr, F->dBr, n, tol, maxits, anorm, res ? res + q0 : nullptr);
+    k_perm_scatter<<<nblk(n, 256), 256, 0, st>>>(n, nq, d_perm, F->dXr, d_x + (size_t) q0 * n);
+    count_launch();
+    if (!cuda_ok(cudaGetLastError(), "permute")) return -1;
+    if (s < 0) worst_steps = -1;
+    else if (worst_steps >= 0) worst_steps = std::max(worst_steps, s);
+  }
+  return worst_steps;
 }
 
 int solve_refine_device(Factor* F, int nrhs, double* dX, const double* dB, int ld, double tol, int maxits,

@@ -47,8 +47,9 @@ namespace tb {
 
 Factor* symbolic(taucs_ccs_matrix* A, int max_depth);
 int numeric_device(Factor* F, const double* d_vals, bool wait);
-int solve_refine_host(Factor* F, taucs_ccs_matrix* A, int nrhs, double* X, const double* B, double tol, int maxits,
-                      double* res);
+int gather_values_device(long nnz, const int* d_vmap, const double* d_raw, double* d_out);
+int solve_refine_permuted(Factor* F, int nrhs, double* d_x, const double* d_b, const int* d_perm, double tol,
+                          int maxits, double* res);
 
 // factor instances kept per pattern while the budget allows (each holds one
 // resident numeric factor)
@@ -63,16 +64,27 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// 64-bit hash of a word array (multiply-xorshift per 8 bytes)
+// 64-bit hash of a byte array: four independent multiply-xorshift lanes over
+// 32-byte strides (so the multiplies of one lane do not wait for the others),
+// folded at the end
+inline uint64_t hash_mix(uint64_t h, uint64_t w) {
+  h ^= w + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
+  return h * 0xff51afd7ed558ccdull;
+}
+
 uint64_t hash_bytes(const void* p, size_t bytes, uint64_t h) {
   const unsigned char* c = (const unsigned char*) p;
+  uint64_t l0 = h, l1 = h ^ 0x243f6a8885a308d3ull, l2 = h ^ 0x13198a2e03707344ull, l3 = h ^ 0xa4093822299f31d0ull;
   size_t i = 0;
-  for (; i + 8 <= bytes; i += 8) {
-    uint64_t w;
-    memcpy(&w, c + i, 8);
-    h ^= w + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
-    h *= 0xff51afd7ed558ccdull;
+  for (; i + 32 <= bytes; i += 32) {
+    uint64_t w[4];
+    memcpy(w, c + i, 32);
+    l0 = hash_mix(l0, w[0]);
+    l1 = hash_mix(l1, w[1]);
+    l2 = hash_mix(l2, w[2]);
+    l3 = hash_mix(l3, w[3]);
   }
+  h = hash_mix(hash_mix(hash_mix(hash_mix(h, l0), l1), l2), l3);
   for (; i < bytes; i++) h = (h ^ c[i]) * 0x100000001b3ull;
   return h ^ (h >> 29);
 }
@@ -96,6 +108,12 @@ struct Pattern {
   std::vector<int> perm;      // P A P^T row i is A's row perm[i]
   std::vector<int> vmap;      // value k of P A P^T is A's value vmap[k]
   Factor* proto = nullptr;    // symbolic factor + plan (host only)
+  // device copies of perm and vmap for the device-side permutations, made
+  // by the first request that needs them (dev_state 0 none, 1 ready, -1 failed)
+  int* d_perm = nullptr;
+  int* d_vmap = nullptr;
+  std::mutex dev_mu;
+  int dev_state = 0;
   size_t inst_bytes = 0;
   int state = 0;              // 0 being built, 1 ready, -1 failed
   int n_created = 0;          // instances made so far
@@ -128,11 +146,14 @@ struct Request {
 struct Worker {
   cudaStream_t stream = nullptr;      // low priority (large systems)
   cudaStream_t stream_hi = nullptr;   // high priority (small systems)
-  double* h_vals = nullptr;   // pinned staging: values of P A P^T
+  double* h_vals = nullptr;   // pinned staging: A's values as given
   size_t h_vals_len = 0;
-  double* h_b = nullptr;      // pinned staging: P b, then P x
+  double* h_b = nullptr;      // pinned staging: b and x in the caller's order
   double* h_x = nullptr;
   size_t h_vec_len = 0;
+  double* d_vals = nullptr;   // device copies of the same (stream-ordered allocations)
+  double* d_b = nullptr;
+  double* d_x = nullptr;
 };
 
 }  // namespace
@@ -154,9 +175,15 @@ class Server {
     for (auto& t : threads_) t.join();
     cudaSetDevice(device_);
     for (auto& I : instances_) taucs_supernodal_factor_free(I->F);
-    for (auto& kv : patterns_)
+    for (auto& kv : patterns_) {
       if (kv.second->proto) taucs_supernodal_factor_free(kv.second->proto);
+      cudaFree(kv.second->d_perm);
+      cudaFree(kv.second->d_vmap);
+    }
     for (auto& w : workers_) {
+      cudaFree(w->d_vals);
+      cudaFree(w->d_b);
+      cudaFree(w->d_x);
       if (w->stream) cudaStreamDestroy(w->stream);
       if (w->stream_hi) cudaStreamDestroy(w->stream_hi);
       if (w->h_vals) cudaFreeHost(w->h_vals);
@@ -244,23 +271,60 @@ class Server {
     }
   }
 
-  bool grow(Worker& W, size_t nvals, size_t nvec) {
+  // staging buffers of a worker, grown to the largest request it has seen;
+  // the device ones come from the stream-ordered allocator (no device-wide
+  // synchronisation) and are ready when the stream has drained
+  bool grow(Worker& W, size_t nvals, size_t nvec, cudaStream_t st) {
+    if (nvals <= W.h_vals_len && nvec <= W.h_vec_len) return true;
     if (nvals > W.h_vals_len) {
       if (W.h_vals) cudaFreeHost(W.h_vals);
+      cudaFreeAsync(W.d_vals, st);
       W.h_vals = nullptr;
-      if (cudaMallocHost((void**) &W.h_vals, sizeof(double) * nvals) != cudaSuccess) return false;
+      W.d_vals = nullptr;
+      if (cudaMallocHost((void**) &W.h_vals, sizeof(double) * nvals) != cudaSuccess ||
+          cudaMallocAsync((void**) &W.d_vals, sizeof(double) * nvals, st) != cudaSuccess)
+        return false;
       W.h_vals_len = nvals;
     }
     if (nvec > W.h_vec_len) {
       if (W.h_b) cudaFreeHost(W.h_b);
       if (W.h_x) cudaFreeHost(W.h_x);
+      cudaFreeAsync(W.d_b, st);
+      cudaFreeAsync(W.d_x, st);
       W.h_b = W.h_x = nullptr;
+      W.d_b = W.d_x = nullptr;
       if (cudaMallocHost((void**) &W.h_b, sizeof(double) * nvec) != cudaSuccess ||
-          cudaMallocHost((void**) &W.h_x, sizeof(double) * nvec) != cudaSuccess)
+          cudaMallocHost((void**) &W.h_x, sizeof(double) * nvec) != cudaSuccess ||
+          cudaMallocAsync((void**) &W.d_b, sizeof(double) * nvec, st) != cudaSuccess ||
+          cudaMallocAsync((void**) &W.d_x, sizeof(double) * nvec, st) != cudaSuccess)
         return false;
       W.h_vec_len = nvec;
     }
-    return true;
+    return cudaStreamSynchronize(st) == cudaSuccess;
+  }
+
+  // device copies of the pattern's permutation and value map, uploaded once
+  // (their bytes count against the budget like an instance's)
+  bool pattern_device(Pattern* P, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(P->dev_mu);
+    if (P->dev_state == 0) {
+      const size_t bytes = sizeof(int) * (P->perm.size() + P->vmap.size());
+      bool ok = cudaMalloc((void**) &P->d_perm, sizeof(int) * std::max<size_t>(P->perm.size(), 1)) == cudaSuccess &&
+                cudaMalloc((void**) &P->d_vmap, sizeof(int) * std::max<size_t>(P->vmap.size(), 1)) == cudaSuccess &&
+                cudaMemcpyAsync(P->d_perm, P->perm.data(), sizeof(int) * P->perm.size(), cudaMemcpyHostToDevice,
+                                st) == cudaSuccess &&
+                cudaMemcpyAsync(P->d_vmap, P->vmap.data(), sizeof(int) * P->vmap.size(), cudaMemcpyHostToDevice,
+                                st) == cudaSuccess &&
+                cudaStreamSynchronize(st) == cudaSuccess;
+      P->dev_state = ok ? 1 : -1;
+      if (ok) {
+        std::lock_guard<std::mutex> lk2(mu_);
+        in_use_ += bytes;
+      } else {
+        set_error("server: could not upload a pattern's permutation to the device");
+      }
+    }
+    return P->dev_state == 1;
   }
 
   int process(Request* r, Worker& W) {
@@ -276,39 +340,37 @@ class Server {
     Instance* I = acquire(P, vkey, &hit);
     if (!I) return -1;
     const size_t nvec = (size_t) n * r->nrhs;
-    int rc = grow(W, (size_t) nnz, nvec) ? 0 : -1;
+    int rc = grow(W, (size_t) nnz, nvec, st) && pattern_device(P, st) ? 0 : -1;
     Factor* F = I->F;
     if (!rc && !hit) {
-      // the values of P A P^T, staged in pinned memory, then FP32 fronts
-      for (int64_t k = 0; k < nnz; k++) W.h_vals[k] = A.values.d[P->vmap[k]];
+      // A's values as given go to the device in one sequential copy; the
+      // values of P A P^T are gathered there through the pattern's value
+      // map, then FP32 fronts
+      memcpy(W.h_vals, A.values.d, sizeof(double) * nnz);
       rc = ensure_device(F);
-      if (!rc && cudaMemcpyAsync(F->dA, W.h_vals, sizeof(double) * nnz, cudaMemcpyHostToDevice, st)
-                     != cudaSuccess)
+      if (!rc && cudaMemcpyAsync(W.d_vals, W.h_vals, sizeof(double) * nnz, cudaMemcpyHostToDevice, st) != cudaSuccess)
         rc = -1;
+      if (!rc) rc = gather_values_device(nnz, P->d_vmap, W.d_vals, F->dA);
       F->precision = 1;
       if (!rc) rc = numeric_device(F, F->dA, true);
       r->factored = true;
     }
     if (!rc) {
-      for (int q = 0; q < r->nrhs; q++) {
-        const double* b = r->B + (size_t) q * n;
-        double* hb = W.h_b + (size_t) q * n;
-        for (int i = 0; i < n; i++) hb[i] = b[P->perm[i]];
-      }
-      // refinement in the instance's own device vectors, 8 columns at a
-      // time, so its recorded launch sequences are replayed by every worker
+      // b in the caller's order to the device; P b, the refinement in the
+      // instance's own vectors (8 columns at a time, so its recorded launch
+      // sequences are replayed by every worker) and x = P^T y on the device
+      memcpy(W.h_b, r->B, sizeof(double) * nvec);
+      if (cudaMemcpyAsync(W.d_b, W.h_b, sizeof(double) * nvec, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = -1;
       std::vector<double> res(r->nrhs, 0.0);
-      const int s = solve_refine_host(F, nullptr, r->nrhs, W.h_x, W.h_b, r->tol, 10, res.data());
+      const int s = rc ? -1 : solve_refine_permuted(F, r->nrhs, W.d_x, W.d_b, P->d_perm, r->tol, 10, res.data());
       if (s < 0) rc = -1;
+      if (!rc && (cudaMemcpyAsync(W.h_x, W.d_x, sizeof(double) * nvec, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                  cudaStreamSynchronize(st) != cudaSuccess))
+        rc = -1;
+      if (!rc) memcpy(r->X, W.h_x, sizeof(double) * nvec);
       r->steps = s;
       r->resid = *std::max_element(res.begin(), res.end());
     }
-    if (!rc)
-      for (int q = 0; q < r->nrhs; q++) {
-        double* x = r->X + (size_t) q * n;
-        const double* hx = W.h_x + (size_t) q * n;
-        for (int i = 0; i < n; i++) x[P->perm[i]] = hx[i];
-      }
     release(I, rc == 0, vkey);
     return rc;
   }
