@@ -223,6 +223,17 @@ int taucs_b200_solve_refine(void* L, taucs_ccs_matrix* A, int nrhs, double* X,
 int taucs_b200_solve_refine_device(void* L, int nrhs, double* d_X, const double* d_B,
                                    int ld, double tol, int maxits, double* res_out);
 
+/* Fallback of the refinement when the FP32 factor's steps stall (a scaled
+ * residual that fails to halve twice in a row, or the step limit): first
+ * preconditioned conjugate gradients (after src/taucs_iter.c:66-223) with the
+ * FP32 factor as preconditioner, up to `maxits` iterations (default 100; 0
+ * skips it), then an FP64 refactorization.  Batches (several systems in one
+ * handle) go straight to FP64.  The report gives how the last refinement
+ * finished: 0 FP32 steps only, 1 PCG, 2 FP64 refactorization; and the PCG
+ * iterations it used. */
+int taucs_b200_set_pcg(void* L, int maxits);
+int taucs_b200_refine_report(void* L, int* fallback, int* pcg_iterations);
+
 /* Inspection of the symbolic factor, in the reference's own arrays (slots
  * 0..n_sn-1, virtual root n_sn) -- used by the parity tests. */
 typedef struct {

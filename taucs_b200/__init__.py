@@ -113,6 +113,8 @@ def lib():
         "taucs_b200_set_precision": (C.c_int, [vp, C.c_int]),
         "taucs_b200_solve_refine": (C.c_int, [vp, pc, C.c_int, _f64p, _f64p, C.c_double, C.c_int, _f64p]),
         "taucs_b200_solve_refine_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_int, _f64p]),
+        "taucs_b200_set_pcg": (C.c_int, [vp, C.c_int]),
+        "taucs_b200_refine_report": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "taucs_b200_batch_analyze": (vp, [C.c_int, C.POINTER(pc)]),
         "taucs_b200_batch_values": (C.c_int, [vp, C.POINTER(pc), _f64p]),
         "taucs_b200_batch_rhs": (C.c_int, [vp, C.POINTER(C.c_void_p), _f64p]),
@@ -376,6 +378,18 @@ class Factor:
 
     def set_precision(self, p):
         return lib().taucs_b200_set_precision(self.h, p)
+
+    def set_pcg(self, maxits):
+        """PCG iterations allowed when FP32 refinement stalls (0: go straight
+        to the FP64 refactorization)."""
+        return lib().taucs_b200_set_pcg(self.h, int(maxits))
+
+    def refine_report(self):
+        """(fallback, pcg_iterations) of the last refinement: fallback 0 FP32
+        steps only, 1 PCG on the FP32 factor, 2 FP64 refactorization."""
+        fb, its = C.c_int(), C.c_int()
+        lib().taucs_b200_refine_report(self.h, C.byref(fb), C.byref(its))
+        return fb.value, its.value
 
     def solve_refine(self, A, b, tol=1e-12, maxits=10):
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -179,6 +179,11 @@ static void free_device(Factor* F) {
   cudaFree(F->dnorm); F->dnorm = nullptr;
   if (F->hnorm) cudaFreeHost(F->hnorm);
   F->hnorm = nullptr;
+  cudaFree(F->dpcg); F->dpcg = nullptr;
+  cudaFree(F->ddot_part); F->ddot_part = nullptr;
+  cudaFree(F->ddot); F->ddot = nullptr;
+  if (F->hdot) cudaFreeHost(F->hdot);
+  F->hdot = nullptr;
   F->refine_ready = false;
   cudaFree(F->dflags); F->dflags = nullptr;
   if (F->hstatus) cudaFreeHost(F->hstatus);

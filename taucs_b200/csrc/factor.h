@@ -60,6 +60,15 @@ struct Factor {
   unsigned long long* dnorm = nullptr;  // 2 x SOLVE_NRHS inf-norm bit patterns
   unsigned long long* hnorm = nullptr;  // pinned readback
   bool refine_ready = false;
+  // PCG fallback of the refinement (preconditioned by the FP32 factor):
+  // p, q, z (3 x n x SOLVE_NRHS), per-block dot partials and the dot results
+  double* dpcg = nullptr;
+  double* ddot_part = nullptr;
+  double* ddot = nullptr;
+  double* hdot = nullptr;              // pinned readback of ddot
+  int pcg_maxits = 100;                // 0: no PCG, stalled refinement refactors in FP64
+  int last_fallback = 0;               // last refinement: 0 FP32 steps, 1 PCG, 2 FP64 refactor
+  int last_pcg_its = 0;
   const double* dvals_cur = nullptr;   // values of the last numeric factorization (device)
   // independent systems held in one factor (a batch): row ranges seg_ptr[s]
   // .. seg_ptr[s+1]; refinement measures every segment's scaled residual on

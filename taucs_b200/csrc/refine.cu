@@ -64,12 +64,13 @@ __device__ __forceinline__ void seg_max(unsigned long long* slots, int sg, int s
   }
 }
 
-// R = B - A X (FP64); inf-norms of R and X per column and segment:
-// norms[(s * SOLVE_NRHS + q) * 2] (r) and [.. + 1] (x); seg == NULL: one segment
+// R = B - A X (FP64; X and B with leading dimension ld, R with ldr);
+// inf-norms of R and X per column and segment: norms[(s * SOLVE_NRHS + q) * 2]
+// (r) and [.. + 1] (x); seg == NULL: one segment
 __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                            const int* __restrict__ vi, const double* __restrict__ vals,
                            const double* __restrict__ X, const double* __restrict__ B, double* __restrict__ R,
-                           int ld, int nrhs, const int* __restrict__ seg, unsigned long long* norms) {
+                           int ld, int ldr, int nrhs, const int* __restrict__ seg, unsigned long long* norms) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int sg = (seg && i < n) ? seg[i] : 0;
   for (int q = 0; q < nrhs; q++) {
@@ -77,7 +78,7 @@ __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restr
     if (i < n) {
       double acc = B[i + (size_t) q * ld];
       for (int e = rp[i]; e < rp[i + 1]; e++) acc -= vals[vi[e]] * X[ci[e] + (size_t) q * ld];
-      R[i + (size_t) q * ld] = acc;
+      R[i + (size_t) q * ldr] = acc;
       r = fabs(acc);
       x = fabs(X[i + (size_t) q * ld]);
     }
@@ -127,10 +128,99 @@ __global__ void k_perm_scatter(int n, int nq, const int* __restrict__ perm, cons
   for (int q = 0; q < nq; q++) dst[pi + (size_t) q * n] = src[i + (size_t) q * n];
 }
 
-__global__ void k_update64(int n, double* __restrict__ X, const double* __restrict__ D, int ld, int nrhs) {
+__global__ void k_update64(int n, double* __restrict__ X, const double* __restrict__ D, int ld, int ldd, int nrhs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  for (int q = 0; q < nrhs; q++) X[i + (size_t) q * ld] += D[i + (size_t) q * ld];
+  for (int q = 0; q < nrhs; q++) X[i + (size_t) q * ld] += D[i + (size_t) q * ldd];
+}
+
+// ---- preconditioned conjugate gradients (fallback of the refinement)
+
+constexpr int DOT_BLOCKS = 296;   // fixed grid, so the summation order never changes
+
+struct Coef {
+  double v[SOLVE_NRHS];
+};
+
+// Y = A X for nq columns (symmetric CSR of both triangles; leading dimension n)
+__global__ void k_spmv(int n, const int* __restrict__ rp, const int* __restrict__ ci, const int* __restrict__ vi,
+                       const double* __restrict__ vals, const double* __restrict__ X, double* __restrict__ Y, int nq) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < nq; q++) {
+    double acc = 0.0;
+    for (int e = rp[i]; e < rp[i + 1]; e++) acc += vals[vi[e]] * X[ci[e] + (size_t) q * n];
+    Y[i + (size_t) q * n] = acc;
+  }
+}
+
+// Z = D d: an FP32 correction scaled back to A's variables
+__global__ void k_scale_up(int n, const float* __restrict__ D, const double* __restrict__ scale, double* __restrict__ Z,
+                           int nq) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < nq; q++) Z[i + (size_t) q * n] = scale[i] * (double) D[i + (size_t) q * n];
+}
+
+// a_q . b_q for nq columns in two fixed-order stages: every block sums a
+// fixed set of rows with a shared-memory tree, then one thread per column
+// adds the block sums in block order
+__global__ void __launch_bounds__(256) k_dot_part(int n, int nq, const double* __restrict__ A,
+                                                  const double* __restrict__ B, double* __restrict__ part) {
+  __shared__ double sh[256];
+  for (int q = 0; q < nq; q++) {
+    double acc = 0.0;
+    for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256)
+      acc += A[i + (size_t) q * n] * B[i + (size_t) q * n];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x * SOLVE_NRHS + q] = sh[0];
+    __syncthreads();
+  }
+}
+
+__global__ void k_dot_final(int nblocks, int nq, const double* __restrict__ part, double* __restrict__ out) {
+  const int q = threadIdx.x;
+  if (q >= nq) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblocks; b++) acc += part[b * SOLVE_NRHS + q];
+  out[q] = acc;
+}
+
+// search direction: P = Z + beta P (P = Z on a (re)start)
+__global__ void k_pcg_dir(int n, int nq, const double* __restrict__ Z, double* __restrict__ Pd, Coef beta, int restart) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < nq; q++) {
+    const size_t k = i + (size_t) q * n;
+    Pd[k] = restart ? Z[k] : Z[k] + beta.v[q] * Pd[k];
+  }
+}
+
+// X += alpha P, R -= alpha Q, and the inf-norms of R and X per column (the
+// one-segment layout of k_residual's norms)
+__global__ void k_pcg_step(int n, int nq, double* __restrict__ X, int ld, double* __restrict__ R,
+                           const double* __restrict__ Pd, const double* __restrict__ Q, Coef alpha,
+                           unsigned long long* norms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int q = 0; q < nq; q++) {
+    double r = 0.0, x = 0.0;
+    if (i < n) {
+      const size_t k = i + (size_t) q * n;
+      const double xi = X[i + (size_t) q * ld] + alpha.v[q] * Pd[k];
+      const double ri = R[k] - alpha.v[q] * Q[k];
+      X[i + (size_t) q * ld] = xi;
+      R[k] = ri;
+      r = fabs(ri);
+      x = fabs(xi);
+    }
+    seg_max(norms + 2 * q, 0, 2 * SOLVE_NRHS, r);
+    seg_max(norms + 2 * q + 1, 0, 2 * SOLVE_NRHS, x);
+  }
 }
 
 __global__ void k_init_status2(int* s) { *s = INT_MAX; }
@@ -245,12 +335,120 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
 
 // Refines X (device, n x nrhs, ld) for B; returns the number of correction
 // steps or -1; res (host, nrhs) gets the final scaled residuals.
+// Preconditioned conjugate gradients for the nq columns of one refinement
+// block, after taucs_conjugate_gradients (src/taucs_iter.c:66-223) with the
+// refinement's scaled-residual test in place of its relative 2-norm test.
+// Starts from the current X; the preconditioner is the FP32 factor applied as
+// the refinement's correction, z = D (L32 L32^T)^-1 D r.  The iteration runs
+// on the recursively updated residual; when every column meets tol there,
+// b - A x confirms it (otherwise all columns restart from the true residual).
+// alpha and beta come from fixed-order dot products, so a rerun gives the same
+// result bit for bit.  A column whose r.z or p.Ap is not positive (the FP32
+// preconditioner is not exactly symmetric) is frozen.  Returns the iterations
+// used; -1 when some column is not within tol after F->pcg_maxits iterations
+// (X then holds the last iterate and F->dR, F->hnorm its true residual); -2 on
+// a CUDA error.
+static int pcg_fp32(Factor* F, int nq, double* X, const double* B, int ld, double tol, double anorm,
+                    const double* bnorm, double* res_q) {
+  const Plan& P = F->plan;
+  const int n = F->n;
+  cudaStream_t st = current_stream();
+  const size_t nv = (size_t) n * SOLVE_NRHS;
+  if (!F->dpcg && !(cuda_ok(cudaMalloc(&F->dpcg, sizeof(double) * 3 * nv), "cudaMalloc(pcg)") &&
+                    cuda_ok(cudaMalloc(&F->ddot_part, sizeof(double) * DOT_BLOCKS * SOLVE_NRHS), "cudaMalloc(pcg)") &&
+                    cuda_ok(cudaMalloc(&F->ddot, sizeof(double) * 2 * SOLVE_NRHS), "cudaMalloc(pcg)") &&
+                    cuda_ok(cudaMallocHost(&F->hdot, sizeof(double) * 2 * SOLVE_NRHS), "cudaMallocHost(pcg)")))
+    return -2;
+  double* Pd = F->dpcg;
+  double* Q = Pd + nv;
+  double* Z = Q + nv;
+  double* R = F->dR;
+  auto dots = [&](const double* a, const double* b, int slot) {
+    k_dot_part<<<DOT_BLOCKS, 256, 0, st>>>(n, nq, a, b, F->ddot_part);
+    k_dot_final<<<1, 32, 0, st>>>(DOT_BLOCKS, nq, F->ddot_part, F->ddot + slot * SOLVE_NRHS);
+    count_launch(2);
+  };
+  auto fetch = [&](void* h, const void* d, size_t bytes) {
+    return cuda_ok(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st), "pcg readback");
+  };
+  auto true_residual = [&]() {
+    cudaMemsetAsync(F->dnorm, 0, norm_bytes(F), st);
+    k_residual<<<nblk(n, 256), 256, 0, st>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, R, ld, n,
+                                             nq, nullptr, F->dnorm);
+    count_launch();
+    return fetch(F->hnorm, F->dnorm, norm_bytes(F)) && cuda_ok(cudaStreamSynchronize(st), "pcg residual");
+  };
+  // worst scaled residual over the columns, from the norms in F->hnorm
+  auto scaled = [&](double* out) {
+    double worst = 0.0;
+    for (int q = 0; q < nq; q++) {
+      double rn, xn;
+      memcpy(&rn, &F->hnorm[(size_t) q * 2], 8);
+      memcpy(&xn, &F->hnorm[(size_t) q * 2 + 1], 8);
+      const double den = anorm * xn + bnorm[q];
+      const double v = den > 0 ? rn / den : 0.0;
+      if (out) out[q] = v;
+      worst = std::max(worst, std::isnan(v) ? INFINITY : v);
+    }
+    return worst;
+  };
+  if (!true_residual()) return -2;
+  std::vector<double> rho(nq), rho_old(nq, 0.0);
+  bool restart = true;
+  for (int it = 0; it < F->pcg_maxits;) {
+    // z = M^-1 r and rho = r.z
+    k_scale_down<<<nblk(n, 256), 256, 0, st>>>(n, R, F->dscale, F->dV32, n, nq);
+    int e = launch_solve_fp32(P, F->dp, F->dL32, F->dDinv32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32, F->dflags,
+                              &F->epoch, F->dstatus + 1, st);
+    k_scale_up<<<nblk(n, 256), 256, 0, st>>>(n, F->dV32, F->dscale, Z, nq);
+    count_launch(2);
+    if (e) return -2;
+    dots(R, Z, 0);
+    if (!fetch(F->hdot, F->ddot, sizeof(double) * SOLVE_NRHS) || !cuda_ok(cudaStreamSynchronize(st), "pcg")) return -2;
+    Coef beta{}, alpha{};
+    for (int q = 0; q < nq; q++) {
+      rho[q] = F->hdot[q];
+      beta.v[q] = (!restart && rho_old[q] > 0 && rho[q] > 0) ? rho[q] / rho_old[q] : 0.0;
+    }
+    // p = z + beta p, q = A p, alpha = rho / p.q
+    k_pcg_dir<<<nblk(n, 256), 256, 0, st>>>(n, nq, Z, Pd, beta, restart ? 1 : 0);
+    k_spmv<<<nblk(n, 256), 256, 0, st>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, Pd, Q, nq);
+    count_launch(2);
+    dots(Pd, Q, 1);
+    if (!fetch(F->hdot + SOLVE_NRHS, F->ddot + SOLVE_NRHS, sizeof(double) * SOLVE_NRHS) ||
+        !cuda_ok(cudaStreamSynchronize(st), "pcg"))
+      return -2;
+    for (int q = 0; q < nq; q++) {
+      const double pq = F->hdot[SOLVE_NRHS + q];
+      alpha.v[q] = (rho[q] > 0 && pq > 0) ? rho[q] / pq : 0.0;
+    }
+    // x += alpha p, r -= alpha q, and the norms of the updated residual
+    cudaMemsetAsync(F->dnorm, 0, norm_bytes(F), st);
+    k_pcg_step<<<nblk(n, 256), 256, 0, st>>>(n, nq, X, ld, R, Pd, Q, alpha, F->dnorm);
+    count_launch();
+    if (!fetch(F->hnorm, F->dnorm, norm_bytes(F)) || !cuda_ok(cudaStreamSynchronize(st), "pcg")) return -2;
+    rho_old = rho;
+    restart = false;
+    it++;
+    if (scaled(nullptr) <= tol) {
+      if (!true_residual()) return -2;
+      if (scaled(res_q) <= tol) return it;
+      restart = true;   // the recursive residual drifted: go on from b - A x
+    }
+  }
+  if (!true_residual()) return -2;
+  scaled(res_q);
+  return -1;
+}
+
 static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int ld, double tol, int maxits,
                          const std::vector<double>& anorm, double* res) {
   const Plan& P = F->plan;
   const int n = F->n, ns = F->nseg();
   cudaStream_t st = current_stream();
   int total = 0;
+  F->last_fallback = 0;
+  F->last_pcg_its = 0;
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
     double* X = dX + (size_t) q0 * ld;
@@ -260,7 +458,7 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     auto residual = [&](cudaStream_t s) {
       cudaMemsetAsync(F->dnorm, 0, norm_bytes(F), s);
       k_residual<<<nblk(n, 256), 256, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, F->dR,
-                                              ld, nq, F->dseg, F->dnorm);
+                                              ld, n, nq, F->dseg, F->dnorm);
       count_launch();
       cudaMemcpyAsync(F->hnorm, F->dnorm, norm_bytes(F), cudaMemcpyDeviceToHost, s);
       return (int) cudaGetLastError();
@@ -269,11 +467,11 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     auto correction = [&](cudaStream_t s, bool u64) {
       int e;
       if (u64) {
-        e = launch_solve_fp64(P, F->dp, F->dL, F->dDinv, nq, F->dR, F->dR, ld, F->dW, F->dpart, F->dflags, &F->epoch,
+        e = launch_solve_fp64(P, F->dp, F->dL, F->dDinv, nq, F->dR, F->dR, n, F->dW, F->dpart, F->dflags, &F->epoch,
                               F->dstatus + 1, s);
-        k_update64<<<nblk(n, 256), 256, 0, s>>>(n, X, F->dR, ld, nq);
+        k_update64<<<nblk(n, 256), 256, 0, s>>>(n, X, F->dR, ld, n, nq);
       } else {
-        k_scale_down<<<nblk(n, 256), 256, 0, s>>>(n, F->dR, F->dscale, F->dV32, ld, nq);
+        k_scale_down<<<nblk(n, 256), 256, 0, s>>>(n, F->dR, F->dscale, F->dV32, n, nq);
         e = launch_solve_fp32(P, F->dp, F->dL32, F->dDinv32, nq, F->dV32, F->dV32, n, F->dW32, F->dpart32,
                               F->dflags, &F->epoch, F->dstatus + 1, s);
         k_update32<<<nblk(n, 256), 256, 0, s>>>(n, X, F->dV32, F->dscale, ld, nq);
@@ -308,9 +506,28 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
         if (worst > 0.5 * prev_worst) slow++;
         else slow = 0;
         if (!use64 && (slow >= 2 || steps >= maxits)) {
-          // refinement stalled with the FP32 factor: finish in FP64
+          // refinement stalled with the FP32 factor: first preconditioned
+          // conjugate gradients on that factor (one system only), then an
+          // FP64 refactorization
+          if (ns == 1 && F->pcg_maxits > 0) {
+            tprintf("\t\trefinement stalled at %.3e after %d steps; PCG on the FP32 factor\n", worst, steps);
+            std::vector<double> rq(nq, 0.0);
+            const int its = pcg_fp32(F, nq, X, B, ld, tol, anorm[0], bnorm.data(), rq.data());
+            if (its == -2) return -1;
+            if (res)
+              for (int q = 0; q < nq; q++) res[q0 + q] = rq[q];
+            F->last_pcg_its += std::max(its, 0);
+            if (its >= 0) {
+              F->last_fallback = std::max(F->last_fallback, 1);
+              steps += its;
+              done = true;
+              continue;
+            }
+            tprintf("\t\tPCG did not converge in %d iterations\n", F->pcg_maxits);
+          }
           tprintf("\t\trefinement stalled at %.3e after %d steps; refactoring in FP64\n", worst, steps);
           if (!F->has_numeric && numeric_fp64_device(F, F->dvals_cur, true)) return -1;
+          F->last_fallback = 2;
           use64 = true;
           slow = 0;
         } else if (use64 && (slow >= 2 || steps >= maxits + 5)) {
@@ -420,6 +637,19 @@ using namespace tb;
 extern "C" int taucs_b200_set_precision(void* L, int precision) {
   if (!L || (precision != 0 && precision != 1)) return -1;
   ((Factor*) L)->precision = precision;
+  return 0;
+}
+
+extern "C" int taucs_b200_set_pcg(void* L, int maxits) {
+  if (!L || maxits < 0) return -1;
+  ((Factor*) L)->pcg_maxits = maxits;
+  return 0;
+}
+
+extern "C" int taucs_b200_refine_report(void* L, int* fallback, int* pcg_iterations) {
+  if (!L) return -1;
+  if (fallback) *fallback = ((Factor*) L)->last_fallback;
+  if (pcg_iterations) *pcg_iterations = ((Factor*) L)->last_pcg_its;
   return 0;
 }
 

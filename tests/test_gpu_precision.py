@@ -75,9 +75,12 @@ def test_stalled_refinement_finishes_in_fp64(tb):
     F.set_precision(1)
     assert F.numeric(P) == 0
     B = np.random.default_rng(4).uniform(-1, 1, (P.n, 2))
-    # maxits = 0: after one FP32 step the driver switches to an FP64 factor
+    # maxits = 0 and no PCG: after one FP32 step the driver switches to an
+    # FP64 factor
+    F.set_pcg(0)
     X, its, res = F.solve_refine(P, B, tol=1e-14, maxits=0)
     assert its >= 1
+    assert F.refine_report()[0] == 2
     for q in range(2):
         assert scaled_residual(P, X[:, q], B[:, q]) <= 1e-14
 
