@@ -142,10 +142,23 @@ void  taucs_dsupernodal_factor_free_numeric(void* L);
 taucs_ccs_matrix* taucs_dsupernodal_factor_to_ccs(void* L);
 double* taucs_dsupernodal_factor_get_diag(void* L);
 
+/* preconditioned conjugate gradients (src/taucs_iter.c:66-223): host
+ * vectors, precond_fn(precond_args, z, r) computes z = M^-1 r (NULL: none),
+ * e.g. taucs_supernodal_solve_llt with a factor; stops when the recursively
+ * updated residual has shrunk by convergetol in the 2-norm, or after
+ * itermax + 1 iterations.  X holds the starting guess on entry.  0, or an
+ * error code when the preconditioner fails. */
+int taucs_conjugate_gradients(taucs_ccs_matrix* A, int (*precond_fn)(void*, void* x, void* b), void* precond_args,
+                              void* X, void* B, int itermax, double convergetol);
+
 /* unified interface (src/taucs_linsolve.c:189-622).  Options understood:
  *   taucs.factor=bool taucs.factor.symbolic=bool taucs.factor.numeric=bool
  *   taucs.factor.LLT=bool taucs.factor.mf=bool taucs.factor.ll=bool
  *   taucs.factor.ordering=string taucs.maxdepth=number
+ *   taucs.solve.cg=bool taucs.solve.maxits=number taucs.solve.convergetol=number
+ *     (conjugate gradients preconditioned by the factor, one column at a
+ *     time, defaults 300 and 1e-6 as in the reference; the starting guess is
+ *     zero, where the reference passes uninitialised memory)
  * plus the additions
  *   taucs.gpu.precision=fp64|mixed   (mixed: FP32 fronts + FP64 refinement)
  *   taucs.gpu.refine.tol=number      (scaled residual target, default 1e-12)

@@ -112,7 +112,8 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
   }
   int opt_factor = 1, opt_symbolic = 1, opt_numeric = 1, opt_llt = 0, opt_lu = 0, opt_mf = 0, opt_ll = 0;
   int opt_ooc = 0, opt_cg = 0, opt_minres = 0;
-  double opt_maxdepth = 0.0, opt_tol = 1e-12, opt_maxits = 10.0, dummy = 0.0;
+  double opt_maxdepth = 0.0, opt_tol = 1e-12, opt_maxits = 10.0;
+  double opt_cg_maxits = 300.0, opt_convergetol = 1e-6;   // src/taucs_linsolve.c:238-239
   const char* opt_ordering = nullptr;
   const char* opt_precision = "fp64";
   const char* sdummy = nullptr;
@@ -132,8 +133,8 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
       u |= get_bool(o, "taucs.ooc", opt_arg, &opt_ooc);
       u |= get_bool(o, "taucs.solve.cg", opt_arg, &opt_cg);
       u |= get_bool(o, "taucs.solve.minres", opt_arg, &opt_minres);
-      u |= get_double(o, "taucs.solve.maxits", opt_arg, &dummy);
-      u |= get_double(o, "taucs.solve.convergetol", opt_arg, &dummy);
+      u |= get_double(o, "taucs.solve.maxits", opt_arg, &opt_cg_maxits);
+      u |= get_double(o, "taucs.solve.convergetol", opt_arg, &opt_convergetol);
       u |= get_string(o, "taucs.ooc.basename", opt_arg, &sdummy);
       u |= get_string(o, "taucs.gpu.precision", opt_arg, &opt_precision);
       u |= get_double(o, "taucs.gpu.refine.tol", opt_arg, &opt_tol);
@@ -143,8 +144,8 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
   }
   (void) opt_mf;
   (void) opt_ll;
-  if (opt_lu || opt_ooc || opt_cg || opt_minres) {
-    taucs_printf((char*) "taucs_linsolve: LU, out-of-core and iterative solvers are not provided by this library\n");
+  if (opt_lu || opt_ooc || opt_minres) {
+    taucs_printf((char*) "taucs_linsolve: LU, out-of-core and MINRES are not provided by this library\n");
     return TAUCS_ERROR_BADARGS;
   }
   const bool mixed = opt_precision && !strcmp(opt_precision, "mixed");
@@ -231,7 +232,15 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
       for (int j = 0; j < nrhs; j++)
         taucs_vec_permute(n, TAUCS_DOUBLE, (double*) B + (size_t) j * n, PB.data() + (size_t) j * n, f->rowperm);
       int rc;
-      if (f->L->precision == 1 || mixed) {
+      if (opt_cg) {
+        // conjugate gradients preconditioned by the factor, one column at a
+        // time (src/taucs_linsolve.c:555-567)
+        if (!PAPT) PAPT = taucs_ccs_permute_symmetrically(A, f->rowperm, f->colperm);
+        rc = PAPT ? 0 : -1;
+        for (int j = 0; j < nrhs && !rc; j++)
+          rc = taucs_conjugate_gradients(PAPT, taucs_supernodal_solve_llt, f->L, PX.data() + (size_t) j * n,
+                                         PB.data() + (size_t) j * n, (int) opt_cg_maxits, opt_convergetol);
+      } else if (f->L->precision == 1 || mixed) {
         if (!PAPT) PAPT = taucs_ccs_permute_symmetrically(A, f->rowperm, f->colperm);
         rc = PAPT ? taucs_b200_solve_refine(f->L, PAPT, nrhs, PX.data(), PB.data(), opt_tol, (int) opt_maxits, nullptr) : -1;
         rc = rc < 0 ? -1 : 0;
