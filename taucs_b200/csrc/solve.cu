@@ -558,47 +558,61 @@ k_gather_upd(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fro
 
 // Backward solve, L21^T x2 split over (column block, 512-row chunk) CTAs so
 // that the whole GPU streams L21; each CTA stores its partial sums, which the
-// chain kernel adds in chunk order.
+// chain kernel adds in chunk order.  The chunk of x2 is staged in shared
+// memory once ([column][row], conflict-free across lanes); each warp takes
+// its 16 columns of the block G = 32 / NQ at a time, so that the G x NQ = 32
+// sums of a pass finish with one warp reduce-scatter (31 shuffles; lane t
+// ends with sum t = column t / NQ, right-hand side t % NQ).
 template <typename T, int NQ, int WS>
 __global__ void __launch_bounds__(128)
 k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts, const T* __restrict__ L,
           const T* __restrict__ W, T* __restrict__ part, int nrhs) {
-  constexpr int G = (16 / NQ) > 1 ? 16 / NQ : 1;
+  constexpr int G = 32 / NQ;
+  static_assert(G * NQ == 32 && G <= 16, "a pass holds 32 sums of at most 16 columns");
+  __shared__ T zs[NQ][SOLVE_RCH];
   const int2_ tk = tasks[blockIdx.x];
   const FrontDesc F = fronts[tk.a];
   const int k = tk.b >> 16, ch = tk.b & 0xffff;
   const int f = F.f, s = F.s, m = f - s;
   const int c0 = k * BR, bw = min(BR, s - c0);
-  const int i0 = ch * SOLVE_RCH, i1 = min(m, i0 + SOLVE_RCH);
+  const int i0 = ch * SOLVE_RCH, nr = min(m - i0, SOLVE_RCH);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const T* z = W + F.v_off * WS + s;
-  const T* P = L + F.l_off;
+  const T* z = W + F.v_off * WS + s + i0;
+  const T* P = L + F.l_off + s + i0;
+  for (int e = threadIdx.x; e < NQ * SOLVE_RCH; e += 128) {
+    const int i = e % SOLVE_RCH, q = e / SOLVE_RCH;
+    zs[q][i] = (i < nr && q < nrhs) ? __ldcg(z + i + (size_t) q * f) : T(0);
+  }
+  __syncthreads();
   for (int cg = warp * 16; cg < warp * 16 + 16; cg += G) {
-    T acc[G][NQ];
+    T v[32];   // v[a * NQ + q]: column cg + a, right-hand side q
 #pragma unroll
-    for (int a_ = 0; a_ < G; a_++)
-#pragma unroll
-      for (int q = 0; q < NQ; q++) acc[a_][q] = 0.0;
-    for (int i = i0 + lane; i < i1; i += 32) {
+    for (int j = 0; j < 32; j++) v[j] = T(0);
+    for (int i = lane; i < nr; i += 32) {
       T zi[NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) zi[q] = (q < nrhs) ? __ldcg(z + i + (size_t) q * f) : 0.0;
+      for (int q = 0; q < NQ; q++) zi[q] = zs[q][i];
 #pragma unroll
-      for (int a_ = 0; a_ < G; a_++) {
-        const T l = (cg + a_ < bw) ? P[(s + i) + (size_t) (c0 + cg + a_) * f] : 0.0;
+      for (int a = 0; a < G; a++) {
+        const T l = (cg + a < bw) ? P[i + (size_t) (c0 + cg + a) * f] : T(0);
 #pragma unroll
-        for (int q = 0; q < NQ; q++) acc[a_][q] += l * zi[q];
+        for (int q = 0; q < NQ; q++) v[a * NQ + q] += l * zi[q];
       }
     }
+    // reduce-scatter: at offset o a lane keeps the half of its remaining
+    // sums that matches its bit o and adds the partner's copy of that half
 #pragma unroll
-    for (int a_ = 0; a_ < G; a_++)
+    for (int o = 16, h = 16; o >= 1; o >>= 1, h >>= 1) {
+      const bool up = (lane & o) != 0;
 #pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        T v = acc[a_][q];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0 && cg + a_ < bw && q < nrhs)
-          part[F.part_off + ((size_t) ch * s + c0 + cg + a_) * SOLVE_NRHS + q] = v;
+      for (int j = 0; j < h; j++) {
+        const T send = up ? v[j] : v[j + h];
+        const T keep = up ? v[j + h] : v[j];
+        v[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
       }
+    }
+    const int a = lane / NQ, q = lane % NQ;
+    if (cg + a < bw && q < nrhs) part[F.part_off + ((size_t) ch * s + c0 + cg + a) * SOLVE_NRHS + q] = v[0];
   }
 }
 
