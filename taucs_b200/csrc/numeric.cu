@@ -745,18 +745,21 @@ static constexpr size_t potrf_smem() { return (2 * PANEL_NB * DLD + 32 * DLD) * 
 
 template <typename T>
 static void set_smem_attrs() {
-  static bool done = false;
-  if (done) return;
-  cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
-  cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) potrf_smem<T>());
-  cudaFuncSetAttribute(k_gemm<T, 64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) GemmCfg<64, 64>::smem<T>());
-  cudaFuncSetAttribute(k_gemm<T, 128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int) GemmCfg<128, 128>::smem<T>());
-  cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       2 * PANEL_NB * TLD * (int) sizeof(T));
-  done = true;
+  // once per process and type; a function-local static, because request-server
+  // workers reach this concurrently
+  static const bool done = [] {
+    cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
+    cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) potrf_smem<T>());
+    cudaFuncSetAttribute(k_gemm<T, 64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int) GemmCfg<64, 64>::smem<T>());
+    cudaFuncSetAttribute(k_gemm<T, 128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int) GemmCfg<128, 128>::smem<T>());
+    cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * PANEL_NB * TLD * (int) sizeof(T));
+    return true;
+  }();
+  (void) done;
 }
 
 template <typename T>

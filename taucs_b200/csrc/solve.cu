@@ -809,22 +809,25 @@ static double solve_pass_bytes(const FrontDesc& F, int nrhs) {
 
 template <typename T>
 static void solve_attrs() {
-  static bool done = false;
-  if (done) return;
-  // static + dynamic shared memory of these kernels can exceed the default
-  // 48 KB (8 columns in FP64)
-  cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
-  cudaFuncSetAttribute(k_fwd_big<T, 4, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
-  cudaFuncSetAttribute(k_fwd_big<T, 8, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
-  cudaFuncSetAttribute(k_fwd_big<T, 1, 1, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
-  cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
-  cudaFuncSetAttribute(k_fwd_big<T, 4, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
-  cudaFuncSetAttribute(k_fwd_big<T, 8, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
-  cudaFuncSetAttribute(k_bwd_big<T, 2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 2>());
-  cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 4>());
-  cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
-  cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
-  done = true;
+  // once per process and type; a function-local static, because request-server
+  // workers reach this concurrently
+  static const bool done = [] {
+    // static + dynamic shared memory of these kernels can exceed the default
+    // 48 KB (8 columns in FP64)
+    cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+    cudaFuncSetAttribute(k_fwd_big<T, 4, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+    cudaFuncSetAttribute(k_fwd_big<T, 8, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+    cudaFuncSetAttribute(k_fwd_big<T, 1, 1, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
+    cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
+    cudaFuncSetAttribute(k_fwd_big<T, 4, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
+    cudaFuncSetAttribute(k_fwd_big<T, 8, SOLVE_NRHS, FWD_CHAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_CHAIN>());
+    cudaFuncSetAttribute(k_bwd_big<T, 2, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 2>());
+    cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 4>());
+    cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
+    cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
+    return true;
+  }();
+  (void) done;
 }
 
 template <typename T>
