@@ -354,9 +354,11 @@ k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
 #pragma unroll
   for (int q = 0; q < 8; q++) X[32 + ci + (cj + q) * DLD] = -c[q];
   __syncthreads();
-  for (int k = tid; k < w * w; k += 128) {
-    const int i = k % w, j = k / w;
-    if (i >= j) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * DLD];
+  // the factored block's lower part (compile-time index arithmetic; w is
+  // below 64 only in a front's last block)
+  for (int k = tid; k < PANEL_NB * PANEL_NB; k += 128) {
+    const int i = k % PANEL_NB, j = k / PANEL_NB;
+    if (i >= j && i < w) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * DLD];
   }
   T* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
   for (int k = tid; k < PANEL_NB * PANEL_NB; k += 128) {
