@@ -137,6 +137,7 @@ __global__ void k_update64(int n, double* __restrict__ X, const double* __restri
 // ---- preconditioned conjugate gradients (fallback of the refinement)
 
 constexpr int DOT_BLOCKS = 296;   // fixed grid, so the summation order never changes
+constexpr int PCG_STALL = 10;     // iterations over which PCG must at least halve its residual
 
 struct Coef {
   double v[SOLVE_NRHS];
@@ -345,9 +346,11 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
 // alpha and beta come from fixed-order dot products, so a rerun gives the same
 // result bit for bit.  A column whose r.z or p.Ap is not positive (the FP32
 // preconditioner is not exactly symmetric) is frozen.  Returns the iterations
-// used; -1 when some column is not within tol after F->pcg_maxits iterations
-// (X then holds the last iterate and F->dR, F->hnorm its true residual); -2 on
-// a CUDA error.
+// used; -1 when some column is not within tol after F->pcg_maxits iterations,
+// or when the worst scaled residual has not at least halved over the last
+// PCG_STALL iterations (each costs about one FP32 solve, so a stagnating PCG
+// hands over to the FP64 refactorization early); X then holds the last
+// iterate and F->dR, F->hnorm its true residual.  -2 on a CUDA error.
 static int pcg_fp32(Factor* F, int nq, double* X, const double* B, int ld, double tol, double anorm,
                     const double* bnorm, double* res_q) {
   const Plan& P = F->plan;
@@ -393,7 +396,8 @@ static int pcg_fp32(Factor* F, int nq, double* X, const double* B, int ld, doubl
     return worst;
   };
   if (!true_residual()) return -2;
-  std::vector<double> rho(nq), rho_old(nq, 0.0);
+  std::vector<double> rho(nq), rho_old(nq, 0.0), hist;   // hist: worst scaled residual per iteration
+  hist.push_back(scaled(nullptr));
   bool restart = true;
   for (int it = 0; it < F->pcg_maxits;) {
     // z = M^-1 r and rho = r.z
@@ -430,11 +434,14 @@ static int pcg_fp32(Factor* F, int nq, double* X, const double* B, int ld, doubl
     rho_old = rho;
     restart = false;
     it++;
-    if (scaled(nullptr) <= tol) {
+    const double worst = scaled(nullptr);
+    if (worst <= tol) {
       if (!true_residual()) return -2;
       if (scaled(res_q) <= tol) return it;
       restart = true;   // the recursive residual drifted: go on from b - A x
     }
+    hist.push_back(worst);
+    if (it >= PCG_STALL && !(worst <= 0.5 * hist[hist.size() - 1 - PCG_STALL])) break;
   }
   if (!true_residual()) return -2;
   scaled(res_q);
