@@ -616,7 +616,7 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
   }
 }
 
-template <typename T, int NQ, int WS, bool PARTS>
+template <typename T, int NQ, int WS, bool PARTS, bool WARPLOOP = (NQ < 8)>
 __global__ void __launch_bounds__(128)
 k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts,
           const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ Dinv, T* __restrict__ X, int ldx,
@@ -694,7 +694,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   }
   __syncthreads();
   const int col = tid % BR, half = tid / BR;
-  if constexpr (NQ >= 8) {
+  if constexpr (!WARPLOOP) {
     // 8 columns: the block of L11 is staged in shared memory before the wait
     // for x_j (measured faster than the warp-level loop below at 8 columns)
     for (int j = nbs - 1; j > k; j--) {
@@ -825,6 +825,7 @@ static void solve_attrs() {
     cudaFuncSetAttribute(k_bwd_big<T, 4, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 4>());
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
     cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
+    cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
     return true;
   }();
   (void) done;
@@ -916,6 +917,9 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
           k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 2>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
           k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 4>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
+        else if (LP.max_s_big >= FWD_CHAIN_MIN_S)
+          // long chains: the barrier-free warp loop (every block's iterations are on the chain)
+          k_bwd_big<T, 8, SOLVE_NRHS, true, true><<<nb, 128, bwd_smem<T, 8>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else
           k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 8>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         count_launch();
