@@ -1,4 +1,4 @@
-"""FP32 fronts + FP64 iterative refinement (north star's precision path).
+"""FP32 fronts + FP64 iterative refinement (the mixed-precision path).
 
 Bars: scaled residual ||Ax-b||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-12
 (the stated target), forward error against the FP64 GPU solution, and the
