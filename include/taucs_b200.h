@@ -274,6 +274,14 @@ int taucs_b200_export_symbolic(void* L, int* sn_size, int* sn_up_size,
 int taucs_b200_export_values(void* L, long* val_ptr, double* vals);
 /* elimination tree of a permuted lower CCS matrix (parent[n], root = n) */
 int taucs_b200_etree(taucs_ccs_matrix* A, int* parent);
+/* device layout of the level plan, for checking it (host memory only): per
+ * front in device order (info.n_live of them) 12 values: level, parent
+ * (device order, -1 root), s, f, and the offsets in elements of its L panel,
+ * update matrix (-1 if none), solve work vector, diagonal-block inverses (-1
+ * if none), first handshake flag (-1 if none), backward partial sums (-1 if
+ * none), its partial-sum row chunks, and its reference slot; totals: L, U,
+ * work-vector, inverse and partial-sum arena lengths and the flag count. */
+int taucs_b200_export_layout(void* L, long long* fronts, long long* totals);
 
 /* 3D 7-point operator with per-edge conductances exp(sigma*N(0,1)) scaled
  * by (ax, ay, az) on an X x Y x Z grid, Dirichlet boundary (boundary faces

@@ -134,6 +134,7 @@ def lib():
         "taucs_b200_export_symbolic": (C.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i64p, _i32p]),
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
         "taucs_b200_etree": (C.c_int, [pc, _i32p]),
+        "taucs_b200_export_layout": (C.c_int, [vp, vp, vp]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
         "taucs_b200_autotune": (C.c_int, [vp, vp, _i32p]),
         "taucs_b200_profile": (C.c_int, [C.c_int]),
@@ -379,6 +380,16 @@ class Factor:
 
     def set_precision(self, p):
         return lib().taucs_b200_set_precision(self.h, p)
+
+    def layout(self):
+        """(fronts, totals): the plan's per-front device layout as an
+        (n_fronts, 12) int64 array and its arena totals
+        (taucs_b200_export_layout)."""
+        nf = self.info().n_live
+        fr = np.zeros((nf, 12), np.int64)
+        tot = np.zeros(6, np.int64)
+        lib().taucs_b200_export_layout(self.h, fr.ctypes.data, tot.ctypes.data)
+        return fr, tot
 
     def set_pcg(self, maxits):
         """PCG iterations allowed when FP32 refinement stalls (0: go straight

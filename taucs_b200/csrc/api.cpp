@@ -649,6 +649,25 @@ int taucs_b200_export_symbolic(void* vL, int* sn_size, int* sn_up_size, int* fir
   return 0;
 }
 
+int taucs_b200_export_layout(void* vL, long long* fronts, long long* totals) {
+  const Factor* F = (const Factor*) vL;
+  if (!F) return -1;
+  const Plan& P = F->plan;
+  if (fronts)
+    for (int i = 0; i < P.n_fronts; i++) {
+      const FrontDesc& D = P.fronts[i];
+      long long* o = fronts + (size_t) i * 12;
+      o[0] = D.level; o[1] = D.parent; o[2] = D.s; o[3] = D.f;
+      o[4] = D.l_off; o[5] = D.u_off; o[6] = D.v_off; o[7] = D.dinv_off;
+      o[8] = D.blk_off; o[9] = D.part_off; o[10] = D.nchunk; o[11] = D.sn;
+    }
+  if (totals) {
+    totals[0] = P.l_len; totals[1] = P.u_len; totals[2] = P.v_len;
+    totals[3] = P.dinv_len; totals[4] = P.part_len; totals[5] = P.n_blk;
+  }
+  return 0;
+}
+
 int taucs_b200_export_values(void* vL, long* val_ptr, double* vals) {
   Factor* F = (Factor*) vL;
   if (!F) return -1;

@@ -1,0 +1,82 @@
+"""Device layout of the level plan (plan.cpp), checked on the host for every
+front: L panels, solve work vectors, diagonal-block inverses and handshake
+flags never overlap and stay inside their arenas; update matrices that are
+live at the same time (from their front's level through their parent's
+level, where the parent's front build reads them) never overlap; backward
+partial sums of one level never overlap.  An overlap would corrupt a
+factorization or a solve only for some inputs, so the plan is checked
+directly.  Host code only."""
+import numpy as np
+import pytest
+
+from tests.helpers import amd_permuted, random_spd_pattern
+
+BR = 64           # rows of a diagonal block / solve block
+SOLVE_NRHS = 8    # right-hand sides per solve pass (partial-sum stride)
+
+
+def _disjoint(name, starts, lens, total):
+    if starts.size == 0:
+        return
+    order = np.argsort(starts, kind="stable")
+    s = starts[order]
+    e = s + lens[order]
+    assert s[0] >= 0 and e.max() <= total, (name, int(s[0]), int(e.max()), int(total))
+    bad = np.nonzero(s[1:] < e[:-1])[0]
+    assert bad.size == 0, (name, int(s[bad[0] + 1]), int(e[bad[0]]))
+
+
+def check_layout(F):
+    fr, tot = F.layout()
+    level, parent, s, f = fr[:, 0], fr[:, 1], fr[:, 2], fr[:, 3]
+    l_off, u_off, v_off, dinv_off, blk_off, part_off, nchunk = (fr[:, k] for k in range(4, 11))
+    m = f - s
+    assert np.all(s >= 1) and np.all(m >= 0)
+    _disjoint("L panels", l_off, f * s, tot[0])
+    _disjoint("work vectors", v_off, f, tot[2])
+    big = dinv_off >= 0
+    nbs = (s + BR - 1) // BR
+    assert np.array_equal(big, blk_off >= 0)
+    _disjoint("inverses", dinv_off[big], nbs[big] * BR * BR, tot[3])
+    _disjoint("flags", blk_off[big], nbs[big], tot[5])
+    hu = u_off >= 0
+    assert np.array_equal(hu, m > 0)
+    assert np.all(parent[m > 0] >= 0), "a front with update rows has a parent"
+    plev = np.where(parent >= 0, level[np.maximum(parent, 0)], level)
+    assert np.all(plev[hu] > level[hu])
+    for L in range(int(level.max()) + 1):
+        live = hu & (level <= L) & (plev >= L)
+        _disjoint("update matrices at level %d" % L, u_off[live], m[live] ** 2, tot[1])
+        sel = (part_off >= 0) & (level == L)
+        _disjoint("partial sums at level %d" % L, part_off[sel], nchunk[sel] * s[sel] * SOLVE_NRHS, tot[4])
+    return fr, tot
+
+
+@pytest.mark.parametrize("case", ["lognormal64", "mesh2d", "random"])
+def test_single_system_layout(tb, case):
+    if case == "lognormal64":
+        A = tb.lognormal(64, 64, 64, 1.0, (1, 1, 1), 1)
+    elif case == "mesh2d":
+        A = tb.mesh2d(90)
+    else:
+        A = random_spd_pattern(3000, 0.002, 5)
+    P, _, _ = amd_permuted(A)
+    F = tb.factor_symbolic(P)
+    fr, tot = check_layout(F)
+    assert (fr[:, 7] >= 0).any() or case == "random"   # big fronts exist on the grids
+    F.free()
+
+
+def test_batch_layout(tb):
+    rng = np.random.default_rng(3)
+    systems = []
+    for i in range(200):
+        if i % 2:
+            k = int(rng.integers(4, 16))
+            systems.append(tb.lognormal(k, k, k, 1.0, (1, 1, 1), 100 + i))
+        else:
+            k = int(rng.integers(8, 60))
+            systems.append(tb.lognormal(k, k, 0, 1.0, (1, 1, 1), 100 + i))
+    B = tb.Batch(systems)
+    check_layout(B)
+    B.free()
