@@ -282,6 +282,10 @@ int taucs_b200_etree(taucs_ccs_matrix* A, int* parent);
  * none), its partial-sum row chunks, and its reference slot; totals: L, U,
  * work-vector, inverse and partial-sum arena lengths and the flag count. */
 int taucs_b200_export_layout(void* L, long long* fronts, long long* totals);
+/* the solve's block lists of level h (host memory only): (front, 64-row
+ * block) pairs in launch order, forward (*n_diag diagonal blocks first, then
+ * update-row blocks) and backward; with NULL arrays only the counts are set. */
+int taucs_b200_export_solve_blocks(void* L, int h, int* fwd, int* n_fwd, int* n_diag, int* bwd, int* n_bwd);
 
 /* 3D 7-point operator with per-edge conductances exp(sigma*N(0,1)) scaled
  * by (ax, ay, az) on an X x Y x Z grid, Dirichlet boundary (boundary faces

@@ -135,6 +135,8 @@ def lib():
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
         "taucs_b200_etree": (C.c_int, [pc, _i32p]),
         "taucs_b200_export_layout": (C.c_int, [vp, vp, vp]),
+        "taucs_b200_export_solve_blocks": (C.c_int, [vp, C.c_int, vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp,
+                                                     C.POINTER(C.c_int)]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
         "taucs_b200_autotune": (C.c_int, [vp, vp, _i32p]),
         "taucs_b200_profile": (C.c_int, [C.c_int]),
@@ -390,6 +392,17 @@ class Factor:
         tot = np.zeros(6, np.int64)
         lib().taucs_b200_export_layout(self.h, fr.ctypes.data, tot.ctypes.data)
         return fr, tot
+
+    def solve_blocks(self, h):
+        """(fwd, n_diag, bwd): level h's solve block lists, (front, block)
+        rows in launch order (taucs_b200_export_solve_blocks)."""
+        nf, nd, nb = C.c_int(), C.c_int(), C.c_int()
+        lib().taucs_b200_export_solve_blocks(self.h, h, None, C.byref(nf), C.byref(nd), None, C.byref(nb))
+        fwd = np.zeros((nf.value, 2), np.int32)
+        bwd = np.zeros((nb.value, 2), np.int32)
+        lib().taucs_b200_export_solve_blocks(self.h, h, fwd.ctypes.data, C.byref(nf), C.byref(nd), bwd.ctypes.data,
+                                             C.byref(nb))
+        return fwd, nd.value, bwd
 
     def set_pcg(self, maxits):
         """PCG iterations allowed when FP32 refinement stalls (0: go straight

@@ -668,6 +668,24 @@ int taucs_b200_export_layout(void* vL, long long* fronts, long long* totals) {
   return 0;
 }
 
+int taucs_b200_export_solve_blocks(void* vL, int h, int* fwd, int* n_fwd, int* n_diag, int* bwd, int* n_bwd) {
+  const Factor* F = (const Factor*) vL;
+  if (!F || h < 0 || h >= F->plan.n_levels) return -1;
+  const LevelPlan& LP = F->plan.levels[h];
+  if (n_fwd) *n_fwd = (int) LP.solve_fwd_blocks.size();
+  if (n_diag) *n_diag = LP.n_fwd_diag;
+  if (n_bwd) *n_bwd = (int) LP.solve_bwd_blocks.size();
+  for (size_t i = 0; fwd && i < LP.solve_fwd_blocks.size(); i++) {
+    fwd[2 * i] = LP.solve_fwd_blocks[i].a;
+    fwd[2 * i + 1] = LP.solve_fwd_blocks[i].b;
+  }
+  for (size_t i = 0; bwd && i < LP.solve_bwd_blocks.size(); i++) {
+    bwd[2 * i] = LP.solve_bwd_blocks[i].a;
+    bwd[2 * i + 1] = LP.solve_bwd_blocks[i].b;
+  }
+  return 0;
+}
+
 int taucs_b200_export_values(void* vL, long* val_ptr, double* vals) {
   Factor* F = (Factor*) vL;
   if (!F) return -1;

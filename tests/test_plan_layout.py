@@ -80,3 +80,47 @@ def test_batch_layout(tb):
     B = tb.Batch(systems)
     check_layout(B)
     B.free()
+
+
+def check_solve_order(F):
+    """Every solve block comes after the blocks of its front that it waits
+    for, in the launch order of its level (a CTA must never wait for a CTA
+    that is launched after it): forward, the diagonal blocks of all big
+    fronts first, each front's in increasing order, then the update-row
+    blocks; backward, each front's column blocks in decreasing order.  Each
+    level's lists cover its big fronts' blocks exactly once."""
+    fr, _ = F.layout()
+    level, s, f, dinv_off = fr[:, 0], fr[:, 2], fr[:, 3], fr[:, 7]
+    nbs = (s + BR - 1) // BR
+    nrb = (f + BR - 1) // BR
+    for h in range(F.info().n_levels):
+        fwd, nd, bwd = F.solve_blocks(h)
+        big = np.nonzero((level == h) & (dinv_off >= 0))[0]
+        if big.size == 0:
+            assert fwd.shape[0] == 0 and bwd.shape[0] == 0
+            continue
+        assert np.all(level[fwd[:, 0]] == h) and np.all(dinv_off[fwd[:, 0]] >= 0)
+        diag, upd = fwd[:nd], fwd[nd:]
+        assert np.all(diag[:, 1] < nbs[diag[:, 0]]), "diagonal blocks first"
+        assert np.all(upd[:, 1] >= nbs[upd[:, 0]])
+        assert np.all(upd[:, 1] < nrb[upd[:, 0]])
+        for fi in big:
+            rows = diag[diag[:, 0] == fi, 1]
+            assert np.array_equal(rows, np.arange(nbs[fi])), ("forward diagonal order", int(fi))
+            assert np.array_equal(np.sort(upd[upd[:, 0] == fi, 1]), np.arange(nbs[fi], nrb[fi]))
+            cols = bwd[bwd[:, 0] == fi, 1]
+            assert np.array_equal(cols, np.arange(nbs[fi])[::-1]), ("backward order", int(fi))
+        assert set(np.unique(bwd[:, 0])) == set(big.tolist())
+
+
+@pytest.mark.parametrize("case", ["lognormal48_aniso", "mesh2d", "batch"])
+def test_solve_block_order(tb, case):
+    if case == "batch":
+        systems = [tb.lognormal(k, k, k, 1.0, (1, 1, 1), k) for k in range(10, 26)]
+        F = tb.Batch(systems)
+    else:
+        A = tb.lognormal(48, 48, 48, 2.0, (1, 1, 100), 0) if case == "lognormal48_aniso" else tb.mesh2d(120)
+        P, _, _ = amd_permuted(A)
+        F = tb.factor_symbolic(P)
+    check_solve_order(F)
+    F.free()
