@@ -275,13 +275,17 @@ int taucs_b200_export_values(void* L, long* val_ptr, double* vals);
 /* elimination tree of a permuted lower CCS matrix (parent[n], root = n) */
 int taucs_b200_etree(taucs_ccs_matrix* A, int* parent);
 /* device layout of the level plan, for checking it (host memory only): per
- * front in device order (info.n_live of them) 12 values: level, parent
+ * front in device order (info.n_live of them) 14 values: level, parent
  * (device order, -1 root), s, f, and the offsets in elements of its L panel,
  * update matrix (-1 if none), solve work vector, diagonal-block inverses (-1
  * if none), first handshake flag (-1 if none), backward partial sums (-1 if
- * none), its partial-sum row chunks, and its reference slot; totals: L, U,
- * work-vector, inverse and partial-sum arena lengths and the flag count. */
+ * none), its partial-sum row chunks, its reference slot, and the offsets of
+ * its row list (f global rows, ascending) and of its map into its parent's
+ * row list (f - s local indices); totals: L, U, work-vector, inverse and
+ * partial-sum arena lengths, the flag count, and the lengths of the row-list
+ * and map arrays that taucs_b200_export_rows_maps fills. */
 int taucs_b200_export_layout(void* L, long long* fronts, long long* totals);
+int taucs_b200_export_rows_maps(void* L, int* rows, int* maps);
 /* the solve's block lists of level h (host memory only): (front, 64-row
  * block) pairs in launch order, forward (*n_diag diagonal blocks first, then
  * update-row blocks) and backward; with NULL arrays only the counts are set. */

@@ -135,6 +135,7 @@ def lib():
         "taucs_b200_export_values": (C.c_int, [vp, _i64p, _f64p]),
         "taucs_b200_etree": (C.c_int, [pc, _i32p]),
         "taucs_b200_export_layout": (C.c_int, [vp, vp, vp]),
+        "taucs_b200_export_rows_maps": (C.c_int, [vp, vp, vp]),
         "taucs_b200_export_solve_blocks": (C.c_int, [vp, C.c_int, vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp,
                                                      C.POINTER(C.c_int)]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
@@ -385,13 +386,22 @@ class Factor:
 
     def layout(self):
         """(fronts, totals): the plan's per-front device layout as an
-        (n_fronts, 12) int64 array and its arena totals
+        (n_fronts, 14) int64 array and its arena totals
         (taucs_b200_export_layout)."""
         nf = self.info().n_live
-        fr = np.zeros((nf, 12), np.int64)
-        tot = np.zeros(6, np.int64)
+        fr = np.zeros((nf, 14), np.int64)
+        tot = np.zeros(8, np.int64)
         lib().taucs_b200_export_layout(self.h, fr.ctypes.data, tot.ctypes.data)
         return fr, tot
+
+    def rows_maps(self):
+        """(rows, maps): the plan's per-front global row lists and
+        child-to-parent maps (offsets in layout() columns 12 and 13)."""
+        _, tot = self.layout()
+        rows = np.zeros(max(int(tot[6]), 1), np.int32)
+        maps = np.zeros(max(int(tot[7]), 1), np.int32)
+        lib().taucs_b200_export_rows_maps(self.h, rows.ctypes.data, maps.ctypes.data)
+        return rows[:int(tot[6])], maps[:int(tot[7])]
 
     def solve_blocks(self, h):
         """(fwd, n_diag, bwd): level h's solve block lists, (front, block)

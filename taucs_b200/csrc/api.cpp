@@ -656,15 +656,25 @@ int taucs_b200_export_layout(void* vL, long long* fronts, long long* totals) {
   if (fronts)
     for (int i = 0; i < P.n_fronts; i++) {
       const FrontDesc& D = P.fronts[i];
-      long long* o = fronts + (size_t) i * 12;
+      long long* o = fronts + (size_t) i * 14;
       o[0] = D.level; o[1] = D.parent; o[2] = D.s; o[3] = D.f;
       o[4] = D.l_off; o[5] = D.u_off; o[6] = D.v_off; o[7] = D.dinv_off;
       o[8] = D.blk_off; o[9] = D.part_off; o[10] = D.nchunk; o[11] = D.sn;
+      o[12] = D.rows_off; o[13] = D.map_off;
     }
   if (totals) {
     totals[0] = P.l_len; totals[1] = P.u_len; totals[2] = P.v_len;
     totals[3] = P.dinv_len; totals[4] = P.part_len; totals[5] = P.n_blk;
+    totals[6] = (long long) P.rows.size(); totals[7] = (long long) P.maps.size();
   }
+  return 0;
+}
+
+int taucs_b200_export_rows_maps(void* vL, int* rows, int* maps) {
+  const Factor* F = (const Factor*) vL;
+  if (!F) return -1;
+  if (rows) std::copy(F->plan.rows.begin(), F->plan.rows.end(), rows);
+  if (maps) std::copy(F->plan.maps.begin(), F->plan.maps.end(), maps);
   return 0;
 }
 

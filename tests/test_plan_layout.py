@@ -124,3 +124,41 @@ def test_solve_block_order(tb, case):
         F = tb.factor_symbolic(P)
     check_solve_order(F)
     F.free()
+
+
+def check_rows_maps(F, n):
+    """Row lists ascend and lie in [0, n); the pivot rows of all fronts cover
+    every row exactly once; each child-to-parent map ascends strictly and
+    points at the same global rows in the parent's list (what extend-add and
+    the solve gathers rely on)."""
+    fr, _ = F.layout()
+    rows, maps = F.rows_maps()
+    parent, s, f, roff, moff = fr[:, 1], fr[:, 2], fr[:, 3], fr[:, 12], fr[:, 13]
+    seen = np.zeros(n, np.int32)
+    for i in range(fr.shape[0]):
+        R = rows[roff[i]:roff[i] + f[i]]
+        assert R.size == f[i] and np.all(np.diff(R) > 0) and R[0] >= 0 and R[-1] < n, i
+        seen[R[:s[i]]] += 1
+        m = f[i] - s[i]
+        if m > 0:
+            p = parent[i]
+            Rp = rows[roff[p]:roff[p] + f[p]]
+            mp = maps[moff[i]:moff[i] + m]
+            assert np.all(np.diff(mp) > 0) and mp[0] >= 0 and mp[-1] < f[p], i
+            assert np.array_equal(Rp[mp], R[s[i]:]), i
+    assert np.all(seen == 1)
+
+
+@pytest.mark.parametrize("case", ["lognormal40", "random", "batch"])
+def test_rows_and_maps(tb, case):
+    if case == "batch":
+        systems = [tb.lognormal(k, k, 0, 1.0, (1, 1, 1), k) for k in range(6, 70, 3)]
+        F = tb.Batch(systems)
+        n = F.n
+    else:
+        A = tb.lognormal(40, 40, 40, 1.0, (1, 1, 1), 2) if case == "lognormal40" else random_spd_pattern(2500, 0.003, 9)
+        P, _, _ = amd_permuted(A)
+        F = tb.factor_symbolic(P)
+        n = P.n
+    check_rows_maps(F, n)
+    F.free()
