@@ -51,6 +51,13 @@ SAMPLE_GRID = 56          # bounded CPU sample of the lognormal workload
 
 KC = dict(small_front=0, build=1, potrf=2, trsm=3, gemm_panel=4, gemm_u=5, solve_fwd=6, solve_bwd=7)
 TENSOR_KC = {"gemm_panel", "gemm_u", "trsm", "potrf"}
+# DRAM traffic per algorithmic byte of a kernel class, from one ncu capture
+# of a 56^3 update-matrix launch (FP32 fronts): dram read + write 109.7 MB
+# against 146.7 MB of L21 read once and U read and written once; the bench
+# scales it to its own per-launch algorithmic bytes
+TRAFFIC_PER_ALG_BYTE = {"gemm_u": (109.7 / 146.7, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 56^3 "
+                                                  "update-matrix launch, scaled by algorithmic bytes (L21 read once, "
+                                                  "U read and written once) to this launch size")}
 
 
 def parse():
@@ -754,12 +761,21 @@ def roofline(kern, tensor_peak, tensor_src, hbm_peak):
     dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])[0]
     d = kern[dom]
     per_launch_ms = d["ms_per_step"] / max(d["launches_per_step"], 1)
+    bytes_per_launch = d.get("gb_per_step", 0.0) / max(d["launches_per_step"], 1) * 1e9
+    traffic, traffic_src = None, None
+    if dom in TRAFFIC_PER_ALG_BYTE and bytes_per_launch > 0:
+        ratio, traffic_src = TRAFFIC_PER_ALG_BYTE[dom]
+        traffic = ratio * bytes_per_launch
     if dom in TENSOR_KC:
         ach = d["gflop_per_step"] / d["ms_per_step"]  # GFLOP/ms = TFLOP/s
-        return {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": tensor_peak, "unit": "TFLOP/s",
-                "frac": ach / tensor_peak, "peak_source": tensor_src,
-                "algorithmic_per_launch": d["gflop_per_step"] / max(d["launches_per_step"], 1) * 1e9,
-                "avg_launch_ms": per_launch_ms, "traffic": None}
+        out = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": tensor_peak, "unit": "TFLOP/s",
+               "frac": ach / tensor_peak, "peak_source": tensor_src,
+               "algorithmic_per_launch": d["gflop_per_step"] / max(d["launches_per_step"], 1) * 1e9,
+               "avg_launch_ms": per_launch_ms, "traffic": traffic,
+               "algorithmic_bytes_per_launch": bytes_per_launch}
+        if traffic_src:
+            out["traffic_source"] = traffic_src
+        return out
     ach = d["gb_per_step"] / d["ms_per_step"] * 1e3
     return {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
             "frac": ach / hbm_peak if hbm_peak else None,

@@ -690,22 +690,25 @@ static double front_flops(const FrontDesc& F) {
   return fl;
 }
 
-static double build_bytes(const Plan& P, const FrontDesc& F) {
+// algorithmic bytes of building one front, values of esz bytes: children's U
+// read once (plus their maps), panel and U written once, A entries (value +
+// row index)
+static double build_bytes(const Plan& P, const FrontDesc& F, double esz) {
   double by = 0.0;
   for (int ci = F.child_begin; ci < F.child_end; ci++) {
     const FrontDesc& C = P.fronts[P.children[ci]];
     const double mc = C.f - C.s;
-    by += 8.0 * mc * (mc + 1.0) / 2.0 + 4.0 * mc;
+    by += esz * mc * (mc + 1.0) / 2.0 + 4.0 * mc;
   }
   const double m = F.f - F.s;
-  by += 8.0 * ((double) F.f * F.s - (double) F.s * (F.s - 1) / 2.0) + 8.0 * m * (m + 1.0) / 2.0;
-  by += 12.0 * (P.acol_ptr[F.acol_off + F.s] - P.acol_ptr[F.acol_off]);
+  by += esz * ((double) F.f * F.s - (double) F.s * (F.s - 1) / 2.0) + esz * m * (m + 1.0) / 2.0;
+  by += (esz + 4.0) * (P.acol_ptr[F.acol_off + F.s] - P.acol_ptr[F.acol_off]);
   return by;
 }
 
 // small fronts: read children's U and A once, write panel and U once
-static double front_bytes(const Plan& P, const FrontDesc& F) {
-  return build_bytes(P, F);
+static double front_bytes(const Plan& P, const FrontDesc& F, double esz) {
+  return build_bytes(P, F, esz);
 }
 
 // GEMM variant of level h for the panel updates (kind 0) or the update
@@ -789,7 +792,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
             for (int q = b; q < e; q++) {
               const FrontDesc& F = P.fronts[LP.small_fronts[q]];
               fl += front_flops(F);
-              by += front_bytes(P, F);
+              by += front_bytes(P, F, sizeof(T));
             }
           prof_begin(KC_SMALL, st);
           k_small_front<T><<<e - b, 128, smem, st>>>(lst + b, D.fronts, D.children, D.maps, D.rows,
@@ -807,7 +810,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
     {
       double by = 0.0;
       if (prof_enabled())
-        for (int fi : LP.big_fronts) by += build_bytes(P, P.fronts[fi]);
+        for (int fi : LP.big_fronts) by += build_bytes(P, P.fronts[fi], sizeof(T));
       prof_begin(KC_BUILD, st);
       k_build<T><<<ntiles, 256, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
                                       D.a_rows, D.a_idx, vals, L, U, status);
@@ -832,9 +835,9 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
         if (prof_enabled()) {
           const double ww = w, below = F.f - kb - w;
           fp += ww * ww * ww / 3.0;
-          bp += 8.0 * ww * ww;
+          bp += sizeof(T) * ww * ww;
           ft += 2.0 * below * ww * ww;
-          bt += 16.0 * below * ww + 8.0 * ww * ww;
+          bt += 2.0 * sizeof(T) * below * ww + sizeof(T) * ww * ww;
         }
       }
       prof_begin(KC_POTRF, st);
@@ -863,7 +866,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
           const double c = ce - c_lo, below = F.f - ce, k = k_hi - k_lo;
           const double entries = c * (c + 1.0) / 2.0 + below * c;
           fg += 2.0 * k * entries;
-          bg += 16.0 * entries + 8.0 * k * (F.f - c_lo);
+          bg += 2.0 * sizeof(T) * entries + sizeof(T) * k * (F.f - c_lo);
         }
       }
       if (gx64 == 0) return;
@@ -901,7 +904,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
           const FrontDesc& F = P.fronts[fi];
           const double m = F.f - F.s;
           fu += 2.0 * F.s * m * (m + 1.0) / 2.0;
-          bu += 16.0 * m * (m + 1.0) / 2.0 + 8.0 * m * F.s;
+          bu += 2.0 * sizeof(T) * m * (m + 1.0) / 2.0 + sizeof(T) * m * F.s;
         }
       prof_begin(KC_GEMM_U, st);
       (void) maxm;

@@ -802,9 +802,11 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 
 // algorithmic bytes of one pass over a front: the lower panel once, its
 // row indices, and the gather/scatter of nrhs vector entries per row
-static double solve_pass_bytes(const FrontDesc& F, int nrhs) {
+// algorithmic bytes of one solve pass over a front, values of esz bytes: the
+// lower panel read once, its row list, the work vector read and written
+static double solve_pass_bytes(const FrontDesc& F, int nrhs, double esz) {
   const double s = F.s, m = F.f - F.s;
-  return 8.0 * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * 8.0 * nrhs * F.f;
+  return esz * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * esz * nrhs * F.f;
 }
 
 template <typename T>
@@ -848,7 +850,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       const LevelPlan& LP = P.levels[h];
       double by = 0.0;
       if (prof_enabled())
-        for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq);
+        for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq, sizeof(T));
       prof_begin(KC_SOLVE_FWD, st);
       const int ns = (int) LP.small_fronts.size();
       if (ns > 0) {
@@ -897,7 +899,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
       const LevelPlan& LP = P.levels[h];
       double by = 0.0;
       if (prof_enabled())
-        for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq);
+        for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq, sizeof(T));
       prof_begin(KC_SOLVE_BWD, st);
       const int nb = (int) LP.solve_bwd_blocks.size();
       if (nb > 0) {
