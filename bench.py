@@ -755,7 +755,10 @@ def read_profile(tb, nsteps):
     return kern
 
 
-def roofline(kern, tensor_peak, tensor_src, hbm_peak):
+def roofline(kern, tensor_peak, tensor_src, hbm_peak, traffic_table=None):
+    """The dominant kernel's roofline.  traffic_table (kernel class ->
+    (DRAM bytes per algorithmic byte, source)) is passed only for the run whose
+    kernel and sizes the ncu capture matches (FP32 fronts at 80^3)."""
     if not kern:
         return None
     dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])[0]
@@ -763,8 +766,8 @@ def roofline(kern, tensor_peak, tensor_src, hbm_peak):
     per_launch_ms = d["ms_per_step"] / max(d["launches_per_step"], 1)
     bytes_per_launch = d.get("gb_per_step", 0.0) / max(d["launches_per_step"], 1) * 1e9
     traffic, traffic_src = None, None
-    if dom in TRAFFIC_PER_ALG_BYTE and bytes_per_launch > 0:
-        ratio, traffic_src = TRAFFIC_PER_ALG_BYTE[dom]
+    if traffic_table and dom in traffic_table and bytes_per_launch > 0:
+        ratio, traffic_src = traffic_table[dom]
         traffic = ratio * bytes_per_launch
     if dom in TENSOR_KC:
         ach = d["gflop_per_step"] / d["ms_per_step"]  # GFLOP/ms = TFLOP/s
@@ -942,7 +945,7 @@ def run_ours(args):
     else:
         tensor_peak = fp64_gemm_peak()
         tensor_src = "FP64: cuBLAS DGEMM 8192^3 measured in this run (of measured)"
-    roof = roofline(kern, tensor_peak, tensor_src, hbm_peak)
+    roof = roofline(kern, tensor_peak, tensor_src, hbm_peak, TRAFFIC_PER_ALG_BYTE if mixed else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
