@@ -530,7 +530,7 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
               done = true;
               continue;
             }
-            tprintf("\t\tPCG did not converge in %d iterations\n", F->pcg_maxits);
+            tprintf("\t\tPCG did not reach the tolerance (stalled, or %d iterations)\n", F->pcg_maxits);
           }
           tprintf("\t\trefinement stalled at %.3e after %d steps; refactoring in FP64\n", worst, steps);
           if (!F->has_numeric && numeric_fp64_device(F, F->dvals_cur, true)) return -1;
