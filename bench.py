@@ -220,123 +220,181 @@ def tf32_gemm_peak():
 
 # ---------------------------------------------------------------- CPU (reference)
 
-def ref_system(workload, g):
-    """The workload's PAP^T in the reference library (oracle/_ref): the matrix
-    comes from the same generator, the ordering from the reference's AMD."""
-    import taucs_b200 as tb
-    from oracle.bindings import Ref
-    R = Ref()
+def ref_inputs(workload, g):
+    """The workload's P A P^T for the reference library, built without the
+    product library: the oracle's independent statement of the lognormal
+    generator (bit-identical to the product's, tests/test_oracle.py) or the
+    reference's own mesh3d, then the reference's AMD ordering and symmetric
+    permutation.  Returns (Ref, n, colptr, rowind, values, B)."""
+    from oracle.bindings import Port, Ref, ref_available
+    if not ref_available():
+        raise RuntimeError("oracle/_ref/libtaucs_ref.so was not built")
+    R, port = Ref(), Port()
     if workload == "mixed80":
-        A = tb.lognormal(g, g, g, 2.0, (1.0, 1.0, 100.0), 0)
-        n, cp, ri, va = A.n, A.colptr, A.rowind, A.values
+        n, cp, ri, va = port.lognormal(g, g, g, 2.0, (1.0, 1.0, 100.0), 0)
     else:
         n, cp, ri, va = R.mesh3d(g, g, g)
     perm, iperm = R.order(n, cp, ri, va, "amd")
     _, pc, pr, pv = R.permute(n, cp, ri, va, perm, iperm)
-    return R, n, pc, pr, pv
-
-
-def ref_step(R, L, n, pc, pr, pv, B):
-    assert R.numeric(L, n, pc, pr, pv) == 0
-    X = np.empty_like(B)
-    for q in range(B.shape[1]):       # the reference solves one right-hand side per call
-        X[:, q] = R.solve(L, np.ascontiguousarray(B[:, q]))
-    return X
-
-
-def cpu_reference(workload, g, n_threads, steps=1, warmup=0):
-    """The reference's CPU multifrontal path (sources + OpenBLAS) on this
-    host's cores.  mixed80: a bounded sample -- the same generator at
-    SAMPLE_GRID^3 -- whose time is scaled by the reference's flop count to the
-    full grid; fp64-64: the full system.  Returns (seconds per full system,
-    description, kind, cores)."""
-    from oracle.bindings import Port, Ref, ref_available
-    os.environ["OPENBLAS_NUM_THREADS"] = str(n_threads)
-    if not ref_available():
-        raise RuntimeError("oracle/_ref/libtaucs_ref.so was not built")
-    gs = SAMPLE_GRID if workload == "mixed80" else g
-    R, n, pc, pr, pv = ref_system(workload, gs)
-    R.set_threads(n_threads)
-    L = R.symbolic(n, pc, pr, pv)
-    flops_s = R.dump_symbolic(L).flops()
     rng = np.random.default_rng(0)
-    B = rng.uniform(-1, 1, (n, NRHS)) if workload == "mixed80" else \
-        Port().spmv(n, pc, pr, pv, rng.uniform(-1, 1, n)).reshape(-1, 1)
-    for _ in range(warmup):
-        ref_step(R, L, n, pc, pr, pv, B)
-        R.free_numeric(L)
-    times = []
+    if workload == "mixed80":
+        B = rng.uniform(-1, 1, (n, NRHS))
+    else:
+        B = port.spmv(n, pc, pr, pv, rng.uniform(-1, 1, n)).reshape(-1, 1)
+    return R, port, n, pc, pr, pv, B
+
+
+def ref_steps(R, L, n, pc, pr, pv, B, steps, threads):
+    """`steps` runs of the reference's pattern-reuse path (numeric factor on
+    the analysed pattern, src/taucs_sn_llt.c:2169-2209, then one
+    taucs_supernodal_solve_llt per right-hand side, :2844-2885) with
+    `threads` OpenBLAS threads.  Returns (factor s, solve s) per step and the
+    last step's X."""
+    R.set_threads(threads)
+    tf, ts, X = [], [], None
     for _ in range(steps):
         t0 = time.perf_counter()
-        ref_step(R, L, n, pc, pr, pv, B)
-        times.append(time.perf_counter() - t0)
+        if R.numeric(L, n, pc, pr, pv) != 0:
+            raise RuntimeError("reference numeric factorization failed")
+        t1 = time.perf_counter()
+        X = np.empty_like(B)
+        for q in range(B.shape[1]):       # the reference solves one right-hand side per call
+            X[:, q] = R.solve(L, np.ascontiguousarray(B[:, q]))
+        ts.append(time.perf_counter() - t1)
+        tf.append(t1 - t0)
         R.free_numeric(L)
+    return tf, ts, X
+
+
+def lower_inf_norm(n, cp, ri, va):
+    """||A||_inf of the symmetric matrix stored as its lower triangle."""
+    col = np.repeat(np.arange(n), np.diff(cp))
+    a = np.abs(va)
+    rs = np.zeros(n)
+    np.add.at(rs, ri, a)
+    np.add.at(rs, col[ri != col], a[ri != col])
+    return float(rs.max())
+
+
+def x_checksum(X):
+    """Per-column sums and max-abs of a solution block (compared across arms)."""
+    return {"sum": [float(v) for v in X.sum(axis=0)], "max_abs": [float(v) for v in np.abs(X).max(axis=0)]}
+
+
+def cpu_baseline_sample(workload, g_full, flops_full, threads_list, g_sample=SAMPLE_GRID):
+    """The bounded CPU-baseline leg of this arm: the reference (sources +
+    OpenBLAS 0.3.15) on a smaller grid of the same generator, one factor + all
+    solves per thread count, its time scaled by the reference's flop count to
+    the full grid.  Returns the cpu_baseline object."""
+    if workload != "mixed80":
+        g_sample = g_full
+    R, _, n, pc, pr, pv, B = ref_inputs(workload, g_sample)
+    L = R.symbolic(n, pc, pr, pv)
+    fl = R.dump_symbolic(L).flops()
+    scale = flops_full / fl if workload == "mixed80" else 1.0
+    out = {}
+    for th in threads_list:
+        tf, ts, _ = ref_steps(R, L, n, pc, pr, pv, B, 1, th)
+        out[th] = (tf[0] + ts[0]) * scale, tf[0] + ts[0]
     R.free(L)
-    dt = sum(times) / len(times)
-    if workload == "mixed80":
-        import taucs_b200 as tb
-        A, _, _, P, _ = make_system(workload, g)
-        flops_f = tb.factor_symbolic(P).info().flops
-        scale = flops_f / flops_s
-        desc = (f"reference FP64 factor + {NRHS} one-RHS solves of the {gs}^3 lognormal system "
-                f"(same generator, sigma=2, aniso 1:1:100, AMD), {dt:.2f} s, scaled by the reference's "
-                f"flop count x{scale:.2f} to {g}^3; sources + OpenBLAS 0.3.15, {n_threads} threads")
-        return dt * scale, desc, "reference", n_threads
-    desc = (f"reference FP64 numeric factor + 1-RHS solve of the full {g}^3 system "
-            f"(sources + OpenBLAS 0.3.15, {n_threads} threads)")
-    return dt, desc, "reference", n_threads
+    th0 = threads_list[0]
+    what = (f"reference FP64 numeric factor + {B.shape[1]} one-RHS solves of the {g_sample}^3 system of the same "
+            f"generator (sigma=2, aniso 1:1:100, AMD)") if workload == "mixed80" else \
+        f"reference FP64 numeric factor + 1-RHS solve of the full {g_full}^3 system"
+    res = {"value": 1.0 / out[th0][0], "unit": UNIT, "cores": th0, "kind": "reference",
+           "sample": what + (f", scaled by the reference's flop count x{scale:.2f} to {g_full}^3" if scale != 1.0
+                             else "") + "; sources + OpenBLAS 0.3.15",
+           "per_thread_count": {str(th): {"systems_per_s": 1.0 / v[0], "sample_s": v[1]} for th, v in out.items()}}
+    return res
 
 
 def run_reference(args):
+    """The reference's own CPU multifrontal path on the FULL workload (no
+    sampling, no scaling), in a process that loads only the oracle libraries
+    (oracle/_ref): numeric factor + solves of the same seeded system, timed at
+    all host threads; one more step at one OpenBLAS thread is reported beside
+    it.  Each step takes about a minute on the box, so at most two timed
+    steps run (no warm-up: nothing is compiled or cached between steps; the
+    reference allocates its fronts afresh every time)."""
     rank, _, world = dist_env()
     if rank != 0:
         return
-    g = args.grid or (80 if args.workload == "mixed80" else 64)
-    n_threads = os.cpu_count() or 1
     if args.workload == "batch4096":
-        try:
-            import taucs_b200 as tb
-            systems, bs = batch_systems(tb, args.batch_count)
-            flops = 0.0
-            for A in systems:
-                p, ip = tb.order(A, "amd")
-                F = tb.factor_symbolic(A.permute(p, ip))
-                flops += F.info().flops
-                F.free()
-            t_s, fl_s, ns = cpu_reference_batch(systems, bs, n_threads)
-            sec = t_s * flops / fl_s
-        except Exception as exc:
-            print(json.dumps({"impl": "reference", "unavailable": repr(exc)}))
-            return
-        val = args.batch_count / sec
-        desc = (f"reference FP64 factor + solve of {ns} evenly spaced systems of the batch one at a time "
-                f"({t_s:.2f} s), scaled by the reference's flop count to all {args.batch_count} systems; "
-                f"sources + OpenBLAS 0.3.15, {n_threads} threads")
-        print(json.dumps({"impl": "reference", "metric": METRIC_BATCH, "value": val, "unit": UNIT, "n_gpus": world,
-                          "steps": 1, "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True,
-                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                          "config": {"workload": f"{args.batch_count} systems"},
-                          "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                          "cpu_baseline": {"value": val, "unit": UNIT, "cores": n_threads, "kind": "reference",
-                                           "sample": desc}}))
-        return
+        return run_reference_batch(args, world)
+    g = args.grid or (80 if args.workload == "mixed80" else 64)
+    nproc = os.cpu_count() or 1
     try:
-        # bounded: one warm-up and at most 3 timed steps of the bounded sample
-        warm = min(args.warmup, 1)
-        steps = max(1, min(args.steps, 3))
-        sec, desc, kind, cores = cpu_reference(args.workload, g, n_threads, steps=steps, warmup=warm)
+        t_setup = time.perf_counter()
+        R, port, n, pc, pr, pv, B = ref_inputs(args.workload, g)
+        L = R.symbolic(n, pc, pr, pv)
+        sym = R.dump_symbolic(L)
+        flops = sym.flops()
+        t_setup = time.perf_counter() - t_setup
+        steps = max(1, min(args.steps, 2))
+        tf, ts, X = ref_steps(R, L, n, pc, pr, pv, B, steps, nproc)
+        tf1, ts1, _ = ref_steps(R, L, n, pc, pr, pv, B, 1, 1)
+        R.free(L)
     except Exception as exc:  # one line, never a traceback
         print(json.dumps({"impl": "reference", "unavailable": repr(exc)}))
         return
+    anorm = lower_inf_norm(n, pc, pr, pv)
+    res = max(float(np.max(np.abs(port.spmv(n, pc, pr, pv, X[:, q]) - B[:, q])) /
+                    (anorm * np.max(np.abs(X[:, q])) + np.max(np.abs(B[:, q])))) for q in range(B.shape[1]))
+    sec = (sum(tf) + sum(ts)) / steps
+    sec1 = tf1[0] + ts1[0]
     val = 1.0 / sec
     metric = METRIC_MIXED if args.workload == "mixed80" else METRIC_FP64
+    desc = (f"reference FP64 numeric factor + {B.shape[1]} one-RHS solves of the full {g}^3 system "
+            f"({steps} timed steps at {nproc} threads); sources + OpenBLAS 0.3.15")
     out = {"impl": "reference", "metric": metric, "value": val, "unit": UNIT, "n_gpus": world,
-           "steps": steps, "warmup": warm, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+           "steps": steps, "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": workload_name(args.workload, g)},
+           "config": workload_config(args.workload, g, n, len(pv), B.shape[1]),
            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-           "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}}
+           "cpu_baseline": {"value": val, "unit": UNIT, "cores": nproc, "kind": "reference", "sample": desc},
+           "steps_note": (f"{args.steps} steps requested; each full step takes about a minute of CPU time, so "
+                          f"{steps} are timed"),
+           "factor_s": sum(tf) / steps, "solve_s": sum(ts) / steps, "setup_s": t_setup,
+           "factor_gflop_s": flops / (sum(tf) / steps) / 1e9, "flops": flops,
+           "supernodes": int(np.count_nonzero(sym.sn_size)),
+           "one_thread": {"value": 1.0 / sec1, "unit": UNIT, "factor_s": tf1[0], "solve_s": ts1[0],
+                          "factor_gflop_s": flops / tf1[0] / 1e9},
+           "scaled_residual": res, "x_checksum": x_checksum(X)}
     print(json.dumps(out))
+
+
+def run_reference_batch(args, world):
+    try:
+        import taucs_b200 as tb
+        systems, bs = batch_systems(tb, args.batch_count)
+        flops = 0.0
+        for A in systems:
+            p, ip = tb.order(A, "amd")
+            F = tb.factor_symbolic(A.permute(p, ip))
+            flops += F.info().flops
+            F.free()
+        n_threads = os.cpu_count() or 1
+        t_s, fl_s, ns = cpu_reference_batch(systems, bs, n_threads)
+        sec = t_s * flops / fl_s
+    except Exception as exc:
+        print(json.dumps({"impl": "reference", "unavailable": repr(exc)}))
+        return
+    val = args.batch_count / sec
+    desc = (f"reference FP64 factor + solve of {ns} evenly spaced systems of the batch one at a time "
+            f"({t_s:.2f} s), scaled by the reference's flop count to all {args.batch_count} systems; "
+            f"sources + OpenBLAS 0.3.15, {n_threads} threads")
+    print(json.dumps({"impl": "reference", "metric": METRIC_BATCH, "value": val, "unit": UNIT, "n_gpus": world,
+                      "steps": 1, "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": f"{args.batch_count} systems"},
+                      "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                      "cpu_baseline": {"value": val, "unit": UNIT, "cores": n_threads, "kind": "reference",
+                                       "sample": desc}}))
+
+
+def workload_config(workload, g, n, nnz, nrhs):
+    """The `config` object both arms print (it names the workload only)."""
+    return {"workload": workload_name(workload, g), "n": int(n), "nnz_lower": int(nnz), "nrhs": int(nrhs)}
 
 
 def workload_name(workload, g):
@@ -950,9 +1008,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            nth = os.cpu_count() or 1
-            sec, desc, kind, cores = cpu_reference(args.workload, g, nth)
-            cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
+            cpu = cpu_baseline_sample(args.workload, g, info.flops, [os.cpu_count() or 1, 1])
         except Exception as exc:  # report, never hide
             cpu = {"error": repr(exc)}
 
@@ -971,8 +1027,8 @@ def run_ours(args):
         "metric": METRIC_MIXED if mixed else METRIC_FP64, "value": world * K / (ms * 1e-3), "unit": UNIT,
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.workload, g), "n": n, "nnz_lower": nnz, "nrhs": nrhs,
-                   "flops": info.flops, "supernodes": info.n_live, "levels": info.n_levels,
+        "config": workload_config(args.workload, g, n, nnz, nrhs),
+        "problem": {"flops": info.flops, "supernodes": info.n_live, "levels": info.n_levels,
                    "max_front": info.max_front, "l_gb_fp64": info.l_bytes / 1e9,
                    "u_arena_gb_fp64": info.u_bytes / 1e9,
                    "l2_policy": "inputs larger than L2 (several GB of L and update arena touched per step)",
@@ -986,6 +1042,7 @@ def run_ours(args):
         "kernels": kern,
         "cpu_baseline": cpu,
         "scaled_residual": {"device": res_main, "e2e": res_e2e},
+        "x_checksum": x_checksum(X),
     }
     if mixed:
         out["refinement_steps"] = steps_main

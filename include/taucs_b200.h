@@ -199,20 +199,31 @@ int taucs_b200_factor_status(void* L);
 int taucs_b200_solve_device(void* L, int nrhs, double* d_X, const double* d_B, int ld);
 
 /* No counterpart in the reference.  The same device solve for callers that
- * must not allocate device memory: code that runs while a stream is being
- * captured into a CUDA graph, where an allocation would break the capture,
- * and serving threads that live inside a fixed, pre-reserved memory budget.
- * Work vectors, handshake flags and the status word live in one static
- * device array of this library (32 MiB of work vectors + 16384 flags; every
- * GPU that loads the library holds it until exit), so the call allocates
- * nothing; factors needing more work space are rejected with -1 and a
- * message in taucs_b200_last_error().  Right-hand sides are solved one per
- * pass.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the array: calls whose work overlaps on the GPU (different
- * streams, or different host threads on one device) race and must be
- * serialised by the caller.  Asynchronous on the current stream. */
+ * must not allocate device memory: serving threads that live inside a fixed,
+ * pre-reserved memory budget they may not grow, latency-critical threads
+ * that may not call cudaMalloc/cudaFree (which can synchronise the device
+ * and stall other streams), and hosts whose own caching allocator already
+ * holds the rest of the GPU's memory.  Work vectors, handshake flags and the
+ * status word live in one static device array of this library (32 MiB of
+ * work vectors + 16384 flags; every GPU that loads the library holds it
+ * until exit), so the call allocates nothing; factors needing more work
+ * space are rejected with -1 and a message in taucs_b200_last_error(), and
+ * so is a call made while another device than the factor's is current.
+ * Right-hand sides are solved one per pass.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) and sets the solve
+ * kernels' shared-memory limits on that device, so make that first call
+ * before any stream capture.  All calls share the array: calls whose work
+ * overlaps on the GPU (different streams, or different host threads on one
+ * device) race and must be serialised by the caller.  Asynchronous on the
+ * current stream. */
 int taucs_b200_solve_device_noalloc(void* L, int nrhs, double* d_X, const double* d_B, int ld);
+/* Status of the no-alloc solves on the current device: waits for the current
+ * stream, then returns 0, or -1 when a bounded wait between thread blocks
+ * gave up in one of them (the solution is then not valid; the message is in
+ * taucs_b200_last_error()).  Each no-alloc solve clears the status word when
+ * it starts, so the status covers the last no-alloc solve issued on the
+ * device: call this after each one whose result you need. */
+int taucs_b200_solve_device_noalloc_status(void);
 
 /* nrhs right-hand sides in HOST memory (column-major, leading dimension n) */
 int taucs_b200_solve_many(void* L, int nrhs, double* X, const double* B);

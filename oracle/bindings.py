@@ -67,11 +67,11 @@ class Symbolic:
         """The reference's relaxed flop count, src/taucs_sn_llt.c:3957-3965."""
         s = self.sn_size.astype(np.float64)
         f = self.sn_up_size.astype(np.float64)
-        tot = 0.0
-        for sn in range(self.n_sn):
-            c = f[sn] - np.arange(int(s[sn]))
-            tot += float(np.sum(1.0 + c * c))
-        return tot
+
+        def sq(x):   # sum of c^2 for c = 1..x
+            return x * (x + 1.0) * (2.0 * x + 1.0) / 6.0
+        # sum over the s columns of 1 + c^2, c = f, f-1, ..., f-s+1
+        return float(np.sum(s + sq(f) - sq(f - s)))
 
 
 def dense_lower_entries(sym, val_ptr, vals):
@@ -295,6 +295,9 @@ class Port:
         L.orc_values.argtypes = [C.c_void_p, _i64p, _f64p]
         L.orc_solve.argtypes = [C.c_void_p, _f64p, _f64p]
         L.orc_spmv_sym_lower.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+        L.orc_generate_lognormal.restype = C.c_long
+        L.orc_generate_lognormal.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                             C.c_double, C.c_ulonglong, _i32p, _i32p, _f64p]
 
     def etree(self, n, cp, ri):
         par = np.empty(n, np.int32)
@@ -344,3 +347,17 @@ class Port:
         y = np.empty(n, np.float64)
         self.lib.orc_spmv_sym_lower(n, cp, ri, va, np.ascontiguousarray(x, np.float64), y)
         return y
+
+    def lognormal(self, X, Y, Z, sigma, aniso, seed):
+        """The benchmarks' lognormal-coefficient operator, stated independently
+        of the product library: (n, colptr, rowind, values) of the lower CCS."""
+        N = X * Y * max(Z, 1)
+        per = 3 if Z == 0 else 4
+        cp = np.empty(N + 1, np.int32)
+        ri = np.empty(per * N, np.int32)
+        va = np.empty(per * N, np.float64)
+        nnz = self.lib.orc_generate_lognormal(X, Y, Z, float(sigma), float(aniso[0]), float(aniso[1]),
+                                              float(aniso[2]), int(seed), cp, ri, va)
+        if nnz < 0:
+            raise ValueError("bad grid")
+        return N, cp, ri[:nnz].copy(), va[:nnz].copy()

@@ -647,3 +647,87 @@ void orc_spmv_sym_lower(int n, const int* colptr, const int* rowind, const doubl
       if (i != j) y[j] += x[i] * val[ip];
     }
 }
+
+/* ----------------------------------------------- lognormal operator inputs */
+
+/* The seeded lognormal-coefficient 7-point (or, Z == 0, 5-point) operator the
+ * benchmarks factor.  The reference has no generator for it, so this is a
+ * second, independent statement of the input generator of the product
+ * library (taucs_b200_generate_lognormal), kept here so that a process that
+ * times the reference can build its inputs without loading the product:
+ * per-edge conductance scale * exp(sigma * N(0,1)), N(0,1) by Box-Muller on
+ * two splitmix64-hashed uniforms of the edge's stream id; off-diagonal -c,
+ * the diagonal accumulates c (and the Dirichlet boundary faces' conductances);
+ * lower CCS in the row order of taucs_ccs_generate_mesh3d
+ * (src/taucs_ccs_generators.c:197-261).  The arrays hold at least X*Y*Z + 1
+ * column pointers and (Z == 0 ? 3 : 4) * X*Y*Z entries; returns the entry
+ * count, or -1 for bad sizes. */
+static unsigned long long orc_splitmix64(unsigned long long x)
+{
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+static double orc_cond(unsigned long long seed, unsigned long long k, double sigma, double scale)
+{
+  unsigned long long a = orc_splitmix64(seed ^ (2 * k));
+  unsigned long long b = orc_splitmix64(seed ^ (2 * k + 1) ^ 0xD1B54A32D192ED03ull);
+  double u1 = ((double) (a >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+  double u2 = (double) (b >> 11) * (1.0 / 9007199254740992.0);
+  double g = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+  return scale * exp(sigma * g);
+}
+
+long orc_generate_lognormal(int X, int Y, int Z, double sigma, double ax, double ay, double az,
+                            unsigned long long seed, int* colptr, int* rowind, double* val)
+{
+  int two_d = (Z == 0), x, y, z, j, N, ip = 0;
+  unsigned long long NN, fb;
+  double* diag;
+  if (two_d) Z = 1;
+  if (X <= 0 || Y <= 0 || Z <= 0) return -1;
+  N = X * Y * Z;
+  NN = (unsigned long long) N;
+  diag = (double*) calloc((size_t) N, sizeof(double));
+  if (!diag) return -1;
+  for (z = 0; z < Z; z++)
+    for (y = 0; y < Y; y++)
+      for (x = 0; x < X; x++) {
+        double c;
+        j = z * X * Y + y * X + x;
+        colptr[j] = ip;
+        if (x < X - 1) {
+          c = orc_cond(seed, 3 * (unsigned long long) j + 0, sigma, ax);
+          rowind[ip] = j + 1; val[ip] = -c; ip++;
+          diag[j] += c; diag[j + 1] += c;
+        }
+        if (y < Y - 1) {
+          c = orc_cond(seed, 3 * (unsigned long long) j + 1, sigma, ay);
+          rowind[ip] = j + X; val[ip] = -c; ip++;
+          diag[j] += c; diag[j + X] += c;
+        }
+        if (!two_d && z < Z - 1) {
+          c = orc_cond(seed, 3 * (unsigned long long) j + 2, sigma, az);
+          rowind[ip] = j + X * Y; val[ip] = -c; ip++;
+          diag[j] += c; diag[j + X * Y] += c;
+        }
+        fb = 3 * NN + 6 * (unsigned long long) j;
+        if (x == 0) diag[j] += orc_cond(seed, fb + 0, sigma, ax);
+        if (x == X - 1) diag[j] += orc_cond(seed, fb + 1, sigma, ax);
+        if (y == 0) diag[j] += orc_cond(seed, fb + 2, sigma, ay);
+        if (y == Y - 1) diag[j] += orc_cond(seed, fb + 3, sigma, ay);
+        if (!two_d) {
+          if (z == 0) diag[j] += orc_cond(seed, fb + 4, sigma, az);
+          if (z == Z - 1) diag[j] += orc_cond(seed, fb + 5, sigma, az);
+        }
+        rowind[ip] = j;
+        val[ip] = 0.0;
+        ip++;
+      }
+  colptr[N] = ip;
+  for (j = 0; j < N; j++) val[colptr[j + 1] - 1] = diag[j];
+  free(diag);
+  return ip;
+}

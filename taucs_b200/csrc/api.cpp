@@ -278,22 +278,35 @@ int numeric_fp64_device(Factor* F, const double* d_vals, bool wait) {
   F->has_numeric = true;
   if (!wait) return 0;
   if (!cuda_ok(cudaStreamSynchronize(st), "numeric factorization")) return -1;
-  if (*F->hstatus != INT_MAX) {
-    tprintf("\t\tLL^T Factorization: Matrix is not positive definite.\n");
-    tprintf("\t\t                    nonpositive pivot in column %d\n", *F->hstatus);
+  if (numeric_status_check(*F->hstatus, "LL^T Factorization") != 0) {
     free_numeric(F);
     return -1;
   }
   return 0;
 }
 
-int numeric_fp32_device(Factor* F, const double* d_vals);
+int numeric_status_check(int word, const char* what) {
+  if (word == INT_MAX) return 0;
+  if (word == NUMERIC_TIMEOUT) {
+    set_error(std::string(what) + ": a bounded wait between thread blocks timed out; the factor is not valid");
+    tprintf("\t\t%s: a bounded device wait timed out\n", what);
+    return -1;
+  }
+  set_error(std::string(what) + ": matrix is not positive definite (nonpositive pivot in column " +
+            std::to_string(word) + ")");
+  tprintf("\t\t%s: Matrix is not positive definite.\n", what);
+  tprintf("\t\t                    nonpositive pivot in column %d\n", word);
+  return 1;
+}
+
 
 int numeric_device(Factor* F, const double* d_vals, bool wait) {
   if (F->precision == 1) {
-    // FP32 fronts; a nonpositive FP32 pivot falls back to the FP64 factor
+    // FP32 fronts; only a nonpositive FP32 pivot falls back to the FP64
+    // factor (a timed-out wait or a CUDA error is reported as it is)
     invalidate_numeric(F);
-    if (numeric_fp32_device(F, d_vals) == 0) return 0;
+    const int r = numeric_fp32_device(F, d_vals);
+    if (r <= 0) return r;
     tprintf("\t\tFP32 factorization failed; refactoring in FP64\n");
     return numeric_fp64_device(F, d_vals, true);
   }
@@ -514,7 +527,7 @@ int taucs_b200_factor_status(void* vL) {
   if (!F || (!F->has_numeric && !F->has_numeric32)) return -1;
   if (!F->has_numeric) return 0;
   if (!cuda_ok(cudaStreamSynchronize(current_stream()), "status")) return -1;
-  if (*F->hstatus != INT_MAX) { free_numeric(F); return -1; }
+  if (numeric_status_check(*F->hstatus, "LL^T Factorization") != 0) { free_numeric(F); return -1; }
   return 0;
 }
 

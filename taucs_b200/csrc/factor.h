@@ -114,5 +114,12 @@ void free_numeric(Factor* F);
 // marks the numeric factors stale without freeing their buffers
 void invalidate_numeric(Factor* F);
 int numeric_fp64_device(Factor* F, const double* d_vals, bool wait);
+// FP32 fronts: 0 on success, 1 on a nonpositive pivot (the caller may
+// refactor in FP64), -1 on any other failure (message set)
+int numeric_fp32_device(Factor* F, const double* d_vals);
+// Reads a numeric factorization's status word: 0 (INT_MAX, success), 1 (a
+// nonpositive pivot; its column is logged) or -1 (NUMERIC_TIMEOUT: a bounded
+// device wait gave up).  Sets the error message for both failures.
+int numeric_status_check(int word, const char* what);
 
 }  // namespace tb

@@ -350,16 +350,15 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
 // variant 0: two-stage ring (65 KB), 128 producers, three CTAs per SM;
 // variant 1: three-stage ring (97 KB), 256 producers, two CTAs per SM
 bool gemm_tc_init() {
-  // once per process (a function-local static: request-server workers reach
-  // this concurrently)
-  static const bool ready = [] {
+  // once per device (request-server workers reach this concurrently)
+  static PerDeviceOnce pd;
+  return per_device_once(pd, [] {
     const cudaError_t e0 = cudaFuncSetAttribute(k_gemm_tc<2, 3, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int) tc_smem<2>());
     const cudaError_t e1 = cudaFuncSetAttribute(k_gemm_tc<3, 2, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int) tc_smem<3>());
     return e0 == cudaSuccess && e1 == cudaSuccess;
-  }();
-  return ready;
+  });
 }
 
 int gemm_tc_tiles(int rows, int cols) {

@@ -49,7 +49,7 @@ extern "C" int taucs_conjugate_gradients(taucs_ccs_matrix* A, int (*precond_fn)(
   taucs_ccs_times_vec(A, X, R.data());
   for (int i = 0; i < n; i++) R[i] = B[i] - R[i];
   double res_norm = two_norm(n, R.data()), init_norm = res_norm;
-  tprintf("cg: two norm of initial residual %.2e\n", init_norm);
+  tprintf("cg: starting residual, 2-norm %.2e\n", init_norm);
   if (init_norm == 0.0) init_norm = 1.0;
   double ratio = 1.0, rho0 = 0.0;
   int iter = 0;
@@ -78,13 +78,13 @@ extern "C" int taucs_conjugate_gradients(taucs_ccs_matrix* A, int (*precond_fn)(
     res_norm = two_norm(n, R.data());
     ratio = res_norm / init_norm;
     if (iter % 25 == 0)
-      tprintf("cg: n=%d at iteration %d the convergence ratio is %.2e, Rnorm %.2e\n", n, iter, ratio, res_norm);
+      tprintf("cg: iteration %d (n=%d): residual reduced by %.2e, 2-norm %.2e\n", iter, n, ratio, res_norm);
   }
   if (iter > 0) {
-    tprintf("cg: n=%d iterations = %d Reduction in residual norm %.2e, Rnorm %.2e\n", n, iter, ratio, res_norm);
+    tprintf("cg: stopped after %d iterations (n=%d): residual reduced by %.2e, 2-norm %.2e\n", iter, n, ratio, res_norm);
     taucs_ccs_times_vec(A, X, R.data());
     for (int i = 0; i < n; i++) R[i] = B[i] - R[i];
-    tprintf("cg: true residual norm %.2e\n", two_norm(n, R.data()));
+    tprintf("cg: recomputed residual b - A x, 2-norm %.2e\n", two_norm(n, R.data()));
   }
   return TAUCS_SUCCESS;
 }

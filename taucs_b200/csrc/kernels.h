@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <mutex>
 #include <vector>
 #include <cuda_runtime.h>
 
@@ -118,6 +119,18 @@ int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, const flo
 
 // launch accounting
 void count_launch(long k = 1);
+
+// Per-device one-time setup.  Function attributes such as the dynamic
+// shared-memory limit belong to the device that is current when they are
+// set, so every launcher runs its setup once on each device it is used on.
+// Returns the setup's result for the current device (false if there is no
+// current device).  Safe to call from several host threads at once.
+constexpr int MAX_DEVICES = 64;
+struct PerDeviceOnce {
+  std::once_flag once[MAX_DEVICES];
+  bool ok[MAX_DEVICES] = {};
+};
+bool per_device_once(PerDeviceOnce& pd, bool (*setup)());
 
 // Optional per-kernel-class timing: when enabled, launchers bracket every
 // launch of a class with CUDA events on the launch stream and record the

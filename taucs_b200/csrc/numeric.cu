@@ -750,9 +750,9 @@ static constexpr size_t potrf_smem() { return (2 * PANEL_NB * DLD + 32 * DLD) * 
 
 template <typename T>
 static void set_smem_attrs() {
-  // once per process and type; a function-local static, because request-server
-  // workers reach this concurrently
-  static const bool done = [] {
+  // once per device and type (request-server workers reach this concurrently)
+  static PerDeviceOnce pd;
+  per_device_once(pd, [] {
     cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
     cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) potrf_smem<T>());
@@ -763,8 +763,7 @@ static void set_smem_attrs() {
     cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          2 * PANEL_NB * TLD * (int) sizeof(T));
     return true;
-  }();
-  (void) done;
+  });
 }
 
 template <typename T>

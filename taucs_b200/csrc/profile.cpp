@@ -8,6 +8,13 @@
 
 namespace tb {
 
+bool per_device_once(PerDeviceOnce& pd, bool (*setup)()) {
+  int d = -1;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= MAX_DEVICES) return false;
+  std::call_once(pd.once[d], [&] { pd.ok[d] = setup(); });
+  return pd.ok[d];
+}
+
 namespace {
 
 struct Rec {

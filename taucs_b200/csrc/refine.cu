@@ -318,7 +318,7 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
   if (!cuda_ok(cudaStreamSynchronize(st), "scaling")) return -1;
   if (*F->hstatus != INT_MAX) {
     tprintf("\t\tscaling: nonpositive diagonal in column %d\n", *F->hstatus);
-    return -1;
+    return 1;
   }
   int e = run_graphed(F, GraphKey{2, (uint64_t) F->dA32, 0, 0, 0, 0}, st, [&](cudaStream_t s) {
     return launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dstatus, s);
@@ -326,10 +326,8 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (!cuda_ok(cudaStreamSynchronize(st), "numeric factorization (FP32)")) return -1;
-  if (*F->hstatus != INT_MAX) {
-    tprintf("\t\tFP32 fronts: nonpositive pivot in column %d\n", *F->hstatus);
-    return -1;
-  }
+  const int rc = numeric_status_check(*F->hstatus, "FP32 fronts");
+  if (rc != 0) return rc;
   F->has_numeric32 = true;
   return 0;
 }

@@ -811,9 +811,9 @@ static double solve_pass_bytes(const FrontDesc& F, int nrhs, double esz) {
 
 template <typename T>
 static void solve_attrs() {
-  // once per process and type; a function-local static, because request-server
-  // workers reach this concurrently
-  static const bool done = [] {
+  // once per device and type (request-server workers reach this concurrently)
+  static PerDeviceOnce pd;
+  per_device_once(pd, [] {
     // static + dynamic shared memory of these kernels can exceed the default
     // 48 KB (8 columns in FP64)
     cudaFuncSetAttribute(k_fwd_big<T, 2, SOLVE_NRHS, FWD_ALL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) fwd_smem<T, FWD_ALL>());
@@ -829,8 +829,7 @@ static void solve_attrs() {
     cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
     return true;
-  }();
-  (void) done;
+  });
 }
 
 template <typename T>
@@ -963,14 +962,16 @@ int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, const flo
 // ------------------------------------------------------------------------
 // Solve without any allocation.
 //
-// Callers that must not allocate device memory -- code running while a CUDA
-// stream is being captured into a graph (a cudaMalloc there breaks the
-// capture), or a latency-critical serving thread that works inside a fixed,
-// pre-reserved memory budget and may not grow it -- can still solve with an
-// existing factor: taucs_b200_solve_device_noalloc keeps the solve's work
-// vectors, handshake flags and status word in the one static device array
-// below instead of the factor's own buffers.  It is the same level-scheduled
-// solve as taucs_b200_solve_device, run one right-hand side per pass.
+// Some callers must not allocate device memory: a serving thread that works
+// inside a fixed, pre-reserved memory budget it may not grow; a latency-
+// critical thread that may not call cudaMalloc/cudaFree because they can
+// synchronise the device and stall every other stream; a host framework whose
+// caching allocator already holds the rest of the GPU's memory.  They can
+// still solve with an existing factor: taucs_b200_solve_device_noalloc keeps
+// the solve's work vectors, handshake flags and status word in the one static
+// device array below instead of the factor's own buffers.  It is the same
+// level-scheduled solve as taucs_b200_solve_device, run one right-hand side
+// per pass.  taucs_b200_solve_device_noalloc_status reads the status word.
 // ------------------------------------------------------------------------
 
 namespace tb {
@@ -1074,6 +1075,11 @@ extern "C" int taucs_b200_solve_device_noalloc(void* vL, int nrhs, double* d_X, 
     set_error("taucs_b200_solve_device_noalloc: the factor has no numeric part");
     return -1;
   }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != F->device) {
+    set_error("taucs_b200_solve_device_noalloc: the current device is not the one the factor lives on");
+    return -1;
+  }
   if (nrhs == 0) return 0;
   double* base = nullptr;
   if (noalloc_scratch(&base)) return -1;
@@ -1097,6 +1103,28 @@ extern "C" int taucs_b200_solve_device_noalloc(void* vL, int nrhs, double* d_X, 
       set_error(std::string("taucs_b200_solve_device_noalloc: ") + cudaGetErrorString(e));
       return -1;
     }
+  }
+  return 0;
+}
+
+// Status of the no-alloc solves issued on the current device: waits for the
+// current stream, then reads the status word that those solves share.
+extern "C" int taucs_b200_solve_device_noalloc_status(void) {
+  using namespace tb;
+  double* base = nullptr;
+  if (noalloc_scratch(&base)) return -1;
+  const int* status = (const int*) (base + NOALLOC_W_DOUBLES) + NOALLOC_FLAGS;
+  cudaError_t e = cudaStreamSynchronize(current_stream());
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    set_error(std::string("taucs_b200_solve_device_noalloc_status: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  if (h != 0) {
+    set_error("taucs_b200_solve_device_noalloc: a bounded wait between thread blocks timed out; "
+              "the solution is not valid");
+    return -1;
   }
   return 0;
 }

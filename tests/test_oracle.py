@@ -73,3 +73,17 @@ def test_port_maxdepth(port):
     h = port.analyze(n, cp, ri, 10000)
     assert h
     port.free(h)
+
+
+@pytest.mark.parametrize("args", [(80, 80, 80, 2.0, (1, 1, 100), 0), (7, 5, 3, 1.0, (1, 2, 3), 9),
+                                  (30, 20, 0, 1.5, (1, 1, 1), 4), (1, 1, 1, 1.0, (1, 1, 1), 2)])
+def test_port_lognormal_generator_is_the_products(args, port):
+    """The oracle's own statement of the lognormal operator (used by the
+    reference timing arm, which must not load the product library) gives the
+    product generator's matrix bit for bit."""
+    import taucs_b200 as tb
+    A = tb.lognormal(*args)
+    n, cp, ri, va = port.lognormal(*args)
+    assert n == A.n
+    assert np.array_equal(cp, A.colptr) and np.array_equal(ri, A.rowind)
+    assert np.array_equal(va, A.values)
