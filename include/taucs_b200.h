@@ -281,7 +281,10 @@ int taucs_b200_export_symbolic(void* L, int* sn_size, int* sn_up_size,
                                int* first_child, int* next_child,
                                long* struct_ptr, int* struct_idx);
 /* numeric panels as f x s column-major per supernode, rows in sn_struct order
- * (the reference's order), val_ptr[n_sn+1] offsets */
+ * (the reference's order), val_ptr[n_sn+1] offsets.  The FP64 factor; a
+ * handle that holds only an FP32 factor (taucs_b200_set_precision(L, 1))
+ * exports that one, the factor of the scaled matrix D A D with
+ * D = diag(A)^-1/2, widened to double. */
 int taucs_b200_export_values(void* L, long* val_ptr, double* vals);
 /* elimination tree of a permuted lower CCS matrix (parent[n], root = n) */
 int taucs_b200_etree(taucs_ccs_matrix* A, int* parent);
@@ -341,6 +344,12 @@ long taucs_b200_profile_log(int* kernel_class, float* ms, long cap);
  * receives the variant per level: [2h] panel, [2h + 1] update matrix.
  * Returns 0, or -1 when a factorization failed. */
 int taucs_b200_autotune(void* L, const double* d_values, int* choices);
+
+/* Sets the GEMM variant per level and product for `precision` (0 FP64
+ * fronts, 1 FP32 fronts) -- e.g. choices an earlier taucs_b200_autotune
+ * returned for the same pattern, kept by the caller.  count = 2 x levels
+ * (layout as in taucs_b200_autotune), or 0 for the default variants. */
+int taucs_b200_set_gemm_choices(void* L, int precision, int count, const int* choices);
 
 /* CUDA kernel launches issued by this library on the calling thread since
  * the last reset (for launch accounting in benchmarks). */

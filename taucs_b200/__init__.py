@@ -140,6 +140,8 @@ def lib():
                                                      C.POINTER(C.c_int)]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
         "taucs_b200_autotune": (C.c_int, [vp, vp, _i32p]),
+        "taucs_b200_set_gemm_choices": (C.c_int, [vp, C.c_int, C.c_int, _i32p]),
+        "taucs_b200_solve_device_noalloc_status": (C.c_int, []),
         "taucs_b200_profile": (C.c_int, [C.c_int]),
         "taucs_b200_profile_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]),
@@ -383,6 +385,13 @@ class Factor:
 
     def set_precision(self, p):
         return lib().taucs_b200_set_precision(self.h, p)
+
+    def set_gemm_choices(self, precision, choices):
+        """GEMM variant per level and product (taucs_b200_set_gemm_choices);
+        an empty sequence restores the defaults."""
+        ch = np.ascontiguousarray(choices, dtype=np.int32)
+        if lib().taucs_b200_set_gemm_choices(self.h, precision, ch.size, ch if ch.size else np.zeros(1, np.int32)):
+            raise RuntimeError("set_gemm_choices failed: " + last_error())
 
     def layout(self):
         """(fronts, totals): the plan's per-front device layout as an

@@ -373,38 +373,76 @@ int solve_host(Factor* F, int nrhs, double* X, const double* B) {
   return solve_status(F, st);
 }
 
-// L panels in the reference's row order (f x s per slot, ld f)
-static int download_ref_panels(Factor* F, std::vector<long>& vptr, std::vector<double>& vals) {
-  if (!F->has_numeric) return -1;
-  const Plan& P = F->plan;
-  const Symbolic& S = F->sym;
-  std::vector<double> hL((size_t) P.l_len);
-  cudaStream_t st = current_stream();
-  if (!cuda_ok(cudaMemcpyAsync(hL.data(), F->dL, sizeof(double) * (size_t) P.l_len, cudaMemcpyDeviceToHost, st), "L download")) return -1;
-  if (!cuda_ok(cudaStreamSynchronize(st), "L download")) return -1;
-  vptr.assign(S.n_sn + 1, 0);
+// Panel offsets in the reference's slot layout: s x f doubles per slot.
+static long ref_panel_offsets(const Symbolic& S, long* vptr) {
   long tot = 0;
   for (int sn = 0; sn < S.n_sn; sn++) { vptr[sn] = tot; tot += (long) S.sn_size[sn] * S.sn_up_size[sn]; }
   vptr[S.n_sn] = tot;
-  vals.assign(std::max(tot, 1L), 0.0);
+  return tot;
+}
+
+// L panels in the reference's row order (f x s per slot, ld f) written into
+// out (ref_panel_offsets layout).  The FP64 factor when there is one, else the
+// FP32 factor (of the scaled matrix D A D) widened to double.  The device
+// arena is copied one level at a time, so the host holds out plus one
+// level's panels.
+static int download_ref_panels_into(Factor* F, const long* vptr, double* out) {
+  const bool f64 = F->has_numeric;
+  if (!f64 && !F->has_numeric32) return -1;
+  const Plan& P = F->plan;
+  const Symbolic& S = F->sym;
+  cudaStream_t st = current_stream();
+  std::vector<double> hL;
+  std::vector<float> hL32;
   std::vector<int> local;
-  for (const FrontDesc& Fd : P.fronts) {
-    const int sn = Fd.sn, s = Fd.s, f = Fd.f;
-    const std::vector<int>& st_ = S.sn_struct[sn];
-    const int* rw = P.rows.data() + Fd.rows_off;
-    local.resize(f);
-    for (int k = 0; k < f; k++) local[k] = (int) (std::lower_bound(rw, rw + f, st_[k]) - rw);
-    const double* pan = hL.data() + Fd.l_off;
-    double* out = vals.data() + vptr[sn];
-    for (int jp = 0; jp < s; jp++) {
-      const int lj = local[jp];
-      for (int ip = jp; ip < f; ip++) {
-        const int li = local[ip];
-        out[(size_t) jp * f + ip] = (li >= lj) ? pan[li + (size_t) lj * f] : 0.0;
+  for (const LevelPlan& LP : P.levels) {
+    if (LP.front_begin >= LP.front_end) continue;
+    // a level's panels are contiguous in the L arena
+    int64_t lo = INT64_MAX, hi = 0;
+    for (int i = LP.front_begin; i < LP.front_end; i++) {
+      const FrontDesc& Fd = P.fronts[i];
+      lo = std::min(lo, Fd.l_off);
+      hi = std::max(hi, Fd.l_off + (int64_t) Fd.f * Fd.s);
+    }
+    const size_t cnt = (size_t) (hi - lo);
+    bool ok;
+    if (f64) {
+      hL.resize(cnt);
+      ok = cuda_ok(cudaMemcpyAsync(hL.data(), F->dL + lo, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st), "L download");
+    } else {
+      hL32.resize(cnt);
+      ok = cuda_ok(cudaMemcpyAsync(hL32.data(), F->dL32 + lo, sizeof(float) * cnt, cudaMemcpyDeviceToHost, st), "L download");
+    }
+    if (!ok || !cuda_ok(cudaStreamSynchronize(st), "L download")) return -1;
+    for (int i = LP.front_begin; i < LP.front_end; i++) {
+      const FrontDesc& Fd = P.fronts[i];
+      const int sn = Fd.sn, s = Fd.s, f = Fd.f;
+      const std::vector<int>& st_ = S.sn_struct[sn];
+      const int* rw = P.rows.data() + Fd.rows_off;
+      local.resize(f);
+      for (int k = 0; k < f; k++) local[k] = (int) (std::lower_bound(rw, rw + f, st_[k]) - rw);
+      const size_t base = (size_t) (Fd.l_off - lo);
+      double* o = out + vptr[sn];
+      for (int jp = 0; jp < s; jp++) {
+        const int lj = local[jp];
+        for (int ip = 0; ip < jp; ip++) o[(size_t) jp * f + ip] = 0.0;
+        for (int ip = jp; ip < f; ip++) {
+          const int li = local[ip];
+          const size_t at = base + li + (size_t) lj * f;
+          o[(size_t) jp * f + ip] = (li >= lj) ? (f64 ? hL[at] : (double) hL32[at]) : 0.0;
+        }
       }
     }
   }
   return 0;
+}
+
+static int download_ref_panels(Factor* F, std::vector<long>& vptr, std::vector<double>& vals) {
+  if (!F->has_numeric) return -1;
+  vptr.assign(F->sym.n_sn + 1, 0);
+  const long tot = ref_panel_offsets(F->sym, vptr.data());
+  vals.assign(std::max(tot, 1L), 0.0);
+  return download_ref_panels_into(F, vptr.data(), vals.data());
 }
 
 static int order_identity(int n, int* p, int* ip) {
@@ -466,6 +504,28 @@ int taucs_b200_autotune(void* L, const double* d_values, int* choices) {
   drop_graphs(F);
   tprintf("\t\tautotune (%s fronts): GEMM time %.2f ms with the default variants, %.2f ms with the chosen ones\n",
           pi ? "FP32" : "FP64", before, after);
+  return 0;
+}
+
+int taucs_b200_set_gemm_choices(void* L, int precision, int count, const int* choices) {
+  Factor* F = (Factor*) L;
+  if (!F || (precision != 0 && precision != 1) || count < 0 || (count > 0 && !choices)) return -1;
+  const int H = F->plan.n_levels;
+  if (count != 0 && count != 2 * H) {
+    set_error("taucs_b200_set_gemm_choices: expected 2 x levels (" + std::to_string(2 * H) + ") choices");
+    return -1;
+  }
+  std::vector<uint8_t>& c = F->plan.gemm_choice[precision];
+  c.assign((size_t) count, 0);
+  for (int i = 0; i < count; i++) {
+    if (choices[i] != 0 && choices[i] != 1) {
+      c.clear();
+      set_error("taucs_b200_set_gemm_choices: a choice is neither 0 nor 1");
+      return -1;
+    }
+    c[i] = (uint8_t) choices[i];
+  }
+  drop_graphs(F);
   return 0;
 }
 
@@ -712,12 +772,12 @@ int taucs_b200_export_solve_blocks(void* vL, int h, int* fwd, int* n_fwd, int* n
 int taucs_b200_export_values(void* vL, long* val_ptr, double* vals) {
   Factor* F = (Factor*) vL;
   if (!F) return -1;
-  std::vector<long> vp;
-  std::vector<double> v;
-  if (download_ref_panels(F, vp, v)) return -1;
-  std::copy(vp.begin(), vp.end(), val_ptr);
-  std::copy(v.begin(), v.begin() + vp.back(), vals);
-  return 0;
+  if (!F->has_numeric && !F->has_numeric32) {
+    set_error("taucs_b200_export_values: the factor has no numeric part");
+    return -1;
+  }
+  ref_panel_offsets(F->sym, val_ptr);
+  return download_ref_panels_into(F, val_ptr, vals);
 }
 
 int taucs_b200_etree(taucs_ccs_matrix* A, int* parent) {

@@ -111,3 +111,24 @@ def test_maxdepth_symbolic(tb):
 def test_unknown_ordering_fails(tb):
     A = tb.mesh2d(5)
     assert tb.order(A, "colamd") == (None, None)
+
+
+@pytest.mark.parametrize("which", ["mesh3d_64", "lognormal_80"])
+def test_host_phase_matches_reference_at_benchmark_sizes(tb, ref, which):
+    """The two benchmark systems (64^3 mesh3d, 35,565 live supernodes; 80^3
+    lognormal, 70,679): AMD permutation, etree and the whole supernodal
+    structure bit-exact against the reference at full size."""
+    A = tb.mesh3d(64) if which == "mesh3d_64" else tb.lognormal(80, 80, 80, 2.0, (1, 1, 100), 0)
+    perm_r, iperm_r = ref.order(*A.arrays(), "amd")
+    perm, iperm = tb.order(A, "amd")
+    assert np.array_equal(perm, perm_r) and np.array_equal(iperm, iperm_r)
+    P = A.permute(perm, iperm)
+    assert np.array_equal(tb.etree(P), ref.etree(*P.arrays()))
+    Lr = ref.symbolic(*P.arrays())
+    F = tb.factor_symbolic(P)
+    sr = ref.dump_symbolic(Lr)
+    assert same_symbolic(F.export_symbolic(), sr)
+    assert int(np.count_nonzero(sr.sn_size)) == F.info().n_live
+    assert abs(F.info().flops - sr.flops()) <= 1e-9 * sr.flops()
+    ref.free(Lr)
+    F.free()

@@ -1,12 +1,13 @@
 """The allocation-free device solve (taucs_b200_solve_device_noalloc).
 
-Callers inside a CUDA-graph capture or inside a fixed device-memory budget
-cannot allocate; this entry point serves them from a static device array.
-Checked through the C ABI against the regular device solve on the same
-factor and right-hand sides, twice in a row (the static array keeps the
-previous call's contents, so the second call also checks that whatever
-must start at zero is cleared), plus the size limit.  This file is named so
-that pytest collects it last.
+Callers that work inside a fixed, pre-reserved device-memory budget, or may
+not call cudaMalloc at all, cannot let the solve allocate its work vectors;
+this entry point serves them from a static device array.  Checked through
+the C ABI against the regular device solve on the same factor and
+right-hand sides, twice in a row (the static array keeps the previous
+call's contents, so the second call also checks that whatever must start at
+zero is cleared), with the status query after each call, plus the size
+limit.  This file is named so that pytest collects it last.
 """
 import ctypes as C
 
@@ -41,6 +42,7 @@ def test_noalloc_solve_matches_device_solve_twice(tb):
     for out in (out1, out2):
         rc = lib.taucs_b200_solve_device_noalloc(F.h, nrhs, C.c_void_p(out.data_ptr()), C.c_void_p(dB.data_ptr()), n)
         assert rc == 0, tb.last_error()
+        assert lib.taucs_b200_solve_device_noalloc_status() == 0, tb.last_error()
     torch.cuda.synchronize()
     xr, x1, x2 = ref.cpu().numpy(), out1.cpu().numpy(), out2.cpu().numpy()
     for x in (x1, x2):
