@@ -807,6 +807,15 @@ void taucs_ccs_order(taucs_ccs_matrix* A, int** perm, int** invperm, char* which
     } else {
       rc = amd_order(n, A->colptr, A->rowind, p, ip);
     }
+  } else if (!strcmp(which, "genmmd")) {
+    // src/taucs_ccs_order.c:262-442
+    if (!(A->flags & (TAUCS_SYMMETRIC | TAUCS_HERMITIAN))) {
+      tprintf("taucs_ccs_genmmd: GENMMD ordering only works on symmetric matrices.\n");
+    } else if (!(A->flags & TAUCS_LOWER)) {
+      tprintf("taucs_ccs_genmmd: the lower part of the matrix must be represented.\n");
+    } else {
+      rc = mmd_order(n, A->colptr, A->rowind, p, ip);
+    }
   } else {
     tprintf("taucs_ccs_order: ordering %s is not available in this build\n", which);
   }

@@ -38,6 +38,8 @@ int symbolic_analyze(int n, const int* colptr, const int* rowind, int max_depth,
 
 // ------------------------------------------------------------ AMD ordering
 int amd_order(int n, const int* colptr, const int* rowind, int* perm, int* invperm);
+// multiple minimum external degree (the reference's "genmmd" ordering)
+int mmd_order(int n, const int* colptr, const int* rowind, int* perm, int* invperm);
 
 // ------------------------------------------------------------------- plan
 // Front-build tile: rows [r0, r0+TILE_R) x columns [c0, c0+TILE_C) of the

@@ -165,7 +165,8 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
     f->flags = A->flags;
     f->rowperm = f->colperm = nullptr;
     f->L = nullptr;
-    if (!opt_ordering) opt_ordering = "amd";
+    // the reference's default for LL^T without METIS (src/taucs_linsolve.c:319-329)
+    if (!opt_ordering) opt_ordering = "genmmd";
     taucs_ccs_order(A, &f->rowperm, &f->colperm, (char*) opt_ordering);
     if (!f->rowperm) {
       taucs_printf((char*) "taucs_factor: ordering failed\n");

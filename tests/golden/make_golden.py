@@ -2,7 +2,7 @@
 itself (oracle/_ref/libtaucs_ref.so, built from the unmodified sources by
 oracle/Makefile).  The reference ships no golden vectors of its own, so these
 pin the oracle and the product to the reference's actual outputs:
-AMD permutation, elimination tree, supernodal structure (slots, sizes,
+AMD and GENMMD permutations, elimination tree, supernodal structure (slots, sizes,
 sn_struct rows, child lists), the L panels (small cases) or their checksums,
 and the solution of A x = b for x_true ~ U(-1,1) with seed 0.
 
@@ -33,6 +33,7 @@ def main():
     for name, gen, args, full in CASES:
         n, cp, ri, va = getattr(R, gen)(*args)
         perm, iperm = R.order(n, cp, ri, va, "amd")
+        perm_g, iperm_g = R.order(n, cp, ri, va, "genmmd")
         _, pc, pr, pv = R.permute(n, cp, ri, va, perm, iperm)
         parent = R.etree(n, pc, pr, pv)
         L = R.factor_mf(n, pc, pr, pv)
@@ -47,6 +48,7 @@ def main():
         np.add.at(b, cols[off], pv[off] * xt[pr[off]])
         x = R.solve(L, b)
         out = dict(n=n, colptr=cp, rowind=ri, values=va, perm=perm, iperm=iperm, parent=parent,
+                   perm_genmmd=perm_g, iperm_genmmd=iperm_g,
                    n_sn=sym.n_sn, sn_size=sym.sn_size, sn_up_size=sym.sn_up_size,
                    first_child=sym.first_child, next_child=sym.next_child,
                    struct_ptr=sym.struct_ptr, struct_idx=sym.struct_idx, val_ptr=vp,

@@ -80,7 +80,7 @@ def test_four_rhs(tb, system):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("opts", [[LLT, "taucs.factor.mf=true"], [LLT, "taucs.factor.ll=true"],
-                                  [LLT, "taucs.factor.ordering=amd"]])
+                                  [LLT, "taucs.factor.ordering=amd"], [LLT, "taucs.factor.ordering=genmmd"]])
 def test_spd_factorizations(tb, system, opts):
     A, X, B = system
     Y = np.zeros((A.n, 1), order="F")

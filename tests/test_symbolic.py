@@ -18,6 +18,8 @@ GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.n
 def test_symbolic_matches_golden(tb, path):
     g = np.load(path)
     A = tb.Matrix(int(g["n"]), g["colptr"], g["rowind"], g["values"])
+    perm, iperm = tb.order(A, "genmmd")
+    assert np.array_equal(perm, g["perm_genmmd"]) and np.array_equal(iperm, g["iperm_genmmd"])
     perm, iperm = tb.order(A, "amd")
     assert np.array_equal(perm, g["perm"]) and np.array_equal(iperm, g["iperm"])
     P = A.permute(perm, iperm)
@@ -64,6 +66,38 @@ def test_host_phase_matches_reference(tb, ref, idx):
     F = tb.factor_symbolic(P)
     assert same_symbolic(F.export_symbolic(), ref.dump_symbolic(Lr)), name
     ref.free(Lr)
+
+
+@pytest.mark.parametrize("idx", range(17))
+def test_genmmd_matches_reference(tb, ref, idx):
+    """GENMMD (src/taucs_ccs_order.c:262-442, external/src/genmmd.c) bit for
+    bit, and the supernodal structure of the matrix it orders."""
+    name, A = _cases(tb)[idx]
+    perm_r, iperm_r = ref.order(*A.arrays(), "genmmd")
+    perm, iperm = tb.order(A, "genmmd")
+    assert np.array_equal(perm, perm_r) and np.array_equal(iperm, iperm_r), name
+    P = A.permute(perm, iperm)
+    Lr = ref.symbolic(*P.arrays())
+    F = tb.factor_symbolic(P)
+    assert same_symbolic(F.export_symbolic(), ref.dump_symbolic(Lr)), name
+    ref.free(Lr)
+
+
+@pytest.mark.parametrize("which", ["mesh3d_64", "lognormal_80"])
+def test_genmmd_matches_reference_at_benchmark_sizes(tb, ref, which):
+    A = tb.mesh3d(64) if which == "mesh3d_64" else tb.lognormal(80, 80, 80, 2.0, (1, 1, 100), 0)
+    perm_r, iperm_r = ref.order(*A.arrays(), "genmmd")
+    perm, iperm = tb.order(A, "genmmd")
+    assert np.array_equal(perm, perm_r) and np.array_equal(iperm, iperm_r)
+
+
+def test_genmmd_diagonal_and_empty(tb, ref):
+    """Every node isolated (diagonal matrix), and a 1x1 matrix."""
+    for n in (1, 50):
+        A = tb.Matrix(n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.ones(n))
+        perm_r, _ = ref.order(*A.arrays(), "genmmd")
+        perm, _ = tb.order(A, "genmmd")
+        assert np.array_equal(perm, perm_r)
 
 
 @pytest.mark.parametrize("order", ["identity", "random"])
