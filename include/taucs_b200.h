@@ -351,6 +351,29 @@ int taucs_b200_autotune(void* L, const double* d_values, int* choices);
  * (layout as in taucs_b200_autotune), or 0 for the default variants. */
 int taucs_b200_set_gemm_choices(void* L, int precision, int count, const int* choices);
 
+/* Device-memory allocation tracking, after the reference's host allocation
+ * tracking (src/taucs_malloc.c:127-250).  Every device and pinned-host
+ * allocation this library makes counts as one attempt.
+ * taucs_b200_allocation_induce_failure(i) makes attempt i (counted from the
+ * last mark) fail as if the device were out of memory;
+ * taucs_b200_allocation_mark_clean() restarts the attempt count;
+ * taucs_b200_allocation_live() returns the number of the library's live
+ * allocations (and their bytes).  A call whose allocation fails returns NULL
+ * or -1 and leaves nothing allocated once its handle is freed. */
+void taucs_b200_allocation_induce_failure(int i);
+int  taucs_b200_allocation_attempts(void);
+void taucs_b200_allocation_mark_clean(void);
+int  taucs_b200_allocation_live(double* bytes);
+
+/* Testing aid for the failure paths (no counterpart in the reference): sets,
+ * on the current device, the polling limit of the bounded waits between
+ * thread blocks (default 4194304 polls) and an offset added to the value
+ * they wait for (default 0).  A nonzero offset makes every such wait run
+ * out: the call that launched it then returns -1 with a timeout message,
+ * without a fault or a hang, and the device stays usable.  Restore with
+ * (4194304, 0). */
+int taucs_b200_debug_waits(int limit, int skew);
+
 /* CUDA kernel launches issued by this library on the calling thread since
  * the last reset (for launch accounting in benchmarks). */
 long taucs_b200_launch_count(int reset);

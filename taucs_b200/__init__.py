@@ -142,6 +142,11 @@ def lib():
         "taucs_b200_autotune": (C.c_int, [vp, vp, _i32p]),
         "taucs_b200_set_gemm_choices": (C.c_int, [vp, C.c_int, C.c_int, _i32p]),
         "taucs_b200_solve_device_noalloc_status": (C.c_int, []),
+        "taucs_b200_debug_waits": (C.c_int, [C.c_int, C.c_int]),
+        "taucs_b200_allocation_induce_failure": (None, [C.c_int]),
+        "taucs_b200_allocation_attempts": (C.c_int, []),
+        "taucs_b200_allocation_mark_clean": (None, []),
+        "taucs_b200_allocation_live": (C.c_int, [C.POINTER(C.c_double)]),
         "taucs_b200_profile": (C.c_int, [C.c_int]),
         "taucs_b200_profile_read": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_long),
                                               C.POINTER(C.c_double), C.POINTER(C.c_double)]),

@@ -32,7 +32,7 @@ bool cuda_ok(cudaError_t e, const char* what) {
 template <class T>
 static bool dev_upload(T** dst, const T* src, size_t n, cudaStream_t st) {
   if (n == 0) n = 1;
-  if (!cuda_ok(cudaMalloc((void**) dst, n * sizeof(T)), "cudaMalloc")) return false;
+  if (!cuda_ok(tb::dmalloc((void**) dst, n * sizeof(T)), "cudaMalloc")) return false;
   if (src) return cuda_ok(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
   return true;
 }
@@ -75,10 +75,10 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
 }
 
 void devplan_free(DevPlan* D) {
-  cudaFree(D->fronts); cudaFree(D->children); cudaFree(D->rows); cudaFree(D->maps);
-  cudaFree(D->acol_ptr); cudaFree(D->a_rows); cudaFree(D->a_idx);
-  cudaFree(D->small_list); cudaFree(D->big_list); cudaFree(D->tiles);
-  cudaFree(D->sfwd); cudaFree(D->sbwd); cudaFree(D->sl21);
+  tb::dfree(D->fronts); tb::dfree(D->children); tb::dfree(D->rows); tb::dfree(D->maps);
+  tb::dfree(D->acol_ptr); tb::dfree(D->a_rows); tb::dfree(D->a_idx);
+  tb::dfree(D->small_list); tb::dfree(D->big_list); tb::dfree(D->tiles);
+  tb::dfree(D->sfwd); tb::dfree(D->sbwd); tb::dfree(D->sl21);
   *D = DevPlan();
 }
 
@@ -140,12 +140,12 @@ void invalidate_numeric(Factor* F) {
 
 void free_numeric(Factor* F) {
   drop_graphs(F);
-  cudaFree(F->dL); F->dL = nullptr;
-  cudaFree(F->dU); F->dU = nullptr;
-  cudaFree(F->dDinv); F->dDinv = nullptr;
-  cudaFree(F->dL32); F->dL32 = nullptr;
-  cudaFree(F->dU32); F->dU32 = nullptr;
-  cudaFree(F->dDinv32); F->dDinv32 = nullptr;
+  tb::dfree(F->dL); F->dL = nullptr;
+  tb::dfree(F->dU); F->dU = nullptr;
+  tb::dfree(F->dDinv); F->dDinv = nullptr;
+  tb::dfree(F->dL32); F->dL32 = nullptr;
+  tb::dfree(F->dU32); F->dU32 = nullptr;
+  tb::dfree(F->dDinv32); F->dDinv32 = nullptr;
   F->has_numeric = false;
   F->has_numeric32 = false;
 }
@@ -155,38 +155,38 @@ static void free_device(Factor* F) {
   if (F->cap_stream) cudaStreamDestroy(F->cap_stream);
   F->cap_stream = nullptr;
   if (F->dev_ready) devplan_free(&F->dp);
-  cudaFree(F->dA); F->dA = nullptr;
-  cudaFree(F->dstatus); F->dstatus = nullptr;
-  cudaFree(F->dW); F->dW = nullptr;
-  cudaFree(F->dpart); F->dpart = nullptr;
-  cudaFree(F->dX); F->dX = nullptr;
-  cudaFree(F->dscale); F->dscale = nullptr;
-  cudaFree(F->dcolptr); F->dcolptr = nullptr;
-  cudaFree(F->drowind); F->drowind = nullptr;
-  cudaFree(F->dA32); F->dA32 = nullptr;
-  cudaFree(F->dW32); F->dW32 = nullptr;
-  cudaFree(F->dpart32); F->dpart32 = nullptr;
-  cudaFree(F->dV32); F->dV32 = nullptr;
-  cudaFree(F->dcolidx); F->dcolidx = nullptr;
-  cudaFree(F->ddiagpos); F->ddiagpos = nullptr;
-  cudaFree(F->dcsr_ptr); F->dcsr_ptr = nullptr;
-  cudaFree(F->dcsr_col); F->dcsr_col = nullptr;
-  cudaFree(F->dcsr_val); F->dcsr_val = nullptr;
-  cudaFree(F->dR); F->dR = nullptr;
-  cudaFree(F->dseg); F->dseg = nullptr;
-  cudaFree(F->dXr); F->dXr = nullptr;
-  cudaFree(F->dBr); F->dBr = nullptr;
-  cudaFree(F->dnorm); F->dnorm = nullptr;
-  if (F->hnorm) cudaFreeHost(F->hnorm);
+  tb::dfree(F->dA); F->dA = nullptr;
+  tb::dfree(F->dstatus); F->dstatus = nullptr;
+  tb::dfree(F->dW); F->dW = nullptr;
+  tb::dfree(F->dpart); F->dpart = nullptr;
+  tb::dfree(F->dX); F->dX = nullptr;
+  tb::dfree(F->dscale); F->dscale = nullptr;
+  tb::dfree(F->dcolptr); F->dcolptr = nullptr;
+  tb::dfree(F->drowind); F->drowind = nullptr;
+  tb::dfree(F->dA32); F->dA32 = nullptr;
+  tb::dfree(F->dW32); F->dW32 = nullptr;
+  tb::dfree(F->dpart32); F->dpart32 = nullptr;
+  tb::dfree(F->dV32); F->dV32 = nullptr;
+  tb::dfree(F->dcolidx); F->dcolidx = nullptr;
+  tb::dfree(F->ddiagpos); F->ddiagpos = nullptr;
+  tb::dfree(F->dcsr_ptr); F->dcsr_ptr = nullptr;
+  tb::dfree(F->dcsr_col); F->dcsr_col = nullptr;
+  tb::dfree(F->dcsr_val); F->dcsr_val = nullptr;
+  tb::dfree(F->dR); F->dR = nullptr;
+  tb::dfree(F->dseg); F->dseg = nullptr;
+  tb::dfree(F->dXr); F->dXr = nullptr;
+  tb::dfree(F->dBr); F->dBr = nullptr;
+  tb::dfree(F->dnorm); F->dnorm = nullptr;
+  if (F->hnorm) tb::hfree(F->hnorm);
   F->hnorm = nullptr;
-  cudaFree(F->dpcg); F->dpcg = nullptr;
-  cudaFree(F->ddot_part); F->ddot_part = nullptr;
-  cudaFree(F->ddot); F->ddot = nullptr;
-  if (F->hdot) cudaFreeHost(F->hdot);
+  tb::dfree(F->dpcg); F->dpcg = nullptr;
+  tb::dfree(F->ddot_part); F->ddot_part = nullptr;
+  tb::dfree(F->ddot); F->ddot = nullptr;
+  if (F->hdot) tb::hfree(F->hdot);
   F->hdot = nullptr;
   F->refine_ready = false;
-  cudaFree(F->dflags); F->dflags = nullptr;
-  if (F->hstatus) cudaFreeHost(F->hstatus);
+  tb::dfree(F->dflags); F->dflags = nullptr;
+  if (F->hstatus) tb::hfree(F->hstatus);
   F->hstatus = nullptr;
   F->dev_ready = false;
 }
@@ -216,7 +216,7 @@ int ensure_device(Factor* F) {
          && dev_upload(&F->dX, (const double*) nullptr, (size_t) F->n * SOLVE_NRHS, st)
          && dev_upload(&F->dcolptr, F->colptr.data(), F->colptr.size(), st)
          && dev_upload(&F->drowind, F->rowind.data(), F->rowind.size(), st)
-         && cuda_ok(cudaMallocHost((void**) &F->hstatus, 2 * sizeof(int)), "cudaMallocHost");
+         && cuda_ok(tb::hmalloc((void**) &F->hstatus, 2 * sizeof(int)), "cudaMallocHost");
   if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "upload");
   if (!ok) { free_device(F); return -1; }
   return 0;
@@ -260,12 +260,12 @@ int numeric_fp64_device(Factor* F, const double* d_vals, bool wait) {
   if (ensure_device(F)) return -1;
   cudaStream_t st = current_stream();
   const Plan& P = F->plan;
-  if (!F->dL && !cuda_ok(cudaMalloc(&F->dL, sizeof(double) * (size_t) P.l_len), "cudaMalloc(L)")) return -1;
-  if (!F->dU && !cuda_ok(cudaMalloc(&F->dU, sizeof(double) * (size_t) P.u_len), "cudaMalloc(U)")) {
+  if (!F->dL && !cuda_ok(tb::dmalloc(&F->dL, sizeof(double) * (size_t) P.l_len), "cudaMalloc(L)")) return -1;
+  if (!F->dU && !cuda_ok(tb::dmalloc(&F->dU, sizeof(double) * (size_t) P.u_len), "cudaMalloc(U)")) {
     free_numeric(F);
     return -1;
   }
-  if (!F->dDinv && !cuda_ok(cudaMalloc(&F->dDinv, sizeof(double) * (size_t) P.dinv_len), "cudaMalloc(Dinv)")) {
+  if (!F->dDinv && !cuda_ok(tb::dmalloc(&F->dDinv, sizeof(double) * (size_t) P.dinv_len), "cudaMalloc(Dinv)")) {
     free_numeric(F);
     return -1;
   }
@@ -527,6 +527,11 @@ int taucs_b200_set_gemm_choices(void* L, int precision, int count, const int* ch
   }
   drop_graphs(F);
   return 0;
+}
+
+int taucs_b200_debug_waits(int limit, int skew) {
+  if (limit < 0) return -1;
+  return cuda_ok((cudaError_t) solve_set_wait_controls(limit, skew), "taucs_b200_debug_waits") ? 0 : -1;
 }
 
 long taucs_b200_launch_count(int reset) {

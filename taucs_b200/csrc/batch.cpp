@@ -215,9 +215,9 @@ extern "C" int taucs_b200_batch_solve(void* L, double* const* X, const double* c
   if (taucs_b200_batch_rhs(L, B, b.data())) return -1;
   double *db = nullptr, *dx = nullptr;
   cudaStream_t st = current_stream();
-  if (!cuda_ok(cudaMalloc(&db, sizeof(double) * n), "cudaMalloc") ||
-      !cuda_ok(cudaMalloc(&dx, sizeof(double) * n), "cudaMalloc")) {
-    cudaFree(db);
+  if (!cuda_ok(tb::dmalloc(&db, sizeof(double) * n), "cudaMalloc") ||
+      !cuda_ok(tb::dmalloc(&dx, sizeof(double) * n), "cudaMalloc")) {
+    tb::dfree(db);
     return -1;
   }
   int steps = -1;
@@ -227,8 +227,8 @@ extern "C" int taucs_b200_batch_solve(void* L, double* const* X, const double* c
         !cuda_ok(cudaStreamSynchronize(st), "batch solve"))
       steps = -1;
   }
-  cudaFree(db);
-  cudaFree(dx);
+  tb::dfree(db);
+  tb::dfree(dx);
   if (steps >= 0) taucs_b200_batch_split(L, x.data(), X);
   return steps;
 }

@@ -117,6 +117,21 @@ int launch_solve_fp32(const Plan& P, const DevPlan& D, const float* L, const flo
                       const float* B, int ld, float* W, float* part, int* flags, int* epoch, int* status,
                       cudaStream_t st);
 
+// sets the polling limit and the test offset of the solve's handshake waits
+// on the current device (returns a cudaError_t code)
+int solve_set_wait_controls(int limit, int skew);
+
+// Device and pinned-host allocations of the library (alloc.cpp): counted,
+// and failable on request (taucs_b200_allocation_induce_failure)
+cudaError_t dmalloc_raw(void** p, size_t bytes);
+cudaError_t dfree(void* p);
+cudaError_t hmalloc_raw(void** p, size_t bytes);
+cudaError_t hfree(void* p);
+template <typename T>
+inline cudaError_t dmalloc(T** p, size_t bytes) { return dmalloc_raw((void**) p, bytes); }
+template <typename T>
+inline cudaError_t hmalloc(T** p, size_t bytes) { return hmalloc_raw((void**) p, bytes); }
+
 // launch accounting
 void count_launch(long k = 1);
 

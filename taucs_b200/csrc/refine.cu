@@ -273,7 +273,7 @@ static int ensure_refine(Factor* F) {
     }
   cudaStream_t st = current_stream();
   auto up = [&](int** d, const std::vector<int>& h) {
-    return cuda_ok(cudaMalloc(d, sizeof(int) * h.size()), "cudaMalloc") &&
+    return cuda_ok(tb::dmalloc(d, sizeof(int) * h.size()), "cudaMalloc") &&
            cuda_ok(cudaMemcpyAsync(*d, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st), "copy");
   };
   const size_t nv = (size_t) n * SOLVE_NRHS;
@@ -285,13 +285,13 @@ static int ensure_refine(Factor* F) {
   }
   bool ok = up(&F->dcolidx, colidx) && up(&F->ddiagpos, diagpos) && up(&F->dcsr_ptr, cnt) && up(&F->dcsr_col, ccol) &&
             up(&F->dcsr_val, cval) &&
-            cuda_ok(cudaMalloc(&F->dscale, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
-            cuda_ok(cudaMalloc(&F->dR, sizeof(double) * nv), "cudaMalloc") &&
-            cuda_ok(cudaMalloc(&F->dXr, sizeof(double) * nv), "cudaMalloc") &&
-            cuda_ok(cudaMalloc(&F->dBr, sizeof(double) * nv), "cudaMalloc") &&
-            cuda_ok(cudaMalloc(&F->dV32, sizeof(float) * nv), "cudaMalloc") &&
-            cuda_ok(cudaMalloc(&F->dnorm, norm_bytes(F)), "cudaMalloc") &&
-            cuda_ok(cudaMallocHost(&F->hnorm, norm_bytes(F)), "cudaMallocHost") &&
+            cuda_ok(tb::dmalloc(&F->dscale, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
+            cuda_ok(tb::dmalloc(&F->dR, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(tb::dmalloc(&F->dXr, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(tb::dmalloc(&F->dBr, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(tb::dmalloc(&F->dV32, sizeof(float) * nv), "cudaMalloc") &&
+            cuda_ok(tb::dmalloc(&F->dnorm, norm_bytes(F)), "cudaMalloc") &&
+            cuda_ok(tb::hmalloc(&F->hnorm, norm_bytes(F)), "cudaMallocHost") &&
             cuda_ok(cudaStreamSynchronize(st), "refine setup");
   if (!ok) return -1;
   F->refine_ready = true;
@@ -302,7 +302,7 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
   if (ensure_device(F) || ensure_refine(F)) return -1;
   const Plan& P = F->plan;
   cudaStream_t st = current_stream();
-  auto al = [&](float** d, size_t n, const char* w) { return *d || cuda_ok(cudaMalloc(d, sizeof(float) * std::max<size_t>(n, 1)), w); };
+  auto al = [&](float** d, size_t n, const char* w) { return *d || cuda_ok(tb::dmalloc(d, sizeof(float) * std::max<size_t>(n, 1)), w); };
   if (!al(&F->dL32, P.l_len, "cudaMalloc(L32)") || !al(&F->dU32, P.u_len, "cudaMalloc(U32)") ||
       !al(&F->dDinv32, P.dinv_len, "cudaMalloc(Dinv32)") || !al(&F->dA32, P.nnz, "cudaMalloc(A32)") ||
       !al(&F->dW32, (size_t) P.v_len * SOLVE_NRHS, "cudaMalloc(W32)") || !al(&F->dpart32, P.part_len, "cudaMalloc(part32)")) {
@@ -355,10 +355,10 @@ static int pcg_fp32(Factor* F, int nq, double* X, const double* B, int ld, doubl
   const int n = F->n;
   cudaStream_t st = current_stream();
   const size_t nv = (size_t) n * SOLVE_NRHS;
-  if (!F->dpcg && !(cuda_ok(cudaMalloc(&F->dpcg, sizeof(double) * 3 * nv), "cudaMalloc(pcg)") &&
-                    cuda_ok(cudaMalloc(&F->ddot_part, sizeof(double) * DOT_BLOCKS * SOLVE_NRHS), "cudaMalloc(pcg)") &&
-                    cuda_ok(cudaMalloc(&F->ddot, sizeof(double) * 2 * SOLVE_NRHS), "cudaMalloc(pcg)") &&
-                    cuda_ok(cudaMallocHost(&F->hdot, sizeof(double) * 2 * SOLVE_NRHS), "cudaMallocHost(pcg)")))
+  if (!F->dpcg && !(cuda_ok(tb::dmalloc(&F->dpcg, sizeof(double) * 3 * nv), "cudaMalloc(pcg)") &&
+                    cuda_ok(tb::dmalloc(&F->ddot_part, sizeof(double) * DOT_BLOCKS * SOLVE_NRHS), "cudaMalloc(pcg)") &&
+                    cuda_ok(tb::dmalloc(&F->ddot, sizeof(double) * 2 * SOLVE_NRHS), "cudaMalloc(pcg)") &&
+                    cuda_ok(tb::hmalloc(&F->hdot, sizeof(double) * 2 * SOLVE_NRHS), "cudaMallocHost(pcg)")))
     return -2;
   double* Pd = F->dpcg;
   double* Q = Pd + nv;

@@ -177,18 +177,18 @@ class Server {
     for (auto& I : instances_) taucs_supernodal_factor_free(I->F);
     for (auto& kv : patterns_) {
       if (kv.second->proto) taucs_supernodal_factor_free(kv.second->proto);
-      cudaFree(kv.second->d_perm);
-      cudaFree(kv.second->d_vmap);
+      tb::dfree(kv.second->d_perm);
+      tb::dfree(kv.second->d_vmap);
     }
     for (auto& w : workers_) {
-      cudaFree(w->d_vals);
-      cudaFree(w->d_b);
-      cudaFree(w->d_x);
+      tb::dfree(w->d_vals);
+      tb::dfree(w->d_b);
+      tb::dfree(w->d_x);
       if (w->stream) cudaStreamDestroy(w->stream);
       if (w->stream_hi) cudaStreamDestroy(w->stream_hi);
-      if (w->h_vals) cudaFreeHost(w->h_vals);
-      if (w->h_b) cudaFreeHost(w->h_b);
-      if (w->h_x) cudaFreeHost(w->h_x);
+      if (w->h_vals) tb::hfree(w->h_vals);
+      if (w->h_b) tb::hfree(w->h_b);
+      if (w->h_x) tb::hfree(w->h_x);
     }
     for (auto& kv : reqs_) delete kv.second;
   }
@@ -277,24 +277,24 @@ class Server {
   bool grow(Worker& W, size_t nvals, size_t nvec, cudaStream_t st) {
     if (nvals <= W.h_vals_len && nvec <= W.h_vec_len) return true;
     if (nvals > W.h_vals_len) {
-      if (W.h_vals) cudaFreeHost(W.h_vals);
+      if (W.h_vals) tb::hfree(W.h_vals);
       cudaFreeAsync(W.d_vals, st);
       W.h_vals = nullptr;
       W.d_vals = nullptr;
-      if (cudaMallocHost((void**) &W.h_vals, sizeof(double) * nvals) != cudaSuccess ||
+      if (tb::hmalloc((void**) &W.h_vals, sizeof(double) * nvals) != cudaSuccess ||
           cudaMallocAsync((void**) &W.d_vals, sizeof(double) * nvals, st) != cudaSuccess)
         return false;
       W.h_vals_len = nvals;
     }
     if (nvec > W.h_vec_len) {
-      if (W.h_b) cudaFreeHost(W.h_b);
-      if (W.h_x) cudaFreeHost(W.h_x);
+      if (W.h_b) tb::hfree(W.h_b);
+      if (W.h_x) tb::hfree(W.h_x);
       cudaFreeAsync(W.d_b, st);
       cudaFreeAsync(W.d_x, st);
       W.h_b = W.h_x = nullptr;
       W.d_b = W.d_x = nullptr;
-      if (cudaMallocHost((void**) &W.h_b, sizeof(double) * nvec) != cudaSuccess ||
-          cudaMallocHost((void**) &W.h_x, sizeof(double) * nvec) != cudaSuccess ||
+      if (tb::hmalloc((void**) &W.h_b, sizeof(double) * nvec) != cudaSuccess ||
+          tb::hmalloc((void**) &W.h_x, sizeof(double) * nvec) != cudaSuccess ||
           cudaMallocAsync((void**) &W.d_b, sizeof(double) * nvec, st) != cudaSuccess ||
           cudaMallocAsync((void**) &W.d_x, sizeof(double) * nvec, st) != cudaSuccess)
         return false;
@@ -309,8 +309,8 @@ class Server {
     std::lock_guard<std::mutex> lk(P->dev_mu);
     if (P->dev_state == 0) {
       const size_t bytes = sizeof(int) * (P->perm.size() + P->vmap.size());
-      bool ok = cudaMalloc((void**) &P->d_perm, sizeof(int) * std::max<size_t>(P->perm.size(), 1)) == cudaSuccess &&
-                cudaMalloc((void**) &P->d_vmap, sizeof(int) * std::max<size_t>(P->vmap.size(), 1)) == cudaSuccess &&
+      bool ok = tb::dmalloc((void**) &P->d_perm, sizeof(int) * std::max<size_t>(P->perm.size(), 1)) == cudaSuccess &&
+                tb::dmalloc((void**) &P->d_vmap, sizeof(int) * std::max<size_t>(P->vmap.size(), 1)) == cudaSuccess &&
                 cudaMemcpyAsync(P->d_perm, P->perm.data(), sizeof(int) * P->perm.size(), cudaMemcpyHostToDevice,
                                 st) == cudaSuccess &&
                 cudaMemcpyAsync(P->d_vmap, P->vmap.data(), sizeof(int) * P->vmap.size(), cudaMemcpyHostToDevice,

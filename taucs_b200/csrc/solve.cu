@@ -257,32 +257,45 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+}  // namespace
+
+// Controls of the handshake waits on this device: the polling limit, and an
+// offset added to the flag value waited for (0; any other value makes every
+// wait run out -- a testing aid for the timeout reporting, set through
+// taucs_b200_debug_waits).
+__device__ int g_solve_wait_limit = 1 << 22;
+__device__ int g_solve_wait_skew = 0;
+
+int solve_set_wait_controls(int limit, int skew) {
+  cudaError_t e = cudaMemcpyToSymbol(g_solve_wait_limit, &limit, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_solve_wait_skew, &skew, sizeof(int));
+  return (int) e;
+}
+
+namespace {
+
+// polls flag until it holds epoch (plus the wait offset); on giving up,
+// records SOLVE_TIMEOUT
+__device__ __forceinline__ void poll_epoch(const int* flag, int epoch, int* status) {
+  const int want = epoch + g_solve_wait_skew, limit = g_solve_wait_limit;
+  int it = 0;
+  while (ld_acquire(flag) != want) {
+    if (++it > limit) {
+      atomicExch(status, SOLVE_TIMEOUT);
+      break;
+    }
+    __nanosleep(32);
+  }
+}
+
 // the same wait for one warp: lane 0 polls, the warp follows it
 __device__ void wait_epoch_warp(const int* flag, int epoch, int* status) {
-  if ((threadIdx.x & 31) == 0) {
-    int it = 0;
-    while (ld_acquire(flag) != epoch) {
-      if (++it > (1 << 22)) {
-        atomicExch(status, SOLVE_TIMEOUT);
-        break;
-      }
-      __nanosleep(32);
-    }
-  }
+  if ((threadIdx.x & 31) == 0) poll_epoch(flag, epoch, status);
   __syncwarp();   // orders the lanes' later loads after lane 0's acquire
 }
 
 __device__ void wait_epoch(const int* flag, int epoch, int* status) {
-  if (threadIdx.x == 0) {
-    int it = 0;
-    while (ld_acquire(flag) != epoch) {
-      if (++it > (1 << 22)) {
-        atomicExch(status, SOLVE_TIMEOUT);
-        break;
-      }
-      __nanosleep(32);
-    }
-  }
+  if (threadIdx.x == 0) poll_epoch(flag, epoch, status);
   __syncthreads();
 }
 
