@@ -101,6 +101,9 @@ int               taucs_vec_write_binary(int n, int flags, void* v, char* filena
 void taucs_vec_permute(int n, int flags, void* v, void* pv, int p[]);
 void taucs_vec_ipermute(int n, int flags, void* pv, void* v, int invp[]);
 void taucs_dvec_permute(int n, double v[], double pv[], int p[]);
+/* axpby = a x + b y, and the 2-norm (src/taucs_vec_base.c:29-92) */
+void   taucs_vec_axpby(int n, int flags, double a, void* x, double b, void* y, void* axpby);
+double taucs_vec_norm2(int n, int flags, void* x);
 void taucs_dvec_ipermute(int n, double pv[], double v[], int invp[]);
 
 /* generators (src/taucs_ccs_generators.c:89-261) */

@@ -206,6 +206,37 @@ void taucs_vec_ipermute(int n, int flags, void* pv, void* v, int invp[]) {
     for (int i = 0; i < n; i++) ((float*) v)[invp[i]] = ((float*) pv)[i];
 }
 
+// axpby = a x + b y (src/taucs_vec_base.c:56-92); the output may alias x or y
+void taucs_vec_axpby(int n, int flags, double a, void* x, double b, void* y, void* axpby) {
+  if (flags & TAUCS_DOUBLE) {
+    const double *xv = (const double*) x, *yv = (const double*) y;
+    double* o = (double*) axpby;
+    for (int i = 0; i < n; i++) o[i] = a * xv[i] + b * yv[i];
+  } else if (flags & TAUCS_SINGLE) {
+    const float *xv = (const float*) x, *yv = (const float*) y;
+    float* o = (float*) axpby;
+    for (int i = 0; i < n; i++) o[i] = (float) a * xv[i] + (float) b * yv[i];
+  }
+}
+
+// Euclidean norm (src/taucs_vec_base.c:29-53, BLAS nrm2 there), accumulated
+// with a running scale so that no square overflows or underflows
+double taucs_vec_norm2(int n, int flags, void* x) {
+  double scale = 0.0, ssq = 1.0;
+  for (int i = 0; i < n; i++) {
+    const double v = (flags & TAUCS_SINGLE) ? (double) ((const float*) x)[i] : ((const double*) x)[i];
+    if (v == 0.0) continue;
+    const double a = std::fabs(v);
+    if (scale < a) {
+      ssq = 1.0 + ssq * (scale / a) * (scale / a);
+      scale = a;
+    } else {
+      ssq += (a / scale) * (a / scale);
+    }
+  }
+  return scale * std::sqrt(ssq);
+}
+
 taucs_ccs_matrix* taucs_ccs_generate_mesh2d(int n, char* which) {
   if (n <= 0 || !which) return nullptr;
   const int N = n * n;
