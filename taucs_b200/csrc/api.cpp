@@ -57,7 +57,13 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
     sb.insert(sb.end(), LP.solve_bwd_blocks.begin(), LP.solve_bwd_blocks.end());
     sl.insert(sl.end(), LP.solve_l21_tasks.begin(), LP.solve_l21_tasks.end());
   }
+  std::vector<int2_> dblk;
+  for (int i = 0; i < (int) P.fronts.size(); i++)
+    if (P.fronts[i].dinv_off >= 0)
+      for (int b = 0; b * PANEL_NB < P.fronts[i].s; b++) dblk.push_back(int2_{i, b});
+  D->n_dblk = (int) dblk.size();
   bool ok = dev_upload(&D->fronts, P.fronts.data(), P.fronts.size(), st)
+         && dev_upload(&D->dblk, dblk.data(), dblk.size(), st)
          && dev_upload(&D->children, P.children.data(), P.children.size(), st)
          && dev_upload(&D->rows, P.rows.data(), P.rows.size(), st)
          && dev_upload(&D->maps, P.maps.data(), P.maps.size(), st)
@@ -78,7 +84,7 @@ void devplan_free(DevPlan* D) {
   tb::dfree(D->fronts); tb::dfree(D->children); tb::dfree(D->rows); tb::dfree(D->maps);
   tb::dfree(D->acol_ptr); tb::dfree(D->a_rows); tb::dfree(D->a_idx);
   tb::dfree(D->small_list); tb::dfree(D->big_list); tb::dfree(D->tiles);
-  tb::dfree(D->sfwd); tb::dfree(D->sbwd); tb::dfree(D->sl21);
+  tb::dfree(D->sfwd); tb::dfree(D->sbwd); tb::dfree(D->sl21); tb::dfree(D->dblk);
   *D = DevPlan();
 }
 

@@ -69,6 +69,8 @@ struct DevPlan {
   int2_* sfwd = nullptr;       // solve blocks, all levels concatenated
   int2_* sbwd = nullptr;
   int2_* sl21 = nullptr;
+  int2_* dblk = nullptr;       // (front, 64-column block) of every big front's diagonal blocks
+  int n_dblk = 0;
   std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off, sl21_off;  // per level (host)
   std::vector<int> lvl_max_f_small;               // per level (host)
 };

@@ -15,15 +15,16 @@
 //                   part gathers A's entries and the children's update
 //                   matrices into shared memory in a fixed child order
 //                   (deterministic, no atomics) and writes the tile once;
-//   k_potrf_diag    blocked partial Cholesky, step kb: one CTA per front
-//                   factors the 64x64 diagonal block in place and forms its
-//                   inverse;
-//   k_trsm          then one CTA per 64-row slab below it computes
-//                   X L_kk^-T = X Dinv^T on DMMA;
+//   k_leaf          blocked partial Cholesky, step kb: one launch factors
+//                   the 64x64 diagonal block and applies it to every row
+//                   below it (one CTA per 64-row slab, each factoring the
+//                   diagonal block itself);
 //   k_gemm          C -= A B^T on DMMA (mma.sync m16n8k8 f64) tiles: the
 //                   panel updates of a recursive (left half, GEMM, right
 //                   half) panel factorization, and the update matrix
-//                   U -= L21 L21^T with k = s at the end.
+//                   U -= L21 L21^T with k = s at the end;
+//   k_dinv          after all levels, the inverses of every big front's
+//                   64x64 diagonal blocks (used by the solve).
 //
 // Every kernel first reads the status word and returns when an earlier front
 // hit a nonpositive pivot; the smallest failing global column is recorded
@@ -187,183 +188,247 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
   }
 }
 
-// ------------------------------------------------------- blocked POTRF+TRSM
+// ---------------------------------------------------------- panel leaves
 
-constexpr int DLD = PANEL_NB + 1;  // padded column stride of the diagonal block
+// Panel leaf, step kb: the columns [kb, kb + w) of the level's big fronts, w =
+// min(64, s - kb), factored and applied to every row below them in ONE
+// launch (the reference's POTRF :1131 and TRSM :1150 on a 64-column piece).
+// CTA x of front y owns the 64 rows [kb + w + 64 x, ...) below the diagonal
+// block; CTA 0 also writes the factored diagonal block.  Every CTA factors
+// the 64x64 diagonal block itself -- a redundant Cholesky instead of waiting
+// for the CTA that owns it -- in four 16-column steps: one warp factors the
+// 16x16 diagonal piece and inverts it in registers, then all warps apply it
+// to the rows below, in the diagonal block and in the CTA's own slab (one row
+// per thread), and update the columns to the right.  The inverses of the
+// 64x64 diagonal blocks, which the solve applies, are formed afterwards for
+// all fronts at once (k_dinv).
+constexpr int LLD = PANEL_NB + 4;   // padded column stride of the leaf's blocks in shared memory
+constexpr int LQ = 16;              // column step inside a leaf
+constexpr int LYD = LQ + 1;         // column stride of a 16x16 inverse
 
-// Lower Cholesky of an n x n (n <= 32) block held in shared memory (ld `ld`),
-// by one warp: lane i keeps row i in registers and the right-looking updates
-// exchange L[k][j] with shuffles.  The critical path per column is one
-// shuffle, one reciprocal square root and one multiply; every division of
-// the textbook loop is replaced by a multiply with rsqrt(pivot).  Returns the
+template <typename T>
+constexpr size_t leaf_smem() { return (2 * PANEL_NB * LLD + LQ * LYD) * sizeof(T); }
+template <typename T>
+constexpr size_t dinv_smem() { return (2 * PANEL_NB * LLD + (PANEL_NB / LQ) * LQ * LYD) * sizeof(T); }
+
+// Inverse of the lower-triangular 16x16 factor held one row per lane (a[k] =
+// L[i][k], i = lane & 15, k <= i) into Y (column-major, ld LYD): lane t forms
+// column t by forward substitution, reading L[r][k] by broadcast shuffles.
+template <typename T>
+__device__ __forceinline__ void warp_inv16_rows(const T (&a)[LQ], T* Y) {
+  const int i = threadIdx.x & 15;
+  T y[LQ];
+#pragma unroll
+  for (int r = 0; r < LQ; r++) {
+    T acc = (r == i) ? T(1) : T(0);
+#pragma unroll
+    for (int k = 0; k < r; k++) acc -= __shfl_sync(0xffffffffu, a[k], r) * y[k];
+    const T lrr = __shfl_sync(0xffffffffu, a[r], r);
+    y[r] = (r >= i) ? acc * (T(1) / lrr) : T(0);
+  }
+  if ((threadIdx.x & 31) < LQ) {
+#pragma unroll
+    for (int r = 0; r < LQ; r++) Y[r + i * LYD] = y[r];
+  }
+}
+
+// One warp: Cholesky of the 16x16 block S (ld LLD, lower part) in place and
+// its inverse into Y.  Lanes 0-15 hold one row each (lanes 16-31 repeat
+// them); the right-looking updates broadcast L[k][j] by shuffles, and the
+// division of the textbook loop is a multiply by rsqrt(pivot).  Returns the
 // first nonpositive pivot (or -1) in every lane.
 template <typename T>
-__device__ int warp_potrf32(T* S, int ld, int n) {
-  const int lane = threadIdx.x & 31;
-  T a[32];
+__device__ int warp_chol_inv16(T* S, T* Y) {
+  const int i = threadIdx.x & 15;
+  T a[LQ];
 #pragma unroll
-  for (int k = 0; k < 32; k++) a[k] = (lane < n && k <= lane) ? S[lane + k * ld] : 0.0;
+  for (int k = 0; k < LQ; k++) a[k] = (k <= i) ? S[i + k * LLD] : T(0);
   int bad = -1;
 #pragma unroll
-  for (int j = 0; j < 32; j++) {
-    if (j < n) {
-      const T d = __shfl_sync(0xffffffffu, a[j], j);
-      if (!(d > 0.0) && bad < 0) bad = j;
-      const T r = rsqrt_t(d);
-      a[j] = (lane == j) ? d * r : a[j] * r;
+  for (int j = 0; j < LQ; j++) {
+    const T d = __shfl_sync(0xffffffffu, a[j], j);
+    if (!(d > T(0)) && bad < 0) bad = j;
+    const T r = rsqrt_t(d);
+    a[j] = (i == j) ? d * r : a[j] * r;
 #pragma unroll
-      for (int k = j + 1; k < 32; k++) {
-        const T lkj = __shfl_sync(0xffffffffu, a[j], k);
-        if (lane >= k) a[k] -= a[j] * lkj;
-      }
+    for (int k = j + 1; k < LQ; k++) {
+      const T lkj = __shfl_sync(0xffffffffu, a[j], k);
+      if (i >= k) a[k] -= a[j] * lkj;
     }
   }
+  if ((threadIdx.x & 31) < LQ) {
 #pragma unroll
-  for (int k = 0; k < 32; k++)
-    if (lane < n && k <= lane) S[lane + k * ld] = a[k];
+    for (int k = 0; k < LQ; k++)
+      if (k <= i) S[i + k * LLD] = a[k];
+  }
+  if (bad < 0) warp_inv16_rows(a, Y);
   return bad;
 }
 
-// Inverse of an n x n (n <= 32) lower-triangular block by one warp: lane t
-// computes column t by forward substitution; L is read as broadcasts, the
-// reciprocal diagonal is formed once in parallel, and each dot product is
-// split over four accumulators to shorten the dependent FMA chain.
-template <typename T>
-__device__ void warp_trinv32(const T* S, int ld, T* X, int ldx, int n) {
-  const int t = threadIdx.x & 31;
-  const T rd_own = (t < n) ? T(1) / S[t + t * ld] : T(0);
-  T x[32];
-#pragma unroll
-  for (int i = 0; i < 32; i++) {
-    T a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-#pragma unroll
-    for (int k = 0; k < i; k++) {
-      const T p = S[i + k * ld] * x[k];
-      if ((k & 3) == 0) a0 += p;
-      else if ((k & 3) == 1) a1 += p;
-      else if ((k & 3) == 2) a2 += p;
-      else a3 += p;
-    }
-    const T rdi = __shfl_sync(0xffffffffu, rd_own, i);
-    x[i] = (i < n) ? (((i == t) ? T(1) : T(0)) - ((a0 + a1) + (a2 + a3))) * rdi : 0.0;
-  }
-#pragma unroll
-  for (int i = 0; i < 32; i++) X[i + t * ldx] = (t < n) ? x[i] : 0.0;
-}
-
-// C (32x32, ld DLD) = A (32x32, ld lda) * op(B) for the 2x2 recursion of the
-// diagonal block.  Thread (i = tid % 32, warp w) owns C[i][8w .. 8w+7]: eight
-// independent accumulation chains, A read with unit stride across lanes and
-// B read as warp-wide broadcasts.  TRANSB selects B^T.
-template <bool TRANSB, typename T>
-__device__ __forceinline__ void prod32(const T* A, int lda, const T* B, int ldb, T (&c)[8]) {
-  const int i = threadIdx.x & 31, j0 = (threadIdx.x >> 5) * 8;
-#pragma unroll
-  for (int q = 0; q < 8; q++) c[q] = 0.0;
-#pragma unroll 8
-  for (int k = 0; k < 32; k++) {
-    const T a = A[i + k * lda];
-#pragma unroll
-    for (int q = 0; q < 8; q++) c[q] += a * (TRANSB ? B[(j0 + q) + k * ldb] : B[k + (j0 + q) * ldb]);
-  }
-}
-
-// Step kb, one CTA (4 warps) per front: factor the w x w diagonal block in
-// place as a 2 x 2 recursion over 32-blocks -- warp-level POTRF of the
-// diagonal blocks, L21 = D21 L11^-T, D22 -= L21 L21^T -- and store the inverse
-// of the factored block (lower, ld PANEL_NB) for the TRSM of the rows below.
-// The block is padded with the identity to 64 x 64 so that the warp routines
-// always run at their compile-time size.
 template <typename T>
 __global__ void __launch_bounds__(128)
-k_potrf_diag(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-             const int* __restrict__ rows, T* __restrict__ L, T* __restrict__ Dinv, int kb,
-             int* status) {
+k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
+       T* __restrict__ L, int kb, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  T* D = sm;                        // the block, col-major, ld DLD
-  T* X = sm + PANEL_NB * DLD;       // its inverse
-  T* Ts = X + PANEL_NB * DLD;       // 32 x DLD scratch
-  __shared__ int bad;
+  T* D = reinterpret_cast<T*>(smraw);   // diagonal block, 64 x 64, ld LLD
+  T* A = D + PANEL_NB * LLD;            // this CTA's slab of rows below it, 64 x 64, ld LLD
+  T* Y = A + PANEL_NB * LLD;            // inverse of the current 16x16 piece, ld LYD
+  __shared__ int bad_s;
   if (failed(status)) return;
-  const FrontDesc F = fronts[list[blockIdx.x]];
+  const FrontDesc F = fronts[list[blockIdx.y]];
   const int f = F.f, s = F.s;
   if (kb >= s) return;
   const int w = min(PANEL_NB, s - kb);
+  const int r0 = kb + w + blockIdx.x * PANEL_NB;
+  const int nr = max(0, min(PANEL_NB, f - r0));
+  if (blockIdx.x > 0 && nr == 0) return;
   const int tid = threadIdx.x, warp = tid >> 5;
   T* P = L + F.l_off;
+  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
+    const int i = e % PANEL_NB, j = e / PANEL_NB;
+    D[i + j * LLD] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
+    A[i + j * LLD] = (i < nr && j < w) ? P[(r0 + i) + (size_t) (kb + j) * f] : T(0);
+  }
+  __syncthreads();
+  // thread -> the row it carries: threads 0-63 the slab's rows, threads 64..
+  // the diagonal block's rows below the current piece
+  for (int b = 0; b < PANEL_NB / LQ; b++) {
+    const int c0 = b * LQ;
+    if (warp == 0) {
+      const int bd = warp_chol_inv16(D + c0 + c0 * LLD, Y);
+      if (tid == 0) bad_s = bd;
+    }
+    __syncthreads();
+    if (bad_s >= 0) {
+      if (tid == 0 && blockIdx.x == 0 && c0 + bad_s < w) atomicMin(status, rows[F.rows_off + kb + c0 + bad_s]);
+      return;
+    }
+    const int nd = PANEL_NB - c0 - LQ;
+    T* M = nullptr;
+    int r = 0;
+    if (tid < PANEL_NB) {
+      M = A;
+      r = tid;
+    } else if (tid - PANEL_NB < nd) {
+      M = D;
+      r = c0 + LQ + (tid - PANEL_NB);
+    }
+    T x[LQ];
+    if (M) {
+      // X[r][c] = sum_{k <= c} M[r][c0 + k] Y[c][k], in place in row r
+      T v[LQ];
+#pragma unroll
+      for (int k = 0; k < LQ; k++) v[k] = M[r + (c0 + k) * LLD];
+#pragma unroll
+      for (int c = 0; c < LQ; c++) {
+        T acc = T(0);
+#pragma unroll
+        for (int k = 0; k <= c; k++) acc += v[k] * Y[c + k * LYD];
+        x[c] = acc;
+      }
+#pragma unroll
+      for (int c = 0; c < LQ; c++) M[r + (c0 + c) * LLD] = x[c];
+    }
+    __syncthreads();   // every row's piece of L is in place before it is read below
+    if (M) {
+      // the columns right of the piece (in D only the lower part):
+      // M[r][c] -= sum_k X[r][k] L[c][c0 + k]
+      const int cend = (M == A) ? PANEL_NB : r + 1;
+      for (int c = c0 + LQ; c < cend; c++) {
+        T acc = M[r + c * LLD];
+#pragma unroll
+        for (int k = 0; k < LQ; k++) acc -= x[k] * D[c + (c0 + k) * LLD];
+        M[r + c * LLD] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x == 0)
+    for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
+      const int i = e % PANEL_NB, j = e / PANEL_NB;
+      if (i >= j && i < w) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * LLD];
+    }
+  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
+    const int i = e % PANEL_NB, j = e / PANEL_NB;
+    if (i < nr && j < w) P[(r0 + i) + (size_t) (kb + j) * f] = A[i + j * LLD];
+  }
+}
+
+// Inverses of the 64x64 diagonal blocks of every big front's factored panel
+// (L_kk^-1, lower, zero beyond the block's width), which the solve applies;
+// one CTA per block.  Warp q inverts the 16x16 diagonal piece q; then warp b
+// forms block column b below the diagonal, X_cb = -X_cc sum_{b<=k<c} L_ck X_kb.
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_dinv(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts, const T* __restrict__ L,
+       T* __restrict__ Dinv, const int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* S = reinterpret_cast<T*>(smraw);   // L_kk, 64 x 64, ld LLD (identity beyond w)
+  T* X = S + PANEL_NB * LLD;            // its inverse, ld LLD
+  T* Tm = X + PANEL_NB * LLD;           // per warp: a 16x16 partial sum, ld LYD
+  if (failed(status)) return;
+  const int2_ bl = blocks[blockIdx.x];
+  const FrontDesc F = fronts[bl.a];
+  const int f = F.f, kb = bl.b * PANEL_NB;
+  const int w = min(PANEL_NB, F.s - kb);
+  const T* P = L + F.l_off;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
+    const int i = e % PANEL_NB, j = e / PANEL_NB;
+    S[i + j * LLD] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
+    X[i + j * LLD] = T(0);
+  }
+  __syncthreads();
   {
-    T v[PANEL_NB * PANEL_NB / 128];
+    const int q0 = warp * LQ, i = lane & 15;
+    T a[LQ];
 #pragma unroll
-    for (int q = 0; q < PANEL_NB * PANEL_NB / 128; q++) {
-      const int k = tid + q * 128, i = k % PANEL_NB, j = k / PANEL_NB;
-      v[q] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
+    for (int k = 0; k < LQ; k++) a[k] = (k <= i) ? S[(q0 + i) + (q0 + k) * LLD] : T(0);
+    T* Yq = Tm + warp * LQ * LYD;
+    warp_inv16_rows(a, Yq);
+    __syncwarp();
+    if (lane < LQ)
+      for (int r = 0; r < LQ; r++) X[(q0 + r) + (q0 + lane) * LLD] = Yq[r + lane * LYD];
+  }
+  __syncthreads();
+  if (warp < PANEL_NB / LQ - 1) {
+    const int b0 = warp * LQ, t = lane & 15;
+    T* Tw = Tm + warp * LQ * LYD;
+    for (int c = warp + 1; c < PANEL_NB / LQ; c++) {
+      const int c0 = c * LQ;
+      // Tw[:, t] = sum_{k=b}^{c-1} L_ck X_kb[:, t]
+      T acc[LQ];
+#pragma unroll
+      for (int r = 0; r < LQ; r++) acc[r] = T(0);
+      for (int j = b0; j < c0; j++) {
+        const T xj = X[j + (b0 + t) * LLD];
+#pragma unroll
+        for (int r = 0; r < LQ; r++) acc[r] += S[(c0 + r) + j * LLD] * xj;
+      }
+      __syncwarp();
+      if (lane < LQ)
+#pragma unroll
+        for (int r = 0; r < LQ; r++) Tw[r + t * LYD] = acc[r];
+      __syncwarp();
+      // X_cb[:, t] = -X_cc Tw[:, t]
+#pragma unroll
+      for (int r = 0; r < LQ; r++) acc[r] = T(0);
+      for (int j = 0; j < LQ; j++) {
+        const T tj = Tw[j + t * LYD];
+#pragma unroll
+        for (int r = 0; r < LQ; r++) acc[r] += X[(c0 + r) + (c0 + j) * LLD] * tj;
+      }
+      if (lane < LQ)
+#pragma unroll
+        for (int r = 0; r < LQ; r++) X[(c0 + r) + (b0 + t) * LLD] = -acc[r];
+      __syncwarp();
     }
-#pragma unroll
-    for (int q = 0; q < PANEL_NB * PANEL_NB / 128; q++) {
-      const int k = tid + q * 128, i = k % PANEL_NB, j = k / PANEL_NB;
-      D[i + j * DLD] = v[q];
-      X[i + j * DLD] = 0.0;
-    }
-  }
-  if (tid == 0) bad = -1;
-  __syncthreads();
-  T c[8];
-  const int ci = tid & 31, cj = (tid >> 5) * 8;
-  T* D21 = D + 32;
-  T* D22 = D + 32 + 32 * DLD;
-  T* X22 = X + 32 + 32 * DLD;
-  if (warp == 0) {
-    const int b = warp_potrf32(D, DLD, 32);
-    if (b < 0) warp_trinv32(D, DLD, X, DLD, 32);
-    if ((tid & 31) == 0) bad = b;
   }
   __syncthreads();
-  if (bad >= 0) {
-    if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
-    return;
-  }
-  // L21 = D21 X11^T
-  prod32<true>(D21, DLD, X, DLD, c);
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 8; q++) D21[ci + (cj + q) * DLD] = c[q];
-  __syncthreads();
-  // D22 -= L21 L21^T (lower part)
-  prod32<true>(D21, DLD, D21, DLD, c);
-#pragma unroll
-  for (int q = 0; q < 8; q++)
-    if (ci >= cj + q) D22[ci + (cj + q) * DLD] -= c[q];
-  __syncthreads();
-  if (warp == 0) {
-    const int b = warp_potrf32(D22, DLD, 32);
-    if (b < 0) warp_trinv32(D22, DLD, X22, DLD, 32);
-    if ((tid & 31) == 0) bad = b < 0 ? -1 : 32 + b;
-  }
-  __syncthreads();
-  if (bad >= 0) {
-    if (tid == 0) atomicMin(status, rows[F.rows_off + kb + bad]);
-    return;
-  }
-  // X21 = -X22 (L21 X11)
-  prod32<false>(D21, DLD, X, DLD, c);
-#pragma unroll
-  for (int q = 0; q < 8; q++) Ts[ci + (cj + q) * DLD] = c[q];
-  __syncthreads();
-  prod32<false>(X22, DLD, Ts, DLD, c);
-#pragma unroll
-  for (int q = 0; q < 8; q++) X[32 + ci + (cj + q) * DLD] = -c[q];
-  __syncthreads();
-  // the factored block's lower part (compile-time index arithmetic; w is
-  // below 64 only in a front's last block)
-  for (int k = tid; k < PANEL_NB * PANEL_NB; k += 128) {
-    const int i = k % PANEL_NB, j = k / PANEL_NB;
-    if (i >= j && i < w) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * DLD];
-  }
-  T* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
-  for (int k = tid; k < PANEL_NB * PANEL_NB; k += 128) {
-    const int i = k % PANEL_NB, j = k / PANEL_NB;
-    Di[k] = (i < w && j < w) ? X[i + j * DLD] : 0.0;
+  T* Di = Dinv + F.dinv_off + (size_t) bl.b * PANEL_NB * PANEL_NB;
+  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
+    const int i = e % PANEL_NB, j = e / PANEL_NB;
+    Di[e] = (i < w && j < w) ? X[i + j * LLD] : T(0);
   }
 }
 
@@ -454,73 +519,6 @@ __device__ __forceinline__ void mma_block(float (&acc)[MI][NI][4], const float (
       mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
       mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
     }
-}
-
-constexpr int TLD = PANEL_NB + 8;  // padded k-row stride of the TRSM operands
-
-// Step kb: rows below the diagonal block, X := X L_kk^-T = X * Dinv^T, one
-// CTA per 64-row slab, DMMA m16n8k8; in place (the slab is staged first).
-template <typename T>
-__global__ void __launch_bounds__(128)
-k_trsm(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-       T* __restrict__ L, const T* __restrict__ Dinv, int kb, const int* status) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* sm = reinterpret_cast<T*>(smraw);
-  T* As = sm;                        // [k][r]: slab, k-major
-  T* Bs = sm + PANEL_NB * TLD;       // [k][c]: Dinv[c][k]
-  if (failed(status)) return;
-  const FrontDesc F = fronts[list[blockIdx.y]];
-  const int f = F.f, s = F.s;
-  if (kb >= s) return;
-  const int w = min(PANEL_NB, s - kb);
-  const int r0 = kb + w + blockIdx.x * TRSM_ROWS;
-  if (r0 >= f) return;
-  const int nr = min(TRSM_ROWS, f - r0);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  T* P = L + F.l_off;
-  const T* Di = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
-  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
-    const int r = e % PANEL_NB, k = e / PANEL_NB;
-    As[k * TLD + r] = (r < nr && k < w) ? P[(r0 + r) + (size_t) (kb + k) * f] : 0.0;
-    Bs[k * TLD + r] = Di[r + k * PANEL_NB];
-  }
-  __syncthreads();
-  const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
-  T acc[2][4][4];
-#pragma unroll
-  for (int a = 0; a < 2; a++)
-#pragma unroll
-    for (int b = 0; b < 4; b++)
-#pragma unroll
-      for (int c = 0; c < 4; c++) acc[a][b][c] = 0.0;
-  for (int kk = 0; kk < PANEL_NB; kk += 8) {
-    T a[2][4], b[4][2];
-#pragma unroll
-    for (int mi = 0; mi < 2; mi++) {
-      const int r = wm * 32 + mi * 16 + g;
-      a[mi][0] = As[(kk + t) * TLD + r];
-      a[mi][1] = As[(kk + t) * TLD + r + 8];
-      a[mi][2] = As[(kk + t + 4) * TLD + r];
-      a[mi][3] = As[(kk + t + 4) * TLD + r + 8];
-    }
-#pragma unroll
-    for (int ni = 0; ni < 4; ni++) {
-      const int c = wn * 32 + ni * 8 + g;
-      b[ni][0] = Bs[(kk + t) * TLD + c];
-      b[ni][1] = Bs[(kk + t + 4) * TLD + c];
-    }
-    mma_block<2, 4>(acc, a, b);
-  }
-#pragma unroll
-  for (int mi = 0; mi < 2; mi++)
-#pragma unroll
-    for (int ni = 0; ni < 4; ni++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int r = wm * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
-        const int c = wn * 32 + ni * 8 + 2 * t + (q & 1);
-        if (r < nr && c < w) P[(r0 + r) + (size_t) (kb + c) * f] = acc[mi][ni][q];
-      }
 }
 
 constexpr int GEMM_STAGES = 3;
@@ -746,22 +744,18 @@ static void launch_gemm(bool alt, int gx128, int gx64, int nb, const int* blst, 
 }
 
 template <typename T>
-static constexpr size_t potrf_smem() { return (2 * PANEL_NB * DLD + 32 * DLD) * sizeof(T); }
-
-template <typename T>
 static void set_smem_attrs() {
   // once per device and type (request-server workers reach this concurrently)
   static PerDeviceOnce pd;
   per_device_once(pd, [] {
     cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
-    cudaFuncSetAttribute(k_potrf_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) potrf_smem<T>());
+    cudaFuncSetAttribute(k_leaf<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) leaf_smem<T>());
+    cudaFuncSetAttribute(k_dinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dinv_smem<T>());
     cudaFuncSetAttribute(k_gemm<T, 64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int) GemmCfg<64, 64>::smem<T>());
     cudaFuncSetAttribute(k_gemm<T, 128, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int) GemmCfg<128, 128>::smem<T>());
-    cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         2 * PANEL_NB * TLD * (int) sizeof(T));
     return true;
   });
 }
@@ -816,39 +810,31 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
       prof_end(KC_BUILD, st, 0.0, by);
       count_launch();
     }
-    const size_t trsm_smem = 2 * PANEL_NB * TLD * sizeof(T);
     // recursive panel factorization over aligned column intervals: factor
     // the left half, update the right half with one GEMM (K = half width),
-    // factor the right half; leaves are 64-column POTRF + TRSM steps
+    // factor the right half; leaves are 64-column steps (k_leaf: POTRF of
+    // the diagonal block and TRSM of the rows below in one launch)
     const int S = LP.max_s_big;
     int span = PANEL_NB;
     while (span < S) span *= 2;
     auto leaf = [&](int kb) {
-      int gx_t = 0;
-      double fp = 0.0, ft = 0.0, bp = 0.0, bt = 0.0;
+      int gx = 1;
+      double fl = 0.0, by = 0.0;
       for (int fi : LP.big_fronts) {
         const FrontDesc& F = P.fronts[fi];
         if (kb >= F.s) continue;
         const int w = std::min(PANEL_NB, F.s - kb);
-        gx_t = std::max(gx_t, (F.f - kb - w + TRSM_ROWS - 1) / TRSM_ROWS);
+        gx = std::max(gx, (F.f - kb - w + PANEL_NB - 1) / PANEL_NB);
         if (prof_enabled()) {
           const double ww = w, below = F.f - kb - w;
-          fp += ww * ww * ww / 3.0;
-          bp += sizeof(T) * ww * ww;
-          ft += 2.0 * below * ww * ww;
-          bt += 2.0 * sizeof(T) * below * ww + sizeof(T) * ww * ww;
+          fl += ww * ww * ww / 3.0 + below * ww * ww;
+          by += 2.0 * sizeof(T) * (ww * (ww + 1.0) / 2.0 + below * ww);
         }
       }
       prof_begin(KC_POTRF, st);
-      k_potrf_diag<T><<<nb, 128, potrf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, Dinv, kb, status);
-      prof_end(KC_POTRF, st, fp, bp);
+      k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, kb, status);
+      prof_end(KC_POTRF, st, fl, by);
       count_launch();
-      if (gx_t > 0) {
-        prof_begin(KC_TRSM, st);
-        k_trsm<T><<<dim3(gx_t, nb), 128, trsm_smem, st>>>(blst, D.fronts, L, Dinv, kb, status);
-        prof_end(KC_TRSM, st, ft, bt);
-        count_launch();
-      }
     };
     auto update = [&](int c_lo, int c_hi, int k_lo, int k_hi) {
       int gx = 0, gx64 = 0, maxc = 0, maxr = 0;
@@ -913,6 +899,13 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
     }
   }
   prof_tag(-1);
+  if (D.n_dblk > 0) {
+    prof_begin(KC_TRSM, st);
+    k_dinv<T><<<D.n_dblk, 128, dinv_smem<T>(), st>>>(D.dblk, D.fronts, L, Dinv, status);
+    prof_end(KC_TRSM, st, (double) D.n_dblk * PANEL_NB * PANEL_NB * PANEL_NB / 3.0,
+             2.0 * sizeof(T) * D.n_dblk * PANEL_NB * PANEL_NB);
+    count_launch();
+  }
   return (int) cudaGetLastError();
 }
 
