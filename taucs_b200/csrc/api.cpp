@@ -150,6 +150,7 @@ void free_numeric(Factor* F) {
   tb::dfree(F->dU); F->dU = nullptr;
   tb::dfree(F->dDinv); F->dDinv = nullptr;
   tb::dfree(F->dL32); F->dL32 = nullptr;
+  tb::dfree(F->dSp32); F->dSp32 = nullptr;
   tb::dfree(F->dU32); F->dU32 = nullptr;
   tb::dfree(F->dDinv32); F->dDinv32 = nullptr;
   F->has_numeric = false;

@@ -39,6 +39,7 @@ struct Factor {
 
   // FP32 fronts (precision 1) and iterative refinement
   float* dL32 = nullptr;
+  float* dSp32 = nullptr;      // split arena: TF32 hi/lo copies of a level's panels (Plan::sp_len)
   float* dU32 = nullptr;
   float* dDinv32 = nullptr;
   float* dA32 = nullptr;       // scaled values D A D in FP32

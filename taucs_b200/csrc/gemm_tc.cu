@@ -345,7 +345,234 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
   }
 }
 
+// ------------------------------------------------------------------------
+// The same products with the operands already split: the panel leaves
+// write every final value of a big FP32 front as TF32 hi and lo parts into
+// the split arena, in the operand layout of the MMAs (16-byte chunks of 4
+// columns for 8 rows; FrontDesc::sp_off).  A 128-row slab of one 4-column
+// chunk is 2 KB of contiguous memory there, so a K-slab of 16 columns of
+// the four operand parts (A hi/lo, B hi/lo) arrives in shared memory as 16
+// bulk copies (cp.async.bulk, completion counted in bytes on the stage's
+// mbarrier), issued by 16 lanes of warp 0 -- no thread touches an operand
+// value on the way.  Warp 1's lane 0 issues the MMAs (lo*hi + hi*lo +
+// hi*hi per 8 columns of K); all four warps then run the epilogue from TMEM.
+// The tiles of the update matrix (mode 1) start at the row group of row s,
+// so a tile may hold up to 7 rows of the panel above U; they are masked.
+
+constexpr int SP_BK = 16;                      // K per pipeline stage
+constexpr int SP_CHUNK = 16 * 128;             // bytes of one 4-column chunk of a 128-row slab
+constexpr int SP_PARTB = (SP_BK / 4) * SP_CHUNK;
+constexpr int SP_STAGE = 4 * SP_PARTB;         // A hi, A lo, B hi, B lo: 32 KB
+template <int STAGES>
+constexpr size_t sp_smem() { return (size_t) STAGES * SP_STAGE + 1024; }
+
+// K-major, no swizzle, chunk-major: the two 16-byte K halves of one MMA are
+// LBO = one chunk (2 KB) apart, consecutive 8-row groups SBO = 128 B apart
+__device__ __forceinline__ uint64_t sp_desc(unsigned addr) {
+  return (uint64_t) ((addr >> 4) & 0x3FFFu) | ((uint64_t) (SP_CHUNK >> 4) << 16) | ((uint64_t) (128 >> 4) << 32) |
+         (1ull << 46);
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+template <int STAGES>
+__global__ void __launch_bounds__(128, 2)
+k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const float* __restrict__ sp,
+          float* __restrict__ L, float* __restrict__ U, int c_lo, int c_hi, int k_lo, int k_hi, int mode,
+          int* status) {
+  __shared__ __align__(8) unsigned long long bars[2 * STAGES + 1];   // full[S], empty[S], done
+  __shared__ unsigned tmem_slot;
+  __shared__ int abort_cta;
+  extern __shared__ __align__(16) unsigned char sp_raw[];
+  if (*(volatile const int*) status != INT_MAX) return;
+  const FrontDesc F = fronts[list[blockIdx.y]];
+  const int f = F.f, s = F.s, m = f - s;
+  // tile grid origin (a row-group boundary), the valid rows/columns and K
+  int base, rows, cols, lo, kbeg, kend;
+  if (mode == 0) {
+    const int ce = min(c_hi, s);
+    if (c_lo >= ce) return;
+    base = c_lo; rows = f - c_lo; cols = ce - c_lo; lo = c_lo;
+    kbeg = k_lo; kend = k_hi;
+  } else {
+    if (m <= 0 || s <= 0) return;
+    base = s & ~7; rows = f - base; cols = f - base; lo = s;
+    kbeg = 0; kend = s;
+  }
+  if (kend <= kbeg) return;
+  int idx = blockIdx.x, c0 = 0;
+  for (;;) {
+    if (c0 >= cols) return;
+    const int nt_c = (rows - c0 + TC_BM - 1) / TC_BM;
+    if (idx < nt_c) break;
+    idx -= nt_c;
+    c0 += TC_BN;
+  }
+  const int r0 = c0 + idx * TC_BM;
+  const int R0 = base + r0, C0 = base + c0;            // first front row of the tile's rows / columns
+  const int nr = min(TC_BM, rows - r0), nc = min(TC_BN, cols - c0);
+  const int nmma = (nc + 15) & ~15;
+  const int nk = (kend - kbeg + SP_BK - 1) / SP_BK;
+  const int rg = (int) sp_rgroups(f);
+  const float* part0 = sp + F.sp_off;
+  const float* part1 = part0 + sp_part(F);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const unsigned sbase = (smem_u32(sp_raw) + 1023u) & ~1023u;
+  const unsigned full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[STAGES]),
+                 done = smem_u32(&bars[2 * STAGES]);
+  if (tid == 0) {
+    for (int i = 0; i < STAGES; i++) {
+      mbar_init(full0 + 8 * i, 1);
+      mbar_init(empty0 + 8 * i, 1);
+    }
+    mbar_init(done, 1);
+    abort_cta = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = tmem_slot;
+
+  if (warp == 0) {
+    // ---- producer: lane q < 16 copies chunk q % 4 of operand part q / 4
+    const int p = lane >> 2, c = lane & 3;
+    const float* pb = (p & 1) ? part1 : part0;
+    const int g0 = ((p < 2) ? R0 : C0) >> 3;
+    for (int kt = 0; kt < nk; kt++) {
+      const int stg = kt % STAGES, use = kt / STAGES;
+      if (use > 0) {
+        int got = 1;
+        if (lane == 0) got = mbar_wait(empty0 + 8 * stg, (use - 1) & 1);
+        got = __shfl_sync(0xffffffffu, got, 0);
+        if (!got) {
+          if (lane == 0) {
+            record_timeout(status);
+            abort_cta = 1;
+          }
+          break;
+        }
+      }
+      if (lane == 0) mbar_expect_tx(full0 + 8 * stg, SP_STAGE);
+      __syncwarp();
+      if (lane < 16) {
+        const int64_t kc = (kbeg + kt * SP_BK) / 4 + c;
+        const float* src = pb + (kc * rg + g0) * 32;
+        bulk_g2s(sbase + stg * SP_STAGE + p * SP_PARTB + c * SP_CHUNK, src, SP_CHUNK, full0 + 8 * stg);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issue, one thread
+    const unsigned idesc = tc_idesc(nmma);
+    bool ok = true;
+    for (int kt = 0; kt < nk; kt++) {
+      const int stg = kt % STAGES, use = kt / STAGES;
+      if (!mbar_wait(full0 + 8 * stg, use & 1)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const unsigned st = sbase + stg * SP_STAGE;
+#pragma unroll
+      for (int j = 0; j < SP_BK / 8; j++) {
+        const unsigned o = 2 * j * SP_CHUNK;
+        const uint64_t ah = sp_desc(st + 0 * SP_PARTB + o), al = sp_desc(st + 1 * SP_PARTB + o);
+        const uint64_t bh = sp_desc(st + 2 * SP_PARTB + o), bl = sp_desc(st + 3 * SP_PARTB + o);
+        tc_mma(tmem, al, bh, idesc, (kt | j) != 0);
+        tc_mma(tmem, ah, bl, idesc, 1u);
+        tc_mma(tmem, ah, bh, idesc, 1u);
+      }
+      tc_commit(empty0 + 8 * stg);
+    }
+    if (!ok) {
+      record_timeout(status);
+      abort_cta = 1;
+    }
+    // done fires once every MMA issued above has completed
+    tc_commit(done);
+  }
+  // ---- epilogue: warp w owns TMEM lanes (tile rows) 32 w .. 32 w + 31
+  int gd = 1;
+  if (lane == 0) gd = mbar_wait(done, 0);
+  const bool got = __shfl_sync(0xffffffffu, gd, 0) != 0;
+  __syncwarp();
+  if (!got && lane == 0) record_timeout(status);
+  tc_fence_after();
+  const int er = warp * 32 + lane;
+  const int row = R0 + er;
+  const bool rv = er < nr && row >= lo;
+  float* Cp = nullptr;
+  int64_t ldc = 0;
+  if (mode == 0) {
+    Cp = L + F.l_off + row;
+    ldc = f;
+  } else {
+    Cp = U + F.u_off + (row - s);
+    ldc = m;
+  }
+  const int coff = (mode == 0) ? 0 : s;
+  // tcgen05.ld is warp-collective: the decision must be warp-uniform
+  if (__all_sync(0xffffffffu, got && !*(volatile int*) &abort_cta)) {
+    const unsigned tl = tmem + ((unsigned) (warp * 32) << 16);
+    for (int cb = 0; cb < nc; cb += 32) {
+      unsigned v[32];
+      tmem_ld32(tl + cb, v);
+      if (rv) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int col = C0 + cb + j;
+          if (cb + j < nc && col >= lo && row >= col) {
+            float* cpt = Cp + (int64_t) (col - coff) * ldc;
+            *cpt = *cpt - __uint_as_float(v[j]);
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+  }
+}
+
 }  // namespace
+
+bool gemm_sp_init() {
+  static PerDeviceOnce pd;
+  return per_device_once(pd, [] {
+    return cudaFuncSetAttribute(k_gemm_sp<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sp_smem<3>()) ==
+           cudaSuccess;
+  });
+}
+
+// tiles of one front in mode 1 start at the row group of row s
+int gemm_sp_tiles_u(int s, int f) {
+  const int n = f - (s & ~7);
+  return gemm_tc_tiles(n, n);
+}
+
+void launch_gemm_sp(int gx, int nb, const int* list, const FrontDesc* fronts, const float* sp, float* L, float* U,
+                    int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
+  k_gemm_sp<3><<<dim3(gx, nb), 128, sp_smem<3>(), st>>>(list, fronts, sp, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
+}
 
 // variant 0: two-stage ring (65 KB), 128 producers, three CTAs per SM;
 // variant 1: three-stage ring (97 KB), 256 producers, two CTAs per SM

@@ -80,7 +80,24 @@ struct FrontDesc {
   int level;
   int parent;         // device-order parent index, -1 for roots
   int sn;             // reference slot
+  int64_t sp_off;     // FP32 fronts: offset (floats) of the panel's split copy in the level's split
+                      // arena (layout below), -1 for fronts factored whole in shared memory
 };
+
+// Split copy of an FP32 front's panel for the tensor-core products: TF32
+// hi and lo parts of every value, each part laid out as 16-byte chunks of 4
+// consecutive columns (k) for 8 consecutive rows (r): element (r, k) of part
+// p at p * sp_part(F) + ((k / 4) * rg + r / 8) * 32 + (r % 8) * 4 + k % 4,
+// rg = ceil(f / 8) row groups; the columns run to a multiple of SP_KPAD.
+#ifdef __CUDACC__
+#define TB_HD __host__ __device__
+#else
+#define TB_HD
+#endif
+constexpr int SP_KPAD = 16;
+TB_HD inline int64_t sp_kchunks(int s) { return ((int64_t) (s + SP_KPAD - 1) / SP_KPAD) * (SP_KPAD / 4); }
+TB_HD inline int64_t sp_rgroups(int f) { return (f + 7) / 8; }
+TB_HD inline int64_t sp_part(const FrontDesc& F) { return sp_kchunks(F.s) * sp_rgroups(F.f) * 32; }
 
 struct LevelPlan {
   int front_begin, front_end;      // fronts of this level (device order)
@@ -110,6 +127,7 @@ struct Plan {
   int64_t dinv_len = 0;            // doubles of diagonal-block inverses
   int n_blk = 0;                   // solve flags
   int64_t part_len = 0;            // doubles of backward partial sums
+  int64_t sp_len = 0;              // floats of the split arena (the largest level's split copies)
   int64_t nnz = 0;
   std::vector<FrontDesc> fronts;
   std::vector<int> children;       // device-order child indices

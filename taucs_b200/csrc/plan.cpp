@@ -346,6 +346,23 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
       }
     }
     P.part_len = std::max<int64_t>(poff, 32);
+    // split copies of the big fronts' panels for the FP32 tensor-core
+    // products; the levels run one after another, so each level starts the
+    // arena afresh.  One tile of slack at the end: the bulk copies of a
+    // 128-row tile may read past the last row group of the last front.
+    int64_t soff = 0, smax = 0;
+    for (int i = 0; i < nf; i++) {
+      FrontDesc& F = P.fronts[i];
+      if (i > 0 && P.fronts[i - 1].level != F.level) soff = 0;
+      if (F.f > SMALL_F_MAX) {
+        F.sp_off = soff;
+        soff += 2 * sp_part(F);
+        smax = std::max(smax, soff);
+      } else {
+        F.sp_off = -1;
+      }
+    }
+    P.sp_len = smax + 16 * 32 * 4;
   }
 
   // levels, front classes, build tiles

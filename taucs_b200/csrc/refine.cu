@@ -304,6 +304,7 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
   cudaStream_t st = current_stream();
   auto al = [&](float** d, size_t n, const char* w) { return *d || cuda_ok(tb::dmalloc(d, sizeof(float) * std::max<size_t>(n, 1)), w); };
   if (!al(&F->dL32, P.l_len, "cudaMalloc(L32)") || !al(&F->dU32, P.u_len, "cudaMalloc(U32)") ||
+      !al(&F->dSp32, P.sp_len, "cudaMalloc(split arena)") ||
       !al(&F->dDinv32, P.dinv_len, "cudaMalloc(Dinv32)") || !al(&F->dA32, P.nnz, "cudaMalloc(A32)") ||
       !al(&F->dW32, (size_t) P.v_len * SOLVE_NRHS, "cudaMalloc(W32)") || !al(&F->dpart32, P.part_len, "cudaMalloc(part32)")) {
     free_numeric(F);
@@ -321,7 +322,7 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
     return 1;
   }
   int e = run_graphed(F, GraphKey{2, (uint64_t) F->dA32, 0, 0, 0, 0}, st, [&](cudaStream_t s) {
-    return launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dstatus, s);
+    return launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dSp32, F->dstatus, s);
   });
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
