@@ -259,6 +259,19 @@ int taucs_b200_solve_refine_device(void* L, int nrhs, double* d_X, const double*
  * finished: 0 FP32 steps only, 1 PCG, 2 FP64 refactorization; and the PCG
  * iterations it used. */
 int taucs_b200_set_pcg(void* L, int maxits);
+/* How taucs_b200_solve_refine[_device] refines with an FP32 factor: 0
+ * (default) refinement steps x += (L32 L32^T)^-1 r, with PCG only when they
+ * stall; 1 conjugate gradients preconditioned by the FP32 factor from the
+ * first step (one system per handle; batches keep method 0).  Either falls
+ * back to an FP64 refactorization when it does not reach the tolerance. */
+int taucs_b200_set_refinement(void* L, int method);
+/* Operand format of the FP32 fronts' tensor-core products (no counterpart
+ * in the reference): 0 (default) TF32 hi + lo parts, three TF32 MMAs per
+ * product; 1 FP16 hi + lo parts (lo scaled by 2^11), three FP16 MMAs at
+ * twice the TF32 rate.  Both keep about 21 bits of every operand; the FP16
+ * form relies on the diagonal scaling of the FP32 fronts, which bounds every
+ * factor entry by 1 in magnitude. */
+int taucs_b200_set_split_format(void* L, int fmt);
 int taucs_b200_refine_report(void* L, int* fallback, int* pcg_iterations);
 
 /* Inspection of the symbolic factor, in the reference's own arrays (slots

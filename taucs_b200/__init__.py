@@ -114,6 +114,8 @@ def lib():
         "taucs_b200_solve_refine": (C.c_int, [vp, pc, C.c_int, _f64p, _f64p, C.c_double, C.c_int, _f64p]),
         "taucs_b200_solve_refine_device": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_double, C.c_int, _f64p]),
         "taucs_b200_set_pcg": (C.c_int, [vp, C.c_int]),
+        "taucs_b200_set_refinement": (C.c_int, [vp, C.c_int]),
+        "taucs_b200_set_split_format": (C.c_int, [vp, C.c_int]),
         "taucs_conjugate_gradients": (C.c_int, [pc, vp, vp, _f64p, _f64p, C.c_int, C.c_double]),
         "taucs_b200_refine_report": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "taucs_b200_batch_analyze": (vp, [C.c_int, C.POINTER(pc)]),

@@ -39,7 +39,8 @@ struct Factor {
 
   // FP32 fronts (precision 1) and iterative refinement
   float* dL32 = nullptr;
-  float* dSp32 = nullptr;      // split arena: TF32 hi/lo copies of a level's panels (Plan::sp_len)
+  float* dSp32 = nullptr;      // split arena: split copies of a level's panels (Plan::sp_len)
+  int sp_fmt = 0;              // split format of the tensor-core products: 0 TF32 x3, 1 FP16 x3
   float* dU32 = nullptr;
   float* dDinv32 = nullptr;
   float* dA32 = nullptr;       // scaled values D A D in FP32
@@ -68,6 +69,7 @@ struct Factor {
   double* ddot = nullptr;
   double* hdot = nullptr;              // pinned readback of ddot
   int pcg_maxits = 100;                // 0: no PCG, stalled refinement refactors in FP64
+  int refine_method = 0;               // 0: refinement steps (PCG on stall), 1: PCG from the first step
   int last_fallback = 0;               // last refinement: 0 FP32 steps, 1 PCG, 2 FP64 refactor
   int last_pcg_its = 0;
   const double* dvals_cur = nullptr;   // values of the last numeric factorization (device)

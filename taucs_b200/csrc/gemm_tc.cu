@@ -347,24 +347,41 @@ k_gemm_tc(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, fl
 
 // ------------------------------------------------------------------------
 // The same products with the operands already split: the panel leaves
-// write every final value of a big FP32 front as TF32 hi and lo parts into
-// the split arena, in the operand layout of the MMAs (16-byte chunks of 4
-// columns for 8 rows; FrontDesc::sp_off).  A 128-row slab of one 4-column
-// chunk is 2 KB of contiguous memory there, so a K-slab of 16 columns of
-// the four operand parts (A hi/lo, B hi/lo) arrives in shared memory as 16
-// bulk copies (cp.async.bulk, completion counted in bytes on the stage's
-// mbarrier), issued by 16 lanes of warp 0 -- no thread touches an operand
-// value on the way.  Warp 1's lane 0 issues the MMAs (lo*hi + hi*lo +
-// hi*hi per 8 columns of K); all four warps then run the epilogue from TMEM.
-// The tiles of the update matrix (mode 1) start at the row group of row s,
-// so a tile may hold up to 7 rows of the panel above U; they are masked.
+// write every final value of a big FP32 front, split, into the split arena
+// in the operand layout of the MMAs (16-byte chunks of consecutive columns
+// for 8 rows; FrontDesc::sp_off), either as TF32 hi and lo (FMT 0) or as
+// FP16 hi and lo scaled by 2^11 (FMT 1).  A 128-row slab of one chunk is 2 KB
+// of contiguous memory there, so four chunks (K = 16 TF32 or 32 FP16
+// columns) of the four operand parts (A hi/lo, B hi/lo) arrive in shared
+// memory as 16 bulk copies (cp.async.bulk, completion counted in bytes on the
+// stage's mbarrier), issued by 16 lanes of warp 0 -- no thread touches an
+// operand value on the way.  Warp 1's lane 0 issues the MMAs: TF32,
+// lo*hi + hi*lo + hi*hi into one accumulator; FP16 (kind::f16, twice the
+// TF32 rate), hi*hi into one accumulator and hi*lo + lo*hi into a second,
+// combined in the epilogue as acc0 + acc1 / 2048.  All four warps then run
+// the epilogue from TMEM.  The tiles of the update matrix (mode 1) start at
+// the row group of row s, so a tile may hold up to 7 rows of the panel above
+// U; they are masked.
 
-constexpr int SP_BK = 16;                      // K per pipeline stage
-constexpr int SP_CHUNK = 16 * 128;             // bytes of one 4-column chunk of a 128-row slab
-constexpr int SP_PARTB = (SP_BK / 4) * SP_CHUNK;
+constexpr int SP_CHUNK = 16 * 128;             // bytes of one 16-byte-wide chunk of a 128-row slab
+constexpr int SP_PARTB = 4 * SP_CHUNK;         // four chunks per stage
 constexpr int SP_STAGE = 4 * SP_PARTB;         // A hi, A lo, B hi, B lo: 32 KB
 template <int STAGES>
 constexpr size_t sp_smem() { return (size_t) STAGES * SP_STAGE + 1024; }
+
+// kind::f16 instruction descriptor: D f32, A/B f16, both K-major, M = 128
+__device__ __forceinline__ unsigned f16_idesc(int n) {
+  return (1u << 4) | ((unsigned) (n >> 3) << 17) | ((unsigned) (TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void f16_mma(unsigned tmem, uint64_t a, uint64_t b, unsigned idesc, unsigned acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
 
 // K-major, no swizzle, chunk-major: the two 16-byte K halves of one MMA are
 // LBO = one chunk (2 KB) apart, consecutive 8-row groups SBO = 128 B apart
@@ -384,7 +401,7 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
       : "memory");
 }
 
-template <int STAGES>
+template <int STAGES, int FMT>
 __global__ void __launch_bounds__(128, 2)
 k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const float* __restrict__ sp,
           float* __restrict__ L, float* __restrict__ U, int c_lo, int c_hi, int k_lo, int k_hi, int mode,
@@ -421,10 +438,13 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
   const int R0 = base + r0, C0 = base + c0;            // first front row of the tile's rows / columns
   const int nr = min(TC_BM, rows - r0), nc = min(TC_BN, cols - c0);
   const int nmma = (nc + 15) & ~15;
-  const int nk = (kend - kbeg + SP_BK - 1) / SP_BK;
+  constexpr int CW = FMT ? 8 : 4;               // columns per chunk
+  constexpr int BK = 4 * CW;                     // K per stage
+  constexpr unsigned TMEM_COLS = FMT ? 2 * TC_TMEM_COLS : TC_TMEM_COLS;
+  const int nk = (kend - kbeg + BK - 1) / BK;
   const int rg = (int) sp_rgroups(f);
-  const float* part0 = sp + F.sp_off;
-  const float* part1 = part0 + sp_part(F);
+  const unsigned char* part0 = reinterpret_cast<const unsigned char*>(sp + F.sp_off);
+  const unsigned char* part1 = part0 + sp_part_bytes(F, FMT);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const unsigned sbase = (smem_u32(sp_raw) + 1023u) & ~1023u;
@@ -441,7 +461,7 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(TC_TMEM_COLS)
+                 "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -453,7 +473,7 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
   if (warp == 0) {
     // ---- producer: lane q < 16 copies chunk q % 4 of operand part q / 4
     const int p = lane >> 2, c = lane & 3;
-    const float* pb = (p & 1) ? part1 : part0;
+    const unsigned char* pb = (p & 1) ? part1 : part0;
     const int g0 = ((p < 2) ? R0 : C0) >> 3;
     for (int kt = 0; kt < nk; kt++) {
       const int stg = kt % STAGES, use = kt / STAGES;
@@ -472,14 +492,14 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
       if (lane == 0) mbar_expect_tx(full0 + 8 * stg, SP_STAGE);
       __syncwarp();
       if (lane < 16) {
-        const int64_t kc = (kbeg + kt * SP_BK) / 4 + c;
-        const float* src = pb + (kc * rg + g0) * 32;
+        const int64_t kc = (kbeg + kt * BK) / CW + c;
+        const unsigned char* src = pb + (kc * rg + g0) * 128;
         bulk_g2s(sbase + stg * SP_STAGE + p * SP_PARTB + c * SP_CHUNK, src, SP_CHUNK, full0 + 8 * stg);
       }
     }
   } else if (warp == 1 && lane == 0) {
-    // ---- MMA issue, one thread
-    const unsigned idesc = tc_idesc(nmma);
+    // ---- MMA issue, one thread: two MMAs of K = 2 chunks per stage
+    const unsigned idesc = FMT ? f16_idesc(nmma) : tc_idesc(nmma);
     bool ok = true;
     for (int kt = 0; kt < nk; kt++) {
       const int stg = kt % STAGES, use = kt / STAGES;
@@ -490,13 +510,20 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
       tc_fence_after();
       const unsigned st = sbase + stg * SP_STAGE;
 #pragma unroll
-      for (int j = 0; j < SP_BK / 8; j++) {
+      for (int j = 0; j < 2; j++) {
         const unsigned o = 2 * j * SP_CHUNK;
         const uint64_t ah = sp_desc(st + 0 * SP_PARTB + o), al = sp_desc(st + 1 * SP_PARTB + o);
         const uint64_t bh = sp_desc(st + 2 * SP_PARTB + o), bl = sp_desc(st + 3 * SP_PARTB + o);
-        tc_mma(tmem, al, bh, idesc, (kt | j) != 0);
-        tc_mma(tmem, ah, bl, idesc, 1u);
-        tc_mma(tmem, ah, bh, idesc, 1u);
+        const unsigned first = (kt | j) != 0;
+        if (FMT == 0) {
+          tc_mma(tmem, al, bh, idesc, first);
+          tc_mma(tmem, ah, bl, idesc, 1u);
+          tc_mma(tmem, ah, bh, idesc, 1u);
+        } else {
+          f16_mma(tmem, ah, bh, idesc, first);
+          f16_mma(tmem + TC_TMEM_COLS, ah, bl, idesc, first);
+          f16_mma(tmem + TC_TMEM_COLS, al, bh, idesc, 1u);
+        }
       }
       tc_commit(empty0 + 8 * stg);
     }
@@ -533,6 +560,13 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
     for (int cb = 0; cb < nc; cb += 32) {
       unsigned v[32];
       tmem_ld32(tl + cb, v);
+      if (FMT) {
+        unsigned v1[32];
+        tmem_ld32(tl + TC_TMEM_COLS + cb, v1);
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(v1[j]) * (1.0f / 2048.0f));
+      }
       if (rv) {
 #pragma unroll
         for (int j = 0; j < 32; j++) {
@@ -549,7 +583,7 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
   }
 }
 
@@ -558,8 +592,10 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
 bool gemm_sp_init() {
   static PerDeviceOnce pd;
   return per_device_once(pd, [] {
-    return cudaFuncSetAttribute(k_gemm_sp<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sp_smem<3>()) ==
-           cudaSuccess;
+    return cudaFuncSetAttribute(k_gemm_sp<3, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sp_smem<3>()) ==
+               cudaSuccess &&
+           cudaFuncSetAttribute(k_gemm_sp<3, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sp_smem<3>()) ==
+               cudaSuccess;
   });
 }
 
@@ -569,9 +605,14 @@ int gemm_sp_tiles_u(int s, int f) {
   return gemm_tc_tiles(n, n);
 }
 
-void launch_gemm_sp(int gx, int nb, const int* list, const FrontDesc* fronts, const float* sp, float* L, float* U,
-                    int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
-  k_gemm_sp<3><<<dim3(gx, nb), 128, sp_smem<3>(), st>>>(list, fronts, sp, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
+void launch_gemm_sp(int fmt, int gx, int nb, const int* list, const FrontDesc* fronts, const float* sp, float* L,
+                    float* U, int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st) {
+  if (fmt)
+    k_gemm_sp<3, 1><<<dim3(gx, nb), 128, sp_smem<3>(), st>>>(list, fronts, sp, L, U, c_lo, c_hi, k_lo, k_hi, mode,
+                                                             status);
+  else
+    k_gemm_sp<3, 0><<<dim3(gx, nb), 128, sp_smem<3>(), st>>>(list, fronts, sp, L, U, c_lo, c_hi, k_lo, k_hi, mode,
+                                                             status);
 }
 
 // variant 0: two-stage ring (65 KB), 128 producers, three CTAs per SM;

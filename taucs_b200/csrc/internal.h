@@ -84,20 +84,26 @@ struct FrontDesc {
                       // arena (layout below), -1 for fronts factored whole in shared memory
 };
 
-// Split copy of an FP32 front's panel for the tensor-core products: TF32
-// hi and lo parts of every value, each part laid out as 16-byte chunks of 4
-// consecutive columns (k) for 8 consecutive rows (r): element (r, k) of part
-// p at p * sp_part(F) + ((k / 4) * rg + r / 8) * 32 + (r % 8) * 4 + k % 4,
-// rg = ceil(f / 8) row groups; the columns run to a multiple of SP_KPAD.
+// Split copy of an FP32 front's panel for the tensor-core products, in one
+// of two formats: 0, TF32 hi and lo parts of every value (x = hi + lo, 4-byte
+// elements); 1, FP16 hi and scaled lo parts (x = hi + lo / 2048, 2-byte
+// elements).  Each part is laid out as 16-byte chunks of consecutive columns
+// (4 or 8) for 8 consecutive rows: element (r, k) of part p at byte
+// p * sp_part_bytes + ((k / cw) * rg + r / 8) * 128 + (r % 8) * 16 + (k % cw) * esz,
+// cw = sp_chunk_cols, rg = ceil(f / 8) row groups; the columns run to a
+// multiple of 4 chunks (one pipeline stage of the products).
 #ifdef __CUDACC__
 #define TB_HD __host__ __device__
 #else
 #define TB_HD
 #endif
-constexpr int SP_KPAD = 16;
-TB_HD inline int64_t sp_kchunks(int s) { return ((int64_t) (s + SP_KPAD - 1) / SP_KPAD) * (SP_KPAD / 4); }
+TB_HD inline int sp_chunk_cols(int fmt) { return fmt ? 8 : 4; }
+TB_HD inline int64_t sp_kchunks(int s, int fmt) {
+  const int kst = 4 * sp_chunk_cols(fmt);
+  return ((int64_t) (s + kst - 1) / kst) * 4;
+}
 TB_HD inline int64_t sp_rgroups(int f) { return (f + 7) / 8; }
-TB_HD inline int64_t sp_part(const FrontDesc& F) { return sp_kchunks(F.s) * sp_rgroups(F.f) * 32; }
+TB_HD inline int64_t sp_part_bytes(const FrontDesc& F, int fmt) { return sp_kchunks(F.s, fmt) * sp_rgroups(F.f) * 128; }
 
 struct LevelPlan {
   int front_begin, front_end;      // fronts of this level (device order)

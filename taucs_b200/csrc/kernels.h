@@ -85,9 +85,10 @@ int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, dou
                         double* U, double* Dinv, int* status, cudaStream_t st);
 // the same factorization with FP32 fronts (TF32x3 tensor products)
 // sp: the split arena (Plan::sp_len floats; its contents are produced by the
-// factorization itself), or nullptr to factor without it
+// factorization itself), or nullptr to factor without it; sp_fmt its format
+// (0 TF32 hi/lo, 1 FP16 hi/scaled lo)
 int launch_numeric_fp32(const Plan& P, const DevPlan& D, const float* vals, float* L,
-                        float* U, float* Dinv, float* sp, int* status, cudaStream_t st);
+                        float* U, float* Dinv, float* sp, int sp_fmt, int* status, cudaStream_t st);
 
 // status value recorded when a bounded device wait of the factorization gave
 // up (never a column index)
@@ -105,7 +106,7 @@ int gemm_tc_tiles(int rows, int cols);
 // the tcgen05 GEMM fed from the split arena by bulk copies (same modes)
 bool gemm_sp_init();
 int gemm_sp_tiles_u(int s, int f);
-void launch_gemm_sp(int gx, int nb, const int* list, const FrontDesc* fronts, const float* sp, float* L, float* U,
+void launch_gemm_sp(int fmt, int gx, int nb, const int* list, const FrontDesc* fronts, const float* sp, float* L, float* U,
                     int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st);
 void launch_gemm_tc(int variant, int gx, int nb, const int* list, const FrontDesc* fronts, float* L, float* U,
                     int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st);

@@ -7,8 +7,10 @@
 //  * all nrhs columns are solved in one multi-RHS device solve instead of a
 //    per-column loop (:556-583);
 //  * taucs.gpu.precision=mixed factors in FP32 and refines in FP64.
-// Orderings, LU, OOC, CG/MINRES and preconditioners are outside this
-// library; requesting them returns TAUCS_ERROR_BADARGS.
+//  * taucs.ooc=true (out-of-core LL^T) gets the same factor, held in device
+//    memory, after the reference's checks of its file options.
+// LU, MINRES, the orderings other than AMD and GENMMD, and preconditioners
+// are outside this library; requesting them returns an error.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -116,7 +118,9 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
   double opt_cg_maxits = 300.0, opt_convergetol = 1e-6;   // src/taucs_linsolve.c:238-239
   const char* opt_ordering = nullptr;
   const char* opt_precision = "fp64";
-  const char* sdummy = nullptr;
+  const char* opt_ooc_name = nullptr;
+  double opt_ooc_memory = -1.0;
+  int opt_ooc_handle = 0;
   if (options) {
     for (int i = 0; options[i]; i++) {
       const char* o = options[i];
@@ -135,7 +139,12 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
       u |= get_bool(o, "taucs.solve.minres", opt_arg, &opt_minres);
       u |= get_double(o, "taucs.solve.maxits", opt_arg, &opt_cg_maxits);
       u |= get_double(o, "taucs.solve.convergetol", opt_arg, &opt_convergetol);
-      u |= get_string(o, "taucs.ooc.basename", opt_arg, &sdummy);
+      u |= get_string(o, "taucs.ooc.basename", opt_arg, &opt_ooc_name);
+      u |= get_double(o, "taucs.ooc.memory", opt_arg, &opt_ooc_memory);
+      if (!strncmp(o, "taucs.ooc.iohandle=", 19)) {
+        opt_ooc_handle = 1;
+        u = 1;
+      }
       u |= get_string(o, "taucs.gpu.precision", opt_arg, &opt_precision);
       u |= get_double(o, "taucs.gpu.refine.tol", opt_arg, &opt_tol);
       u |= get_double(o, "taucs.gpu.refine.maxits", opt_arg, &opt_maxits);
@@ -144,9 +153,22 @@ extern "C" int taucs_linsolve(taucs_ccs_matrix* A, void** F, int nrhs, void* X, 
   }
   (void) opt_mf;
   (void) opt_ll;
-  if (opt_lu || opt_ooc || opt_minres) {
-    taucs_printf((char*) "taucs_linsolve: LU, out-of-core and MINRES are not provided by this library\n");
+  if (opt_lu || opt_minres) {
+    taucs_printf((char*) "taucs_linsolve: LU and MINRES are not provided by this library\n");
     return TAUCS_ERROR_BADARGS;
+  }
+  (void) opt_ooc_memory;
+  if (opt_ooc && opt_factor) {
+    // the reference's out-of-core LL^T (src/taucs_linsolve.c:366-402) keeps
+    // the factor in a file because it may not fit in memory; here it is the
+    // same multifrontal factor held in device memory.  The option checks are
+    // the reference's: exactly one of a file name and an I/O handle.
+    if ((opt_ooc_name != nullptr) == (opt_ooc_handle != 0)) {
+      taucs_printf((char*) "taucs_linsolve: ooc factorization requires exactly one of basename or iohandle\n");
+      return TAUCS_ERROR_BADARGS;
+    }
+    taucs_printf((char*) "taucs_linsolve: taucs.ooc: the LL^T factor is kept in device memory; no out-of-core "
+                         "file is written\n");
   }
   const bool mixed = opt_precision && !strcmp(opt_precision, "mixed");
 

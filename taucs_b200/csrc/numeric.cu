@@ -31,6 +31,7 @@
 // with atomicMin (the reference reports the failing column, :1139-1145).
 #include <climits>
 #include <cstdio>
+#include <cuda_fp16.h>
 
 #include "kernels.h"
 
@@ -268,7 +269,7 @@ __device__ int warp_chol_inv16(T* S, T* Y) {
 template <typename T>
 __global__ void __launch_bounds__(128)
 k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
-       T* __restrict__ L, float* __restrict__ sp, int kb, int* status) {
+       T* __restrict__ L, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* D = reinterpret_cast<T*>(smraw);   // diagonal block, 64 x 64, ld LLD
   T* A = D + PANEL_NB * LLD;            // this CTA's slab of rows below it, 64 x 64, ld LLD
@@ -353,29 +354,46 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
     if (i < nr && j < w) P[(r0 + i) + (size_t) (kb + j) * f] = A[i + j * LLD];
   }
   if (sizeof(T) == 4 && sp != nullptr && F.sp_off >= 0) {
-    // the slab's final values, split into TF32 hi/lo, into the split arena
-    // for the tensor-core products; the front's last leaf also writes the
-    // zero columns that pad K to the products' stage width
-    const int rg = (int) sp_rgroups(f);
-    const int64_t part = sp_part(F);
-    float* base = sp + F.sp_off;
-    const int kc_end = (kb + w == s) ? (int) sp_kchunks(s) : (kb + w) / 4;
-    const int nch = kc_end - kb / 4;
+    // the slab's final values, split, into the split arena for the tensor-
+    // core products; the front's last leaf also writes the zero columns that
+    // pad K to the products' stage width
+    const int rg = (int) sp_rgroups(f), cw = sp_chunk_cols(sp_fmt);
+    const int64_t part = sp_part_bytes(F, sp_fmt);
+    unsigned char* base = reinterpret_cast<unsigned char*>(sp + F.sp_off);
+    const int kc_end = (kb + w == s) ? (int) sp_kchunks(s, sp_fmt) : (kb + w) / cw;
+    const int nch = kc_end - kb / cw;
     for (int e = tid; e < nch * PANEL_NB; e += 128) {
       const int i = e % PANEL_NB, c = e / PANEL_NB;
       if (i >= nr) continue;
-      const int r = r0 + i, k0 = kb + 4 * c;
-      unsigned h[4], l[4];
+      const int r = r0 + i, k0 = kb + cw * c;
+      const int64_t o = ((int64_t) (k0 / cw) * rg + (r >> 3)) * 128 + (r & 7) * 16;
+      if (sp_fmt == 0) {
+        unsigned h[4], l[4];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int kk = k0 + q - kb;
-        const float x = (k0 + q < kb + w) ? (float) A[i + kk * LLD] : 0.0f;
-        h[q] = __float_as_uint(x) & 0xffffe000u;
-        l[q] = __float_as_uint(x - __uint_as_float(h[q]));
+        for (int q = 0; q < 4; q++) {
+          const float x = (k0 + q < kb + w) ? (float) A[i + (k0 + q - kb) * LLD] : 0.0f;
+          h[q] = __float_as_uint(x) & 0xffffe000u;
+          l[q] = __float_as_uint(x - __uint_as_float(h[q]));
+        }
+        *reinterpret_cast<uint4*>(base + o) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(base + part + o) = make_uint4(l[0], l[1], l[2], l[3]);
+      } else {
+        unsigned short h[8], l[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const float x = (k0 + q < kb + w) ? (float) A[i + (k0 + q - kb) * LLD] : 0.0f;
+          const __half hh = __float2half_rn(x);
+          h[q] = __half_as_ushort(hh);
+          l[q] = __half_as_ushort(__float2half_rn((x - __half2float(hh)) * 2048.0f));
+        }
+        uint4 vh, vl;
+        vh.x = h[0] | (unsigned) h[1] << 16; vh.y = h[2] | (unsigned) h[3] << 16;
+        vh.z = h[4] | (unsigned) h[5] << 16; vh.w = h[6] | (unsigned) h[7] << 16;
+        vl.x = l[0] | (unsigned) l[1] << 16; vl.y = l[2] | (unsigned) l[3] << 16;
+        vl.z = l[4] | (unsigned) l[5] << 16; vl.w = l[6] | (unsigned) l[7] << 16;
+        *reinterpret_cast<uint4*>(base + o) = vh;
+        *reinterpret_cast<uint4*>(base + part + o) = vl;
       }
-      const int64_t o = ((int64_t) (k0 / 4) * rg + (r >> 3)) * 32 + (r & 7) * 4;
-      *reinterpret_cast<uint4*>(base + o) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(base + part + o) = make_uint4(l[0], l[1], l[2], l[3]);
     }
   }
 }
@@ -750,7 +768,7 @@ static bool gemm_alt(const Plan& P, int h, int kind) {
 template <typename T>
 static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, T* L, T* U,
                         int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st,
-                        const float* = nullptr, int = 0) {
+                        const float* = nullptr, int = 0, int = 0) {
   if (big)
     k_gemm<T, 128, 128><<<dim3(gx128, nb), GemmCfg<128, 128>::THREADS, GemmCfg<128, 128>::smem<T>(), st>>>(
         blst, D.fronts, L, U, c_lo, c_hi, k_lo, k_hi, mode, status);
@@ -764,9 +782,9 @@ static void launch_gemm(bool big, int gx128, int gx64, int nb, const int* blst, 
 // producer warps split the operands as they load them
 static void launch_gemm(bool alt, int gx128, int gx64, int nb, const int* blst, const DevPlan& D, float* L, float* U,
                         int c_lo, int c_hi, int k_lo, int k_hi, int mode, int* status, cudaStream_t st,
-                        const float* sp = nullptr, int gx_sp = 0) {
+                        const float* sp = nullptr, int gx_sp = 0, int sp_fmt = 0) {
   if (!alt && sp && gemm_sp_init()) {
-    launch_gemm_sp(gx_sp, nb, blst, D.fronts, sp, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
+    launch_gemm_sp(sp_fmt, gx_sp, nb, blst, D.fronts, sp, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
     return;
   }
   if (gemm_tc_init()) {
@@ -795,7 +813,7 @@ static void set_smem_attrs() {
 
 template <typename T>
 static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, T* U, T* Dinv, float* sp,
-                          int* status, cudaStream_t st) {
+                          int sp_fmt, int* status, cudaStream_t st) {
   set_smem_attrs<T>();
   k_init_status<<<1, 1, 0, st>>>(status);
   count_launch();
@@ -865,7 +883,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
         }
       }
       prof_begin(KC_POTRF, st);
-      k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, sp, kb, status);
+      k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, sp, sp_fmt, kb, status);
       prof_end(KC_POTRF, st, fl, by);
       count_launch();
     };
@@ -890,7 +908,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
       if (gx64 == 0) return;
       prof_begin(KC_GEMM_PANEL, st);
       (void) maxr; (void) maxc;
-      launch_gemm(gemm_alt<T>(P, h, 0), gx, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, 0, status, st, sp, gx);
+      launch_gemm(gemm_alt<T>(P, h, 0), gx, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, 0, status, st, sp, gx, sp_fmt);
       prof_end(KC_GEMM_PANEL, st, fg, bg);
       count_launch();
     };
@@ -927,7 +945,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
         }
       prof_begin(KC_GEMM_U, st);
       (void) maxm;
-      launch_gemm(gemm_alt<T>(P, h, 1), gx_u, gx_u64, nb, blst, D, L, U, 0, 0, 0, 0, 1, status, st, sp, gx_usp);
+      launch_gemm(gemm_alt<T>(P, h, 1), gx_u, gx_u64, nb, blst, D, L, U, 0, 0, 0, 0, 1, status, st, sp, gx_usp, sp_fmt);
       prof_end(KC_GEMM_U, st, fu, bu);
       count_launch();
     }
@@ -945,12 +963,12 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
 
 int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L, double* U, double* Dinv,
                         int* status, cudaStream_t st) {
-  return launch_numeric<double>(P, D, vals, L, U, Dinv, nullptr, status, st);
+  return launch_numeric<double>(P, D, vals, L, U, Dinv, nullptr, 0, status, st);
 }
 
 int launch_numeric_fp32(const Plan& P, const DevPlan& D, const float* vals, float* L, float* U, float* Dinv,
-                        float* sp, int* status, cudaStream_t st) {
-  return launch_numeric<float>(P, D, vals, L, U, Dinv, sp, status, st);
+                        float* sp, int sp_fmt, int* status, cudaStream_t st) {
+  return launch_numeric<float>(P, D, vals, L, U, Dinv, sp, sp_fmt, status, st);
 }
 
 }  // namespace tb

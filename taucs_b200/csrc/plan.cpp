@@ -356,7 +356,7 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
       if (i > 0 && P.fronts[i - 1].level != F.level) soff = 0;
       if (F.f > SMALL_F_MAX) {
         F.sp_off = soff;
-        soff += 2 * sp_part(F);
+        soff += 2 * sp_part_bytes(F, 0) / 4;   // format 0 is the larger one
         smax = std::max(smax, soff);
       } else {
         F.sp_off = -1;

@@ -322,7 +322,7 @@ int numeric_fp32_device(Factor* F, const double* d_vals) {
     return 1;
   }
   int e = run_graphed(F, GraphKey{2, (uint64_t) F->dA32, 0, 0, 0, 0}, st, [&](cudaStream_t s) {
-    return launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dSp32, F->dstatus, s);
+    return launch_numeric_fp32(P, F->dp, F->dA32, F->dL32, F->dU32, F->dDinv32, F->dSp32, F->sp_fmt, F->dstatus, s);
   });
   if (!cuda_ok((cudaError_t) e, "numeric launch")) return -1;
   cudaMemcpyAsync(F->hstatus, F->dstatus, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -493,6 +493,30 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     double prev_worst = INFINITY;
     int slow = 0, steps = 0;
     bool done = false;
+    if (!use64 && ns == 1 && F->refine_method == 1 && F->pcg_maxits > 0) {
+      // conjugate gradients preconditioned by the FP32 factor from the start
+      // (from x = 0); the FP64 refactorization below only if they fail
+      if (!cuda_ok(cudaStreamSynchronize(st), "refinement")) return -1;
+      for (int q = 0; q < nq; q++) memcpy(&bnorm[q], &F->hnorm[(size_t) q * 2], 8);
+      std::vector<double> rq(nq, 0.0);
+      const int its = pcg_fp32(F, nq, X, B, ld, tol, anorm[0], bnorm.data(), rq.data());
+      if (its == -2) return -1;
+      if (res)
+        for (int q = 0; q < nq; q++) res[q0 + q] = rq[q];
+      F->last_pcg_its += std::max(its, 0);
+      if (its >= 0) {
+        F->last_fallback = std::max(F->last_fallback, 1);
+        total = std::max(total, its);
+        continue;
+      }
+      tprintf("\t\tPCG did not reach the tolerance; refactoring in FP64\n");
+      if (!F->has_numeric && numeric_fp64_device(F, F->dvals_cur, true)) return -1;
+      F->last_fallback = 2;
+      use64 = true;
+      cudaMemsetAsync(X, 0, sizeof(double) * ((size_t) ld * (nq - 1) + n), st);
+      if (run_graphed(F, GraphKey{6, (uint64_t) nq, (uint64_t) X, (uint64_t) B, (uint64_t) ld, 0}, st, residual))
+        return -1;
+    }
     for (int it = 0; !done; it++) {
       if (!cuda_ok(cudaStreamSynchronize(st), "refinement")) return -1;
       double worst = 0.0;
@@ -643,6 +667,20 @@ using namespace tb;
 extern "C" int taucs_b200_set_precision(void* L, int precision) {
   if (!L || (precision != 0 && precision != 1)) return -1;
   ((Factor*) L)->precision = precision;
+  return 0;
+}
+
+extern "C" int taucs_b200_set_split_format(void* L, int fmt) {
+  if (!L || fmt < 0 || fmt > 1) return -1;
+  Factor* F = (Factor*) L;
+  if (F->sp_fmt != fmt) drop_graphs(F);
+  F->sp_fmt = fmt;
+  return 0;
+}
+
+extern "C" int taucs_b200_set_refinement(void* L, int method) {
+  if (!L || method < 0 || method > 1) return -1;
+  ((Factor*) L)->refine_method = method;
   return 0;
 }
 
