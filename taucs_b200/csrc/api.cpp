@@ -38,12 +38,14 @@ static bool dev_upload(T** dst, const T* src, size_t n, cudaStream_t st) {
 }
 
 int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
-  std::vector<int> small, big;
+  std::vector<int> small, big, small_num;
   std::vector<Tile> tiles;
   std::vector<int2_> sf, sb, sl;
   D->small_off.clear(); D->big_off.clear(); D->tile_off.clear(); D->sfwd_off.clear(); D->sbwd_off.clear();
-  D->sl21_off.clear();
+  D->sl21_off.clear(); D->small_num_off.clear();
   for (const LevelPlan& LP : P.levels) {
+    D->small_num_off.push_back((int) small_num.size());
+    small_num.insert(small_num.end(), LP.small_numeric.begin(), LP.small_numeric.end());
     D->small_off.push_back((int) small.size());
     D->big_off.push_back((int) big.size());
     D->tile_off.push_back((int) tiles.size());
@@ -62,7 +64,13 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
     if (P.fronts[i].dinv_off >= 0)
       for (int b = 0; b * PANEL_NB < P.fronts[i].s; b++) dblk.push_back(int2_{i, b});
   D->n_dblk = (int) dblk.size();
+  D->n_pers = (int) P.pers_fronts.size();
   bool ok = dev_upload(&D->fronts, P.fronts.data(), P.fronts.size(), st)
+         && dev_upload(&D->small_num, small_num.data(), small_num.size(), st)
+         && dev_upload(&D->pers_list, P.pers_fronts.data(), P.pers_fronts.size(), st)
+         && dev_upload(&D->pers_parent, P.pers_parent.data(), P.pers_parent.size(), st)
+         && dev_upload(&D->pers_pending0, P.pers_pending.data(), P.pers_pending.size(), st)
+         && dev_upload(&D->pers_work, (const int*) nullptr, P.pers_fronts.size() + 1, st)
          && dev_upload(&D->dblk, dblk.data(), dblk.size(), st)
          && dev_upload(&D->children, P.children.data(), P.children.size(), st)
          && dev_upload(&D->rows, P.rows.data(), P.rows.size(), st)
@@ -85,6 +93,8 @@ void devplan_free(DevPlan* D) {
   tb::dfree(D->acol_ptr); tb::dfree(D->a_rows); tb::dfree(D->a_idx);
   tb::dfree(D->small_list); tb::dfree(D->big_list); tb::dfree(D->tiles);
   tb::dfree(D->sfwd); tb::dfree(D->sbwd); tb::dfree(D->sl21); tb::dfree(D->dblk);
+  tb::dfree(D->small_num); tb::dfree(D->pers_list); tb::dfree(D->pers_parent); tb::dfree(D->pers_pending0);
+  tb::dfree(D->pers_work);
   *D = DevPlan();
 }
 

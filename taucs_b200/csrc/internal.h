@@ -115,6 +115,10 @@ struct LevelPlan {
   // small fronts, fused kernel (sorted by order f); the first small_warp of
   // them are small enough for the one-warp-per-front solve kernels
   std::vector<int> small_fronts;
+  // the small fronts that the level launches of the numeric factorization
+  // take (those with a big front below them); the others are factored by
+  // the persistent launch (Plan::pers_fronts).  Sorted by order f.
+  std::vector<int> small_numeric;
   int small_warp = 0;
   // medium/large fronts
   std::vector<int> big_fronts;
@@ -134,6 +138,13 @@ struct Plan {
   int n_blk = 0;                   // solve flags
   int64_t part_len = 0;            // doubles of backward partial sums
   int64_t sp_len = 0;              // floats of the split arena (the largest level's split copies)
+  // small fronts whose whole subtree is small, in device (level) order: one
+  // persistent launch factors them all, taking them from a device-side queue
+  // in this order, each once its children are done.  pers_parent: the task
+  // index of the front's parent when that parent is in the list too, else -1;
+  // pers_pending: the front's number of children (all of them in the list).
+  std::vector<int> pers_fronts, pers_parent, pers_pending;
+  int pers_fmax = 0;               // largest order f among them
   int64_t nnz = 0;
   std::vector<FrontDesc> fronts;
   std::vector<int> children;       // device-order child indices

@@ -71,7 +71,13 @@ struct DevPlan {
   int2_* sl21 = nullptr;
   int2_* dblk = nullptr;       // (front, 64-column block) of every big front's diagonal blocks
   int n_dblk = 0;
-  std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off, sl21_off;  // per level (host)
+  int* small_num = nullptr;    // LevelPlan::small_numeric, all levels concatenated
+  int* pers_list = nullptr;    // Plan::pers_fronts, pers_parent, pers_pending
+  int* pers_parent = nullptr;
+  int* pers_pending0 = nullptr;
+  int* pers_work = nullptr;    // per factorization: pending counts (n_pers) + the queue head
+  int n_pers = 0;
+  std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off, sl21_off, small_num_off;  // per level (host)
   std::vector<int> lvl_max_f_small;               // per level (host)
 };
 

@@ -6,7 +6,9 @@
 // (:1131), TRSM (:1150) and SYRK (:1180).  Here every front of one level of
 // the supernodal tree is processed by the same launches:
 //
-//   k_small_front   fronts of order <= SMALL_F_MAX: one CTA builds the whole
+//   k_small_persistent  the small fronts with only small fronts below them,
+//                   all levels in one launch from a device-side queue;
+//   k_small_front   the other fronts of order <= SMALL_F_MAX: one CTA builds the whole
 //                   front in shared memory (zero + assemble + extend-add),
 //                   factors it (right-looking partial Cholesky of the first s
 //                   columns, i.e. POTRF+TRSM+SYRK fused) and writes the panel
@@ -50,18 +52,18 @@ __global__ void k_init_status(int* status) { *status = INT_MAX; }
 
 // ------------------------------------------------------------ small fronts
 
+// One small front by one CTA (128 threads) in shared memory W (f x f): zero,
+// assemble A's columns, extend-add the children's update matrices in child
+// order, partial Cholesky of the first s columns, then write the panel and
+// the update matrix.  Every thread returns together; on a nonpositive pivot
+// the front's global column is recorded and it returns early.
 template <typename T>
-__global__ void __launch_bounds__(128)
-k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
-              const int* __restrict__ children, const int* __restrict__ maps,
-              const int* __restrict__ rows, const int* __restrict__ acol_ptr,
-              const int* __restrict__ a_rows, const int* __restrict__ a_idx,
-              const T* __restrict__ vals, T* __restrict__ L, T* __restrict__ U,
-              int* status) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* W = reinterpret_cast<T*>(smraw);
-  if (failed(status)) return;
-  const FrontDesc F = fronts[list[blockIdx.x]];
+__device__ void small_front(const FrontDesc& F, const FrontDesc* __restrict__ fronts, T* W,
+                            const int* __restrict__ children,
+                            const int* __restrict__ maps, const int* __restrict__ rows,
+                            const int* __restrict__ acol_ptr, const int* __restrict__ a_rows,
+                            const int* __restrict__ a_idx, const T* __restrict__ vals, T* __restrict__ L,
+                            T* __restrict__ U, int* status) {
   const int f = F.f, s = F.s, m = f - s;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
 
@@ -109,6 +111,73 @@ k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts
     for (int k = tid; k < m * m; k += nt) {
       const int i = k % m, c = k / m;
       Up[k] = W[(s + i) + (s + c) * f];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_small_front(const int* __restrict__ list, const FrontDesc* __restrict__ fronts,
+              const int* __restrict__ children, const int* __restrict__ maps,
+              const int* __restrict__ rows, const int* __restrict__ acol_ptr,
+              const int* __restrict__ a_rows, const int* __restrict__ a_idx,
+              const T* __restrict__ vals, T* __restrict__ L, T* __restrict__ U,
+              int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  if (failed(status)) return;
+  small_front<T>(fronts[list[blockIdx.x]], fronts, reinterpret_cast<T*>(smraw), children, maps, rows, acol_ptr, a_rows,
+                 a_idx, vals, L, U, status);
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The small fronts whose whole subtree is small (Plan::pers_fronts), in one
+// launch of resident CTAs: each CTA takes the next front from a device-side
+// queue (an atomic counter over the fronts in level order), waits until the
+// front's children are done (its pending count, decremented by each child's
+// CTA after its update matrix is written), factors it, and marks it done
+// for its parent.  A front is only taken after all fronts before it in level
+// order were taken by running CTAs, so every wait ends; the waits are bounded
+// all the same (NUMERIC_TIMEOUT).  After a nonpositive pivot anywhere the
+// remaining fronts are only marked done.
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_small_persistent(const int* __restrict__ tasks, int ntask, const int* __restrict__ parent_task, int* pending,
+                   int* next, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+                   const int* __restrict__ maps, const int* __restrict__ rows, const int* __restrict__ acol_ptr,
+                   const int* __restrict__ a_rows, const int* __restrict__ a_idx, const T* __restrict__ vals,
+                   T* __restrict__ L, T* __restrict__ U, int* status) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ int t_s, skip_s;
+  T* W = reinterpret_cast<T*>(smraw);
+  for (;;) {
+    if (threadIdx.x == 0) t_s = atomicAdd(next, 1);
+    __syncthreads();
+    const int t = t_s;
+    if (t >= ntask) break;
+    if (threadIdx.x == 0) {
+      int it = 0;
+      while (ld_acquire_gpu(pending + t) != 0) {
+        if (++it > (1 << 22)) {
+          atomicMin(status, NUMERIC_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+      skip_s = failed(status);
+    }
+    __syncthreads();
+    if (!skip_s)
+      small_front<T>(fronts[tasks[t]], fronts, W, children, maps, rows, acol_ptr, a_rows, a_idx, vals, L, U, status);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const int pt = parent_task[t];
+      if (pt >= 0) atomicSub(pending + pt, 1);
     }
   }
 }
@@ -794,12 +863,37 @@ static void launch_gemm(bool alt, int gx128, int gx64, int nb, const int* blst, 
   launch_gemm<float>(false, gx128, gx64, nb, blst, D, L, U, c_lo, c_hi, k_lo, k_hi, mode, status, st);
 }
 
+// CTAs of the persistent small-front launch: all that fit on the device at
+// once with `smem` bytes each (computed once per device and type, at the
+// largest shared-memory size)
+template <typename T>
+static int pers_grid(size_t smem) {
+  static PerDeviceOnce pd;
+  static int per_sm[MAX_DEVICES], sms[MAX_DEVICES];
+  per_device_once(pd, [] {
+    int d = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&sms[d], cudaDevAttrMultiProcessorCount, d);
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_small_persistent<T>, 128,
+                                                  (size_t) SMALL_F_MAX * SMALL_F_MAX * sizeof(T));
+    per_sm[d] = std::max(b, 1);
+    return true;
+  });
+  int d = 0;
+  cudaGetDevice(&d);
+  (void) smem;
+  return std::max(1, per_sm[d] * sms[d]);
+}
+
 template <typename T>
 static void set_smem_attrs() {
   // once per device and type (request-server workers reach this concurrently)
   static PerDeviceOnce pd;
   per_device_once(pd, [] {
     cudaFuncSetAttribute(k_small_front<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
+    cudaFuncSetAttribute(k_small_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
     cudaFuncSetAttribute(k_leaf<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) leaf_smem<T>());
     cudaFuncSetAttribute(k_dinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dinv_smem<T>());
@@ -817,24 +911,44 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
   set_smem_attrs<T>();
   k_init_status<<<1, 1, 0, st>>>(status);
   count_launch();
+  if (D.n_pers > 0) {
+    // every small front with only small fronts below it, in one launch
+    cudaMemcpyAsync(D.pers_work, D.pers_pending0, sizeof(int) * D.n_pers, cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(D.pers_work + D.n_pers, 0, sizeof(int), st);
+    const size_t smem = (size_t) P.pers_fmax * P.pers_fmax * sizeof(T);
+    const int grid = std::min(D.n_pers, pers_grid<T>(smem));
+    double fl = 0.0, by = 0.0;
+    if (prof_enabled())
+      for (int i : P.pers_fronts) {
+        fl += front_flops(P.fronts[i]);
+        by += front_bytes(P, P.fronts[i], sizeof(T));
+      }
+    prof_begin(KC_SMALL, st);
+    k_small_persistent<T><<<grid, 128, smem, st>>>(D.pers_list, D.n_pers, D.pers_parent, D.pers_work,
+                                                   D.pers_work + D.n_pers, D.fronts, D.children, D.maps, D.rows,
+                                                   D.acol_ptr, D.a_rows, D.a_idx, vals, L, U, status);
+    prof_end(KC_SMALL, st, fl, by);
+    count_launch();
+  }
   for (int h = 0; h < P.n_levels; h++) {
     const LevelPlan& LP = P.levels[h];
     prof_tag(h);
-    // small fronts, in size classes so that the shared-memory request fits the class
-    const int ns = (int) LP.small_fronts.size();
+    // small fronts above a big one (the rest went through the persistent
+    // launch), in size classes so that the shared-memory request fits the class
+    const int ns = (int) LP.small_numeric.size();
     if (ns > 0) {
-      const int* lst = D.small_list + D.small_off[h];
+      const int* lst = D.small_num + D.small_num_off[h];
       int b = 0;
       const int classes[3] = {32, 64, SMALL_F_MAX};
       for (int cl = 0; cl < 3 && b < ns; cl++) {
         int e = b;
-        while (e < ns && P.fronts[LP.small_fronts[e]].f <= classes[cl]) e++;
+        while (e < ns && P.fronts[LP.small_numeric[e]].f <= classes[cl]) e++;
         if (e > b) {
           const size_t smem = (size_t) classes[cl] * classes[cl] * sizeof(T);
           double fl = 0.0, by = 0.0;
           if (prof_enabled())
             for (int q = b; q < e; q++) {
-              const FrontDesc& F = P.fronts[LP.small_fronts[q]];
+              const FrontDesc& F = P.fronts[LP.small_numeric[q]];
               fl += front_flops(F);
               by += front_bytes(P, F, sizeof(T));
             }

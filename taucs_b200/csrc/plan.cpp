@@ -411,6 +411,30 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
     }
   }
 
+  // the persistent set: small fronts with only small fronts below them
+  // (children come before parents in device order)
+  {
+    std::vector<int> task(nf, -1);
+    for (int i = 0; i < nf; i++) {
+      const FrontDesc& F = P.fronts[i];
+      bool pure = F.f <= SMALL_F_MAX;
+      for (int ci = F.child_begin; pure && ci < F.child_end; ci++) pure = task[P.children[ci]] >= 0;
+      if (!pure) continue;
+      task[i] = (int) P.pers_fronts.size();
+      P.pers_fronts.push_back(i);
+      P.pers_pending.push_back(F.child_end - F.child_begin);
+      P.pers_fmax = std::max(P.pers_fmax, F.f);
+    }
+    P.pers_parent.assign(P.pers_fronts.size(), -1);
+    for (size_t t = 0; t < P.pers_fronts.size(); t++) {
+      const int par = P.fronts[P.pers_fronts[t]].parent;
+      if (par >= 0) P.pers_parent[t] = task[par];
+    }
+    for (LevelPlan& LP : P.levels)
+      for (int i : LP.small_fronts)
+        if (task[i] < 0) LP.small_numeric.push_back(i);
+  }
+
   // statistics: the reference's relaxed flop count (src/taucs_sn_llt.c:3957-3965)
   double flops = 0.0, ea = 0.0, sb = 0.0;
   for (int i = 0; i < nf; i++) {
