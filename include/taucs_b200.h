@@ -361,11 +361,24 @@ long taucs_b200_profile_log(int* kernel_class, float* ms, long cap);
  * Returns 0, or -1 when a factorization failed. */
 int taucs_b200_autotune(void* L, const double* d_values, int* choices);
 
+/* The autotuner's measurements also go into a process-wide table keyed by
+ * precision, product and the shape class of each level's largest product
+ * (rows and K in powers of two); every handle analysed afterwards (including
+ * the request server's and batches) takes its per-level variants from the
+ * table.  The table can be saved to and loaded from a text file, so a tuning
+ * run carries over to later processes; load returns the entries read. */
+int  taucs_b200_tuning_save(const char* path);
+int  taucs_b200_tuning_load(const char* path);
+int  taucs_b200_tuning_entries(void);
+void taucs_b200_tuning_clear(void);
+
 /* Sets the GEMM variant per level and product for `precision` (0 FP64
  * fronts, 1 FP32 fronts) -- e.g. choices an earlier taucs_b200_autotune
  * returned for the same pattern, kept by the caller.  count = 2 x levels
  * (layout as in taucs_b200_autotune), or 0 for the default variants. */
 int taucs_b200_set_gemm_choices(void* L, int precision, int count, const int* choices);
+/* the current variants (2 x levels values) */
+int taucs_b200_get_gemm_choices(void* L, int precision, int* choices);
 
 /* Device-memory allocation tracking, after the reference's host allocation
  * tracking (src/taucs_malloc.c:127-250).  Every device and pinned-host

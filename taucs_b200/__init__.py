@@ -143,6 +143,11 @@ def lib():
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),
         "taucs_b200_autotune": (C.c_int, [vp, vp, _i32p]),
         "taucs_b200_set_gemm_choices": (C.c_int, [vp, C.c_int, C.c_int, _i32p]),
+        "taucs_b200_get_gemm_choices": (C.c_int, [vp, C.c_int, _i32p]),
+        "taucs_b200_tuning_save": (C.c_int, [C.c_char_p]),
+        "taucs_b200_tuning_load": (C.c_int, [C.c_char_p]),
+        "taucs_b200_tuning_entries": (C.c_int, []),
+        "taucs_b200_tuning_clear": (None, []),
         "taucs_b200_solve_device_noalloc_status": (C.c_int, []),
         "taucs_b200_debug_waits": (C.c_int, [C.c_int, C.c_int]),
         "taucs_b200_allocation_induce_failure": (None, [C.c_int]),
@@ -392,6 +397,11 @@ class Factor:
 
     def set_precision(self, p):
         return lib().taucs_b200_set_precision(self.h, p)
+
+    def gemm_choices(self, precision):
+        ch = np.zeros(2 * max(self.info().n_levels, 1), np.int32)
+        lib().taucs_b200_get_gemm_choices(self.h, precision, ch)
+        return ch
 
     def set_gemm_choices(self, precision, choices):
         """GEMM variant per level and product (taucs_b200_set_gemm_choices);

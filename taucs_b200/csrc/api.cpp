@@ -265,6 +265,9 @@ Factor* symbolic(taucs_ccs_matrix* A, int max_depth) {
   if (rc != TAUCS_SUCCESS) { delete F; return nullptr; }
   rc = build_plan(F->sym, A->n, A->colptr, A->rowind, &F->plan);
   if (rc != TAUCS_SUCCESS) { delete F; return nullptr; }
+  // GEMM variants measured on earlier factors of similar shape
+  tune_apply(&F->plan, 0);
+  tune_apply(&F->plan, 1);
   F->colptr.assign(A->colptr, A->colptr + A->n + 1);
   F->rowind.assign(A->rowind, A->rowind + A->colptr[A->n]);
   tprintf("\t\tSymbolic Analysis            = % 10.3f seconds\n", taucs_wtime() - wt);
@@ -510,6 +513,7 @@ int taucs_b200_autotune(void* L, const double* d_values, int* choices) {
       }
     }
   }
+  tune_record(F->plan, pi, t);
   std::vector<uint8_t>& c = F->plan.gemm_choice[pi];
   double before = 0.0, after = 0.0;
   for (int i = 0; i < 2 * H; i++) {
@@ -521,6 +525,14 @@ int taucs_b200_autotune(void* L, const double* d_values, int* choices) {
   drop_graphs(F);
   tprintf("\t\tautotune (%s fronts): GEMM time %.2f ms with the default variants, %.2f ms with the chosen ones\n",
           pi ? "FP32" : "FP64", before, after);
+  return 0;
+}
+
+int taucs_b200_get_gemm_choices(void* L, int precision, int* choices) {
+  Factor* F = (Factor*) L;
+  if (!F || (precision != 0 && precision != 1) || !choices) return -1;
+  const std::vector<uint8_t>& c = F->plan.gemm_choice[precision];
+  for (int i = 0; i < 2 * F->plan.n_levels; i++) choices[i] = (size_t) i < c.size() ? c[i] : 0;
   return 0;
 }
 

@@ -146,6 +146,8 @@ extern "C" void* taucs_b200_batch_analyze(int count, taucs_ccs_matrix* const* A)
     set_error("batch_analyze: plan construction failed");
     return nullptr;
   }
+  tune_apply(&F->plan, 0);
+  tune_apply(&F->plan, 1);
   F->colptr = std::move(colptr);
   F->rowind = std::move(rowind);
   F->seg_ptr = std::move(seg_ptr);

@@ -148,6 +148,11 @@ inline cudaError_t dmalloc(T** p, size_t bytes) { return dmalloc_raw((void**) p,
 template <typename T>
 inline cudaError_t hmalloc(T** p, size_t bytes) { return hmalloc_raw((void**) p, bytes); }
 
+// GEMM tuning table (tune.cpp): record one factor's per-level times of both
+// variants (t[v][2h + kind], ms), and fill a plan's choices from the table
+void tune_record(const Plan& P, int prec, const std::vector<double> (&t)[2]);
+bool tune_apply(Plan* P, int prec);
+
 // launch accounting
 void count_launch(long k = 1);
 
