@@ -73,6 +73,10 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="duration of the Poisson request stream at 2000 req/s (the configuration's 60 s)")
+    ap.add_argument("--split-format", type=int, default=0, choices=[0, 1],
+                    help="operand format of the FP32 fronts' tensor-core products: 0 TF32x3, 1 FP16x3")
+    ap.add_argument("--refinement", type=int, default=0, choices=[0, 1],
+                    help="0 refinement steps (PCG on stall), 1 PCG on the FP32 factor from the first step")
     ap.add_argument("--no-extra-legs", action="store_true",
                     help="skip the fp64-64 and batch4096 legs that the default run reports beside its line")
     return ap.parse_args()
@@ -866,6 +870,8 @@ def run_ours(args):
     # ---- setup (untimed): generator, AMD, permutation, symbolic analysis
     A, perm, iperm, P, B = make_system(args.workload, g)
     F = tb.factor_symbolic(P)
+    tb.lib().taucs_b200_set_split_format(F.h, args.split_format)
+    tb.lib().taucs_b200_set_refinement(F.h, args.refinement)
     info = F.info()
     n, nnz, nrhs = A.n, P.nnz, B.shape[1]
     Bf = np.asfortranarray(B)

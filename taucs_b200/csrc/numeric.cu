@@ -264,14 +264,18 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
 // min(64, s - kb), factored and applied to every row below them in ONE
 // launch (the reference's POTRF :1131 and TRSM :1150 on a 64-column piece).
 // CTA x of front y owns the 64 rows [kb + w + 64 x, ...) below the diagonal
-// block; CTA 0 also writes the factored diagonal block.  Every CTA factors
+// block.  Every CTA of the launch reads the diagonal block as it was before
+// the step, so CTA 0 parks the factored block in the block's slot of the
+// inverse array rather than in the panel; k_dinv moves it into the panel
+// after the factorization and replaces it there by its inverse.  Every CTA factors
 // the 64x64 diagonal block itself -- a redundant Cholesky instead of waiting
 // for the CTA that owns it -- in four 16-column steps: one warp factors the
 // 16x16 diagonal piece and inverts it in registers, then all warps apply it
 // to the rows below, in the diagonal block and in the CTA's own slab (one row
 // per thread), and update the columns to the right.  The inverses of the
 // 64x64 diagonal blocks, which the solve applies, are formed afterwards for
-// all fronts at once (k_dinv).
+// all fronts at once (k_dinv).  Nothing reads a diagonal block of the panel
+// between its leaf and k_dinv: the later products read rows below it only.
 constexpr int LLD = PANEL_NB + 4;   // padded column stride of the leaf's blocks in shared memory
 constexpr int LQ = 16;              // column step inside a leaf
 constexpr int LYD = LQ + 1;         // column stride of a 16x16 inverse
@@ -338,7 +342,7 @@ __device__ int warp_chol_inv16(T* S, T* Y) {
 template <typename T>
 __global__ void __launch_bounds__(128)
 k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
-       T* __restrict__ L, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
+       T* __restrict__ L, T* __restrict__ Dinv, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* D = reinterpret_cast<T*>(smraw);   // diagonal block, 64 x 64, ld LLD
   T* A = D + PANEL_NB * LLD;            // this CTA's slab of rows below it, 64 x 64, ld LLD
@@ -413,11 +417,13 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
     }
     __syncthreads();
   }
-  if (blockIdx.x == 0)
+  if (blockIdx.x == 0) {
+    T* Dk = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
     for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
       const int i = e % PANEL_NB, j = e / PANEL_NB;
-      if (i >= j && i < w) P[(kb + i) + (size_t) (kb + j) * f] = D[i + j * LLD];
+      Dk[e] = (i >= j && i < w) ? D[i + j * LLD] : T(0);
     }
+  }
   for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
     const int i = e % PANEL_NB, j = e / PANEL_NB;
     if (i < nr && j < w) P[(r0 + i) + (size_t) (kb + j) * f] = A[i + j * LLD];
@@ -467,13 +473,15 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
   }
 }
 
-// Inverses of the 64x64 diagonal blocks of every big front's factored panel
-// (L_kk^-1, lower, zero beyond the block's width), which the solve applies;
-// one CTA per block.  Warp q inverts the 16x16 diagonal piece q; then warp b
-// forms block column b below the diagonal, X_cb = -X_cc sum_{b<=k<c} L_ck X_kb.
+// After the factorization, one CTA per 64x64 diagonal block of every big
+// front: the factored block L_kk that its leaf parked in the block's slot of
+// Dinv goes into the panel, and the slot receives L_kk^-1 (lower, zero
+// beyond the block's width), which the solve applies.  Warp q inverts the
+// 16x16 diagonal piece q; then warp b forms block column b below the
+// diagonal, X_cb = -X_cc sum_{b<=k<c} L_ck X_kb.
 template <typename T>
 __global__ void __launch_bounds__(128)
-k_dinv(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts, const T* __restrict__ L,
+k_dinv(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts, T* __restrict__ L,
        T* __restrict__ Dinv, const int* status) {
   extern __shared__ __align__(16) unsigned char smraw[];
   T* S = reinterpret_cast<T*>(smraw);   // L_kk, 64 x 64, ld LLD (identity beyond w)
@@ -484,12 +492,15 @@ k_dinv(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts, c
   const FrontDesc F = fronts[bl.a];
   const int f = F.f, kb = bl.b * PANEL_NB;
   const int w = min(PANEL_NB, F.s - kb);
-  const T* P = L + F.l_off;
+  T* P = L + F.l_off;
+  T* Di = Dinv + F.dinv_off + (size_t) bl.b * PANEL_NB * PANEL_NB;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
     const int i = e % PANEL_NB, j = e / PANEL_NB;
-    S[i + j * LLD] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
+    const T v = (i < w && j < w && i >= j) ? Di[e] : (i == j ? T(1) : T(0));
+    S[i + j * LLD] = v;
     X[i + j * LLD] = T(0);
+    if (i < w && j < w && i >= j) P[(kb + i) + (size_t) (kb + j) * f] = v;
   }
   __syncthreads();
   {
@@ -538,7 +549,6 @@ k_dinv(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts, c
     }
   }
   __syncthreads();
-  T* Di = Dinv + F.dinv_off + (size_t) bl.b * PANEL_NB * PANEL_NB;
   for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
     const int i = e % PANEL_NB, j = e / PANEL_NB;
     Di[e] = (i < w && j < w) ? X[i + j * LLD] : T(0);
@@ -997,7 +1007,8 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
         }
       }
       prof_begin(KC_POTRF, st);
-      k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, sp, sp_fmt, kb, status);
+      k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, Dinv, sp, sp_fmt, kb,
+                                                           status);
       prof_end(KC_POTRF, st, fl, by);
       count_launch();
     };

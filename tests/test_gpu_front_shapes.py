@@ -11,10 +11,12 @@ front of order m + g.  Every front has order > 96, so the tiled path runs
 
 * FP64 fronts (DMMA GEMM, both tile shapes): L within 1e-10 relative
   Frobenius of the reference (src/taucs_sn_llt.c:1084-1194).
-* FP32 fronts (tcgen05 TF32x3 GEMM, both pipeline shapes): the FP32 factor
-  of the scaled matrix D A D (D = diag(A)^-1/2) within 2e-5 relative
-  Frobenius of the reference's FP64 factor of the same scaled matrix, per
-  supernode (FP32 rounding is ~1e-7; a tile or mask error is O(1)).
+* FP32 fronts (the tcgen05 GEMMs: split-fed TF32x3 and FP16x3, and the
+  producer-split one): the FP32 factor of the scaled matrix D A D
+  (D = diag(A)^-1/2) within 1e-4 relative Frobenius of the reference's FP64
+  factor of the same scaled matrix, per supernode (an FP32 Cholesky of a
+  supernode of s columns is accurate to about s * 2^-24, 3e-5 at s = 513; a
+  tile or mask error is O(1)).
 """
 import numpy as np
 import pytest
@@ -115,13 +117,14 @@ def test_fp64_fronts_match_reference(tb, ref, shape, variant):
 
 @pytest.mark.parametrize("shape", SHAPES, ids=[f"{a}_{b}_{c}" for a, b, c in SHAPES])
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", ["split_tf32", "split_fp16", "producer_split"])
 def test_fp32_fronts_match_reference_scaled(tb, ref, shape, variant):
     A = blocks_and_separator(tb, *shape, seed=sum(shape))
     n, cp, ri, va = A.arrays()
     F = tb.factor_symbolic(A)
     F.set_precision(1)
-    F.set_gemm_choices(1, [variant] * (2 * F.info().n_levels))
+    tb.lib().taucs_b200_set_split_format(F.h, 1 if variant == "split_fp16" else 0)
+    F.set_gemm_choices(1, [1 if variant == "producer_split" else 0] * (2 * F.info().n_levels))
     assert F.numeric(A) == 0, tb.last_error()
     Lr = ref.factor_mf(n, cp, ri, _scaled(A))
     sym = ref.dump_symbolic(Lr)
@@ -129,6 +132,6 @@ def test_fp32_fronts_match_reference_scaled(tb, ref, shape, variant):
     vp_g, v_g = F.export_values()
     assert np.array_equal(vp_r, vp_g)
     err = _per_supernode_err(sym, vp_r, v_g, v_r)
-    assert err <= 2e-5, (shape, _fronts(F), err)
+    assert err <= 1e-4, (shape, _fronts(F), err)
     ref.free(Lr)
     F.free()
