@@ -226,16 +226,47 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
     moff += m;
   }
 
-  // update arena: lifetime [level(front), level(parent)]
+  // small fronts with only small fronts below them (children come before
+  // parents in device order): one persistent launch factors all of them
+  // before the level launches (numeric.cu)
+  std::vector<char> pure(nf, 0);
+  for (int i = 0; i < nf; i++) {
+    const FrontDesc& F = P.fronts[i];
+    bool ok = F.f <= SMALL_F_MAX;
+    for (int ci = F.child_begin; ok && ci < F.child_end; ci++) ok = pure[P.children[ci]];
+    pure[i] = ok;
+  }
+
+  // update arena.  The persistent launch runs the small fronts of all levels
+  // in no fixed order among unrelated subtrees, so their update matrices get
+  // slots of their own, live from the start: released at its end when the
+  // consumer is in the persistent set too, else at the consumer's level.
+  // The other fronts' update matrices live over [level(front), level(parent)].
   {
     ArenaPlanner ap;
     std::vector<std::vector<int>> free_at(H + 1);
+    std::vector<int> free_now;
+    for (int i = 0; i < nf; i++) {
+      FrontDesc& F = P.fronts[i];
+      const int64_t m = F.f - F.s;
+      if (!pure[i]) continue;
+      F.u_off = -1;
+      if (m <= 0) continue;
+      F.u_off = ap.alloc(m * m);
+      if (pure[F.parent]) free_now.push_back(i);
+      else free_at[P.fronts[F.parent].level].push_back(i);
+    }
+    for (int i : free_now) {
+      const int64_t m = P.fronts[i].f - P.fronts[i].s;
+      ap.release(P.fronts[i].u_off, m * m);
+    }
     int fi = 0;
     for (int h = 0; h < H; h++) {
       int fe = fi;
       while (fe < nf && P.fronts[fe].level == h) fe++;
       for (int i = fi; i < fe; i++) {
         FrontDesc& F = P.fronts[i];
+        if (pure[i]) continue;
         const int64_t m = F.f - F.s;
         if (m > 0) {
           F.u_off = ap.alloc(m * m);
@@ -411,15 +442,12 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
     }
   }
 
-  // the persistent set: small fronts with only small fronts below them
-  // (children come before parents in device order)
+  // the persistent set, in device (level) order
   {
     std::vector<int> task(nf, -1);
     for (int i = 0; i < nf; i++) {
       const FrontDesc& F = P.fronts[i];
-      bool pure = F.f <= SMALL_F_MAX;
-      for (int ci = F.child_begin; pure && ci < F.child_end; ci++) pure = task[P.children[ci]] >= 0;
-      if (!pure) continue;
+      if (!pure[i]) continue;
       task[i] = (int) P.pers_fronts.size();
       P.pers_fronts.push_back(i);
       P.pers_pending.push_back(F.child_end - F.child_begin);

@@ -1,9 +1,13 @@
 """Device layout of the level plan (plan.cpp), checked on the host for every
 front: L panels, solve work vectors, diagonal-block inverses and handshake
 flags never overlap and stay inside their arenas; update matrices that are
-live at the same time (from their front's level through their parent's
-level, where the parent's front build reads them) never overlap; backward
-partial sums of one level never overlap.  An overlap would corrupt a
+live at the same time never overlap; backward partial sums of one level
+never overlap.  Lifetimes of update matrices: the small fronts with only
+small fronts below them are factored by one persistent launch before the
+level launches, in no fixed order among unrelated subtrees, so their update
+matrices are live from that launch until it ends (consumer in the same set)
+or until the consumer's level; every other update matrix is live from its
+front's level through its parent's level.  An overlap would corrupt a
 factorization or a solve only for some inputs, so the plan is checked
 directly.  Host code only."""
 import numpy as np
@@ -44,9 +48,18 @@ def check_layout(F):
     assert np.all(parent[m > 0] >= 0), "a front with update rows has a parent"
     plev = np.where(parent >= 0, level[np.maximum(parent, 0)], level)
     assert np.all(plev[hu] > level[hu])
+    # the persistent set: f <= 96 and every child in it (children have lower levels)
+    pure = f <= 96
+    for i in np.argsort(level, kind="stable"):
+        if parent[i] >= 0 and not pure[i]:
+            pure[parent[i]] = False
+    # live intervals on the time axis -1 (the persistent launch), 0, 1, ...
+    start = np.where(pure, -1, level)
+    end = np.where(pure & pure[np.maximum(parent, 0)] & (parent >= 0), -1, plev)
+    for t in range(-1, int(level.max()) + 1):
+        live = hu & (start <= t) & (end >= t)
+        _disjoint("update matrices at time %d" % t, u_off[live], m[live] ** 2, tot[1])
     for L in range(int(level.max()) + 1):
-        live = hu & (level <= L) & (plev >= L)
-        _disjoint("update matrices at level %d" % L, u_off[live], m[live] ** 2, tot[1])
         sel = (part_off >= 0) & (level == L)
         _disjoint("partial sums at level %d" % L, part_off[sel], nchunk[sel] * s[sel] * SOLVE_NRHS, tot[4])
     return fr, tot
