@@ -71,6 +71,7 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
          && dev_upload(&D->pers_parent, P.pers_parent.data(), P.pers_parent.size(), st)
          && dev_upload(&D->pers_pending0, P.pers_pending.data(), P.pers_pending.size(), st)
          && dev_upload(&D->pers_work, (const int*) nullptr, P.pers_fronts.size() + 1, st)
+         && dev_upload(&D->pers_solve, (const int*) nullptr, 2 * P.pers_fronts.size() + 2, st)
          && dev_upload(&D->dblk, dblk.data(), dblk.size(), st)
          && dev_upload(&D->children, P.children.data(), P.children.size(), st)
          && dev_upload(&D->rows, P.rows.data(), P.rows.size(), st)
@@ -94,7 +95,7 @@ void devplan_free(DevPlan* D) {
   tb::dfree(D->small_list); tb::dfree(D->big_list); tb::dfree(D->tiles);
   tb::dfree(D->sfwd); tb::dfree(D->sbwd); tb::dfree(D->sl21); tb::dfree(D->dblk);
   tb::dfree(D->small_num); tb::dfree(D->pers_list); tb::dfree(D->pers_parent); tb::dfree(D->pers_pending0);
-  tb::dfree(D->pers_work);
+  tb::dfree(D->pers_work); tb::dfree(D->pers_solve);
   *D = DevPlan();
 }
 

@@ -119,6 +119,7 @@ struct LevelPlan {
   // take (those with a big front below them); the others are factored by
   // the persistent launch (Plan::pers_fronts).  Sorted by order f.
   std::vector<int> small_numeric;
+  int small_numeric_warp = 0;      // the first ones small enough for the one-warp solve kernels
   int small_warp = 0;
   // medium/large fronts
   std::vector<int> big_fronts;

@@ -76,6 +76,7 @@ struct DevPlan {
   int* pers_parent = nullptr;
   int* pers_pending0 = nullptr;
   int* pers_work = nullptr;    // per factorization: pending counts (n_pers) + the queue head
+  int* pers_solve = nullptr;   // per solve: pending counts and done flags (n_pers each) + two queue heads
   int n_pers = 0;
   std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off, sl21_off, small_num_off;  // per level (host)
   std::vector<int> lvl_max_f_small;               // per level (host)

@@ -458,9 +458,13 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
       const int par = P.fronts[P.pers_fronts[t]].parent;
       if (par >= 0) P.pers_parent[t] = task[par];
     }
-    for (LevelPlan& LP : P.levels)
+    for (LevelPlan& LP : P.levels) {
       for (int i : LP.small_fronts)
         if (task[i] < 0) LP.small_numeric.push_back(i);
+      while (LP.small_numeric_warp < (int) LP.small_numeric.size() &&
+             P.fronts[LP.small_numeric[LP.small_numeric_warp]].f <= SOLVE_WARP_F)
+        LP.small_numeric_warp++;
+    }
   }
 
   // statistics: the reference's relaxed flop count (src/taucs_sn_llt.c:3957-3965)

@@ -36,17 +36,13 @@ __device__ __forceinline__ void group_sync() {
   else __syncthreads();
 }
 
+// forward step of one small front by a group of G threads; xs: the group's
+// shared staging of one substitution block
 template <typename T, int WS, int G>
-__global__ void __launch_bounds__(256)
-k_fwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
-      const int* __restrict__ maps, const int* __restrict__ rows, const T* __restrict__ L,
-      const T* __restrict__ B, int ldb, T* __restrict__ W, int nrhs) {
-  constexpr int GPC = 256 / G;   // fronts per CTA: one per group of G threads
-  __shared__ T xs_all[GPC][SB][SOLVE_NRHS];
-  const int grp = threadIdx.x / G, li = blockIdx.x * GPC + grp;
-  if (li >= count) return;
-  T (&xs)[SB][SOLVE_NRHS] = xs_all[grp];
-  const FrontDesc F = fronts[list[li]];
+__device__ void fwd_small(const FrontDesc& F, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+                          const int* __restrict__ maps, const int* __restrict__ rows, const T* __restrict__ L,
+                          const T* __restrict__ B, int ldb, T* __restrict__ W, int nrhs,
+                          T (&xs)[SB][SOLVE_NRHS]) {
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x % G, nt = G, lane = tid & 31, warp = tid >> 5;
   T* Wf = W + F.v_off * WS;
@@ -119,15 +115,20 @@ k_fwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fro
 
 template <typename T, int WS, int G>
 __global__ void __launch_bounds__(256)
-k_bwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
-      const T* __restrict__ L, T* __restrict__ X, int ldx, T* __restrict__ W,
-      int nrhs) {
-  constexpr int GPC = 256 / G;
+k_fwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+      const int* __restrict__ maps, const int* __restrict__ rows, const T* __restrict__ L,
+      const T* __restrict__ B, int ldb, T* __restrict__ W, int nrhs) {
+  constexpr int GPC = 256 / G;   // fronts per CTA: one per group of G threads
   __shared__ T xs_all[GPC][SB][SOLVE_NRHS];
   const int grp = threadIdx.x / G, li = blockIdx.x * GPC + grp;
   if (li >= count) return;
-  T (&xs)[SB][SOLVE_NRHS] = xs_all[grp];
-  const FrontDesc F = fronts[list[li]];
+  fwd_small<T, WS, G>(fronts[list[li]], fronts, children, maps, rows, L, B, ldb, W, nrhs, xs_all[grp]);
+}
+
+// backward step of one small front by a group of G threads
+template <typename T, int WS, int G>
+__device__ void bwd_small(const FrontDesc& F, const int* __restrict__ rows, const T* __restrict__ L,
+                          T* __restrict__ X, int ldx, T* __restrict__ W, int nrhs, T (&xs)[SB][SOLVE_NRHS]) {
   const int f = F.f, s = F.s;
   const int tid = threadIdx.x % G, nt = G, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   T* Wf = W + F.v_off * WS;
@@ -229,6 +230,100 @@ k_bwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fro
   for (int k = tid; k < s * nrhs; k += nt) {
     const int r = k % s, q = k / s;
     X[rw[r] + (size_t) q * ldx] = Wf[r + q * f];
+  }
+}
+
+template <typename T, int WS, int G>
+__global__ void __launch_bounds__(256)
+k_bwd(const int* __restrict__ list, int count, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
+      const T* __restrict__ L, T* __restrict__ X, int ldx, T* __restrict__ W,
+      int nrhs) {
+  constexpr int GPC = 256 / G;
+  __shared__ T xs_all[GPC][SB][SOLVE_NRHS];
+  const int grp = threadIdx.x / G, li = blockIdx.x * GPC + grp;
+  if (li >= count) return;
+  bwd_small<T, WS, G>(fronts[list[li]], rows, L, X, ldx, W, nrhs, xs_all[grp]);
+}
+
+__device__ __forceinline__ int ld_acquire_i(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The small fronts with only small fronts below them (Plan::pers_fronts), in
+// one launch per direction; each warp takes the next front from a device-
+// side queue.  Forward, in level order: a front waits until its children's
+// update vectors are in place (pending count), and counts itself off at its
+// parent.  Backward, in reverse level order: a front waits until its parent
+// has written x at its update rows (done flag = epoch; parents outside the
+// set ran in the level launches before this one).  Every wait is bounded
+// (SOLVE_TIMEOUT).
+template <typename T, int WS>
+__global__ void __launch_bounds__(256)
+k_fwd_pers(const int* __restrict__ tasks, int ntask, const int* __restrict__ parent_task, int* pending, int* next,
+           const FrontDesc* __restrict__ fronts, const int* __restrict__ children, const int* __restrict__ maps,
+           const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ B, int ldb,
+           T* __restrict__ W, int nrhs, int* status) {
+  __shared__ T xs_all[8][SB][SOLVE_NRHS];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(next, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= ntask) break;
+    if (lane == 0) {
+      int it = 0;
+      while (ld_acquire_i(pending + t) != 0) {
+        if (++it > (1 << 22)) {
+          atomicExch(status, SOLVE_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __syncwarp();
+    fwd_small<T, WS, 32>(fronts[tasks[t]], fronts, children, maps, rows, L, B, ldb, W, nrhs, xs_all[wi]);
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      const int pt = parent_task[t];
+      if (pt >= 0) atomicSub(pending + pt, 1);
+    }
+  }
+}
+
+template <typename T, int WS>
+__global__ void __launch_bounds__(256)
+k_bwd_pers(const int* __restrict__ tasks, int ntask, const int* __restrict__ parent_task, int* done, int* next,
+           int epoch, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows, const T* __restrict__ L,
+           T* __restrict__ X, int ldx, T* __restrict__ W, int nrhs, int* status) {
+  __shared__ T xs_all[8][SB][SOLVE_NRHS];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(next, 1);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= ntask) break;
+    const int t = ntask - 1 - q;
+    const int pt = parent_task[t];
+    if (lane == 0 && pt >= 0) {
+      int it = 0;
+      while (ld_acquire_i(done + pt) != epoch) {
+        if (++it > (1 << 22)) {
+          atomicExch(status, SOLVE_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __syncwarp();
+    bwd_small<T, WS, 32>(fronts[tasks[t]], rows, L, X, ldx, W, nrhs, xs_all[wi]);
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      atomicExch(done + t, epoch);
+    }
   }
 }
 
@@ -845,6 +940,22 @@ static void solve_attrs() {
   });
 }
 
+// CTAs (eight warps each) of the persistent small-front solve launches: up
+// to four per SM, no more than the fronts need
+static int pers_solve_grid(int ntask) {
+  static PerDeviceOnce pd;
+  static int sms[MAX_DEVICES];
+  per_device_once(pd, [] {
+    int d = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&sms[d], cudaDevAttrMultiProcessorCount, d);
+    return true;
+  });
+  int d = 0;
+  cudaGetDevice(&d);
+  return std::max(1, std::min((ntask + 7) / 8, 4 * std::max(sms[d], 1)));
+}
+
 template <typename T>
 static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Dinv, int nrhs, T* X, const T* B, int ld, T* W,
                         T* part, int* flags, int* epoch, int* status, cudaStream_t st) {
@@ -852,22 +963,38 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
   // the handshake flags restart from zero on every call, so the epochs of a
   // call are always 1, 2, ... and a recorded launch sequence stays valid
   cudaMemsetAsync(flags, 0, sizeof(int) * (size_t) P.n_blk, st);
+  const int np = D.n_pers;
+  if (np > 0) cudaMemsetAsync(D.pers_solve, 0, sizeof(int) * (size_t) (2 * np + 2), st);
   int ep = 0;
   for (int q0 = 0; q0 < nrhs; q0 += SOLVE_NRHS) {
     const int nq = std::min(SOLVE_NRHS, nrhs - q0);
     const T* Bq = B + (size_t) q0 * ld;
     T* Xq = X + (size_t) q0 * ld;
     const int ef = ++ep;
+    if (np > 0) {
+      // every small front with only small fronts below it, one launch
+      cudaMemcpyAsync(D.pers_solve, D.pers_pending0, sizeof(int) * np, cudaMemcpyDeviceToDevice, st);
+      cudaMemsetAsync(D.pers_solve + 2 * np, 0, 2 * sizeof(int), st);
+      double by = 0.0;
+      if (prof_enabled())
+        for (int i : P.pers_fronts) by += solve_pass_bytes(P.fronts[i], nq, sizeof(T));
+      prof_begin(KC_SOLVE_FWD, st);
+      k_fwd_pers<T, SOLVE_NRHS><<<pers_solve_grid(np), 256, 0, st>>>(
+          D.pers_list, np, D.pers_parent, D.pers_solve, D.pers_solve + 2 * np, D.fronts, D.children, D.maps, D.rows,
+          L, Bq, ld, W, nq, status);
+      prof_end(KC_SOLVE_FWD, st, 0.0, by);
+      count_launch();
+    }
     for (int h = 0; h < P.n_levels; h++) {
       const LevelPlan& LP = P.levels[h];
       double by = 0.0;
       if (prof_enabled())
         for (int i = LP.front_begin; i < LP.front_end; i++) by += solve_pass_bytes(P.fronts[i], nq, sizeof(T));
       prof_begin(KC_SOLVE_FWD, st);
-      const int ns = (int) LP.small_fronts.size();
+      const int ns = (int) LP.small_numeric.size();
       if (ns > 0) {
-        const int* sl = D.small_list + D.small_off[h];
-        const int nw = LP.small_warp;
+        const int* sl = D.small_num + D.small_num_off[h];
+        const int nw = LP.small_numeric_warp;
         if (nw > 0) {
           k_fwd<T, SOLVE_NRHS, 32><<<(nw + 7) / 8, 256, 0, st>>>(sl, nw, D.fronts, D.children, D.maps, D.rows, L,
                                                                  Bq, ld, W, nq);
@@ -938,10 +1065,10 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
           k_bwd_big<T, 8, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 8>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         count_launch();
       }
-      const int ns = (int) LP.small_fronts.size();
+      const int ns = (int) LP.small_numeric.size();
       if (ns > 0) {
-        const int* sl = D.small_list + D.small_off[h];
-        const int nw = LP.small_warp;
+        const int* sl = D.small_num + D.small_num_off[h];
+        const int nw = LP.small_numeric_warp;
         if (nw > 0) {
           k_bwd<T, SOLVE_NRHS, 32><<<(nw + 7) / 8, 256, 0, st>>>(sl, nw, D.fronts, D.rows, L, Xq, ld, W, nq);
           count_launch();
@@ -952,6 +1079,17 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         }
       }
       prof_end(KC_SOLVE_BWD, st, 0.0, by);
+    }
+    if (np > 0) {
+      double by = 0.0;
+      if (prof_enabled())
+        for (int i : P.pers_fronts) by += solve_pass_bytes(P.fronts[i], nq, sizeof(T));
+      prof_begin(KC_SOLVE_BWD, st);
+      k_bwd_pers<T, SOLVE_NRHS><<<pers_solve_grid(np), 256, 0, st>>>(
+          D.pers_list, np, D.pers_parent, D.pers_solve + np, D.pers_solve + 2 * np + 1, eb, D.fronts, D.rows, L, Xq, ld,
+          W, nq, status);
+      prof_end(KC_SOLVE_BWD, st, 0.0, by);
+      count_launch();
     }
   }
   (void) epoch;
