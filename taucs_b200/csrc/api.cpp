@@ -170,6 +170,12 @@ void free_numeric(Factor* F) {
 
 static void free_device(Factor* F) {
   free_numeric(F);
+  tb::dfree(F->batch.d_cvmap); F->batch.d_cvmap = nullptr;
+  tb::dfree(F->batch.d_cperm); F->batch.d_cperm = nullptr;
+  tb::dfree(F->batch.d_raw); F->batch.d_raw = nullptr;
+  tb::dfree(F->batch.d_b); F->batch.d_b = nullptr;
+  tb::dfree(F->batch.d_x); F->batch.d_x = nullptr;
+  tb::hfree(F->batch.h_raw); F->batch.h_raw = nullptr;
   if (F->cap_stream) cudaStreamDestroy(F->cap_stream);
   F->cap_stream = nullptr;
   if (F->dev_ready) devplan_free(&F->dp);

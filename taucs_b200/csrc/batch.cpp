@@ -195,14 +195,81 @@ extern "C" int taucs_b200_batch_split(void* L, const double* combined, double* c
   return 0;
 }
 
+// The device side of the batch entry points, set up on first use: the maps
+// from the combined order to the systems' own orders concatenated, the
+// device buffers, and the pinned staging area.
+static int batch_device(Factor* F) {
+  Factor::BatchMap& M = F->batch;
+  if (M.h_raw) return 0;
+  if (ensure_device(F)) return -1;
+  const int64_t nnz = F->plan.nnz;
+  const int n = F->n, count = F->nseg();
+  std::vector<int> cvmap((size_t) nnz), cperm((size_t) n);
+  for (int s = 0; s < count; s++) {
+    for (int64_t k = M.nnz_off[s]; k < M.nnz_off[s + 1]; k++) cvmap[k] = (int) (M.nnz_off[s] + M.vmap[k]);
+    for (int i = F->seg_ptr[s]; i < F->seg_ptr[s + 1]; i++) cperm[i] = F->seg_ptr[s] + M.perm[i];
+  }
+  const size_t raw = (size_t) std::max<int64_t>(nnz, n);
+  cudaStream_t st = current_stream();
+  bool ok = cuda_ok(dmalloc(&M.d_cvmap, sizeof(int) * std::max<int64_t>(nnz, 1)), "cudaMalloc") &&
+            cuda_ok(dmalloc(&M.d_cperm, sizeof(int) * std::max(n, 1)), "cudaMalloc") &&
+            cuda_ok(dmalloc(&M.d_raw, sizeof(double) * raw), "cudaMalloc") &&
+            cuda_ok(dmalloc(&M.d_b, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
+            cuda_ok(dmalloc(&M.d_x, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
+            cuda_ok(hmalloc(&M.h_raw, sizeof(double) * raw), "cudaMallocHost") &&
+            cuda_ok(cudaMemcpyAsync(M.d_cvmap, cvmap.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, st), "map") &&
+            cuda_ok(cudaMemcpyAsync(M.d_cperm, cperm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st), "map") &&
+            cuda_ok(cudaStreamSynchronize(st), "batch maps");
+  if (!ok) {
+    dfree(M.d_cvmap); dfree(M.d_cperm); dfree(M.d_raw); dfree(M.d_b); dfree(M.d_x); hfree(M.h_raw);
+    M.d_cvmap = M.d_cperm = nullptr;
+    M.d_raw = M.d_b = M.d_x = M.h_raw = nullptr;
+    return -1;
+  }
+  return 0;
+}
+
+// body(s) for every system s, on up to 16 host threads
+template <typename Body>
+static void for_systems(int count, Body body) {
+  const int nt = (int) std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (nt <= 1 || count < 64) {
+    for (int s = 0; s < count; s++) body(s);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&, t] {
+      for (int s = t; s < count; s += nt) body(s);
+    });
+  for (auto& x : th) x.join();
+}
+
+int gather_values_device(long nnz, const int* d_vmap, const double* d_raw, double* d_out);
+int perm_gather_device(int n, const int* d_perm, const double* src, double* dst);
+int perm_scatter_device(int n, const int* d_perm, const double* src, double* dst);
+
 extern "C" int taucs_b200_batch_factor(void* L, taucs_ccs_matrix* const* A) {
   Factor* F = (Factor*) L;
   if (!is_batch(F)) { set_error("batch_factor: not a batch handle"); return -1; }
-  if (ensure_device(F)) return -1;
-  std::vector<double> v((size_t) F->plan.nnz);
-  if (taucs_b200_batch_values(L, A, v.data())) return -1;
+  if (!A) { set_error("batch_factor: no systems"); return -1; }
+  if (batch_device(F)) return -1;
+  Factor::BatchMap& M = F->batch;
+  const int count = F->nseg();
+  for (int s = 0; s < count; s++)
+    if (!A[s] || A[s]->colptr[A[s]->n] != M.nnz_off[s + 1] - M.nnz_off[s]) {
+      set_error("batch_factor: system " + std::to_string(s) + " does not match the analysed pattern");
+      return -1;
+    }
+  // the values as given, back to back in pinned memory; one copy; the
+  // combined order is gathered on the device
+  for_systems(count, [&](int s) {
+    memcpy(M.h_raw + M.nnz_off[s], A[s]->values.d, sizeof(double) * (size_t) (M.nnz_off[s + 1] - M.nnz_off[s]));
+  });
   cudaStream_t st = current_stream();
-  if (!cuda_ok(cudaMemcpyAsync(F->dA, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, st), "values"))
+  const int64_t nnz = F->plan.nnz;
+  if (!cuda_ok(cudaMemcpyAsync(M.d_raw, M.h_raw, sizeof(double) * nnz, cudaMemcpyHostToDevice, st), "values") ||
+      gather_values_device(nnz, M.d_cvmap, M.d_raw, F->dA))
     return -1;
   return numeric_device(F, F->dA, true);
 }
@@ -212,26 +279,27 @@ extern "C" int taucs_b200_batch_solve(void* L, double* const* X, const double* c
   Factor* F = (Factor*) L;
   if (!is_batch(F)) { set_error("batch_solve: not a batch handle"); return -1; }
   if (!F->has_numeric && !F->has_numeric32) { set_error("batch_solve: no numeric factor"); return -1; }
-  const int n = F->n;
-  std::vector<double> b(n), x(n);
-  if (taucs_b200_batch_rhs(L, B, b.data())) return -1;
-  double *db = nullptr, *dx = nullptr;
+  if (!X || !B) { set_error("batch_solve: no vectors"); return -1; }
+  if (batch_device(F)) return -1;
+  Factor::BatchMap& M = F->batch;
+  const int n = F->n, count = F->nseg();
+  // right-hand sides as given, back to back; permuted on the device
+  for_systems(count, [&](int s) {
+    memcpy(M.h_raw + F->seg_ptr[s], B[s], sizeof(double) * (size_t) (F->seg_ptr[s + 1] - F->seg_ptr[s]));
+  });
   cudaStream_t st = current_stream();
-  if (!cuda_ok(tb::dmalloc(&db, sizeof(double) * n), "cudaMalloc") ||
-      !cuda_ok(tb::dmalloc(&dx, sizeof(double) * n), "cudaMalloc")) {
-    tb::dfree(db);
+  if (!cuda_ok(cudaMemcpyAsync(M.d_raw, M.h_raw, sizeof(double) * n, cudaMemcpyHostToDevice, st), "rhs") ||
+      perm_gather_device(n, M.d_cperm, M.d_raw, M.d_b))
     return -1;
-  }
-  int steps = -1;
-  if (cuda_ok(cudaMemcpyAsync(db, b.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st), "rhs")) {
-    steps = solve_refine_device(F, 1, dx, db, n, tol, maxits < 0 ? 0 : maxits, res);
-    if (!cuda_ok(cudaMemcpyAsync(x.data(), dx, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "solution") ||
-        !cuda_ok(cudaStreamSynchronize(st), "batch solve"))
-      steps = -1;
-  }
-  tb::dfree(db);
-  tb::dfree(dx);
-  if (steps >= 0) taucs_b200_batch_split(L, x.data(), X);
+  int steps = solve_refine_device(F, 1, M.d_x, M.d_b, n, tol, maxits < 0 ? 0 : maxits, res);
+  if (steps < 0) return -1;
+  if (perm_scatter_device(n, M.d_cperm, M.d_x, M.d_raw) ||
+      !cuda_ok(cudaMemcpyAsync(M.h_raw, M.d_raw, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "solution") ||
+      !cuda_ok(cudaStreamSynchronize(st), "batch solve"))
+    return -1;
+  for_systems(count, [&](int s) {
+    memcpy(X[s], M.h_raw + F->seg_ptr[s], sizeof(double) * (size_t) (F->seg_ptr[s + 1] - F->seg_ptr[s]));
+  });
   return steps;
 }
 

@@ -85,6 +85,16 @@ struct Factor {
   struct BatchMap {
     std::vector<int64_t> nnz_off;
     std::vector<int> perm, vmap;
+    // device side of taucs_b200_batch_factor / _solve: the systems' values
+    // and vectors travel as they are given, concatenated, and are permuted on
+    // the device: combined value k = raw[cvmap[k]], combined row i = raw row
+    // cperm[i]; pinned host staging for both
+    int* d_cvmap = nullptr;
+    int* d_cperm = nullptr;
+    double* d_raw = nullptr;     // max(nnz, n)
+    double* d_b = nullptr;       // n
+    double* d_x = nullptr;       // n
+    double* h_raw = nullptr;     // pinned, max(nnz, n)
   } batch;
 
   // recorded launch sequences (numeric factorization, solves, refinement

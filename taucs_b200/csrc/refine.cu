@@ -600,6 +600,20 @@ int gather_values_device(long nnz, const int* d_vmap, const double* d_raw, doubl
   return cuda_ok(cudaGetLastError(), "value gather") ? 0 : -1;
 }
 
+int perm_gather_device(int n, const int* d_perm, const double* src, double* dst) {
+  if (n <= 0) return 0;
+  k_perm_gather<<<nblk(n, 256), 256, 0, current_stream()>>>(n, 1, d_perm, src, dst);
+  count_launch();
+  return cuda_ok(cudaGetLastError(), "permutation") ? 0 : -1;
+}
+
+int perm_scatter_device(int n, const int* d_perm, const double* src, double* dst) {
+  if (n <= 0) return 0;
+  k_perm_scatter<<<nblk(n, 256), 256, 0, current_stream()>>>(n, 1, d_perm, src, dst);
+  count_launch();
+  return cuda_ok(cudaGetLastError(), "permutation") ? 0 : -1;
+}
+
 int solve_refine_permuted(Factor* F, int nrhs, double* d_x, const double* d_b, const int* d_perm, double tol,
                           int maxits, double* res) {
   if (!F || (!F->has_numeric && !F->has_numeric32)) { set_error("solve_refine: no numeric factor"); return -1; }
