@@ -245,9 +245,6 @@ static void for_systems(int count, Body body) {
   for (auto& x : th) x.join();
 }
 
-int gather_values_device(long nnz, const int* d_vmap, const double* d_raw, double* d_out);
-int perm_gather_device(int n, const int* d_perm, const double* src, double* dst);
-int perm_scatter_device(int n, const int* d_perm, const double* src, double* dst);
 
 extern "C" int taucs_b200_batch_factor(void* L, taucs_ccs_matrix* const* A) {
   Factor* F = (Factor*) L;

@@ -154,6 +154,12 @@ inline cudaError_t hmalloc(T** p, size_t bytes) { return hmalloc_raw((void**) p,
 void tune_record(const Plan& P, int prec, const std::vector<double> (&t)[2]);
 bool tune_apply(Plan* P, int prec);
 
+// device gathers of the request server and the batch entry points
+// (refine.cu): out[k] = raw[vmap[k]]; dst[i] = src[perm[i]]; dst[perm[i]] = src[i]
+int gather_values_device(long nnz, const int* d_vmap, const double* d_raw, double* d_out);
+int perm_gather_device(int n, const int* d_perm, const double* src, double* dst);
+int perm_scatter_device(int n, const int* d_perm, const double* src, double* dst);
+
 // launch accounting
 void count_launch(long k = 1);
 
