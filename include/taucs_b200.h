@@ -316,6 +316,12 @@ int taucs_b200_etree(taucs_ccs_matrix* A, int* parent);
  * and map arrays that taucs_b200_export_rows_maps fills. */
 int taucs_b200_export_layout(void* L, long long* fronts, long long* totals);
 int taucs_b200_export_rows_maps(void* L, int* rows, int* maps);
+/* the persistent set (small fronts with only small fronts below them, which
+ * one launch factors and one launch per direction solves, from device-side
+ * queues), host memory only: per task in queue order its front (device
+ * order), its parent's task (-1 when the parent is outside the set) and its
+ * number of children; returns the number of tasks (arrays may be NULL) */
+int taucs_b200_export_persistent(void* L, int* tasks, int* parent_task, int* pending);
 /* the solve's block lists of level h (host memory only): (front, 64-row
  * block) pairs in launch order, forward (*n_diag diagonal blocks first, then
  * update-row blocks) and backward; with NULL arrays only the counts are set. */

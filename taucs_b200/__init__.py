@@ -138,6 +138,7 @@ def lib():
         "taucs_b200_etree": (C.c_int, [pc, _i32p]),
         "taucs_b200_export_layout": (C.c_int, [vp, vp, vp]),
         "taucs_b200_export_rows_maps": (C.c_int, [vp, vp, vp]),
+        "taucs_b200_export_persistent": (C.c_int, [vp, vp, vp, vp]),
         "taucs_b200_export_solve_blocks": (C.c_int, [vp, C.c_int, vp, C.POINTER(C.c_int), C.POINTER(C.c_int), vp,
                                                      C.POINTER(C.c_int)]),
         "taucs_b200_launch_count": (C.c_long, [C.c_int]),

@@ -810,6 +810,19 @@ int taucs_b200_export_solve_blocks(void* vL, int h, int* fwd, int* n_fwd, int* n
   return 0;
 }
 
+int taucs_b200_export_persistent(void* vL, int* tasks, int* parent_task, int* pending) {
+  const Factor* F = (const Factor*) vL;
+  if (!F) return -1;
+  const Plan& P = F->plan;
+  const int n = (int) P.pers_fronts.size();
+  for (int t = 0; t < n; t++) {
+    if (tasks) tasks[t] = P.pers_fronts[t];
+    if (parent_task) parent_task[t] = P.pers_parent[t];
+    if (pending) pending[t] = P.pers_pending[t];
+  }
+  return n;
+}
+
 int taucs_b200_export_values(void* vL, long* val_ptr, double* vals) {
   Factor* F = (Factor*) vL;
   if (!F) return -1;

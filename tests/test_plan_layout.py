@@ -175,3 +175,52 @@ def test_rows_and_maps(tb, case):
         n = P.n
     check_rows_maps(F, n)
     F.free()
+
+
+def check_persistent(F):
+    """The persistent set and its device-side queue: every task is a small
+    front (f <= 96) whose children are all tasks, queued after them (level
+    order, so a task is only taken after everything it waits for was taken);
+    every small front whose subtree is small is in the set; parent links and
+    child counts agree with the tree."""
+    import ctypes as C
+    lib = __import__("taucs_b200").lib()
+    fr, _ = F.layout()
+    level, parent, f = fr[:, 0], fr[:, 1], fr[:, 3]
+    n = lib.taucs_b200_export_persistent(F.h, None, None, None)
+    tasks = np.zeros(max(n, 1), np.int32)
+    ptask = np.zeros(max(n, 1), np.int32)
+    pend = np.zeros(max(n, 1), np.int32)
+    lib.taucs_b200_export_persistent(F.h, tasks.ctypes.data, ptask.ctypes.data, pend.ctypes.data)
+    tasks, ptask, pend = tasks[:n], ptask[:n], pend[:n]
+    task_of = np.full(fr.shape[0], -1)
+    task_of[tasks] = np.arange(n)
+    nchild = np.bincount(parent[parent >= 0], minlength=fr.shape[0])
+    assert np.all(f[tasks] <= 96)
+    assert np.all(np.diff(level[tasks]) >= 0), "queue in level order"
+    for t, i in enumerate(tasks):
+        assert pend[t] == nchild[i]
+        kids = np.nonzero(parent == i)[0]
+        assert np.all(task_of[kids] >= 0) and np.all(task_of[kids] < t), "children are queued before the parent"
+        p = parent[i]
+        assert ptask[t] == (task_of[p] if p >= 0 else -1)
+    # completeness: a small front is a task exactly when its whole subtree is small
+    pure = f <= 96
+    for i in np.argsort(level, kind="stable"):
+        if parent[i] >= 0 and not pure[i]:
+            pure[parent[i]] = False
+    assert np.array_equal(task_of >= 0, pure)
+    return n
+
+
+@pytest.mark.parametrize("case", ["lognormal40", "mesh2d", "batch"])
+def test_persistent_queue(tb, case):
+    if case == "batch":
+        systems = [tb.lognormal(k, k, 0, 1.0, (1, 1, 1), k) for k in range(6, 70, 3)]
+        F = tb.Batch(systems)
+    else:
+        A = tb.lognormal(40, 40, 40, 1.0, (1, 1, 1), 2) if case == "lognormal40" else tb.mesh2d(120)
+        P, _, _ = amd_permuted(A)
+        F = tb.factor_symbolic(P)
+    assert check_persistent(F) > 0
+    F.free()
