@@ -137,7 +137,8 @@ struct Plan {
   int64_t v_len = 0;               // doubles of per-front work vectors (1 rhs)
   int64_t dinv_len = 0;            // doubles of diagonal-block inverses
   int n_blk = 0;                   // solve flags
-  int64_t part_len = 0;            // doubles of backward partial sums
+  int64_t part_len = 0;            // doubles of partial sums: the backward ones, then the forward walk's
+  int64_t fpart_off = 0;           // start of the forward walk's partial sums (n_blk x 64 x SOLVE_NRHS)
   int64_t sp_len = 0;              // floats of the split arena (the largest level's split copies)
   // small fronts whose whole subtree is small, in device (level) order: one
   // persistent launch factors them all, taking them from a device-side queue

@@ -376,6 +376,9 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
         F.part_off = -1;
       }
     }
+    // the forward walk's partial sums of every diagonal block follow
+    P.fpart_off = poff;
+    poff += (int64_t) P.n_blk * PANEL_NB * SOLVE_NRHS;
     P.part_len = std::max<int64_t>(poff, 32);
     // split copies of the big fronts' panels for the FP32 tensor-core
     // products; the levels run one after another, so each level starts the

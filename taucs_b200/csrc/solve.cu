@@ -644,6 +644,241 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   if (tid == 0) st_release(flags + F.blk_off + r, epoch);
 }
 
+// Forward solve of the diagonal blocks of levels with long chains, as a
+// walk.  One walker CTA per big front runs the chain y_r = L_rr^-1 (w_r -
+// sum_{k<r} L_rk y_k) itself, block after block, keeping the last WALK_D
+// y's in shared memory: consecutive steps are linked by barriers inside one
+// CTA, not by flags between CTAs.  Helper CTAs, one per diagonal block,
+// gather w_r and subtract the far terms k < r - WALK_D as the walker
+// publishes y_k (flags), then publish the partial p_r (pflags) -- WALK_D
+// steps ahead of the walker; the walker at step r subtracts the WALK_D near
+// terms and applies the block's inverse.  The tiles of step r + 1 (L_{r+1,k}
+// for the near k and the next inverse) are loaded into registers while step
+// r runs.  Walkers have the lowest CTA indices and a helper waits only for
+// the walker of its front, which waits only for helpers of lower index, so
+// in-order dispatch keeps every wait finite; the waits are bounded all the
+// same.  In the last diagonal block rows >= s are update rows of the same
+// front; the walker finishes them too.  The update-row blocks follow in
+// FWD_UPD.  Right-hand sides are processed eight at a time (the layout of
+// the partials).
+constexpr int WALK_D = 2, WALK_T = WALK_D + 1;
+constexpr int WALK_PER = WALK_T * BR * BR / 256;   // staged tile entries per thread
+
+// dynamic shared memory of the walk: the walker's tiles of one step and its
+// ring of y's; the helpers use the first part for their partial sums
+template <typename T>
+constexpr size_t walk_smem() {
+  return (WALK_T * BR * BR + WALK_T * BR * (SOLVE_NRHS + 1)) * sizeof(T);
+}
+
+template <typename T, int WS>
+__global__ void __launch_bounds__(256)
+k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
+           const FrontDesc* __restrict__ fronts, const int* __restrict__ children, const int* __restrict__ maps,
+           const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ Dinv,
+           const T* __restrict__ B, int ldb, T* __restrict__ W, T* __restrict__ fpart, int nrhs,
+           int* __restrict__ flags, int* __restrict__ pflags, int epoch, int* status) {
+  constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
+  static_assert(NQ % 4 == 0, "four thread groups share the right-hand sides");
+  extern __shared__ __align__(16) unsigned char wsm[];
+  __shared__ T pv[BR][NQ + 1];
+  __shared__ int rng[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int row = tid % BR, qg = tid / BR;
+  if (blockIdx.x < nwalk) {
+    // ---------------------------------------------------------------- walker
+    const FrontDesc F = fronts[walk_fronts[blockIdx.x]];
+    const int f = F.f, s = F.s, nbs = (s + BR - 1) / BR;
+    const T* P = L + F.l_off;
+    T* Wf = W + F.v_off * WS;
+    const T* fp = fpart + (size_t) F.blk_off * BR * NQ;
+    // tl[j] for j < WALK_D: L_{r, r-WALK_D+j} (zero before the first block);
+    // tl[WALK_D]: the inverse of block r, and in rows >= bw of the last
+    // block the update rows' entries of L_{., r}; all column-major
+    T (*tl)[BR][BR] = reinterpret_cast<T (*)[BR][BR]>(wsm);
+    T (*yr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * BR * sizeof(T));
+    T pre[WALK_PER];
+    auto fetch = [&](int r) {
+      const int r0 = r * BR, nr = min(BR, f - r0), bw = min(BR, s - r0);
+      const T* Di = Dinv + F.dinv_off + (size_t) r * BR * BR;
+#pragma unroll
+      for (int t = 0; t < WALK_PER; t++) {
+        const int jj = t / TPT, e = tid + 256 * (t % TPT);
+        const int i = e % BR, j = e / BR;
+        T v = 0.0;
+        if (jj < WALK_D) {
+          const int k = r - WALK_D + jj;   // a full block (k < r <= nbs - 1)
+          if (k >= 0 && i < nr) v = P[(r0 + i) + (size_t) (k * BR + j) * f];
+        } else if (j < bw && i < nr) {
+          v = (i < bw) ? (i >= j ? Di[i + j * BR] : T(0)) : P[(r0 + i) + (size_t) (r0 + j) * f];
+        }
+        pre[t] = v;
+      }
+    };
+    auto put = [&]() {
+#pragma unroll
+      for (int t = 0; t < WALK_PER; t++) {
+        const int e = tid + 256 * (t % TPT);
+        tl[t / TPT][e / BR][e % BR] = pre[t];
+      }
+    };
+    auto load_p = [&](int r) {
+      if (tid == 32) poll_epoch(pflags + F.blk_off + r, epoch, status);
+      __syncthreads();
+      for (int e = tid; e < BR * NQ; e += 256) pv[e / NQ][e % NQ] = __ldcg(fp + (size_t) r * BR * NQ + e);
+    };
+    fetch(0);
+    put();
+    load_p(0);
+    for (int r = 0; r < nbs; r++) {
+      const int r0 = r * BR, nr = min(BR, f - r0), bw = min(BR, s - r0);
+      const int slot = r % WALK_T;
+      if (r + 1 < nbs) fetch(r + 1);   // in flight during the step
+      __syncthreads();                  // p_r and the tiles of step r are in place
+      // near terms: p_r -= sum_j L_{r, r-WALK_D+j} y_{r-WALK_D+j}
+      {
+        T u[QG];
+#pragma unroll
+        for (int c = 0; c < QG; c++) u[c] = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < WALK_D; jj++) {
+          const int k = r - WALK_D + jj;
+          if (k < 0) continue;
+          const int sl = k % WALK_T;
+#pragma unroll 8
+          for (int j = 0; j < BR; j++) {
+            const T l = tl[jj][j][row];
+#pragma unroll
+            for (int c = 0; c < QG; c++) u[c] += l * yr[sl][j][qg * QG + c];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < QG; c++) pv[row][qg * QG + c] -= u[c];
+      }
+      __syncthreads();
+      // y_r = L_rr^-1 p_r in rows < bw; the update rows keep p
+      {
+        T y[QG];
+#pragma unroll
+        for (int c = 0; c < QG; c++) y[c] = 0.0;
+        if (row < bw)
+          for (int j = 0; j <= row; j++) {
+            const T d = tl[WALK_D][j][row];
+#pragma unroll
+            for (int c = 0; c < QG; c++) y[c] += d * pv[j][qg * QG + c];
+          }
+#pragma unroll
+        for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] = (row < bw) ? y[c] : pv[row][qg * QG + c];
+      }
+      __syncthreads();
+      if (bw < nr) {
+        // update rows inside the last diagonal block: w_i -= L[i, r] y_r
+        // (reads rows < bw of the ring slot, writes rows >= bw)
+        if (row >= bw) {
+          T v[QG];
+#pragma unroll
+          for (int c = 0; c < QG; c++) v[c] = 0.0;
+          for (int j = 0; j < bw; j++) {
+            const T l = tl[WALK_D][j][row];
+#pragma unroll
+            for (int c = 0; c < QG; c++) v[c] += l * yr[slot][j][qg * QG + c];
+          }
+#pragma unroll
+          for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] -= v[c];
+        }
+        __syncthreads();
+      }
+      for (int e = tid; e < nr * nrhs; e += 256) {
+        const int i = e % nr, q = e / nr;
+        Wf[r0 + i + (size_t) q * f] = yr[slot][i][q];
+      }
+      // the barrier orders every thread's stores before the release, and
+      // every read of this step's tiles and p before they are replaced
+      __syncthreads();
+      if (tid == 0) st_release(flags + F.blk_off + r, epoch);
+      if (r + 1 < nbs) {
+        put();
+        load_p(r + 1);   // thread 32 polls while thread 0 releases
+      }
+    }
+    return;
+  }
+  // ------------------------------------------------------------------ helper
+  const int2_ bk = blocks[blockIdx.x - nwalk];
+  const FrontDesc F = fronts[bk.a];
+  const int r = bk.b, f = F.f, s = F.s;
+  const int r0 = r * BR, nr = min(BR, f - r0);
+  const T* P = L + F.l_off;
+  const T* Wf = W + F.v_off * WS;
+  const int* rw = rows + F.rows_off;
+  T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);   // [4], then ys
+  T (*ys)[NQ] = red[4];
+  // this thread's 16 columns of the first far block, loaded before anything
+  // waits
+  const int kend = max(r - WALK_D, 0);
+  T lv[BR / 4];
+  auto load_l = [&](int k) {
+    const T* pc = P + (r0 + row) + (size_t) (k * BR + qg * (BR / 4)) * f;
+#pragma unroll
+    for (int j = 0; j < BR / 4; j++) lv[j] = (row < nr) ? pc[(size_t) j * f] : T(0);
+  };
+  if (kend > 0) load_l(0);
+  for (int k = tid; k < BR * NQ; k += 256) {
+    const int i = k % BR, q = k / BR;
+    pv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : T(0);
+  }
+  __syncthreads();
+  for (int ci = F.child_begin; ci < F.child_end; ci++) {
+    const FrontDesc C = fronts[children[ci]];
+    const int mc = C.f - C.s;
+    const int* mp = maps + C.map_off;
+    if (warp < 2) {
+      const int x = warp_lower_bound(mp, mc, warp == 0 ? r0 : r0 + nr);
+      if (lane == 0) rng[warp] = x;
+    }
+    __syncthreads();
+    const int ia = rng[0], ib = rng[1];
+    __syncthreads();
+    if (ia >= ib) continue;
+    const T* Wc = W + C.v_off * WS;
+    for (int k = tid; k < (ib - ia) * nrhs; k += 256) {
+      const int i = ia + k % (ib - ia), q = k / (ib - ia);
+      pv[mp[i] - r0][q] += Wc[C.s + i + q * C.f];
+    }
+    __syncthreads();
+  }
+  // far terms k < r - WALK_D: thread (row, quarter qg) sums 16 columns of
+  // each L_rk for every right-hand side, the y_k arriving as the walker
+  // publishes them
+  T acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+  for (int k = 0; k < kend; k++) {
+    wait_epoch(flags + F.blk_off + k, epoch, status);
+    for (int e = tid; e < BR * NQ; e += 256) {
+      const int j = e % BR, q = e / BR;
+      ys[j][q] = (q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < BR / 4; j++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) acc[q] += lv[j] * ys[qg * (BR / 4) + j][q];
+    if (k + 1 < kend) load_l(k + 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; q++) red[qg][row][q] = acc[q];
+  __syncthreads();
+  T* dst = fpart + (size_t) (F.blk_off + r) * BR * NQ;
+  for (int e = tid; e < BR * NQ; e += 256) {
+    const int i = e / NQ, q = e % NQ;
+    dst[e] = pv[i][q] - (red[0][i][q] + red[1][i][q] + red[2][i][q] + red[3][i][q]);
+  }
+  __syncthreads();
+  if (tid == 0) st_release(pflags + F.blk_off + r, epoch);
+}
+
 // x at the update rows of every big front of a level, gathered once into the
 // front's work vector (rows s..f-1) so the backward blocks read it coalesced
 template <typename T, int WS>
@@ -917,6 +1152,18 @@ static double solve_pass_bytes(const FrontDesc& F, int nrhs, double esz) {
   return esz * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * esz * nrhs * F.f;
 }
 
+// the forward walk on levels with long chains of FP32 factors
+// (TAUCS_B200_NO_FWD_WALK=1 selects the flag-chained FWD_CHAIN kernel
+// instead; FP64 keeps FWD_CHAIN: the walker's staged FP64 tiles take 164
+// registers, one CTA per SM, too few resident helpers)
+static bool fwd_walk_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("TAUCS_B200_NO_FWD_WALK");
+    return !(e && *e && strcmp(e, "0") != 0);
+  }();
+  return on;
+}
+
 template <typename T>
 static void solve_attrs() {
   // once per device and type (request-server workers reach this concurrently)
@@ -936,6 +1183,7 @@ static void solve_attrs() {
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
     cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
+    cudaFuncSetAttribute(k_fwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) walk_smem<T>());
     return true;
   });
 }
@@ -962,7 +1210,8 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
   solve_attrs<T>();
   // the handshake flags restart from zero on every call, so the epochs of a
   // call are always 1, 2, ... and a recorded launch sequence stays valid
-  cudaMemsetAsync(flags, 0, sizeof(int) * (size_t) P.n_blk, st);
+  // (the second half: the forward walk's partial-sum flags)
+  cudaMemsetAsync(flags, 0, 2 * sizeof(int) * (size_t) P.n_blk, st);
   const int np = D.n_pers;
   if (np > 0) cudaMemsetAsync(D.pers_solve, 0, sizeof(int) * (size_t) (2 * np + 2), st);
   int ep = 0;
@@ -1014,7 +1263,16 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         // than a one-column instantiation (columns >= nrhs are skipped)
         auto run = [&](auto nqc) {
           constexpr int Q = decltype(nqc)::value;
-          if (LP.max_s_big >= FWD_CHAIN_MIN_S) {
+          if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && fwd_walk_enabled()) {
+            const int nbig = (int) LP.big_fronts.size();
+            k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, 256, walk_smem<T>(), st>>>(
+                D.big_list + D.big_off[h], nbig, bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W,
+                part + P.fpart_off, nq, flags, flags + P.n_blk, ef, status);
+            if (nu)
+              k_fwd_big<T, Q, SOLVE_NRHS, FWD_UPD><<<nu, 128, 0, st>>>(bl + nd, D.fronts, D.children, D.maps, D.rows,
+                                                                      L, Dinv, Bq, ld, W, nq, flags, ef, status);
+            count_launch(nu ? 2 : 1);
+          } else if (LP.max_s_big >= FWD_CHAIN_MIN_S) {
             k_fwd_big<T, Q, SOLVE_NRHS, FWD_CHAIN><<<nd, 128, fwd_smem<T, FWD_CHAIN>(), st>>>(
                 bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, nq, flags, ef, status);
             if (nu)
