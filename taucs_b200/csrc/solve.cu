@@ -375,7 +375,9 @@ __device__ __forceinline__ void poll_epoch(const int* flag, int epoch, int* stat
   const int want = epoch + g_solve_wait_skew, limit = g_solve_wait_limit;
   int it = 0;
   while (ld_acquire(flag) != want) {
-    if (++it > limit) {
+    // a wait that gave up anywhere ends the others at once, so a broken
+    // chain costs one polling limit, not one per wait
+    if (++it > limit || ((it & 1023) == 0 && *(volatile int*) status == SOLVE_TIMEOUT)) {
       atomicExch(status, SOLVE_TIMEOUT);
       break;
     }
@@ -663,12 +665,21 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 // the partials).
 constexpr int WALK_D = 2, WALK_T = WALK_D + 1;
 constexpr int WALK_PER = WALK_T * BR * BR / 256;   // staged tile entries per thread
+// levels with more big fronts keep the flag-chained kernels: every walker
+// must be resident with room to spare for helpers (two CTAs per SM)
+constexpr int WALK_MAX_FRONTS = 64;
 
 // dynamic shared memory of the walk: the walker's tiles of one step and its
 // ring of y's; the helpers use the first part for their partial sums
 template <typename T>
 constexpr size_t walk_smem() {
   return (WALK_T * BR * BR + WALK_T * BR * (SOLVE_NRHS + 1)) * sizeof(T);
+}
+// the backward walker's tiles are [row][column], padded against bank
+// conflicts of the coalesced staging stores
+template <typename T>
+constexpr size_t bwalk_smem() {
+  return (WALK_T * BR * (BR + 1) + WALK_T * BR * (SOLVE_NRHS + 1)) * sizeof(T);
 }
 
 template <typename T, int WS>
@@ -1141,10 +1152,195 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   if (tid == 0) st_release(flags + F.blk_off + k, epoch);
 }
 
+// Backward solve of the diagonal blocks of levels with long chains, as a
+// walk: the mirror of k_fwd_walk.  The walker of a front runs
+// x_k = L_kk^-T (v_k - sum_{j>k} L_jk^T x_j) from the last block to the
+// first, subtracting the WALK_D near terms j = k+1, k+2 itself; helper CTAs,
+// one per diagonal block (listed last block first), form v_k = y_k - L21^T
+// x2 from the chunk partial sums, subtract the far terms j > k + WALK_D as
+// the walker publishes x_j, and publish the partial through the second
+// flag array.  The same in-order dispatch argument as the forward walk
+// keeps every wait finite.
+template <typename T, int WS>
+__global__ void __launch_bounds__(256)
+k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
+           const FrontDesc* __restrict__ fronts, const int* __restrict__ rows, const T* __restrict__ L,
+           const T* __restrict__ Dinv, T* __restrict__ X, int ldx, T* __restrict__ W,
+           const T* __restrict__ part, T* __restrict__ bpart, int nrhs, int* __restrict__ flags,
+           int* __restrict__ pflags, int epoch, int* status) {
+  constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
+  extern __shared__ __align__(16) unsigned char wsm[];
+  __shared__ T pv[BR][NQ + 1];
+  const int tid = threadIdx.x;
+  const int col = tid % BR, qg = tid / BR;
+  if (blockIdx.x < nwalk) {
+    // ---------------------------------------------------------------- walker
+    const FrontDesc F = fronts[walk_fronts[blockIdx.x]];
+    const int f = F.f, s = F.s, nbs = (s + BR - 1) / BR;
+    const T* P = L + F.l_off;
+    T* Wf = W + F.v_off * WS;
+    const int* rw = rows + F.rows_off;
+    const T* bp = bpart + (size_t) F.blk_off * BR * NQ;
+    // tl[j] for j < WALK_D: L_{k+1+j, k} (zero past the last block);
+    // tl[WALK_D]: the inverse of block k; all [row][column]
+    T (*tl)[BR][BR + 1] = reinterpret_cast<T (*)[BR][BR + 1]>(wsm);
+    T (*xr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * (BR + 1) * sizeof(T));
+    T pre[WALK_PER];
+    auto fetch = [&](int k) {
+      const int c0 = k * BR, bw = min(BR, s - c0);
+      const T* Di = Dinv + F.dinv_off + (size_t) k * BR * BR;
+#pragma unroll
+      for (int t = 0; t < WALK_PER; t++) {
+        const int jj = t / TPT, e = tid + 256 * (t % TPT);
+        const int i = e % BR, c = e / BR;
+        T v = 0.0;
+        if (jj < WALK_D) {
+          const int j = k + 1 + jj;
+          if (j < nbs && c < bw && i < min(BR, s - j * BR)) v = P[(j * BR + i) + (size_t) (c0 + c) * f];
+        } else if (c < bw && i < bw && i >= c) {
+          v = Di[i + c * BR];
+        }
+        pre[t] = v;
+      }
+    };
+    auto put = [&]() {
+#pragma unroll
+      for (int t = 0; t < WALK_PER; t++) {
+        const int e = tid + 256 * (t % TPT);
+        tl[t / TPT][e % BR][e / BR] = pre[t];
+      }
+    };
+    auto load_p = [&](int k) {
+      if (tid == 32) poll_epoch(pflags + F.blk_off + k, epoch, status);
+      __syncthreads();
+      for (int e = tid; e < BR * NQ; e += 256) pv[e / NQ][e % NQ] = __ldcg(bp + (size_t) k * BR * NQ + e);
+    };
+    fetch(nbs - 1);
+    put();
+    load_p(nbs - 1);
+    for (int k = nbs - 1; k >= 0; k--) {
+      const int c0 = k * BR, bw = min(BR, s - c0);
+      const int slot = k % WALK_T;
+      if (k > 0) fetch(k - 1);   // in flight during the step
+      __syncthreads();           // p_k and the tiles of step k are in place
+      // near terms: p_k -= sum_j L_{k+1+j, k}^T x_{k+1+j}
+      {
+        T u[QG];
+#pragma unroll
+        for (int c = 0; c < QG; c++) u[c] = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < WALK_D; jj++) {
+          const int j = k + 1 + jj;
+          if (j >= nbs) continue;
+          const int sl = j % WALK_T;
+#pragma unroll 8
+          for (int i = 0; i < BR; i++) {
+            const T l = tl[jj][i][col];
+#pragma unroll
+            for (int c = 0; c < QG; c++) u[c] += l * xr[sl][i][qg * QG + c];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < QG; c++) pv[col][qg * QG + c] -= u[c];
+      }
+      __syncthreads();
+      // x_k = L_kk^-T p_k (the inverse is lower triangular)
+      {
+        T x[QG];
+#pragma unroll
+        for (int c = 0; c < QG; c++) x[c] = 0.0;
+        for (int i = col; i < bw; i++) {
+          const T d = tl[WALK_D][i][col];
+#pragma unroll
+          for (int c = 0; c < QG; c++) x[c] += d * pv[i][qg * QG + c];
+        }
+#pragma unroll
+        for (int c = 0; c < QG; c++) xr[slot][col][qg * QG + c] = (col < bw) ? x[c] : T(0);
+      }
+      __syncthreads();
+      for (int e = tid; e < bw * nrhs; e += 256) {
+        const int c = e % bw, q = e / bw;
+        const T v = xr[slot][c][q];
+        Wf[c0 + c + (size_t) q * f] = v;
+        X[rw[c0 + c] + (size_t) q * ldx] = v;
+      }
+      // the barrier orders every thread's stores before the release, and
+      // every read of this step's tiles and p before they are replaced
+      __syncthreads();
+      if (tid == 0) st_release(flags + F.blk_off + k, epoch);
+      if (k > 0) {
+        put();
+        load_p(k - 1);   // thread 32 polls while thread 0 releases
+      }
+    }
+    return;
+  }
+  // ------------------------------------------------------------------ helper
+  const int2_ bk = blocks[blockIdx.x - nwalk];
+  const FrontDesc F = fronts[bk.a];
+  const int k = bk.b, f = F.f, s = F.s;
+  const int nbs = (s + BR - 1) / BR;
+  const int c0 = k * BR, bw = min(BR, s - c0);
+  const T* P = L + F.l_off;
+  const T* Wf = W + F.v_off * WS;
+  T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);   // [4], then ys
+  T (*ys)[NQ] = red[4];
+  const int jlo = k + WALK_D + 1;   // far blocks j = nbs-1 .. jlo
+  // this thread's 16 rows of column c0 + col of the first far block, loaded
+  // before anything waits
+  T lv[BR / 4];
+  auto load_l = [&](int j) {
+    const int bwj = min(BR, s - j * BR);
+    const T* pc = P + (size_t) (c0 + col) * f + j * BR + qg * (BR / 4);
+#pragma unroll
+    for (int t = 0; t < BR / 4; t++) lv[t] = (col < bw && qg * (BR / 4) + t < bwj) ? __ldg(pc + t) : T(0);
+  };
+  if (nbs - 1 >= jlo) load_l(nbs - 1);
+  // v_k = y_k - L21^T x2, the chunk partial sums added in chunk order
+  for (int e = tid; e < BR * NQ; e += 256) {
+    const int c = e % BR, q = e / BR;
+    T v = 0.0;
+    if (c < bw && q < nrhs) {
+      v = Wf[c0 + c + (size_t) q * f];
+      T acc = 0.0;
+      for (int ch = 0; ch < F.nchunk; ch++)
+        acc += __ldcg(part + F.part_off + ((size_t) ch * s + c0 + c) * SOLVE_NRHS + q);
+      v -= acc;
+    }
+    pv[c][q] = v;
+  }
+  T acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+  for (int j = nbs - 1; j >= jlo; j--) {
+    const int bwj = min(BR, s - j * BR);
+    wait_epoch(flags + F.blk_off + j, epoch, status);
+    for (int e = tid; e < BR * NQ; e += 256) {
+      const int i = e % BR, q = e / BR;
+      ys[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < BR / 4; t++)
+#pragma unroll
+      for (int q = 0; q < NQ; q++) acc[q] += lv[t] * ys[qg * (BR / 4) + t][q];
+    if (j - 1 >= jlo) load_l(j - 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; q++) red[qg][col][q] = acc[q];
+  __syncthreads();
+  T* dst = bpart + (size_t) (F.blk_off + k) * BR * NQ;
+  for (int e = tid; e < BR * NQ; e += 256) {
+    const int c = e / NQ, q = e % NQ;
+    dst[e] = pv[c][q] - (red[0][c][q] + red[1][c][q] + red[2][c][q] + red[3][c][q]);
+  }
+  __syncthreads();
+  if (tid == 0) st_release(pflags + F.blk_off + k, epoch);
+}
+
 }  // namespace
 
-// algorithmic bytes of one pass over a front: the lower panel once, its
-// row indices, and the gather/scatter of nrhs vector entries per row
 // algorithmic bytes of one solve pass over a front, values of esz bytes: the
 // lower panel read once, its row list, the work vector read and written
 static double solve_pass_bytes(const FrontDesc& F, int nrhs, double esz) {
@@ -1152,13 +1348,13 @@ static double solve_pass_bytes(const FrontDesc& F, int nrhs, double esz) {
   return esz * (s * (s + 1.0) / 2.0 + m * s) + 4.0 * F.f + 2.0 * esz * nrhs * F.f;
 }
 
-// the forward walk on levels with long chains of FP32 factors
-// (TAUCS_B200_NO_FWD_WALK=1 selects the flag-chained FWD_CHAIN kernel
-// instead; FP64 keeps FWD_CHAIN: the walker's staged FP64 tiles take 164
+// the forward and backward walks on levels with long chains of FP32
+// factors (TAUCS_B200_NO_SOLVE_WALK=1 selects the flag-chained kernels
+// instead; FP64 keeps them: the walker's staged FP64 tiles take 164
 // registers, one CTA per SM, too few resident helpers)
-static bool fwd_walk_enabled() {
+static bool walk_enabled() {
   static const bool on = [] {
-    const char* e = getenv("TAUCS_B200_NO_FWD_WALK");
+    const char* e = getenv("TAUCS_B200_NO_SOLVE_WALK");
     return !(e && *e && strcmp(e, "0") != 0);
   }();
   return on;
@@ -1184,6 +1380,7 @@ static void solve_attrs() {
     cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
     cudaFuncSetAttribute(k_fwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) walk_smem<T>());
+    cudaFuncSetAttribute(k_bwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwalk_smem<T>());
     return true;
   });
 }
@@ -1263,7 +1460,8 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         // than a one-column instantiation (columns >= nrhs are skipped)
         auto run = [&](auto nqc) {
           constexpr int Q = decltype(nqc)::value;
-          if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && fwd_walk_enabled()) {
+          if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
+            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS) {
             const int nbig = (int) LP.big_fronts.size();
             k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, 256, walk_smem<T>(), st>>>(
                 D.big_list + D.big_off[h], nbig, bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W,
@@ -1312,7 +1510,13 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
           count_launch();
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
-        if (nq <= 2)
+        if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
+            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS) {
+          const int nbig = (int) LP.big_fronts.size();
+          k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, 256, bwalk_smem<T>(), st>>>(
+              D.big_list + D.big_off[h], nbig, bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, part + P.fpart_off,
+              nq, flags, flags + P.n_blk, eb, status);
+        } else if (nq <= 2)
           k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 2>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
           k_bwd_big<T, 4, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 4>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
