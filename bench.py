@@ -49,8 +49,8 @@ NRHS = 8
 TOL = 1e-12
 SAMPLE_GRID = 56          # bounded CPU sample of the lognormal workload
 
-KC = dict(small_front=0, build=1, potrf=2, trsm=3, gemm_panel=4, gemm_u=5, solve_fwd=6, solve_bwd=7)
-TENSOR_KC = {"gemm_panel", "gemm_u", "trsm", "potrf"}
+KC = dict(small_front=0, build=1, leaf=2, dinv=3, gemm_panel=4, gemm_u=5, solve_fwd=6, solve_bwd=7)
+TENSOR_KC = {"gemm_panel", "gemm_u", "dinv", "leaf"}
 # DRAM traffic per algorithmic byte of a kernel class, from one ncu capture
 # of a 56^3 update-matrix launch (FP32 fronts): dram read + write 109.7 MB
 # against 146.7 MB of L21 read once and U read and written once; the bench

@@ -178,7 +178,7 @@ bool per_device_once(PerDeviceOnce& pd, bool (*setup)());
 // Optional per-kernel-class timing: when enabled, launchers bracket every
 // launch of a class with CUDA events on the launch stream and record the
 // algorithmic flops and bytes of that launch.
-enum KernelClass { KC_SMALL = 0, KC_BUILD, KC_POTRF, KC_TRSM, KC_GEMM_PANEL, KC_GEMM_U, KC_SOLVE_FWD,
+enum KernelClass { KC_SMALL = 0, KC_BUILD, KC_LEAF, KC_DINV, KC_GEMM_PANEL, KC_GEMM_U, KC_SOLVE_FWD,
                    KC_SOLVE_BWD, KC_OTHER, KC_COUNT };
 bool prof_enabled();
 // every profiled launch: its class, the tag set when it was issued (the

@@ -1006,10 +1006,10 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
           by += 2.0 * sizeof(T) * (ww * (ww + 1.0) / 2.0 + below * ww);
         }
       }
-      prof_begin(KC_POTRF, st);
+      prof_begin(KC_LEAF, st);
       k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, Dinv, sp, sp_fmt, kb,
                                                            status);
-      prof_end(KC_POTRF, st, fl, by);
+      prof_end(KC_LEAF, st, fl, by);
       count_launch();
     };
     auto update = [&](int c_lo, int c_hi, int k_lo, int k_hi) {
@@ -1077,9 +1077,9 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
   }
   prof_tag(-1);
   if (D.n_dblk > 0) {
-    prof_begin(KC_TRSM, st);
+    prof_begin(KC_DINV, st);
     k_dinv<T><<<D.n_dblk, 128, dinv_smem<T>(), st>>>(D.dblk, D.fronts, L, Dinv, status);
-    prof_end(KC_TRSM, st, (double) D.n_dblk * PANEL_NB * PANEL_NB * PANEL_NB / 3.0,
+    prof_end(KC_DINV, st, (double) D.n_dblk * PANEL_NB * PANEL_NB * PANEL_NB / 3.0,
              2.0 * sizeof(T) * D.n_dblk * PANEL_NB * PANEL_NB);
     count_launch();
   }
