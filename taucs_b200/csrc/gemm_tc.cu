@@ -568,13 +568,19 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
           v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(v1[j]) * (1.0f / 2048.0f));
       }
       if (rv) {
+        // all 32 loads are issued before the first store: interleaved, each
+        // load would wait for the store before it (the compiler cannot rule
+        // out that they alias), one memory latency per element
+        float old[32];
 #pragma unroll
         for (int j = 0; j < 32; j++) {
           const int col = C0 + cb + j;
-          if (cb + j < nc && col >= lo && row >= col) {
-            float* cpt = Cp + (int64_t) (col - coff) * ldc;
-            *cpt = *cpt - __uint_as_float(v[j]);
-          }
+          old[j] = (cb + j < nc && col >= lo && row >= col) ? Cp[(int64_t) (col - coff) * ldc] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const int col = C0 + cb + j;
+          if (cb + j < nc && col >= lo && row >= col) Cp[(int64_t) (col - coff) * ldc] = old[j] - __uint_as_float(v[j]);
         }
       }
     }

@@ -211,12 +211,20 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
   for (int k = tid; k < BUILD_TR * BUILD_TC; k += nt) W[k] = 0.0;
   __syncthreads();
   if (panel) {
-    for (int c = tid; c < nc; c += nt) {
-      const int e1 = acol_ptr[F.acol_off + C0 + c + 1];
-      for (int e = acol_ptr[F.acol_off + C0 + c]; e < e1; e++) {
-        const int r = a_rows[e] - R0;
-        if (r >= 0 && r < nr) W[r + c * BUILD_TR] += vals[a_idx[e]];
-      }
+    // A's entries of the tile's columns: thread (column c, slot q) takes the
+    // column's entries q, q + 8, ... -- the loads of all slots in flight at
+    // once; threads of one column serialize their adds through the barrier
+    // rounds (the entries of one column are distinct rows)
+    const int c = tid % BUILD_TC, q = tid / BUILD_TC;
+    constexpr int NQS = 256 / BUILD_TC;
+    int e = 0, e1 = 0;
+    if (c < nc) {
+      e = __ldg(acol_ptr + F.acol_off + C0 + c) + q;
+      e1 = __ldg(acol_ptr + F.acol_off + C0 + c + 1);
+    }
+    for (; e < e1; e += NQS) {
+      const int r = __ldg(a_rows + e) - R0;
+      if (r >= 0 && r < nr) W[r + c * BUILD_TR] += __ldg(vals + __ldg(a_idx + e));
     }
     __syncthreads();
   }
@@ -235,12 +243,36 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     const int ja = rng[0], jb = rng[1], ia = rng[2], ib = rng[3];
     __syncthreads();
     if (ja >= jb || ia >= ib) continue;
+    // warp w takes the child's columns ja + w + 8u, lane l its rows
+    // ia + l + 32v: every load of the tile's share is issued before the first
+    // add (the children's update matrices were written by earlier launches)
     const T* Uc = U + C.u_off;
-    for (int j = ja + warp; j < jb; j += nw) {
-      const int pj = (mp[j] - C0) * BUILD_TR;
-      const T* uj = Uc + (size_t) j * mc;
-      for (int i = max(ia, j) + lane; i < ib; i += 32) W[(mp[i] - R0) + pj] += uj[i];
+    constexpr int JU = (BUILD_TC + 7) / 8, IU = BUILD_TR / 32;
+    int pi[IU], pj[JU];
+    T val[JU][IU];
+#pragma unroll
+    for (int v = 0; v < IU; v++) {
+      const int i = ia + lane + 32 * v;
+      pi[v] = (i < ib) ? __ldg(mp + i) - R0 : -1;
     }
+#pragma unroll
+    for (int u = 0; u < JU; u++) {
+      const int j = ja + warp + 8 * u;
+      const bool jv = j < jb;
+      pj[u] = jv ? (__ldg(mp + j) - C0) * BUILD_TR : -1;
+#pragma unroll
+      for (int v = 0; v < IU; v++) {
+        const int i = ia + lane + 32 * v;
+        val[u][v] = (jv && i < ib && i >= j) ? __ldg(Uc + (size_t) j * mc + i) : T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < JU; u++)
+#pragma unroll
+      for (int v = 0; v < IU; v++) {
+        const int i = ia + lane + 32 * v, j = ja + warp + 8 * u;
+        if (pj[u] >= 0 && pi[v] >= 0 && i >= j) W[pi[v] + pj[u]] += val[u][v];
+      }
     __syncthreads();
   }
   if (panel) {
@@ -312,22 +344,29 @@ __device__ __forceinline__ void warp_inv16_rows(const T (&a)[LQ], T* Y) {
 // division of the textbook loop is a multiply by rsqrt(pivot).  Returns the
 // first nonpositive pivot (or -1) in every lane.
 template <typename T>
-__device__ int warp_chol_inv16(T* S, T* Y) {
+__device__ __forceinline__ int warp_chol_inv16(T* S, T* Y) {
   const int i = threadIdx.x & 15;
   T a[LQ];
 #pragma unroll
   for (int k = 0; k < LQ; k++) a[k] = (k <= i) ? S[i + k * LLD] : T(0);
   int bad = -1;
-#pragma unroll
+  // column j is picked out of a[] by selects, not by a[j]: the compiler
+  // does not unroll this loop, and an array indexed by the loop variable
+  // would live in local memory, one access per step of the serial chain
+#pragma unroll 1
   for (int j = 0; j < LQ; j++) {
-    const T d = __shfl_sync(0xffffffffu, a[j], j);
+    T aj = T(0);
+#pragma unroll
+    for (int k = 0; k < LQ; k++) aj = (k == j) ? a[k] : aj;
+    const T d = __shfl_sync(0xffffffffu, aj, j);
     if (!(d > T(0)) && bad < 0) bad = j;
     const T r = rsqrt_t(d);
-    a[j] = (i == j) ? d * r : a[j] * r;
+    aj = (i == j) ? d * r : aj * r;
 #pragma unroll
-    for (int k = j + 1; k < LQ; k++) {
-      const T lkj = __shfl_sync(0xffffffffu, a[j], k);
-      if (i >= k) a[k] -= a[j] * lkj;
+    for (int k = 0; k < LQ; k++) {
+      const T lkj = __shfl_sync(0xffffffffu, aj, k);
+      if (k == j) a[k] = aj;
+      else if (k > j && i >= k) a[k] -= aj * lkj;
     }
   }
   if ((threadIdx.x & 31) < LQ) {
@@ -358,10 +397,25 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
   if (blockIdx.x > 0 && nr == 0) return;
   const int tid = threadIdx.x, warp = tid >> 5;
   T* P = L + F.l_off;
-  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
-    const int i = e % PANEL_NB, j = e / PANEL_NB;
-    D[i + j * LLD] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
-    A[i + j * LLD] = (i < nr && j < w) ? P[(r0 + i) + (size_t) (kb + j) * f] : T(0);
+  // the two blocks, LB entries of each per thread in flight at a time (a
+  // loop that stores each entry before loading the next waits one memory
+  // latency per entry)
+  constexpr int LB = sizeof(T) == 4 ? 16 : 8, NE = PANEL_NB * PANEL_NB / 128;
+#pragma unroll 1
+  for (int t0 = 0; t0 < NE; t0 += LB) {
+    T dv[LB], av[LB];
+#pragma unroll
+    for (int t = 0; t < LB; t++) {
+      const int e = tid + 128 * (t0 + t), i = e % PANEL_NB, j = e / PANEL_NB;
+      dv[t] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
+      av[t] = (i < nr && j < w) ? P[(r0 + i) + (size_t) (kb + j) * f] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < LB; t++) {
+      const int e = tid + 128 * (t0 + t), i = e % PANEL_NB, j = e / PANEL_NB;
+      D[i + j * LLD] = dv[t];
+      A[i + j * LLD] = av[t];
+    }
   }
   __syncthreads();
   // thread -> the row it carries: threads 0-63 the slab's rows, threads 64..
@@ -419,13 +473,15 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
   }
   if (blockIdx.x == 0) {
     T* Dk = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
-    for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
-      const int i = e % PANEL_NB, j = e / PANEL_NB;
+#pragma unroll 8
+    for (int t = 0; t < NE; t++) {
+      const int e = tid + 128 * t, i = e % PANEL_NB, j = e / PANEL_NB;
       Dk[e] = (i >= j && i < w) ? D[i + j * LLD] : T(0);
     }
   }
-  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
-    const int i = e % PANEL_NB, j = e / PANEL_NB;
+#pragma unroll 8
+  for (int t = 0; t < NE; t++) {
+    const int e = tid + 128 * t, i = e % PANEL_NB, j = e / PANEL_NB;
     if (i < nr && j < w) P[(r0 + i) + (size_t) (kb + j) * f] = A[i + j * LLD];
   }
   if (sizeof(T) == 4 && sp != nullptr && F.sp_off >= 0) {
@@ -495,8 +551,9 @@ k_dinv(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts, T
   T* P = L + F.l_off;
   T* Di = Dinv + F.dinv_off + (size_t) bl.b * PANEL_NB * PANEL_NB;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  for (int e = tid; e < PANEL_NB * PANEL_NB; e += 128) {
-    const int i = e % PANEL_NB, j = e / PANEL_NB;
+#pragma unroll 8
+  for (int t = 0; t < PANEL_NB * PANEL_NB / 128; t++) {
+    const int e = tid + 128 * t, i = e % PANEL_NB, j = e / PANEL_NB;
     const T v = (i < w && j < w && i >= j) ? Di[e] : (i == j ? T(1) : T(0));
     S[i + j * LLD] = v;
     X[i + j * LLD] = T(0);

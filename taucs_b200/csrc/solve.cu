@@ -453,12 +453,24 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
   if (diag) {
     // staged now, off the chain's critical path
     const T* Di = Dinv + F.dinv_off + (size_t) r * BR * BR;
-    for (int e = tid; e < BR * BR; e += 128) {
-      const int i = e % BR, j = e / BR;
-      T v = 0.0;
-      if (j < bw && i < nr) v = (i < bw) ? (i >= j ? Di[i + j * BR] : T(0)) : P[(r0 + i) + (size_t) (r0 + j) * f];
-      dg[j][i] = v;
-      if (CHAIN && r > 0) mx[j][i] = (i < nr) ? P[(r0 + i) + (size_t) (r0 - BR + j) * f] : T(0);
+    // 16 entries of each tile per thread in flight before they are stored
+#pragma unroll 1
+    for (int t0 = 0; t0 < BR * BR / 128; t0 += 16) {
+      T dv[16], mv[16];
+#pragma unroll
+      for (int t = 0; t < 16; t++) {
+        const int e = tid + 128 * (t0 + t), i = e % BR, j = e / BR;
+        T v = 0.0;
+        if (j < bw && i < nr) v = (i < bw) ? (i >= j ? Di[i + j * BR] : T(0)) : P[(r0 + i) + (size_t) (r0 + j) * f];
+        dv[t] = v;
+        mv[t] = (CHAIN && r > 0 && i < nr) ? P[(r0 + i) + (size_t) (r0 - BR + j) * f] : T(0);
+      }
+#pragma unroll
+      for (int t = 0; t < 16; t++) {
+        const int e = tid + 128 * (t0 + t), i = e % BR, j = e / BR;
+        dg[j][i] = dv[t];
+        if (CHAIN && r > 0) mx[j][i] = mv[t];
+      }
     }
   }
   if (CHAIN && r > 0) {
@@ -933,9 +945,20 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T* z = W + F.v_off * WS + s + i0;
   const T* P = L + F.l_off + s + i0;
-  for (int e = threadIdx.x; e < NQ * SOLVE_RCH; e += 128) {
-    const int i = e % SOLVE_RCH, q = e / SOLVE_RCH;
-    zs[q][i] = (i < nr && q < nrhs) ? __ldcg(z + i + (size_t) q * f) : T(0);
+  // all of this thread's loads in flight before its first store
+  {
+    constexpr int NZ = NQ * SOLVE_RCH / 128;
+    T zv[NZ];
+#pragma unroll
+    for (int t = 0; t < NZ; t++) {
+      const int e = threadIdx.x + 128 * t, i = e % SOLVE_RCH, q = e / SOLVE_RCH;
+      zv[t] = (i < nr && q < nrhs) ? __ldcg(z + i + (size_t) q * f) : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < NZ; t++) {
+      const int e = threadIdx.x + 128 * t;
+      zs[e / SOLVE_RCH][e % SOLVE_RCH] = zv[t];
+    }
   }
   __syncthreads();
   for (int cg = warp * 16; cg < warp * 16 + 16; cg += G) {
@@ -996,9 +1019,19 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 
   // stage the block's inverse now, off the chain's critical path
   const T* Di = Dinv + F.dinv_off + (size_t) k * BR * BR;
-  for (int e = tid; e < BR * BR; e += 128) {
-    const int i = e % BR, c = e / BR;
-    dgb[i][c] = (i < bw && c < bw && i >= c) ? Di[i + c * BR] : T(0);
+#pragma unroll 1
+  for (int t0 = 0; t0 < BR * BR / 128; t0 += 16) {
+    T dv[16];
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      const int e = tid + 128 * (t0 + t), i = e % BR, c = e / BR;
+      dv[t] = (i < bw && c < bw && i >= c) ? Di[i + c * BR] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      const int e = tid + 128 * (t0 + t);
+      dgb[e % BR][e / BR] = dv[t];
+    }
   }
   for (int e = tid; e < BR * NQ; e += 128) {
     const int c = e % BR, q = e / BR;
@@ -1053,9 +1086,19 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
     // for x_j (measured faster than the warp-level loop below at 8 columns)
     for (int j = nbs - 1; j > k; j--) {
       const int bwj = min(BR, s - j * BR);
-      for (int e = tid; e < BR * BR; e += 128) {
-        const int i = e % BR, c = e / BR;
-        tile[c][i] = (i < bwj && c < bw) ? P[(j * BR + i) + (size_t) (c0 + c) * f] : 0.0;
+#pragma unroll 1
+      for (int t0 = 0; t0 < BR * BR / 128; t0 += 16) {
+        T tv[16];
+#pragma unroll
+        for (int t = 0; t < 16; t++) {
+          const int e = tid + 128 * (t0 + t), i = e % BR, c = e / BR;
+          tv[t] = (i < bwj && c < bw) ? P[(j * BR + i) + (size_t) (c0 + c) * f] : T(0);
+        }
+#pragma unroll
+        for (int t = 0; t < 16; t++) {
+          const int e = tid + 128 * (t0 + t);
+          tile[e / BR][e % BR] = tv[t];
+        }
       }
       wait_epoch(flags + F.blk_off + j, epoch, status);
       for (int e = tid; e < BR * NQ; e += 128) {
