@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="duration of the Poisson request stream at 2000 req/s (the configuration's 60 s)")
-    ap.add_argument("--split-format", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--split-format", type=int, default=1, choices=[0, 1],
                     help="operand format of the FP32 fronts' tensor-core products: 0 TF32x3, 1 FP16x3")
     ap.add_argument("--refinement", type=int, default=0, choices=[0, 1],
                     help="0 refinement steps (PCG on stall), 1 PCG on the FP32 factor from the first step")

@@ -266,9 +266,9 @@ int taucs_b200_set_pcg(void* L, int maxits);
  * back to an FP64 refactorization when it does not reach the tolerance. */
 int taucs_b200_set_refinement(void* L, int method);
 /* Operand format of the FP32 fronts' tensor-core products (no counterpart
- * in the reference): 0 (default) TF32 hi + lo parts, three TF32 MMAs per
- * product; 1 FP16 hi + lo parts (lo scaled by 2^11), three FP16 MMAs at
- * twice the TF32 rate.  Both keep about 21 bits of every operand; the FP16
+ * in the reference): 0 TF32 hi + lo parts, three TF32 MMAs per product;
+ * 1 (default) FP16 hi + lo parts (lo scaled by 2^11), three FP16 MMAs at
+ * twice the TF32 rate and half the operand bytes.  Both keep about 21 bits of every operand; the FP16
  * form relies on the diagonal scaling of the FP32 fronts, which bounds every
  * factor entry by 1 in magnitude. */
 int taucs_b200_set_split_format(void* L, int fmt);

@@ -40,7 +40,7 @@ struct Factor {
   // FP32 fronts (precision 1) and iterative refinement
   float* dL32 = nullptr;
   float* dSp32 = nullptr;      // split arena: split copies of a level's panels (Plan::sp_len)
-  int sp_fmt = 0;              // split format of the tensor-core products: 0 TF32 x3, 1 FP16 x3
+  int sp_fmt = 1;              // split format of the tensor-core products: 0 TF32 x3, 1 FP16 x3
   float* dU32 = nullptr;
   float* dDinv32 = nullptr;
   float* dA32 = nullptr;       // scaled values D A D in FP32

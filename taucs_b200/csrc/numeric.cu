@@ -213,8 +213,8 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
   if (panel) {
     // A's entries of the tile's columns: thread (column c, slot q) takes the
     // column's entries q, q + 8, ... -- the loads of all slots in flight at
-    // once; threads of one column serialize their adds through the barrier
-    // rounds (the entries of one column are distinct rows)
+    // once; the adds are atomic, as a column may list a row more than once
+    // (duplicates are summed)
     const int c = tid % BUILD_TC, q = tid / BUILD_TC;
     constexpr int NQS = 256 / BUILD_TC;
     int e = 0, e1 = 0;
@@ -224,7 +224,7 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     }
     for (; e < e1; e += NQS) {
       const int r = __ldg(a_rows + e) - R0;
-      if (r >= 0 && r < nr) W[r + c * BUILD_TR] += __ldg(vals + __ldg(a_idx + e));
+      if (r >= 0 && r < nr) atomicAdd(&W[r + c * BUILD_TR], __ldg(vals + __ldg(a_idx + e)));
     }
     __syncthreads();
   }
@@ -338,6 +338,31 @@ __device__ __forceinline__ void warp_inv16_rows(const T (&a)[LQ], T* Y) {
   }
 }
 
+// One step j of the warp Cholesky below, unrolled through the recursion so
+// that every index into the row held in registers is a constant (a loop the
+// compiler leaves rolled would index the row by the loop variable and keep
+// it in local memory): the pivot by shuffle, the scaled column, and the
+// right-looking update of the columns right of j.
+template <typename T, int J>
+struct CholStep {
+  __device__ __forceinline__ static void run(T (&a)[LQ], int i, int& bad) {
+    const T d = __shfl_sync(0xffffffffu, a[J], J);
+    if (!(d > T(0)) && bad < 0) bad = J;
+    const T r = rsqrt_t(d);
+    a[J] = (i == J) ? d * r : a[J] * r;
+#pragma unroll
+    for (int k = J + 1; k < LQ; k++) {
+      const T lkj = __shfl_sync(0xffffffffu, a[J], k);
+      if (i >= k) a[k] -= a[J] * lkj;
+    }
+    CholStep<T, J + 1>::run(a, i, bad);
+  }
+};
+template <typename T>
+struct CholStep<T, LQ> {
+  __device__ __forceinline__ static void run(T (&)[LQ], int, int&) {}
+};
+
 // One warp: Cholesky of the 16x16 block S (ld LLD, lower part) in place and
 // its inverse into Y.  Lanes 0-15 hold one row each (lanes 16-31 repeat
 // them); the right-looking updates broadcast L[k][j] by shuffles, and the
@@ -350,25 +375,7 @@ __device__ __forceinline__ int warp_chol_inv16(T* S, T* Y) {
 #pragma unroll
   for (int k = 0; k < LQ; k++) a[k] = (k <= i) ? S[i + k * LLD] : T(0);
   int bad = -1;
-  // column j is picked out of a[] by selects, not by a[j]: the compiler
-  // does not unroll this loop, and an array indexed by the loop variable
-  // would live in local memory, one access per step of the serial chain
-#pragma unroll 1
-  for (int j = 0; j < LQ; j++) {
-    T aj = T(0);
-#pragma unroll
-    for (int k = 0; k < LQ; k++) aj = (k == j) ? a[k] : aj;
-    const T d = __shfl_sync(0xffffffffu, aj, j);
-    if (!(d > T(0)) && bad < 0) bad = j;
-    const T r = rsqrt_t(d);
-    aj = (i == j) ? d * r : aj * r;
-#pragma unroll
-    for (int k = 0; k < LQ; k++) {
-      const T lkj = __shfl_sync(0xffffffffu, aj, k);
-      if (k == j) a[k] = aj;
-      else if (k > j && i >= k) a[k] -= aj * lkj;
-    }
-  }
+  CholStep<T, 0>::run(a, i, bad);
   if ((threadIdx.x & 31) < LQ) {
 #pragma unroll
     for (int k = 0; k < LQ; k++)

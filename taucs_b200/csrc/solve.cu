@@ -73,17 +73,37 @@ __device__ void fwd_small(const FrontDesc& F, const FrontDesc* __restrict__ fron
       T v[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && lane < bw) ? Wf[jb + lane + q * f] : T(0);
-      for (int j = 0; j < bw; j++) {
-        const T rj = __shfl_sync(0xffffffffu, rd, j);
-        const T l = (lane > j && lane < bw) ? P[(jb + lane) + (size_t) (jb + j) * f] : T(0);
+      // this lane's row of the block in pieces of 8 columns, the next piece
+      // loaded while the chain runs through the current one
+      T lr[8], ln[8];
+      auto load_row = [&](T (&d)[8], int j0) {
 #pragma unroll
-        for (int q = 0; q < SOLVE_NRHS; q++) {
-          if (q < nrhs) {
-            const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
-            if (lane == j) v[q] = xj;
-            else v[q] -= l * xj;
+        for (int jj = 0; jj < 8; jj++) {
+          const int j = j0 + jj;
+          d[jj] = (j < bw && lane > j && lane < bw) ? P[(jb + lane) + (size_t) (jb + j) * f] : T(0);
+        }
+      };
+      load_row(lr, 0);
+#pragma unroll 1
+      for (int j0 = 0; j0 < bw; j0 += 8) {
+        if (j0 + 8 < bw) load_row(ln, j0 + 8);
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+          const int j = j0 + jj;
+          if (j < bw) {
+            const T rj = __shfl_sync(0xffffffffu, rd, j);
+#pragma unroll
+            for (int q = 0; q < SOLVE_NRHS; q++) {
+              if (q < nrhs) {
+                const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
+                if (lane == j) v[q] = xj;
+                else v[q] -= lr[jj] * xj;
+              }
+            }
           }
         }
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) lr[jj] = ln[jj];
       }
       if (lane < bw) {
 #pragma unroll
@@ -99,11 +119,17 @@ __device__ void fwd_small(const FrontDesc& F, const FrontDesc* __restrict__ fron
       T acc[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
-      for (int j = 0; j < bw; j++) {
-        const T l = P[r + (size_t) (jb + j) * f];
+      // 16 entries of the row in flight at a time
+#pragma unroll 1
+      for (int j0 = 0; j0 < SB; j0 += 16) {
+        T lr[16];
 #pragma unroll
-        for (int q = 0; q < SOLVE_NRHS; q++)
-          if (q < nrhs) acc[q] += l * xs[j][q];
+        for (int jj = 0; jj < 16; jj++) lr[jj] = (j0 + jj < bw) ? P[r + (size_t) (jb + j0 + jj) * f] : T(0);
+#pragma unroll
+        for (int jj = 0; jj < 16; jj++)
+#pragma unroll
+          for (int q = 0; q < SOLVE_NRHS; q++)
+            if (q < nrhs) acc[q] += lr[jj] * xs[j0 + jj][q];
       }
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++)
@@ -202,17 +228,38 @@ __device__ void bwd_small(const FrontDesc& F, const int* __restrict__ rows, cons
       T v[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && lane < bw) ? Wf[jb + lane + q * f] : T(0);
-      for (int j = bw - 1; j >= 0; j--) {
-        const T rj = __shfl_sync(0xffffffffu, rd, j);
-        const T l = (lane < j) ? P[(jb + j) + (size_t) (jb + lane) * f] : T(0);
+      // this lane's column of the block (L[j][lane], j > lane) in pieces of
+      // 8 rows from the last, the next piece loaded during the current one
+      T lc[8], ln[8];
+      auto load_col = [&](T (&d)[8], int j0) {
 #pragma unroll
-        for (int q = 0; q < SOLVE_NRHS; q++) {
-          if (q < nrhs) {
-            const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
-            if (lane == j) v[q] = xj;
-            else v[q] -= l * xj;
+        for (int jj = 0; jj < 8; jj++) {
+          const int j = j0 + jj;
+          d[jj] = (j >= 0 && j < bw && lane < j) ? P[(jb + j) + (size_t) (jb + lane) * f] : T(0);
+        }
+      };
+      const int jtop = ((bw - 1) / 8) * 8;
+      load_col(lc, jtop);
+#pragma unroll 1
+      for (int j0 = jtop; j0 >= 0; j0 -= 8) {
+        if (j0 > 0) load_col(ln, j0 - 8);
+#pragma unroll
+        for (int jj = 7; jj >= 0; jj--) {
+          const int j = j0 + jj;
+          if (j < bw) {
+            const T rj = __shfl_sync(0xffffffffu, rd, j);
+#pragma unroll
+            for (int q = 0; q < SOLVE_NRHS; q++) {
+              if (q < nrhs) {
+                const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
+                if (lane == j) v[q] = xj;
+                else v[q] -= lc[jj] * xj;
+              }
+            }
           }
         }
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) lc[jj] = ln[jj];
       }
       if (lane < bw) {
 #pragma unroll
