@@ -166,6 +166,10 @@ struct Plan {
   std::vector<uint8_t> gemm_choice[2];
 };
 
+// words of the solve's handshake array: a chain flag and a partial-sum flag
+// per 64-row block, and a walk progress word per front
+inline size_t solve_flag_words(const Plan& P) { return 2 * (size_t) P.n_blk + P.fronts.size(); }
+
 int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, Plan* P);
 
 }  // namespace tb

@@ -125,11 +125,15 @@ __device__ void fwd_small(const FrontDesc& F, const FrontDesc* __restrict__ fron
         T lr[16];
 #pragma unroll
         for (int jj = 0; jj < 16; jj++) lr[jj] = (j0 + jj < bw) ? P[r + (size_t) (jb + j0 + jj) * f] : T(0);
+        // rows of xs at or past bw hold stale values (possibly not numbers):
+        // skipped, not multiplied by zero
 #pragma unroll
         for (int jj = 0; jj < 16; jj++)
+          if (j0 + jj < bw) {
 #pragma unroll
-          for (int q = 0; q < SOLVE_NRHS; q++)
-            if (q < nrhs) acc[q] += lr[jj] * xs[j0 + jj][q];
+            for (int q = 0; q < SOLVE_NRHS; q++)
+              if (q < nrhs) acc[q] += lr[jj] * xs[j0 + jj][q];
+          }
       }
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++)
@@ -443,6 +447,22 @@ __device__ void wait_epoch(const int* flag, int epoch, int* status) {
   __syncthreads();
 }
 
+// A walk's progress word holds (epoch << 12) | blocks published.  Polls it
+// until at least count blocks of this epoch are published and returns the
+// number published (count itself after giving up, with SOLVE_TIMEOUT set).
+__device__ __forceinline__ int poll_progress(const int* p, int epoch, int count, int* status) {
+  const int want = ((epoch + g_solve_wait_skew) << 12) | count, limit = g_solve_wait_limit;
+  int it = 0, v;
+  while ((v = ld_acquire(p)) < want) {
+    if (++it > limit || ((it & 1023) == 0 && *(volatile int*) status == SOLVE_TIMEOUT)) {
+      atomicExch(status, SOLVE_TIMEOUT);
+      return count;
+    }
+    __nanosleep(32);
+  }
+  return v & 4095;
+}
+
 // Forward solve of big fronts.  Diagonal block r of L11 gives
 // y_r = L_rr^-1 (w_r - sum_{k<r} L_rk y_k), chained to block r-1 by
 // release/acquire flags; update rows i get w_i - sum_k L_ik y_k.
@@ -741,13 +761,61 @@ constexpr size_t bwalk_smem() {
   return (WALK_T * BR * (BR + 1) + WALK_T * BR * (SOLVE_NRHS + 1)) * sizeof(T);
 }
 
+// The far terms of a walk's helper: blocks t = 0 .. n-1 of the chain in the
+// order the walker publishes them (its progress counts them), each adding
+// acc[q] += sum_jj load_l(t, jj) ys[qg * 16 + jj][q] with ys[i][q] =
+// load_y(t, i, q).  Every round takes all published blocks not used yet, up
+// to WALK_HB, and issues all of their loads before any waits.
+constexpr int WALK_HB = 4;
+template <typename T, int NQ, typename LoadL, typename LoadY>
+__device__ __forceinline__ void walk_far_terms(const int* prog, int epoch, int* status, int n, LoadL load_l,
+                                               LoadY load_y, T (*ysb)[BR][NQ], T (&acc)[NQ], int qg) {
+  __shared__ int avail_s;
+  constexpr int NY = WALK_HB * BR * NQ / 256;
+  int avail = 0;
+  for (int t = 0; t < n;) {
+    if (t >= avail) {
+      if (threadIdx.x == 0) avail_s = poll_progress(prog, epoch, t + 1, status);
+      __syncthreads();
+      avail = max(min(avail_s, n), t + 1);
+    }
+    const int nb = min(avail - t, WALK_HB);
+    T lv[WALK_HB][BR / 4];
+#pragma unroll
+    for (int b = 0; b < WALK_HB; b++)
+#pragma unroll
+      for (int jj = 0; jj < BR / 4; jj++) lv[b][jj] = (b < nb) ? load_l(t + b, jj) : T(0);
+    T yv[NY];
+#pragma unroll
+    for (int u = 0; u < NY; u++) {
+      const int e = threadIdx.x + 256 * u, b = e / (BR * NQ), i = e % BR, q = (e / BR) % NQ;
+      yv[u] = (b < nb) ? load_y(t + b, i, q) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < NY; u++) {
+      const int e = threadIdx.x + 256 * u;
+      ysb[e / (BR * NQ)][e % BR][(e / BR) % NQ] = yv[u];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < WALK_HB; b++)
+      if (b < nb)
+#pragma unroll
+        for (int jj = 0; jj < BR / 4; jj++)
+#pragma unroll
+          for (int q = 0; q < NQ; q++) acc[q] += lv[b][jj] * ysb[b][qg * (BR / 4) + jj][q];
+    __syncthreads();
+    t += nb;
+  }
+}
+
 template <typename T, int WS>
 __global__ void __launch_bounds__(256)
 k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
            const FrontDesc* __restrict__ fronts, const int* __restrict__ children, const int* __restrict__ maps,
            const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ Dinv,
            const T* __restrict__ B, int ldb, T* __restrict__ W, T* __restrict__ fpart, int nrhs,
-           int* __restrict__ flags, int* __restrict__ pflags, int epoch, int* status) {
+           int* __restrict__ flags, int* __restrict__ pflags, int* __restrict__ progress, int epoch, int* status) {
   constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
   static_assert(NQ % 4 == 0, "four thread groups share the right-hand sides");
   extern __shared__ __align__(16) unsigned char wsm[];
@@ -757,7 +825,8 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   const int row = tid % BR, qg = tid / BR;
   if (blockIdx.x < nwalk) {
     // ---------------------------------------------------------------- walker
-    const FrontDesc F = fronts[walk_fronts[blockIdx.x]];
+    const int fi = walk_fronts[blockIdx.x];
+    const FrontDesc F = fronts[fi];
     const int f = F.f, s = F.s, nbs = (s + BR - 1) / BR;
     const T* P = L + F.l_off;
     T* Wf = W + F.v_off * WS;
@@ -863,9 +932,13 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         Wf[r0 + i + (size_t) q * f] = yr[slot][i][q];
       }
       // the barrier orders every thread's stores before the release, and
-      // every read of this step's tiles and p before they are replaced
+      // every read of this step's tiles and p before they are replaced; the
+      // block's own flag is for the update-row blocks of the next launch
       __syncthreads();
-      if (tid == 0) st_release(flags + F.blk_off + r, epoch);
+      if (tid == 0) {
+        flags[F.blk_off + r] = epoch;
+        st_release(progress + fi, (epoch << 12) | (r + 1));
+      }
       if (r + 1 < nbs) {
         put();
         load_p(r + 1);   // thread 32 polls while thread 0 releases
@@ -881,18 +954,9 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   const T* P = L + F.l_off;
   const T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
-  T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);   // [4], then ys
-  T (*ys)[NQ] = red[4];
-  // this thread's 16 columns of the first far block, loaded before anything
-  // waits
+  T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);            // [4]
+  T (*ysb)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm) + 4;         // [WALK_HB]
   const int kend = max(r - WALK_D, 0);
-  T lv[BR / 4];
-  auto load_l = [&](int k) {
-    const T* pc = P + (r0 + row) + (size_t) (k * BR + qg * (BR / 4)) * f;
-#pragma unroll
-    for (int j = 0; j < BR / 4; j++) lv[j] = (row < nr) ? pc[(size_t) j * f] : T(0);
-  };
-  if (kend > 0) load_l(0);
   for (int k = tid; k < BR * NQ; k += 256) {
     const int i = k % BR, q = k / BR;
     pv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : T(0);
@@ -918,25 +982,20 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     __syncthreads();
   }
   // far terms k < r - WALK_D: thread (row, quarter qg) sums 16 columns of
-  // each L_rk for every right-hand side, the y_k arriving as the walker
-  // publishes them
+  // each L_rk for every right-hand side.  The helper reads the walker's
+  // progress and takes every published block it has not used yet, up to
+  // WALK_HB per round with all their loads in flight at once, so a helper
+  // that fell behind catches up in few rounds.
   T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
-  for (int k = 0; k < kend; k++) {
-    wait_epoch(flags + F.blk_off + k, epoch, status);
-    for (int e = tid; e < BR * NQ; e += 256) {
-      const int j = e % BR, q = e / BR;
-      ys[j][q] = (q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : T(0);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < BR / 4; j++)
-#pragma unroll
-      for (int q = 0; q < NQ; q++) acc[q] += lv[j] * ys[qg * (BR / 4) + j][q];
-    if (k + 1 < kend) load_l(k + 1);
-    __syncthreads();
-  }
+  walk_far_terms<T, NQ>(
+      progress + bk.a, epoch, status, kend,
+      [&](int k, int jj) -> T {
+        return (row < nr) ? P[(r0 + row) + (size_t) (k * BR + qg * (BR / 4) + jj) * f] : T(0);
+      },
+      [&](int k, int j, int q) -> T { return (q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : T(0); }, ysb,
+      acc, qg);
 #pragma unroll
   for (int q = 0; q < NQ; q++) red[qg][row][q] = acc[q];
   __syncthreads();
@@ -1257,7 +1316,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
            const FrontDesc* __restrict__ fronts, const int* __restrict__ rows, const T* __restrict__ L,
            const T* __restrict__ Dinv, T* __restrict__ X, int ldx, T* __restrict__ W,
            const T* __restrict__ part, T* __restrict__ bpart, int nrhs, int* __restrict__ flags,
-           int* __restrict__ pflags, int epoch, int* status) {
+           int* __restrict__ pflags, int* __restrict__ progress, int epoch, int* status) {
   constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
   extern __shared__ __align__(16) unsigned char wsm[];
   __shared__ T pv[BR][NQ + 1];
@@ -1265,7 +1324,8 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   const int col = tid % BR, qg = tid / BR;
   if (blockIdx.x < nwalk) {
     // ---------------------------------------------------------------- walker
-    const FrontDesc F = fronts[walk_fronts[blockIdx.x]];
+    const int fi = walk_fronts[blockIdx.x];
+    const FrontDesc F = fronts[fi];
     const int f = F.f, s = F.s, nbs = (s + BR - 1) / BR;
     const T* P = L + F.l_off;
     T* Wf = W + F.v_off * WS;
@@ -1357,7 +1417,10 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
       // the barrier orders every thread's stores before the release, and
       // every read of this step's tiles and p before they are replaced
       __syncthreads();
-      if (tid == 0) st_release(flags + F.blk_off + k, epoch);
+      if (tid == 0) {
+        flags[F.blk_off + k] = epoch;
+        st_release(progress + fi, (epoch << 12) | (nbs - k));
+      }
       if (k > 0) {
         put();
         load_p(k - 1);   // thread 32 polls while thread 0 releases
@@ -1373,19 +1436,9 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   const int c0 = k * BR, bw = min(BR, s - c0);
   const T* P = L + F.l_off;
   const T* Wf = W + F.v_off * WS;
-  T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);   // [4], then ys
-  T (*ys)[NQ] = red[4];
+  T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);            // [4]
+  T (*ysb)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm) + 4;         // [WALK_HB]
   const int jlo = k + WALK_D + 1;   // far blocks j = nbs-1 .. jlo
-  // this thread's 16 rows of column c0 + col of the first far block, loaded
-  // before anything waits
-  T lv[BR / 4];
-  auto load_l = [&](int j) {
-    const int bwj = min(BR, s - j * BR);
-    const T* pc = P + (size_t) (c0 + col) * f + j * BR + qg * (BR / 4);
-#pragma unroll
-    for (int t = 0; t < BR / 4; t++) lv[t] = (col < bw && qg * (BR / 4) + t < bwj) ? __ldg(pc + t) : T(0);
-  };
-  if (nbs - 1 >= jlo) load_l(nbs - 1);
   // v_k = y_k - L21^T x2, the chunk partial sums added in chunk order
   for (int e = tid; e < BR * NQ; e += 256) {
     const int c = e % BR, q = e / BR;
@@ -1399,24 +1452,22 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     }
     pv[c][q] = v;
   }
+  // far terms: blocks j = nbs-1 down to jlo, taken as the walker publishes
+  // them (block t of the helper's order is j = nbs-1-t)
   T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
-  for (int j = nbs - 1; j >= jlo; j--) {
-    const int bwj = min(BR, s - j * BR);
-    wait_epoch(flags + F.blk_off + j, epoch, status);
-    for (int e = tid; e < BR * NQ; e += 256) {
-      const int i = e % BR, q = e / BR;
-      ys[i][q] = (i < bwj && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : T(0);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int t = 0; t < BR / 4; t++)
-#pragma unroll
-      for (int q = 0; q < NQ; q++) acc[q] += lv[t] * ys[qg * (BR / 4) + t][q];
-    if (j - 1 >= jlo) load_l(j - 1);
-    __syncthreads();
-  }
+  walk_far_terms<T, NQ>(
+      progress + bk.a, epoch, status, max(nbs - jlo, 0),
+      [&](int t, int tt) -> T {
+        const int j = nbs - 1 - t, i = qg * (BR / 4) + tt;
+        return (col < bw && i < min(BR, s - j * BR)) ? __ldg(P + (size_t) (c0 + col) * f + j * BR + i) : T(0);
+      },
+      [&](int t, int i, int q) -> T {
+        const int j = nbs - 1 - t;
+        return (i < min(BR, s - j * BR) && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : T(0);
+      },
+      ysb, acc, qg);
 #pragma unroll
   for (int q = 0; q < NQ; q++) red[qg][col][q] = acc[q];
   __syncthreads();
@@ -1497,8 +1548,8 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
   solve_attrs<T>();
   // the handshake flags restart from zero on every call, so the epochs of a
   // call are always 1, 2, ... and a recorded launch sequence stays valid
-  // (the second half: the forward walk's partial-sum flags)
-  cudaMemsetAsync(flags, 0, 2 * sizeof(int) * (size_t) P.n_blk, st);
+  // (with the walks' partial-sum flags and progress words)
+  cudaMemsetAsync(flags, 0, sizeof(int) * solve_flag_words(P), st);
   const int np = D.n_pers;
   if (np > 0) cudaMemsetAsync(D.pers_solve, 0, sizeof(int) * (size_t) (2 * np + 2), st);
   int ep = 0;
@@ -1551,11 +1602,11 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         auto run = [&](auto nqc) {
           constexpr int Q = decltype(nqc)::value;
           if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
-            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS) {
+            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR) {
             const int nbig = (int) LP.big_fronts.size();
             k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, 256, walk_smem<T>(), st>>>(
                 D.big_list + D.big_off[h], nbig, bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W,
-                part + P.fpart_off, nq, flags, flags + P.n_blk, ef, status);
+                part + P.fpart_off, nq, flags, flags + P.n_blk, flags + 2 * (size_t) P.n_blk, ef, status);
             if (nu)
               k_fwd_big<T, Q, SOLVE_NRHS, FWD_UPD><<<nu, 128, 0, st>>>(bl + nd, D.fronts, D.children, D.maps, D.rows,
                                                                       L, Dinv, Bq, ld, W, nq, flags, ef, status);
@@ -1601,11 +1652,11 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
         if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
-            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS) {
+            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR) {
           const int nbig = (int) LP.big_fronts.size();
           k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, 256, bwalk_smem<T>(), st>>>(
               D.big_list + D.big_off[h], nbig, bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, part + P.fpart_off,
-              nq, flags, flags + P.n_blk, eb, status);
+              nq, flags, flags + P.n_blk, flags + 2 * (size_t) P.n_blk, eb, status);
         } else if (nq <= 2)
           k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 2>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
