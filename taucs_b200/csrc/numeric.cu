@@ -192,12 +192,13 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
         const int* __restrict__ a_idx, const T* __restrict__ vals,
         T* __restrict__ L, T* __restrict__ U, const int* status) {
   __shared__ T W[BUILD_TR * BUILD_TC];
-  __shared__ int rng[4];
+  __shared__ int rng[2][4], cmc[2], cmap[2];
+  __shared__ int64_t cuoff[2];
   if (failed(status)) return;
   const Tile tl = tiles[blockIdx.x];
   const FrontDesc F = fronts[tl.front];
   const int f = F.f, s = F.s, m = f - s;
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
   const bool panel = tl.c0 >= 0;
   int R0, C0, nr, nc;
   if (panel) {
@@ -228,52 +229,70 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     }
     __syncthreads();
   }
-  for (int ci = F.child_begin; ci < F.child_end; ci++) {
-    const FrontDesc C = fronts[children[ci]];
-    const int mc = C.f - C.s;
-    const int* mp = maps + C.map_off;
-    // the child's columns and rows that land in this tile: four warps search
-    // the four bounds at once
-    if (warp < 4) {
-      const int key = warp == 0 ? C0 : warp == 1 ? C0 + nc : warp == 2 ? R0 : R0 + nr;
-      const int r = warp_lower_bound(mp, mc, key);
-      if (lane == 0) rng[warp] = r;
+  // children two at a time: warps 0-3 search the four bounds of the first
+  // (its columns and rows that land in this tile), warps 4-7 those of the
+  // second; then every load of both children's shares is issued before the
+  // first add, and the two children add in child order
+  const int nch = F.child_end - F.child_begin;
+  for (int c0 = 0; c0 < nch; c0 += 2) {
+    const int two = min(2, nch - c0);
+    {
+      const int cc = warp >> 2, wb = warp & 3;
+      if (cc < two) {
+        const FrontDesc C = fronts[children[F.child_begin + c0 + cc]];
+        const int key = wb == 0 ? C0 : wb == 1 ? C0 + nc : wb == 2 ? R0 : R0 + nr;
+        const int r = warp_lower_bound(maps + C.map_off, C.f - C.s, key);
+        if (lane == 0) rng[cc][wb] = r;
+        if (wb == 0 && lane == 0) {
+          cmc[cc] = C.f - C.s;
+          cmap[cc] = C.map_off;
+          cuoff[cc] = C.u_off;
+        }
+      }
     }
     __syncthreads();
-    const int ja = rng[0], jb = rng[1], ia = rng[2], ib = rng[3];
-    __syncthreads();
-    if (ja >= jb || ia >= ib) continue;
     // warp w takes the child's columns ja + w + 8u, lane l its rows
-    // ia + l + 32v: every load of the tile's share is issued before the first
-    // add (the children's update matrices were written by earlier launches)
-    const T* Uc = U + C.u_off;
+    // ia + l + 32v (the children's update matrices were written by earlier
+    // launches)
     constexpr int JU = (BUILD_TC + 7) / 8, IU = BUILD_TR / 32;
-    int pi[IU], pj[JU];
-    T val[JU][IU];
+    int pi[2][IU], pj[2][JU];
+    T val[2][JU][IU];
 #pragma unroll
-    for (int v = 0; v < IU; v++) {
-      const int i = ia + lane + 32 * v;
-      pi[v] = (i < ib) ? __ldg(mp + i) - R0 : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < JU; u++) {
-      const int j = ja + warp + 8 * u;
-      const bool jv = j < jb;
-      pj[u] = jv ? (__ldg(mp + j) - C0) * BUILD_TR : -1;
+    for (int cc = 0; cc < 2; cc++) {
+      const int ja = rng[cc][0], jb = rng[cc][1], ia = rng[cc][2], ib = rng[cc][3];
+      const bool live = cc < two && ja < jb && ia < ib;
+      const int mc = live ? cmc[cc] : 0;
+      const int* mp = maps + (live ? cmap[cc] : 0);
+      const T* Uc = U + (live ? cuoff[cc] : 0);
 #pragma unroll
       for (int v = 0; v < IU; v++) {
         const int i = ia + lane + 32 * v;
-        val[u][v] = (jv && i < ib && i >= j) ? __ldg(Uc + (size_t) j * mc + i) : T(0);
+        pi[cc][v] = (live && i < ib) ? __ldg(mp + i) - R0 : -1;
+      }
+#pragma unroll
+      for (int u = 0; u < JU; u++) {
+        const int j = ja + warp + 8 * u;
+        const bool jv = live && j < jb;
+        pj[cc][u] = jv ? (__ldg(mp + j) - C0) * BUILD_TR : -1;
+#pragma unroll
+        for (int v = 0; v < IU; v++) {
+          const int i = ia + lane + 32 * v;
+          val[cc][u][v] = (jv && i < ib && i >= j) ? __ldg(Uc + (size_t) j * mc + i) : T(0);
+        }
       }
     }
 #pragma unroll
-    for (int u = 0; u < JU; u++)
+    for (int cc = 0; cc < 2; cc++) {
+      const int ja = rng[cc][0], ia = rng[cc][2];
 #pragma unroll
-      for (int v = 0; v < IU; v++) {
-        const int i = ia + lane + 32 * v, j = ja + warp + 8 * u;
-        if (pj[u] >= 0 && pi[v] >= 0 && i >= j) W[pi[v] + pj[u]] += val[u][v];
-      }
-    __syncthreads();
+      for (int u = 0; u < JU; u++)
+#pragma unroll
+        for (int v = 0; v < IU; v++) {
+          const int i = ia + lane + 32 * v, j = ja + warp + 8 * u;
+          if (pj[cc][u] >= 0 && pi[cc][v] >= 0 && i >= j) W[pi[cc][v] + pj[cc][u]] += val[cc][u][v];
+        }
+      __syncthreads();
+    }
   }
   if (panel) {
     T* dst = L + F.l_off;
@@ -299,21 +318,22 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
 // block.  Every CTA of the launch reads the diagonal block as it was before
 // the step, so CTA 0 parks the factored block in the block's slot of the
 // inverse array rather than in the panel; k_dinv moves it into the panel
-// after the factorization and replaces it there by its inverse.  Every CTA factors
-// the 64x64 diagonal block itself -- a redundant Cholesky instead of waiting
-// for the CTA that owns it -- in four 16-column steps: one warp factors the
-// 16x16 diagonal piece and inverts it in registers, then all warps apply it
-// to the rows below, in the diagonal block and in the CTA's own slab (one row
-// per thread), and update the columns to the right.  The inverses of the
-// 64x64 diagonal blocks, which the solve applies, are formed afterwards for
-// all fronts at once (k_dinv).  Nothing reads a diagonal block of the panel
-// between its leaf and k_dinv: the later products read rows below it only.
-constexpr int LLD = PANEL_NB + 4;   // padded column stride of the leaf's blocks in shared memory
+// after the factorization and replaces it there by its inverse.  Every CTA
+// factors the 64x64 diagonal block itself -- a redundant Cholesky instead of
+// waiting for the CTA that owns it.  Each thread holds one row in registers
+// (threads 0-63 the slab's rows, 64-127 the diagonal block's), and the block
+// goes in four 16-column steps: the warp whose lanes hold the piece's rows
+// factors the 16x16 piece by shuffles, every row below it solves against
+// the piece by substitution, and every row updates its columns to the right
+// from the diagonal block's new rows (published row-major in shared memory).
+// The inverses of the 64x64 diagonal blocks, which the solve applies, are
+// formed afterwards for all fronts at once (k_dinv).  Nothing reads a
+// diagonal block of the panel between its leaf and k_dinv: the later
+// products read rows below it only.
+constexpr int LLD = PANEL_NB + 4;   // padded column stride of k_dinv's blocks in shared memory
 constexpr int LQ = 16;              // column step inside a leaf
 constexpr int LYD = LQ + 1;         // column stride of a 16x16 inverse
 
-template <typename T>
-constexpr size_t leaf_smem() { return (2 * PANEL_NB * LLD + LQ * LYD) * sizeof(T); }
 template <typename T>
 constexpr size_t dinv_smem() { return (2 * PANEL_NB * LLD + (PANEL_NB / LQ) * LQ * LYD) * sizeof(T); }
 
@@ -338,61 +358,90 @@ __device__ __forceinline__ void warp_inv16_rows(const T (&a)[LQ], T* Y) {
   }
 }
 
-// One step j of the warp Cholesky below, unrolled through the recursion so
-// that every index into the row held in registers is a constant (a loop the
-// compiler leaves rolled would index the row by the loop variable and keep
-// it in local memory): the pivot by shuffle, the scaled column, and the
-// right-looking update of the columns right of j.
+// One pivot J of the 16x16 warp Cholesky of the leaf, unrolled through the
+// recursion so that every index into the row held in registers is a
+// constant: lane base + i holds row i of the piece (a[k] = L[i][k], k <= i);
+// the pivot comes by shuffle, the column is scaled by rsqrt(pivot), and the
+// columns right of J take the right-looking update.  Lanes outside the piece
+// run along on values that are never written back.
 template <typename T, int J>
 struct CholStep {
-  __device__ __forceinline__ static void run(T (&a)[LQ], int i, int& bad) {
-    const T d = __shfl_sync(0xffffffffu, a[J], J);
+  __device__ __forceinline__ static void run(T (&a)[LQ], int i, int base, int& bad) {
+    const T d = __shfl_sync(0xffffffffu, a[J], base + J);
     if (!(d > T(0)) && bad < 0) bad = J;
     const T r = rsqrt_t(d);
     a[J] = (i == J) ? d * r : a[J] * r;
 #pragma unroll
     for (int k = J + 1; k < LQ; k++) {
-      const T lkj = __shfl_sync(0xffffffffu, a[J], k);
+      const T lkj = __shfl_sync(0xffffffffu, a[J], base + k);
       if (i >= k) a[k] -= a[J] * lkj;
     }
-    CholStep<T, J + 1>::run(a, i, bad);
+    CholStep<T, J + 1>::run(a, i, base, bad);
   }
 };
 template <typename T>
 struct CholStep<T, LQ> {
-  __device__ __forceinline__ static void run(T (&)[LQ], int, int&) {}
+  __device__ __forceinline__ static void run(T (&)[LQ], int, int, int&) {}
 };
 
-// One warp: Cholesky of the 16x16 block S (ld LLD, lower part) in place and
-// its inverse into Y.  Lanes 0-15 hold one row each (lanes 16-31 repeat
-// them); the right-looking updates broadcast L[k][j] by shuffles, and the
-// division of the textbook loop is a multiply by rsqrt(pivot).  Returns the
-// first nonpositive pivot (or -1) in every lane.
-template <typename T>
-__device__ __forceinline__ int warp_chol_inv16(T* S, T* Y) {
-  const int i = threadIdx.x & 15;
-  T a[LQ];
+// The split copy of one slab row for the tensor-core products: chunks of CW
+// columns, hi and lo parts, written for chunk indices [0, nch) of the leaf
+// (columns past w are zero: the front's last leaf pads K to the products'
+// stage width).
+template <int CW>
+__device__ __forceinline__ void leaf_split_row(const float (&rw)[PANEL_NB], int w, int nch, unsigned char* base,
+                                               int64_t part, int64_t kc0, int64_t rg, int r) {
+  constexpr int CMAX = PANEL_NB / CW + 4;
 #pragma unroll
-  for (int k = 0; k < LQ; k++) a[k] = (k <= i) ? S[i + k * LLD] : T(0);
-  int bad = -1;
-  CholStep<T, 0>::run(a, i, bad);
-  if ((threadIdx.x & 31) < LQ) {
+  for (int c = 0; c < CMAX; c++) {
+    if (c >= nch) break;
+    const int64_t o = ((kc0 + c) * rg + (r >> 3)) * 128 + (r & 7) * 16;
+    if (CW == 4) {
+      unsigned h[4], l[4];
 #pragma unroll
-    for (int k = 0; k < LQ; k++)
-      if (k <= i) S[i + k * LLD] = a[k];
+      for (int q = 0; q < 4; q++) {
+        const int k = c * 4 + q;
+        const float x = (k < PANEL_NB && k < w) ? rw[k < PANEL_NB ? k : 0] : 0.0f;
+        h[q] = __float_as_uint(x) & 0xffffe000u;
+        l[q] = __float_as_uint(x - __uint_as_float(h[q]));
+      }
+      *reinterpret_cast<uint4*>(base + o) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(base + part + o) = make_uint4(l[0], l[1], l[2], l[3]);
+    } else {
+      unsigned short h[8], l[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int k = c * 8 + q;
+        const float x = (k < PANEL_NB && k < w) ? rw[k < PANEL_NB ? k : 0] : 0.0f;
+        const __half hh = __float2half_rn(x);
+        h[q] = __half_as_ushort(hh);
+        l[q] = __half_as_ushort(__float2half_rn((x - __half2float(hh)) * 2048.0f));
+      }
+      uint4 vh, vl;
+      vh.x = h[0] | (unsigned) h[1] << 16; vh.y = h[2] | (unsigned) h[3] << 16;
+      vh.z = h[4] | (unsigned) h[5] << 16; vh.w = h[6] | (unsigned) h[7] << 16;
+      vl.x = l[0] | (unsigned) l[1] << 16; vl.y = l[2] | (unsigned) l[3] << 16;
+      vl.z = l[4] | (unsigned) l[5] << 16; vl.w = l[6] | (unsigned) l[7] << 16;
+      *reinterpret_cast<uint4*>(base + o) = vh;
+      *reinterpret_cast<uint4*>(base + part + o) = vl;
+    }
   }
-  if (bad < 0) warp_inv16_rows(a, Y);
-  return bad;
 }
+template <int CW>
+__device__ __forceinline__ void leaf_split_row(const double (&)[PANEL_NB], int, int, unsigned char*, int64_t, int64_t,
+                                               int64_t, int) {}
 
 template <typename T>
 __global__ void __launch_bounds__(128)
 k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
        T* __restrict__ L, T* __restrict__ Dinv, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  T* D = reinterpret_cast<T*>(smraw);   // diagonal block, 64 x 64, ld LLD
-  T* A = D + PANEL_NB * LLD;            // this CTA's slab of rows below it, 64 x 64, ld LLD
-  T* Y = A + PANEL_NB * LLD;            // inverse of the current 16x16 piece, ld LYD
+  // Xt[buf][c][k]: the new L[c][c0 + k] of the diagonal block's rows c below
+  // the current piece (row-major, 16-byte aligned rows, two buffers by piece
+  // parity); Lp, rinv: the factored piece and its reciprocal diagonal
+  constexpr int XLD = sizeof(T) == 4 ? LQ + 4 : LQ + 2;
+  __shared__ __align__(16) T Xt[2][PANEL_NB][XLD];
+  __shared__ T Lp[LQ][LQ + 1];
+  __shared__ T rinv[LQ];
   __shared__ int bad_s;
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.y]];
@@ -402,136 +451,109 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
   const int r0 = kb + w + blockIdx.x * PANEL_NB;
   const int nr = max(0, min(PANEL_NB, f - r0));
   if (blockIdx.x > 0 && nr == 0) return;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // threads 0-63: the slab's rows; threads 64-127: the diagonal block's rows
+  // (identity past w); each thread holds its row's 64 entries in registers
+  const bool is_d = tid >= PANEL_NB;
+  const int i = is_d ? tid - PANEL_NB : tid;
   T* P = L + F.l_off;
-  // the two blocks, LB entries of each per thread in flight at a time (a
-  // loop that stores each entry before loading the next waits one memory
-  // latency per entry)
-  constexpr int LB = sizeof(T) == 4 ? 16 : 8, NE = PANEL_NB * PANEL_NB / 128;
-#pragma unroll 1
-  for (int t0 = 0; t0 < NE; t0 += LB) {
-    T dv[LB], av[LB];
+  T rw[PANEL_NB];
+  {
+    const size_t g = is_d ? (size_t) (kb + i) : (size_t) (r0 + i);
+    const bool rv = is_d ? (i < w) : (i < nr);
 #pragma unroll
-    for (int t = 0; t < LB; t++) {
-      const int e = tid + 128 * (t0 + t), i = e % PANEL_NB, j = e / PANEL_NB;
-      dv[t] = (i < w && j < w && i >= j) ? P[(kb + i) + (size_t) (kb + j) * f] : (i == j ? T(1) : T(0));
-      av[t] = (i < nr && j < w) ? P[(r0 + i) + (size_t) (kb + j) * f] : T(0);
-    }
-#pragma unroll
-    for (int t = 0; t < LB; t++) {
-      const int e = tid + 128 * (t0 + t), i = e % PANEL_NB, j = e / PANEL_NB;
-      D[i + j * LLD] = dv[t];
-      A[i + j * LLD] = av[t];
+    for (int c = 0; c < PANEL_NB; c++) {
+      const bool in = rv && c < w && (!is_d || c <= i);
+      rw[c] = in ? P[g + (size_t) (kb + c) * f] : ((is_d && c == i) ? T(1) : T(0));
     }
   }
-  __syncthreads();
-  // thread -> the row it carries: threads 0-63 the slab's rows, threads 64..
-  // the diagonal block's rows below the current piece
+#pragma unroll
   for (int b = 0; b < PANEL_NB / LQ; b++) {
     const int c0 = b * LQ;
-    if (warp == 0) {
-      const int bd = warp_chol_inv16(D + c0 + c0 * LLD, Y);
-      if (tid == 0) bad_s = bd;
+    // the piece's 16 rows are lanes base .. base + 15 of warp 2 + c0 / 32
+    const int base = c0 % 32;
+    if (warp == 2 + c0 / 32) {
+      const int ii = lane - base;
+      T a[LQ];
+#pragma unroll
+      for (int k = 0; k < LQ; k++) a[k] = (k <= ii) ? rw[c0 + k] : T(0);
+      int bad = -1;
+      CholStep<T, 0>::run(a, ii, base, bad);
+      if (ii >= 0 && ii < LQ) {
+        T dg = T(1);
+#pragma unroll
+        for (int k = 0; k < LQ; k++) {
+          if (k <= ii) rw[c0 + k] = a[k];
+          Lp[ii][k] = (k <= ii) ? a[k] : T(0);
+          if (k == ii) dg = a[k];
+        }
+        rinv[ii] = T(1) / dg;
+      }
+      if (lane == 0) bad_s = bad;
     }
     __syncthreads();
     if (bad_s >= 0) {
       if (tid == 0 && blockIdx.x == 0 && c0 + bad_s < w) atomicMin(status, rows[F.rows_off + kb + c0 + bad_s]);
       return;
     }
-    const int nd = PANEL_NB - c0 - LQ;
-    T* M = nullptr;
-    int r = 0;
-    if (tid < PANEL_NB) {
-      M = A;
-      r = tid;
-    } else if (tid - PANEL_NB < nd) {
-      M = D;
-      r = c0 + LQ + (tid - PANEL_NB);
-    }
+    // rows below the piece: X L_p^T = M by substitution (in registers), the
+    // diagonal block's rows also published for the update below
+    const bool below = !is_d || i >= c0 + LQ;
     T x[LQ];
-    if (M) {
-      // X[r][c] = sum_{k <= c} M[r][c0 + k] Y[c][k], in place in row r
-      T v[LQ];
 #pragma unroll
-      for (int k = 0; k < LQ; k++) v[k] = M[r + (c0 + k) * LLD];
+    for (int c = 0; c < LQ; c++) x[c] = rw[c0 + c];
+    if (below) {
 #pragma unroll
       for (int c = 0; c < LQ; c++) {
-        T acc = T(0);
+        x[c] *= rinv[c];
 #pragma unroll
-        for (int k = 0; k <= c; k++) acc += v[k] * Y[c + k * LYD];
-        x[c] = acc;
+        for (int c2 = c + 1; c2 < LQ; c2++) x[c2] -= x[c] * Lp[c2][c];
       }
 #pragma unroll
-      for (int c = 0; c < LQ; c++) M[r + (c0 + c) * LLD] = x[c];
-    }
-    __syncthreads();   // every row's piece of L is in place before it is read below
-    if (M) {
-      // the columns right of the piece (in D only the lower part):
-      // M[r][c] -= sum_k X[r][k] L[c][c0 + k]
-      const int cend = (M == A) ? PANEL_NB : r + 1;
-      for (int c = c0 + LQ; c < cend; c++) {
-        T acc = M[r + c * LLD];
+      for (int c = 0; c < LQ; c++) rw[c0 + c] = x[c];
+      if (is_d) {
 #pragma unroll
-        for (int k = 0; k < LQ; k++) acc -= x[k] * D[c + (c0 + k) * LLD];
-        M[r + c * LLD] = acc;
+        for (int c = 0; c < LQ; c++) Xt[b & 1][i][c] = x[c];
       }
     }
     __syncthreads();
-  }
-  if (blockIdx.x == 0) {
-    T* Dk = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
-#pragma unroll 8
-    for (int t = 0; t < NE; t++) {
-      const int e = tid + 128 * t, i = e % PANEL_NB, j = e / PANEL_NB;
-      Dk[e] = (i >= j && i < w) ? D[i + j * LLD] : T(0);
+    // the columns right of the piece: rw[c] -= sum_k x[k] L[c][c0 + k] (the
+    // diagonal block's rows also compute their upper part, never read)
+    if (below) {
+#pragma unroll
+      for (int c = c0 + LQ; c < PANEL_NB; c++) {
+        const T* xr = Xt[b & 1][c];
+        T acc = rw[c];
+#pragma unroll
+        for (int k = 0; k < LQ; k++) acc -= x[k] * xr[k];
+        rw[c] = acc;
+      }
     }
   }
-#pragma unroll 8
-  for (int t = 0; t < NE; t++) {
-    const int e = tid + 128 * t, i = e % PANEL_NB, j = e / PANEL_NB;
-    if (i < nr && j < w) P[(r0 + i) + (size_t) (kb + j) * f] = A[i + j * LLD];
+  if (is_d) {
+    if (blockIdx.x == 0) {
+      T* Dk = Dinv + F.dinv_off + (size_t) (kb / PANEL_NB) * PANEL_NB * PANEL_NB;
+#pragma unroll
+      for (int c = 0; c < PANEL_NB; c++) Dk[i + c * PANEL_NB] = (c <= i && i < w) ? rw[c] : T(0);
+    }
+    return;
   }
-  if (sizeof(T) == 4 && sp != nullptr && F.sp_off >= 0) {
-    // the slab's final values, split, into the split arena for the tensor-
-    // core products; the front's last leaf also writes the zero columns that
-    // pad K to the products' stage width
-    const int rg = (int) sp_rgroups(f), cw = sp_chunk_cols(sp_fmt);
-    const int64_t part = sp_part_bytes(F, sp_fmt);
-    unsigned char* base = reinterpret_cast<unsigned char*>(sp + F.sp_off);
-    const int kc_end = (kb + w == s) ? (int) sp_kchunks(s, sp_fmt) : (kb + w) / cw;
-    const int nch = kc_end - kb / cw;
-    for (int e = tid; e < nch * PANEL_NB; e += 128) {
-      const int i = e % PANEL_NB, c = e / PANEL_NB;
-      if (i >= nr) continue;
-      const int r = r0 + i, k0 = kb + cw * c;
-      const int64_t o = ((int64_t) (k0 / cw) * rg + (r >> 3)) * 128 + (r & 7) * 16;
-      if (sp_fmt == 0) {
-        unsigned h[4], l[4];
+  if (i < nr) {
+    const size_t g = (size_t) (r0 + i);
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const float x = (k0 + q < kb + w) ? (float) A[i + (k0 + q - kb) * LLD] : 0.0f;
-          h[q] = __float_as_uint(x) & 0xffffe000u;
-          l[q] = __float_as_uint(x - __uint_as_float(h[q]));
-        }
-        *reinterpret_cast<uint4*>(base + o) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(base + part + o) = make_uint4(l[0], l[1], l[2], l[3]);
-      } else {
-        unsigned short h[8], l[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const float x = (k0 + q < kb + w) ? (float) A[i + (k0 + q - kb) * LLD] : 0.0f;
-          const __half hh = __float2half_rn(x);
-          h[q] = __half_as_ushort(hh);
-          l[q] = __half_as_ushort(__float2half_rn((x - __half2float(hh)) * 2048.0f));
-        }
-        uint4 vh, vl;
-        vh.x = h[0] | (unsigned) h[1] << 16; vh.y = h[2] | (unsigned) h[3] << 16;
-        vh.z = h[4] | (unsigned) h[5] << 16; vh.w = h[6] | (unsigned) h[7] << 16;
-        vl.x = l[0] | (unsigned) l[1] << 16; vl.y = l[2] | (unsigned) l[3] << 16;
-        vl.z = l[4] | (unsigned) l[5] << 16; vl.w = l[6] | (unsigned) l[7] << 16;
-        *reinterpret_cast<uint4*>(base + o) = vh;
-        *reinterpret_cast<uint4*>(base + part + o) = vl;
-      }
+    for (int c = 0; c < PANEL_NB; c++)
+      if (c < w) P[g + (size_t) (kb + c) * f] = rw[c];
+    if (sizeof(T) == 4 && sp != nullptr && F.sp_off >= 0) {
+      // the row's final values, split, into the split arena for the tensor-
+      // core products; the front's last leaf also writes the zero columns
+      // that pad K to the products' stage width
+      const int64_t rg = sp_rgroups(f), part = sp_part_bytes(F, sp_fmt);
+      unsigned char* base = reinterpret_cast<unsigned char*>(sp + F.sp_off);
+      const int cw = sp_chunk_cols(sp_fmt);
+      const int kc_end = (kb + w == s) ? (int) sp_kchunks(s, sp_fmt) : (kb + w) / cw;
+      const int nch = kc_end - kb / cw;
+      if (sp_fmt == 0) leaf_split_row<4>(rw, w, nch, base, part, kb / 4, rg, r0 + i);
+      else leaf_split_row<8>(rw, w, nch, base, part, kb / 8, rg, r0 + i);
     }
   }
 }
@@ -969,7 +991,6 @@ static void set_smem_attrs() {
                          SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
     cudaFuncSetAttribute(k_small_persistent<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          SMALL_F_MAX * SMALL_F_MAX * (int) sizeof(T));
-    cudaFuncSetAttribute(k_leaf<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) leaf_smem<T>());
     cudaFuncSetAttribute(k_dinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) dinv_smem<T>());
     cudaFuncSetAttribute(k_gemm<T, 64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int) GemmCfg<64, 64>::smem<T>());
@@ -1071,7 +1092,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
         }
       }
       prof_begin(KC_LEAF, st);
-      k_leaf<T><<<dim3(gx, nb), 128, leaf_smem<T>(), st>>>(blst, D.fronts, D.rows, L, Dinv, sp, sp_fmt, kb,
+      k_leaf<T><<<dim3(gx, nb), 128, 0, st>>>(blst, D.fronts, D.rows, L, Dinv, sp, sp_fmt, kb,
                                                            status);
       prof_end(KC_LEAF, st, fl, by);
       count_launch();

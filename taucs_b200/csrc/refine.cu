@@ -73,13 +73,38 @@ __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restr
                            int ld, int ldr, int nrhs, const int* __restrict__ seg, unsigned long long* norms) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int sg = (seg && i < n) ? seg[i] : 0;
-  for (int q = 0; q < nrhs; q++) {
+  // the row's entries eight at a time, then every column's products with
+  // all loads in flight together; per column the entries are subtracted in
+  // row order
+  double acc[SOLVE_NRHS];
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = (i < n && q < nrhs) ? B[i + (size_t) q * ld] : 0.0;
+  const int e0 = (i < n) ? rp[i] : 0, e1 = (i < n) ? rp[i + 1] : 0;
+  for (int eb = e0; eb < e1; eb += 8) {
+    int c[8];
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) c[u] = (eb + u < e1) ? ci[eb + u] : -1;
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = (c[u] >= 0) ? vals[vi[eb + u]] : 0.0;
+#pragma unroll
+    for (int q = 0; q < SOLVE_NRHS; q++) {
+      if (q >= nrhs) break;
+      double xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) xv[u] = (c[u] >= 0) ? X[c[u] + (size_t) q * ld] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+        if (c[u] >= 0) acc[q] -= v[u] * xv[u];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q++) {
+    if (q >= nrhs) break;
     double r = 0.0, x = 0.0;
     if (i < n) {
-      double acc = B[i + (size_t) q * ld];
-      for (int e = rp[i]; e < rp[i + 1]; e++) acc -= vals[vi[e]] * X[ci[e] + (size_t) q * ld];
-      R[i + (size_t) q * ldr] = acc;
-      r = fabs(acc);
+      R[i + (size_t) q * ldr] = acc[q];
+      r = fabs(acc[q]);
       x = fabs(X[i + (size_t) q * ld]);
     }
     seg_max(norms + 2 * q, sg, 2 * SOLVE_NRHS, r);

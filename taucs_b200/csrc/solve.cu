@@ -1071,15 +1071,30 @@ k_bwd_l21(const int2_* __restrict__ tasks, const FrontDesc* __restrict__ fronts,
     T v[32];   // v[a * NQ + q]: column cg + a, right-hand side q
 #pragma unroll
     for (int j = 0; j < 32; j++) v[j] = T(0);
-    for (int i = lane; i < nr; i += 32) {
-      T zi[NQ];
+    // RU rows per lane per round, 16 loads of the panel in flight at once
+    // (one round per memory latency)
+    constexpr int RU = G >= 16 ? 1 : 16 / G;
+    for (int i0 = lane; i0 < nr; i0 += 32 * RU) {
+      T lv[RU][G];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) zi[q] = zs[q][i];
+      for (int u = 0; u < RU; u++)
 #pragma unroll
-      for (int a = 0; a < G; a++) {
-        const T l = (cg + a < bw) ? P[i + (size_t) (c0 + cg + a) * f] : T(0);
+        for (int a = 0; a < G; a++) {
+          const int i = i0 + 32 * u;
+          lv[u][a] = (i < nr && cg + a < bw) ? P[i + (size_t) (c0 + cg + a) * f] : T(0);
+        }
 #pragma unroll
-        for (int q = 0; q < NQ; q++) v[a * NQ + q] += l * zi[q];
+      for (int u = 0; u < RU; u++) {
+        const int i = i0 + 32 * u;
+        if (i < nr) {
+          T zi[NQ];
+#pragma unroll
+          for (int q = 0; q < NQ; q++) zi[q] = zs[q][i];
+#pragma unroll
+          for (int a = 0; a < G; a++)
+#pragma unroll
+            for (int q = 0; q < NQ; q++) v[a * NQ + q] += lv[u][a] * zi[q];
+        }
       }
     }
     // reduce-scatter: at offset o a lane keeps the half of its remaining
@@ -1150,6 +1165,7 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
       const int c = e % bw, q = e / bw;
       if (q < nrhs) {
         T acc = 0.0;
+#pragma unroll 4
         for (int ch = 0; ch < F.nchunk; ch++)
           acc += __ldcg(part + F.part_off + ((size_t) ch * s + c0 + c) * SOLVE_NRHS + q);
         xv[c][q] -= acc;
@@ -1446,6 +1462,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     if (c < bw && q < nrhs) {
       v = Wf[c0 + c + (size_t) q * f];
       T acc = 0.0;
+#pragma unroll 4
       for (int ch = 0; ch < F.nchunk; ch++)
         acc += __ldcg(part + F.part_off + ((size_t) ch * s + c0 + c) * SOLVE_NRHS + q);
       v -= acc;

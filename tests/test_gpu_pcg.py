@@ -17,11 +17,13 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
-def _factored(tb, A):
+def _factored(tb, A, split_format=None):
     perm, iperm = tb.order(A, "amd")
     P = A.permute(perm, iperm)
     F = tb.factor_symbolic(P)
     F.set_precision(1)
+    if split_format is not None:
+        assert tb.lib().taucs_b200_set_split_format(F.h, split_format) == 0
     assert F.numeric(P) == 0, tb.last_error()
     return P, F
 
@@ -97,8 +99,10 @@ def _shifted_neumann(tb, k, eps):
 
 def test_stalled_refinement_rescued_by_pcg(tb):
     """Condition ~2e8: FP32 refinement stalls; PCG on the same FP32 factor
-    reaches the target without an FP64 refactorization."""
-    P, F = _factored(tb, _shifted_neumann(tb, 24, 1e-8))
+    reaches the target without an FP64 refactorization.  The stall is
+    reproduced with the TF32x3 products (split format 0); with the FP16x3
+    default this matrix refines to the target in one step."""
+    P, F = _factored(tb, _shifted_neumann(tb, 24, 1e-8), split_format=0)
     b = np.random.default_rng(0).uniform(-1, 1, P.n)
     x, its, res = F.solve_refine(P, b, tol=TOL, maxits=10)
     fb, pcg_its = F.refine_report()
