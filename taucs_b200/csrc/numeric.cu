@@ -192,8 +192,7 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
         const int* __restrict__ a_idx, const T* __restrict__ vals,
         T* __restrict__ L, T* __restrict__ U, const int* status) {
   __shared__ T W[BUILD_TR * BUILD_TC];
-  __shared__ int rng[2][4], cmc[2], cmap[2];
-  __shared__ int64_t cuoff[2];
+  __shared__ int rng[4];
   if (failed(status)) return;
   const Tile tl = tiles[blockIdx.x];
   const FrontDesc F = fronts[tl.front];
@@ -229,70 +228,52 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     }
     __syncthreads();
   }
-  // children two at a time: warps 0-3 search the four bounds of the first
-  // (its columns and rows that land in this tile), warps 4-7 those of the
-  // second; then every load of both children's shares is issued before the
-  // first add, and the two children add in child order
-  const int nch = F.child_end - F.child_begin;
-  for (int c0 = 0; c0 < nch; c0 += 2) {
-    const int two = min(2, nch - c0);
-    {
-      const int cc = warp >> 2, wb = warp & 3;
-      if (cc < two) {
-        const FrontDesc C = fronts[children[F.child_begin + c0 + cc]];
-        const int key = wb == 0 ? C0 : wb == 1 ? C0 + nc : wb == 2 ? R0 : R0 + nr;
-        const int r = warp_lower_bound(maps + C.map_off, C.f - C.s, key);
-        if (lane == 0) rng[cc][wb] = r;
-        if (wb == 0 && lane == 0) {
-          cmc[cc] = C.f - C.s;
-          cmap[cc] = C.map_off;
-          cuoff[cc] = C.u_off;
-        }
-      }
+  for (int ci = F.child_begin; ci < F.child_end; ci++) {
+    const FrontDesc C = fronts[children[ci]];
+    const int mc = C.f - C.s;
+    const int* mp = maps + C.map_off;
+    // the child's columns and rows that land in this tile: four warps search
+    // the four bounds at once
+    if (warp < 4) {
+      const int key = warp == 0 ? C0 : warp == 1 ? C0 + nc : warp == 2 ? R0 : R0 + nr;
+      const int r = warp_lower_bound(mp, mc, key);
+      if (lane == 0) rng[warp] = r;
     }
     __syncthreads();
+    const int ja = rng[0], jb = rng[1], ia = rng[2], ib = rng[3];
+    __syncthreads();
+    if (ja >= jb || ia >= ib) continue;
     // warp w takes the child's columns ja + w + 8u, lane l its rows
-    // ia + l + 32v (the children's update matrices were written by earlier
-    // launches)
+    // ia + l + 32v: every load of the tile's share is issued before the first
+    // add (the children's update matrices were written by earlier launches)
+    const T* Uc = U + C.u_off;
     constexpr int JU = (BUILD_TC + 7) / 8, IU = BUILD_TR / 32;
-    int pi[2][IU], pj[2][JU];
-    T val[2][JU][IU];
+    int pi[IU], pj[JU];
+    T val[JU][IU];
 #pragma unroll
-    for (int cc = 0; cc < 2; cc++) {
-      const int ja = rng[cc][0], jb = rng[cc][1], ia = rng[cc][2], ib = rng[cc][3];
-      const bool live = cc < two && ja < jb && ia < ib;
-      const int mc = live ? cmc[cc] : 0;
-      const int* mp = maps + (live ? cmap[cc] : 0);
-      const T* Uc = U + (live ? cuoff[cc] : 0);
+    for (int v = 0; v < IU; v++) {
+      const int i = ia + lane + 32 * v;
+      pi[v] = (i < ib) ? __ldg(mp + i) - R0 : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < JU; u++) {
+      const int j = ja + warp + 8 * u;
+      const bool jv = j < jb;
+      pj[u] = jv ? (__ldg(mp + j) - C0) * BUILD_TR : -1;
 #pragma unroll
       for (int v = 0; v < IU; v++) {
         const int i = ia + lane + 32 * v;
-        pi[cc][v] = (live && i < ib) ? __ldg(mp + i) - R0 : -1;
-      }
-#pragma unroll
-      for (int u = 0; u < JU; u++) {
-        const int j = ja + warp + 8 * u;
-        const bool jv = live && j < jb;
-        pj[cc][u] = jv ? (__ldg(mp + j) - C0) * BUILD_TR : -1;
-#pragma unroll
-        for (int v = 0; v < IU; v++) {
-          const int i = ia + lane + 32 * v;
-          val[cc][u][v] = (jv && i < ib && i >= j) ? __ldg(Uc + (size_t) j * mc + i) : T(0);
-        }
+        val[u][v] = (jv && i < ib && i >= j) ? __ldg(Uc + (size_t) j * mc + i) : T(0);
       }
     }
 #pragma unroll
-    for (int cc = 0; cc < 2; cc++) {
-      const int ja = rng[cc][0], ia = rng[cc][2];
+    for (int u = 0; u < JU; u++)
 #pragma unroll
-      for (int u = 0; u < JU; u++)
-#pragma unroll
-        for (int v = 0; v < IU; v++) {
-          const int i = ia + lane + 32 * v, j = ja + warp + 8 * u;
-          if (pj[cc][u] >= 0 && pi[cc][v] >= 0 && i >= j) W[pi[cc][v] + pj[cc][u]] += val[cc][u][v];
-        }
-      __syncthreads();
-    }
+      for (int v = 0; v < IU; v++) {
+        const int i = ia + lane + 32 * v, j = ja + warp + 8 * u;
+        if (pj[u] >= 0 && pi[v] >= 0 && i >= j) W[pi[v] + pj[u]] += val[u][v];
+      }
+    __syncthreads();
   }
   if (panel) {
     T* dst = L + F.l_off;

@@ -73,37 +73,17 @@ __device__ void fwd_small(const FrontDesc& F, const FrontDesc* __restrict__ fron
       T v[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && lane < bw) ? Wf[jb + lane + q * f] : T(0);
-      // this lane's row of the block in pieces of 8 columns, the next piece
-      // loaded while the chain runs through the current one
-      T lr[8], ln[8];
-      auto load_row = [&](T (&d)[8], int j0) {
+      for (int j = 0; j < bw; j++) {
+        const T rj = __shfl_sync(0xffffffffu, rd, j);
+        const T l = (lane > j && lane < bw) ? P[(jb + lane) + (size_t) (jb + j) * f] : T(0);
 #pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          const int j = j0 + jj;
-          d[jj] = (j < bw && lane > j && lane < bw) ? P[(jb + lane) + (size_t) (jb + j) * f] : T(0);
-        }
-      };
-      load_row(lr, 0);
-#pragma unroll 1
-      for (int j0 = 0; j0 < bw; j0 += 8) {
-        if (j0 + 8 < bw) load_row(ln, j0 + 8);
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          const int j = j0 + jj;
-          if (j < bw) {
-            const T rj = __shfl_sync(0xffffffffu, rd, j);
-#pragma unroll
-            for (int q = 0; q < SOLVE_NRHS; q++) {
-              if (q < nrhs) {
-                const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
-                if (lane == j) v[q] = xj;
-                else v[q] -= lr[jj] * xj;
-              }
-            }
+        for (int q = 0; q < SOLVE_NRHS; q++) {
+          if (q < nrhs) {
+            const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
+            if (lane == j) v[q] = xj;
+            else v[q] -= l * xj;
           }
         }
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) lr[jj] = ln[jj];
       }
       if (lane < bw) {
 #pragma unroll
@@ -119,21 +99,11 @@ __device__ void fwd_small(const FrontDesc& F, const FrontDesc* __restrict__ fron
       T acc[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = 0.0;
-      // 16 entries of the row in flight at a time
-#pragma unroll 1
-      for (int j0 = 0; j0 < SB; j0 += 16) {
-        T lr[16];
+      for (int j = 0; j < bw; j++) {
+        const T l = P[r + (size_t) (jb + j) * f];
 #pragma unroll
-        for (int jj = 0; jj < 16; jj++) lr[jj] = (j0 + jj < bw) ? P[r + (size_t) (jb + j0 + jj) * f] : T(0);
-        // rows of xs at or past bw hold stale values (possibly not numbers):
-        // skipped, not multiplied by zero
-#pragma unroll
-        for (int jj = 0; jj < 16; jj++)
-          if (j0 + jj < bw) {
-#pragma unroll
-            for (int q = 0; q < SOLVE_NRHS; q++)
-              if (q < nrhs) acc[q] += lr[jj] * xs[j0 + jj][q];
-          }
+        for (int q = 0; q < SOLVE_NRHS; q++)
+          if (q < nrhs) acc[q] += l * xs[j][q];
       }
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++)
@@ -232,38 +202,17 @@ __device__ void bwd_small(const FrontDesc& F, const int* __restrict__ rows, cons
       T v[SOLVE_NRHS];
 #pragma unroll
       for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && lane < bw) ? Wf[jb + lane + q * f] : T(0);
-      // this lane's column of the block (L[j][lane], j > lane) in pieces of
-      // 8 rows from the last, the next piece loaded during the current one
-      T lc[8], ln[8];
-      auto load_col = [&](T (&d)[8], int j0) {
+      for (int j = bw - 1; j >= 0; j--) {
+        const T rj = __shfl_sync(0xffffffffu, rd, j);
+        const T l = (lane < j) ? P[(jb + j) + (size_t) (jb + lane) * f] : T(0);
 #pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-          const int j = j0 + jj;
-          d[jj] = (j >= 0 && j < bw && lane < j) ? P[(jb + j) + (size_t) (jb + lane) * f] : T(0);
-        }
-      };
-      const int jtop = ((bw - 1) / 8) * 8;
-      load_col(lc, jtop);
-#pragma unroll 1
-      for (int j0 = jtop; j0 >= 0; j0 -= 8) {
-        if (j0 > 0) load_col(ln, j0 - 8);
-#pragma unroll
-        for (int jj = 7; jj >= 0; jj--) {
-          const int j = j0 + jj;
-          if (j < bw) {
-            const T rj = __shfl_sync(0xffffffffu, rd, j);
-#pragma unroll
-            for (int q = 0; q < SOLVE_NRHS; q++) {
-              if (q < nrhs) {
-                const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
-                if (lane == j) v[q] = xj;
-                else v[q] -= lc[jj] * xj;
-              }
-            }
+        for (int q = 0; q < SOLVE_NRHS; q++) {
+          if (q < nrhs) {
+            const T xj = __shfl_sync(0xffffffffu, v[q], j) * rj;
+            if (lane == j) v[q] = xj;
+            else v[q] -= l * xj;
           }
         }
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++) lc[jj] = ln[jj];
       }
       if (lane < bw) {
 #pragma unroll
@@ -731,45 +680,87 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 // y's in shared memory: consecutive steps are linked by barriers inside one
 // CTA, not by flags between CTAs.  Helper CTAs, one per diagonal block,
 // gather w_r and subtract the far terms k < r - WALK_D as the walker
-// publishes y_k (flags), then publish the partial p_r (pflags) -- WALK_D
-// steps ahead of the walker; the walker at step r subtracts the WALK_D near
-// terms and applies the block's inverse.  The tiles of step r + 1 (L_{r+1,k}
-// for the near k and the next inverse) are loaded into registers while step
-// r runs.  Walkers have the lowest CTA indices and a helper waits only for
-// the walker of its front, which waits only for helpers of lower index, so
-// in-order dispatch keeps every wait finite; the waits are bounded all the
-// same.  In the last diagonal block rows >= s are update rows of the same
-// front; the walker finishes them too.  The update-row blocks follow in
-// FWD_UPD.  Right-hand sides are processed eight at a time (the layout of
-// the partials).
+// publishes y_k (its progress word), then publish the partial p_r (pflags)
+// -- WALK_D steps ahead of the walker -- and pull the walker's tiles of
+// their block into L2; the walker at step r subtracts the WALK_D near terms
+// and applies the block's inverse.  Inside the walker eight compute warps
+// run the arithmetic while a ninth, communication warp takes the waits off
+// their path: it publishes each step's progress once the compute warps
+// signal that y_r is stored, and loads the partial two steps ahead, handing
+// both over through named barriers (one per direction and step parity).
+// The tiles of step r + 1 (L_{r+1,k} for the near k and the next inverse)
+// are loaded into registers while step r runs.  Walkers have the lowest CTA
+// indices and a helper waits only for the walker of its front, which waits
+// only for helpers of lower index, so in-order dispatch keeps every wait
+// finite; the waits are bounded all the same.  In the last diagonal block
+// rows >= s are update rows of the same front; the walker finishes them
+// too.  The update-row blocks follow in FWD_UPD.  Right-hand sides are
+// processed eight at a time (the layout of the partials).
 constexpr int WALK_D = 2, WALK_T = WALK_D + 1;
-constexpr int WALK_PER = WALK_T * BR * BR / 256;   // staged tile entries per thread
+constexpr int WALK_PER = WALK_T * BR * BR / 256;   // staged tile entries per compute thread
+constexpr int WALK_THREADS = 288;                   // eight compute warps and a communication warp
 // levels with more big fronts keep the flag-chained kernels: every walker
 // must be resident with room to spare for helpers (two CTAs per SM)
 constexpr int WALK_MAX_FRONTS = 64;
+// named barriers of the walker (0 is __syncthreads): the compute warps
+// among themselves; partial and tiles of a step ready (+ step parity);
+// y of a step stored (+ step parity)
+constexpr int WB_COMPUTE = 1, WB_READY = 2, WB_STORED = 4;
 
-// dynamic shared memory of the walk: the walker's tiles of one step and its
-// ring of y's; the helpers use the first part for their partial sums
+// barrier ids are immediates, so that the kernel reserves only the ids it uses
+template <int ID, int N>
+__device__ __forceinline__ void nbar_sync() {
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "n"(N) : "memory");
+}
+template <int ID, int N>
+__device__ __forceinline__ void nbar_arrive() {
+  asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(N) : "memory");
+}
+// the hand-over barriers of a step of parity par
+__device__ __forceinline__ void walk_ready_arrive(int par) {
+  if (par) nbar_arrive<WB_READY + 1, WALK_THREADS>();
+  else nbar_arrive<WB_READY, WALK_THREADS>();
+}
+__device__ __forceinline__ void walk_ready_sync(int par) {
+  if (par) nbar_sync<WB_READY + 1, WALK_THREADS>();
+  else nbar_sync<WB_READY, WALK_THREADS>();
+}
+__device__ __forceinline__ void walk_stored_arrive(int par) {
+  if (par) nbar_arrive<WB_STORED + 1, WALK_THREADS>();
+  else nbar_arrive<WB_STORED, WALK_THREADS>();
+}
+__device__ __forceinline__ void walk_stored_sync(int par) {
+  if (par) nbar_sync<WB_STORED + 1, WALK_THREADS>();
+  else nbar_sync<WB_STORED, WALK_THREADS>();
+}
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// dynamic shared memory of the walk: the walker's tiles of one step, its
+// ring of y's and two partial buffers; the helpers use the first part for
+// their partial sums and staged y's
 template <typename T>
 constexpr size_t walk_smem() {
-  return (WALK_T * BR * BR + WALK_T * BR * (SOLVE_NRHS + 1)) * sizeof(T);
+  return (WALK_T * BR * BR + (WALK_T + 2) * BR * (SOLVE_NRHS + 1)) * sizeof(T);
 }
 // the backward walker's tiles are [row][column], padded against bank
 // conflicts of the coalesced staging stores
 template <typename T>
 constexpr size_t bwalk_smem() {
-  return (WALK_T * BR * (BR + 1) + WALK_T * BR * (SOLVE_NRHS + 1)) * sizeof(T);
+  return (WALK_T * BR * (BR + 1) + (WALK_T + 2) * BR * (SOLVE_NRHS + 1)) * sizeof(T);
 }
 
 // The far terms of a walk's helper: blocks t = 0 .. n-1 of the chain in the
 // order the walker publishes them (its progress counts them), each adding
 // acc[q] += sum_jj load_l(t, jj) ys[qg * 16 + jj][q] with ys[i][q] =
 // load_y(t, i, q).  Every round takes all published blocks not used yet, up
-// to WALK_HB, and issues all of their loads before any waits.
+// to WALK_HB, and issues all of their loads before any waits.  Threads past
+// the first 256 (act false) only keep the barriers.
 constexpr int WALK_HB = 4;
 template <typename T, int NQ, typename LoadL, typename LoadY>
 __device__ __forceinline__ void walk_far_terms(const int* prog, int epoch, int* status, int n, LoadL load_l,
-                                               LoadY load_y, T (*ysb)[BR][NQ], T (&acc)[NQ], int qg) {
+                                               LoadY load_y, T (*ysb)[BR][NQ], T (&acc)[NQ], int qg, bool act) {
   __shared__ int avail_s;
   constexpr int NY = WALK_HB * BR * NQ / 256;
   int avail = 0;
@@ -781,36 +772,40 @@ __device__ __forceinline__ void walk_far_terms(const int* prog, int epoch, int* 
     }
     const int nb = min(avail - t, WALK_HB);
     T lv[WALK_HB][BR / 4];
+    if (act) {
 #pragma unroll
-    for (int b = 0; b < WALK_HB; b++)
+      for (int b = 0; b < WALK_HB; b++)
 #pragma unroll
-      for (int jj = 0; jj < BR / 4; jj++) lv[b][jj] = (b < nb) ? load_l(t + b, jj) : T(0);
-    T yv[NY];
+        for (int jj = 0; jj < BR / 4; jj++) lv[b][jj] = (b < nb) ? load_l(t + b, jj) : T(0);
+      T yv[NY];
 #pragma unroll
-    for (int u = 0; u < NY; u++) {
-      const int e = threadIdx.x + 256 * u, b = e / (BR * NQ), i = e % BR, q = (e / BR) % NQ;
-      yv[u] = (b < nb) ? load_y(t + b, i, q) : T(0);
-    }
+      for (int u = 0; u < NY; u++) {
+        const int e = threadIdx.x + 256 * u, b = e / (BR * NQ), i = e % BR, q = (e / BR) % NQ;
+        yv[u] = (b < nb) ? load_y(t + b, i, q) : T(0);
+      }
 #pragma unroll
-    for (int u = 0; u < NY; u++) {
-      const int e = threadIdx.x + 256 * u;
-      ysb[e / (BR * NQ)][e % BR][(e / BR) % NQ] = yv[u];
+      for (int u = 0; u < NY; u++) {
+        const int e = threadIdx.x + 256 * u;
+        ysb[e / (BR * NQ)][e % BR][(e / BR) % NQ] = yv[u];
+      }
     }
     __syncthreads();
+    if (act) {
 #pragma unroll
-    for (int b = 0; b < WALK_HB; b++)
-      if (b < nb)
+      for (int b = 0; b < WALK_HB; b++)
+        if (b < nb)
 #pragma unroll
-        for (int jj = 0; jj < BR / 4; jj++)
+          for (int jj = 0; jj < BR / 4; jj++)
 #pragma unroll
-          for (int q = 0; q < NQ; q++) acc[q] += lv[b][jj] * ysb[b][qg * (BR / 4) + jj][q];
+            for (int q = 0; q < NQ; q++) acc[q] += lv[b][jj] * ysb[b][qg * (BR / 4) + jj][q];
+    }
     __syncthreads();
     t += nb;
   }
 }
 
 template <typename T, int WS>
-__global__ void __launch_bounds__(256)
+__global__ void __maxnreg__(112)
 k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
            const FrontDesc* __restrict__ fronts, const int* __restrict__ children, const int* __restrict__ maps,
            const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ Dinv,
@@ -819,7 +814,7 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
   static_assert(NQ % 4 == 0, "four thread groups share the right-hand sides");
   extern __shared__ __align__(16) unsigned char wsm[];
-  __shared__ T pv[BR][NQ + 1];
+  __shared__ T hpv[BR][NQ + 1];
   __shared__ int rng[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int row = tid % BR, qg = tid / BR;
@@ -836,6 +831,38 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     // block the update rows' entries of L_{., r}; all column-major
     T (*tl)[BR][BR] = reinterpret_cast<T (*)[BR][BR]>(wsm);
     T (*yr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * BR * sizeof(T));
+    T (*pvb)[BR][NQ + 1] = yr + WALK_T;   // [2]: the partials of even and odd steps
+    if (warp == 8) {
+      // ---- communication warp
+      auto load_p = [&](int r, int buf) {
+        if (lane == 0) poll_epoch(pflags + F.blk_off + r, epoch, status);
+        __syncwarp();   // the lanes' loads below follow lane 0's acquire
+        constexpr int NV = BR * NQ / 32;
+        T v[NV];
+#pragma unroll
+        for (int u = 0; u < NV; u++) v[u] = __ldcg(fp + (size_t) r * BR * NQ + lane + 32 * u);
+#pragma unroll
+        for (int u = 0; u < NV; u++) {
+          const int e = lane + 32 * u;
+          pvb[buf][e / NQ][e % NQ] = v[u];
+        }
+        walk_ready_arrive(buf);
+      };
+      load_p(0, 0);
+      if (nbs > 1) load_p(1, 1);
+      for (int r = 0; r < nbs; r++) {
+        walk_stored_sync(r & 1);
+        // y_r is stored: the block's own flag for the update-row blocks of
+        // the next launch, the progress word for the helpers
+        if (lane == 0) {
+          flags[F.blk_off + r] = epoch;
+          st_release(progress + fi, (epoch << 12) | (r + 1));
+        }
+        if (r + 2 < nbs) load_p(r + 2, r & 1);
+      }
+      return;
+    }
+    // ---- compute warps
     T pre[WALK_PER];
     auto fetch = [&](int r) {
       const int r0 = r * BR, nr = min(BR, f - r0), bw = min(BR, s - r0);
@@ -861,19 +888,16 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         tl[t / TPT][e / BR][e % BR] = pre[t];
       }
     };
-    auto load_p = [&](int r) {
-      if (tid == 32) poll_epoch(pflags + F.blk_off + r, epoch, status);
-      __syncthreads();
-      for (int e = tid; e < BR * NQ; e += 256) pv[e / NQ][e % NQ] = __ldcg(fp + (size_t) r * BR * NQ + e);
-    };
     fetch(0);
     put();
-    load_p(0);
     for (int r = 0; r < nbs; r++) {
       const int r0 = r * BR, nr = min(BR, f - r0), bw = min(BR, s - r0);
-      const int slot = r % WALK_T;
+      const int slot = r % WALK_T, buf = r & 1;
+      T (*pv)[NQ + 1] = pvb[buf];
+      // p_r is in place (communication warp) and so are the tiles of step r
+      // (every compute thread put its share before arriving here)
+      walk_ready_sync(buf);
       if (r + 1 < nbs) fetch(r + 1);   // in flight during the step
-      __syncthreads();                  // p_r and the tiles of step r are in place
       // near terms: p_r -= sum_j L_{r, r-WALK_D+j} y_{r-WALK_D+j}
       {
         T u[QG];
@@ -894,7 +918,7 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll
         for (int c = 0; c < QG; c++) pv[row][qg * QG + c] -= u[c];
       }
-      __syncthreads();
+      nbar_sync<WB_COMPUTE, 256>();
       // y_r = L_rr^-1 p_r in rows < bw; the update rows keep p
       {
         T y[QG];
@@ -909,7 +933,7 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll
         for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] = (row < bw) ? y[c] : pv[row][qg * QG + c];
       }
-      __syncthreads();
+      nbar_sync<WB_COMPUTE, 256>();
       if (bw < nr) {
         // update rows inside the last diagonal block: w_i -= L[i, r] y_r
         // (reads rows < bw of the ring slot, writes rows >= bw)
@@ -925,28 +949,23 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll
           for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] -= v[c];
         }
-        __syncthreads();
+        nbar_sync<WB_COMPUTE, 256>();
       }
       for (int e = tid; e < nr * nrhs; e += 256) {
         const int i = e % nr, q = e / nr;
         Wf[r0 + i + (size_t) q * f] = yr[slot][i][q];
       }
-      // the barrier orders every thread's stores before the release, and
-      // every read of this step's tiles and p before they are replaced; the
-      // block's own flag is for the update-row blocks of the next launch
-      __syncthreads();
-      if (tid == 0) {
-        flags[F.blk_off + r] = epoch;
-        st_release(progress + fi, (epoch << 12) | (r + 1));
-      }
-      if (r + 1 < nbs) {
-        put();
-        load_p(r + 1);   // thread 32 polls while thread 0 releases
-      }
+      // every read of this step's tiles is done before they are replaced;
+      // the stores of y_r come before the hand-over to the communication warp
+      nbar_sync<WB_COMPUTE, 256>();
+      walk_stored_arrive(buf);
+      if (r + 1 < nbs) put();
     }
     return;
   }
   // ------------------------------------------------------------------ helper
+  // (the communication warp's threads only keep the barriers here)
+  const bool act = tid < 256;
   const int2_ bk = blocks[blockIdx.x - nwalk];
   const FrontDesc F = fronts[bk.a];
   const int r = bk.b, f = F.f, s = F.s;
@@ -957,9 +976,25 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);            // [4]
   T (*ysb)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm) + 4;         // [WALK_HB]
   const int kend = max(r - WALK_D, 0);
-  for (int k = tid; k < BR * NQ; k += 256) {
+  // the walker's tiles of this block into L2: the near blocks' 64 columns
+  // (two 128-byte lines each, the second while it holds rows of the front)
+  // and the block's inverse
+  {
+    const int ncol = WALK_D * BR, dlines = (int) (BR * BR * sizeof(T) / 128);
+    const T* Di = Dinv + F.dinv_off + (size_t) r * BR * BR;
+    for (int e = tid; e < 2 * ncol + dlines; e += WALK_THREADS) {
+      if (e < 2 * ncol) {
+        const int c = e >> 1, half = e & 1, k = r - WALK_D + c / BR;
+        if (k >= 0 && (half == 0 || r0 + 128 / (int) sizeof(T) < f))
+          prefetch_l2(P + r0 + half * (128 / (int) sizeof(T)) + (size_t) (k * BR + c % BR) * f);
+      } else {
+        prefetch_l2(reinterpret_cast<const unsigned char*>(Di) + (size_t) (e - 2 * ncol) * 128);
+      }
+    }
+  }
+  for (int k = tid; k < BR * NQ; k += WALK_THREADS) {
     const int i = k % BR, q = k / BR;
-    pv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : T(0);
+    hpv[i][q] = (i < nr && q < nrhs && r0 + i < s) ? B[rw[r0 + i] + (size_t) q * ldb] : T(0);
   }
   __syncthreads();
   for (int ci = F.child_begin; ci < F.child_end; ci++) {
@@ -975,17 +1010,14 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     __syncthreads();
     if (ia >= ib) continue;
     const T* Wc = W + C.v_off * WS;
-    for (int k = tid; k < (ib - ia) * nrhs; k += 256) {
+    for (int k = tid; k < (ib - ia) * nrhs; k += WALK_THREADS) {
       const int i = ia + k % (ib - ia), q = k / (ib - ia);
-      pv[mp[i] - r0][q] += Wc[C.s + i + q * C.f];
+      hpv[mp[i] - r0][q] += Wc[C.s + i + q * C.f];
     }
     __syncthreads();
   }
   // far terms k < r - WALK_D: thread (row, quarter qg) sums 16 columns of
-  // each L_rk for every right-hand side.  The helper reads the walker's
-  // progress and takes every published block it has not used yet, up to
-  // WALK_HB per round with all their loads in flight at once, so a helper
-  // that fell behind catches up in few rounds.
+  // each L_rk for every right-hand side
   T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
@@ -995,14 +1027,16 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         return (row < nr) ? P[(r0 + row) + (size_t) (k * BR + qg * (BR / 4) + jj) * f] : T(0);
       },
       [&](int k, int j, int q) -> T { return (q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : T(0); }, ysb,
-      acc, qg);
+      acc, qg, act);
+  if (act) {
 #pragma unroll
-  for (int q = 0; q < NQ; q++) red[qg][row][q] = acc[q];
+    for (int q = 0; q < NQ; q++) red[qg][row][q] = acc[q];
+  }
   __syncthreads();
   T* dst = fpart + (size_t) (F.blk_off + r) * BR * NQ;
-  for (int e = tid; e < BR * NQ; e += 256) {
+  for (int e = tid; e < BR * NQ; e += WALK_THREADS) {
     const int i = e / NQ, q = e % NQ;
-    dst[e] = pv[i][q] - (red[0][i][q] + red[1][i][q] + red[2][i][q] + red[3][i][q]);
+    dst[e] = hpv[i][q] - (red[0][i][q] + red[1][i][q] + red[2][i][q] + red[3][i][q]);
   }
   __syncthreads();
   if (tid == 0) st_release(pflags + F.blk_off + r, epoch);
@@ -1320,14 +1354,15 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 // Backward solve of the diagonal blocks of levels with long chains, as a
 // walk: the mirror of k_fwd_walk.  The walker of a front runs
 // x_k = L_kk^-T (v_k - sum_{j>k} L_jk^T x_j) from the last block to the
-// first, subtracting the WALK_D near terms j = k+1, k+2 itself; helper CTAs,
-// one per diagonal block (listed last block first), form v_k = y_k - L21^T
-// x2 from the chunk partial sums, subtract the far terms j > k + WALK_D as
-// the walker publishes x_j, and publish the partial through the second
-// flag array.  The same in-order dispatch argument as the forward walk
-// keeps every wait finite.
+// first, subtracting the WALK_D near terms j = k+1, k+2 itself, with the
+// same split into compute warps and a communication warp; helper CTAs, one
+// per diagonal block (listed last block first), form v_k = y_k - L21^T x2
+// from the chunk partial sums, subtract the far terms j > k + WALK_D as the
+// walker publishes x_j, publish the partial through the second flag array
+// and pull the walker's tiles of their block into L2.  The same in-order
+// dispatch argument as the forward walk keeps every wait finite.
 template <typename T, int WS>
-__global__ void __launch_bounds__(256)
+__global__ void __maxnreg__(112)
 k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
            const FrontDesc* __restrict__ fronts, const int* __restrict__ rows, const T* __restrict__ L,
            const T* __restrict__ Dinv, T* __restrict__ X, int ldx, T* __restrict__ W,
@@ -1335,8 +1370,8 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
            int* __restrict__ pflags, int* __restrict__ progress, int epoch, int* status) {
   constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
   extern __shared__ __align__(16) unsigned char wsm[];
-  __shared__ T pv[BR][NQ + 1];
-  const int tid = threadIdx.x;
+  __shared__ T hpv[BR][NQ + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int col = tid % BR, qg = tid / BR;
   if (blockIdx.x < nwalk) {
     // ---------------------------------------------------------------- walker
@@ -1351,6 +1386,37 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     // tl[WALK_D]: the inverse of block k; all [row][column]
     T (*tl)[BR][BR + 1] = reinterpret_cast<T (*)[BR][BR + 1]>(wsm);
     T (*xr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * (BR + 1) * sizeof(T));
+    T (*pvb)[BR][NQ + 1] = xr + WALK_T;   // [2]: the partials by step parity
+    if (warp == 8) {
+      // ---- communication warp; step t of the walk is block nbs - 1 - t
+      auto load_p = [&](int t, int buf) {
+        const int k = nbs - 1 - t;
+        if (lane == 0) poll_epoch(pflags + F.blk_off + k, epoch, status);
+        __syncwarp();   // the lanes' loads below follow lane 0's acquire
+        constexpr int NV = BR * NQ / 32;
+        T v[NV];
+#pragma unroll
+        for (int u = 0; u < NV; u++) v[u] = __ldcg(bp + (size_t) k * BR * NQ + lane + 32 * u);
+#pragma unroll
+        for (int u = 0; u < NV; u++) {
+          const int e = lane + 32 * u;
+          pvb[buf][e / NQ][e % NQ] = v[u];
+        }
+        walk_ready_arrive(buf);
+      };
+      load_p(0, 0);
+      if (nbs > 1) load_p(1, 1);
+      for (int t = 0; t < nbs; t++) {
+        walk_stored_sync(t & 1);
+        if (lane == 0) {
+          flags[F.blk_off + nbs - 1 - t] = epoch;
+          st_release(progress + fi, (epoch << 12) | (t + 1));
+        }
+        if (t + 2 < nbs) load_p(t + 2, t & 1);
+      }
+      return;
+    }
+    // ---- compute warps
     T pre[WALK_PER];
     auto fetch = [&](int k) {
       const int c0 = k * BR, bw = min(BR, s - c0);
@@ -1376,19 +1442,15 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         tl[t / TPT][e % BR][e / BR] = pre[t];
       }
     };
-    auto load_p = [&](int k) {
-      if (tid == 32) poll_epoch(pflags + F.blk_off + k, epoch, status);
-      __syncthreads();
-      for (int e = tid; e < BR * NQ; e += 256) pv[e / NQ][e % NQ] = __ldcg(bp + (size_t) k * BR * NQ + e);
-    };
     fetch(nbs - 1);
     put();
-    load_p(nbs - 1);
-    for (int k = nbs - 1; k >= 0; k--) {
+    for (int t = 0; t < nbs; t++) {
+      const int k = nbs - 1 - t;
       const int c0 = k * BR, bw = min(BR, s - c0);
-      const int slot = k % WALK_T;
-      if (k > 0) fetch(k - 1);   // in flight during the step
-      __syncthreads();           // p_k and the tiles of step k are in place
+      const int slot = k % WALK_T, buf = t & 1;
+      T (*pv)[NQ + 1] = pvb[buf];
+      walk_ready_sync(buf);   // p_k and the tiles of step k are in place
+      if (k > 0) fetch(k - 1);                     // in flight during the step
       // near terms: p_k -= sum_j L_{k+1+j, k}^T x_{k+1+j}
       {
         T u[QG];
@@ -1409,7 +1471,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll
         for (int c = 0; c < QG; c++) pv[col][qg * QG + c] -= u[c];
       }
-      __syncthreads();
+      nbar_sync<WB_COMPUTE, 256>();
       // x_k = L_kk^-T p_k (the inverse is lower triangular)
       {
         T x[QG];
@@ -1423,28 +1485,24 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll
         for (int c = 0; c < QG; c++) xr[slot][col][qg * QG + c] = (col < bw) ? x[c] : T(0);
       }
-      __syncthreads();
+      nbar_sync<WB_COMPUTE, 256>();
       for (int e = tid; e < bw * nrhs; e += 256) {
         const int c = e % bw, q = e / bw;
         const T v = xr[slot][c][q];
         Wf[c0 + c + (size_t) q * f] = v;
         X[rw[c0 + c] + (size_t) q * ldx] = v;
       }
-      // the barrier orders every thread's stores before the release, and
-      // every read of this step's tiles and p before they are replaced
-      __syncthreads();
-      if (tid == 0) {
-        flags[F.blk_off + k] = epoch;
-        st_release(progress + fi, (epoch << 12) | (nbs - k));
-      }
-      if (k > 0) {
-        put();
-        load_p(k - 1);   // thread 32 polls while thread 0 releases
-      }
+      // every read of this step's tiles is done before they are replaced;
+      // the stores of x_k come before the hand-over to the communication warp
+      nbar_sync<WB_COMPUTE, 256>();
+      walk_stored_arrive(buf);
+      if (k > 0) put();
     }
     return;
   }
   // ------------------------------------------------------------------ helper
+  // (the communication warp's threads only keep the barriers here)
+  const bool act = tid < 256;
   const int2_ bk = blocks[blockIdx.x - nwalk];
   const FrontDesc F = fronts[bk.a];
   const int k = bk.b, f = F.f, s = F.s;
@@ -1455,8 +1513,25 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);            // [4]
   T (*ysb)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm) + 4;         // [WALK_HB]
   const int jlo = k + WALK_D + 1;   // far blocks j = nbs-1 .. jlo
+  // the walker's tiles of this block into L2: the near blocks' 64-row
+  // column pieces of block column k (two 128-byte lines each, the second
+  // while it holds rows of the near block) and the block's inverse
+  {
+    const int ncol = WALK_D * BR, dlines = (int) (BR * BR * sizeof(T) / 128);
+    const T* Di = Dinv + F.dinv_off + (size_t) k * BR * BR;
+    for (int e = tid; e < 2 * ncol + dlines; e += WALK_THREADS) {
+      if (e < 2 * ncol) {
+        const int c = e >> 1, half = e & 1, j = k + 1 + c / BR;
+        const int rows_j = j < nbs ? min(BR, s - j * BR) : 0;
+        if (c % BR < bw && (half == 0 ? rows_j > 0 : rows_j > 128 / (int) sizeof(T)))
+          prefetch_l2(P + (size_t) j * BR + half * (128 / (int) sizeof(T)) + (size_t) (c0 + c % BR) * f);
+      } else {
+        prefetch_l2(reinterpret_cast<const unsigned char*>(Di) + (size_t) (e - 2 * ncol) * 128);
+      }
+    }
+  }
   // v_k = y_k - L21^T x2, the chunk partial sums added in chunk order
-  for (int e = tid; e < BR * NQ; e += 256) {
+  for (int e = tid; e < BR * NQ; e += WALK_THREADS) {
     const int c = e % BR, q = e / BR;
     T v = 0.0;
     if (c < bw && q < nrhs) {
@@ -1467,7 +1542,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         acc += __ldcg(part + F.part_off + ((size_t) ch * s + c0 + c) * SOLVE_NRHS + q);
       v -= acc;
     }
-    pv[c][q] = v;
+    hpv[c][q] = v;
   }
   // far terms: blocks j = nbs-1 down to jlo, taken as the walker publishes
   // them (block t of the helper's order is j = nbs-1-t)
@@ -1484,14 +1559,16 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         const int j = nbs - 1 - t;
         return (i < min(BR, s - j * BR) && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : T(0);
       },
-      ysb, acc, qg);
+      ysb, acc, qg, act);
+  if (act) {
 #pragma unroll
-  for (int q = 0; q < NQ; q++) red[qg][col][q] = acc[q];
+    for (int q = 0; q < NQ; q++) red[qg][col][q] = acc[q];
+  }
   __syncthreads();
   T* dst = bpart + (size_t) (F.blk_off + k) * BR * NQ;
-  for (int e = tid; e < BR * NQ; e += 256) {
+  for (int e = tid; e < BR * NQ; e += WALK_THREADS) {
     const int c = e / NQ, q = e % NQ;
-    dst[e] = pv[c][q] - (red[0][c][q] + red[1][c][q] + red[2][c][q] + red[3][c][q]);
+    dst[e] = hpv[c][q] - (red[0][c][q] + red[1][c][q] + red[2][c][q] + red[3][c][q]);
   }
   __syncthreads();
   if (tid == 0) st_release(pflags + F.blk_off + k, epoch);
@@ -1621,7 +1698,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
           if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
             (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR) {
             const int nbig = (int) LP.big_fronts.size();
-            k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, 256, walk_smem<T>(), st>>>(
+            k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, WALK_THREADS, walk_smem<T>(), st>>>(
                 D.big_list + D.big_off[h], nbig, bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W,
                 part + P.fpart_off, nq, flags, flags + P.n_blk, flags + 2 * (size_t) P.n_blk, ef, status);
             if (nu)
@@ -1671,7 +1748,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
             (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR) {
           const int nbig = (int) LP.big_fronts.size();
-          k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, 256, bwalk_smem<T>(), st>>>(
+          k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, WALK_THREADS, bwalk_smem<T>(), st>>>(
               D.big_list + D.big_off[h], nbig, bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, part + P.fpart_off,
               nq, flags, flags + P.n_blk, flags + 2 * (size_t) P.n_blk, eb, status);
         } else if (nq <= 2)
