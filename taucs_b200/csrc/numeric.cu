@@ -184,8 +184,12 @@ k_small_persistent(const int* __restrict__ tasks, int ntask, const int* __restri
 
 // --------------------------------------------------------------- front build
 
+// threads of a build CTA: four warps (the four bounds of a child's ranges are
+// searched at once), sixteen CTAs resident per SM
+constexpr int BUILD_THREADS = 128;
+
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(BUILD_THREADS)
 k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
         const int* __restrict__ children, const int* __restrict__ maps,
         const int* __restrict__ acol_ptr, const int* __restrict__ a_rows,
@@ -216,7 +220,7 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     // once; the adds are atomic, as a column may list a row more than once
     // (duplicates are summed)
     const int c = tid % BUILD_TC, q = tid / BUILD_TC;
-    constexpr int NQS = 256 / BUILD_TC;
+    constexpr int NQS = BUILD_THREADS / BUILD_TC;
     int e = 0, e1 = 0;
     if (c < nc) {
       e = __ldg(acol_ptr + F.acol_off + C0 + c) + q;
@@ -243,11 +247,11 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     const int ja = rng[0], jb = rng[1], ia = rng[2], ib = rng[3];
     __syncthreads();
     if (ja >= jb || ia >= ib) continue;
-    // warp w takes the child's columns ja + w + 8u, lane l its rows
+    // warp w takes the child's columns ja + w + NW u, lane l its rows
     // ia + l + 32v: every load of the tile's share is issued before the first
     // add (the children's update matrices were written by earlier launches)
     const T* Uc = U + C.u_off;
-    constexpr int JU = (BUILD_TC + 7) / 8, IU = BUILD_TR / 32;
+    constexpr int NW = BUILD_THREADS / 32, JU = (BUILD_TC + NW - 1) / NW, IU = BUILD_TR / 32;
     int pi[IU], pj[JU];
     T val[JU][IU];
 #pragma unroll
@@ -257,7 +261,7 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     }
 #pragma unroll
     for (int u = 0; u < JU; u++) {
-      const int j = ja + warp + 8 * u;
+      const int j = ja + warp + NW * u;
       const bool jv = j < jb;
       pj[u] = jv ? (__ldg(mp + j) - C0) * BUILD_TR : -1;
 #pragma unroll
@@ -270,7 +274,7 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     for (int u = 0; u < JU; u++)
 #pragma unroll
       for (int v = 0; v < IU; v++) {
-        const int i = ia + lane + 32 * v, j = ja + warp + 8 * u;
+        const int i = ia + lane + 32 * v, j = ja + warp + NW * u;
         if (pj[u] >= 0 && pi[v] >= 0 && i >= j) W[pi[v] + pj[u]] += val[u][v];
       }
     __syncthreads();
@@ -418,11 +422,10 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
        T* __restrict__ L, T* __restrict__ Dinv, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
   // Xt[buf][c][k]: the new L[c][c0 + k] of the diagonal block's rows c below
   // the current piece (row-major, 16-byte aligned rows, two buffers by piece
-  // parity); Lp, rinv: the factored piece and its reciprocal diagonal
+  // parity); Yr: the inverse of the factored piece, row-major
   constexpr int XLD = sizeof(T) == 4 ? LQ + 4 : LQ + 2;
   __shared__ __align__(16) T Xt[2][PANEL_NB][XLD];
-  __shared__ T Lp[LQ][LQ + 1];
-  __shared__ T rinv[LQ];
+  __shared__ __align__(16) T Yr[LQ][XLD];
   __shared__ int bad_s;
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.y]];
@@ -461,14 +464,26 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       int bad = -1;
       CholStep<T, 0>::run(a, ii, base, bad);
       if (ii >= 0 && ii < LQ) {
-        T dg = T(1);
 #pragma unroll
-        for (int k = 0; k < LQ; k++) {
+        for (int k = 0; k < LQ; k++)
           if (k <= ii) rw[c0 + k] = a[k];
-          Lp[ii][k] = (k <= ii) ? a[k] : T(0);
-          if (k == ii) dg = a[k];
+      }
+      // the piece's inverse: lane base + ii forms column ii by forward
+      // substitution, reading L[r][k] from lane base + r by shuffles
+      if (bad < 0) {
+        T y[LQ];
+#pragma unroll
+        for (int r = 0; r < LQ; r++) {
+          T acc = (r == ii) ? T(1) : T(0);
+#pragma unroll
+          for (int k = 0; k < r; k++) acc -= __shfl_sync(0xffffffffu, a[k], base + r) * y[k];
+          const T lrr = __shfl_sync(0xffffffffu, a[r], base + r);
+          y[r] = (r >= ii) ? acc * (T(1) / lrr) : T(0);
         }
-        rinv[ii] = T(1) / dg;
+        if (ii >= 0 && ii < LQ) {
+#pragma unroll
+          for (int r = 0; r < LQ; r++) Yr[r][ii] = y[r];
+        }
       }
       if (lane == 0) bad_s = bad;
     }
@@ -477,18 +492,18 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       if (tid == 0 && blockIdx.x == 0 && c0 + bad_s < w) atomicMin(status, rows[F.rows_off + kb + c0 + bad_s]);
       return;
     }
-    // rows below the piece: X L_p^T = M by substitution (in registers), the
-    // diagonal block's rows also published for the update below
+    // rows below the piece: X = M L_p^-T, every entry an independent dot
+    // product with a row of the inverse (in registers); the diagonal block's
+    // rows also published for the update below
     const bool below = !is_d || i >= c0 + LQ;
     T x[LQ];
-#pragma unroll
-    for (int c = 0; c < LQ; c++) x[c] = rw[c0 + c];
     if (below) {
 #pragma unroll
       for (int c = 0; c < LQ; c++) {
-        x[c] *= rinv[c];
+        T acc = T(0);
 #pragma unroll
-        for (int c2 = c + 1; c2 < LQ; c2++) x[c2] -= x[c] * Lp[c2][c];
+        for (int k = 0; k <= c; k++) acc += rw[c0 + k] * Yr[c][k];
+        x[c] = acc;
       }
 #pragma unroll
       for (int c = 0; c < LQ; c++) rw[c0 + c] = x[c];
@@ -501,13 +516,18 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
     // the columns right of the piece: rw[c] -= sum_k x[k] L[c][c0 + k] (the
     // diagonal block's rows also compute their upper part, never read)
     if (below) {
+      // four columns at a time: four independent accumulation chains
 #pragma unroll
-      for (int c = c0 + LQ; c < PANEL_NB; c++) {
-        const T* xr = Xt[b & 1][c];
-        T acc = rw[c];
+      for (int c = c0 + LQ; c < PANEL_NB; c += 4) {
+        T acc[4];
 #pragma unroll
-        for (int k = 0; k < LQ; k++) acc -= x[k] * xr[k];
-        rw[c] = acc;
+        for (int u = 0; u < 4; u++) acc[u] = T(0);
+#pragma unroll
+        for (int k = 0; k < LQ; k++)
+#pragma unroll
+          for (int u = 0; u < 4; u++) acc[u] += x[k] * Xt[b & 1][c + u][k];
+#pragma unroll
+        for (int u = 0; u < 4; u++) rw[c + u] -= acc[u];
       }
     }
   }
@@ -1046,7 +1066,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
       if (prof_enabled())
         for (int fi : LP.big_fronts) by += build_bytes(P, P.fronts[fi], sizeof(T));
       prof_begin(KC_BUILD, st);
-      k_build<T><<<ntiles, 256, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
+      k_build<T><<<ntiles, BUILD_THREADS, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
                                       D.a_rows, D.a_idx, vals, L, U, status);
       prof_end(KC_BUILD, st, 0.0, by);
       count_launch();
