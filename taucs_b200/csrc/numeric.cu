@@ -422,10 +422,11 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
        T* __restrict__ L, T* __restrict__ Dinv, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
   // Xt[buf][c][k]: the new L[c][c0 + k] of the diagonal block's rows c below
   // the current piece (row-major, 16-byte aligned rows, two buffers by piece
-  // parity); Yr: the inverse of the factored piece, row-major
+  // parity); Lp, rinv: the factored piece and its reciprocal diagonal
   constexpr int XLD = sizeof(T) == 4 ? LQ + 4 : LQ + 2;
   __shared__ __align__(16) T Xt[2][PANEL_NB][XLD];
-  __shared__ __align__(16) T Yr[LQ][XLD];
+  __shared__ T Lp[LQ][LQ + 1];
+  __shared__ T rinv[LQ];
   __shared__ int bad_s;
   if (failed(status)) return;
   const FrontDesc F = fronts[list[blockIdx.y]];
@@ -464,26 +465,14 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       int bad = -1;
       CholStep<T, 0>::run(a, ii, base, bad);
       if (ii >= 0 && ii < LQ) {
+        T dg = T(1);
 #pragma unroll
-        for (int k = 0; k < LQ; k++)
+        for (int k = 0; k < LQ; k++) {
           if (k <= ii) rw[c0 + k] = a[k];
-      }
-      // the piece's inverse: lane base + ii forms column ii by forward
-      // substitution, reading L[r][k] from lane base + r by shuffles
-      if (bad < 0) {
-        T y[LQ];
-#pragma unroll
-        for (int r = 0; r < LQ; r++) {
-          T acc = (r == ii) ? T(1) : T(0);
-#pragma unroll
-          for (int k = 0; k < r; k++) acc -= __shfl_sync(0xffffffffu, a[k], base + r) * y[k];
-          const T lrr = __shfl_sync(0xffffffffu, a[r], base + r);
-          y[r] = (r >= ii) ? acc * (T(1) / lrr) : T(0);
+          Lp[ii][k] = (k <= ii) ? a[k] : T(0);
+          if (k == ii) dg = a[k];
         }
-        if (ii >= 0 && ii < LQ) {
-#pragma unroll
-          for (int r = 0; r < LQ; r++) Yr[r][ii] = y[r];
-        }
+        rinv[ii] = T(1) / dg;
       }
       if (lane == 0) bad_s = bad;
     }
@@ -492,18 +481,18 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       if (tid == 0 && blockIdx.x == 0 && c0 + bad_s < w) atomicMin(status, rows[F.rows_off + kb + c0 + bad_s]);
       return;
     }
-    // rows below the piece: X = M L_p^-T, every entry an independent dot
-    // product with a row of the inverse (in registers); the diagonal block's
-    // rows also published for the update below
+    // rows below the piece: X L_p^T = M by substitution (in registers), the
+    // diagonal block's rows also published for the update below
     const bool below = !is_d || i >= c0 + LQ;
     T x[LQ];
+#pragma unroll
+    for (int c = 0; c < LQ; c++) x[c] = rw[c0 + c];
     if (below) {
 #pragma unroll
       for (int c = 0; c < LQ; c++) {
-        T acc = T(0);
+        x[c] *= rinv[c];
 #pragma unroll
-        for (int k = 0; k <= c; k++) acc += rw[c0 + k] * Yr[c][k];
-        x[c] = acc;
+        for (int c2 = c + 1; c2 < LQ; c2++) x[c2] -= x[c] * Lp[c2][c];
       }
 #pragma unroll
       for (int c = 0; c < LQ; c++) rw[c0 + c] = x[c];
@@ -516,18 +505,13 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
     // the columns right of the piece: rw[c] -= sum_k x[k] L[c][c0 + k] (the
     // diagonal block's rows also compute their upper part, never read)
     if (below) {
-      // four columns at a time: four independent accumulation chains
 #pragma unroll
-      for (int c = c0 + LQ; c < PANEL_NB; c += 4) {
-        T acc[4];
+      for (int c = c0 + LQ; c < PANEL_NB; c++) {
+        const T* xr = Xt[b & 1][c];
+        T acc = rw[c];
 #pragma unroll
-        for (int u = 0; u < 4; u++) acc[u] = T(0);
-#pragma unroll
-        for (int k = 0; k < LQ; k++)
-#pragma unroll
-          for (int u = 0; u < 4; u++) acc[u] += x[k] * Xt[b & 1][c + u][k];
-#pragma unroll
-        for (int u = 0; u < 4; u++) rw[c + u] -= acc[u];
+        for (int k = 0; k < LQ; k++) acc -= x[k] * xr[k];
+        rw[c] = acc;
       }
     }
   }
