@@ -233,8 +233,8 @@ int ensure_device(Factor* F) {
   const Plan& P = F->plan;
   bool ok = dev_upload(&F->dA, (const double*) nullptr, (size_t) P.nnz, st)
          && dev_upload(&F->dstatus, (const int*) nullptr, 2, st)
-         && dev_upload(&F->dflags, (const int*) nullptr, solve_flag_words(P), st)
-         && cuda_ok(cudaMemsetAsync(F->dflags, 0, sizeof(int) * solve_flag_words(P), st), "flags")
+         && dev_upload(&F->dflags, (const int*) nullptr, solve_flag_words(P) + 1, st)
+         && cuda_ok(cudaMemsetAsync(F->dflags, 0, sizeof(int) * (solve_flag_words(P) + 1), st), "flags")
          && dev_upload(&F->dW, (const double*) nullptr, (size_t) P.v_len * SOLVE_NRHS, st)
          && dev_upload(&F->dpart, (const double*) nullptr, (size_t) P.part_len, st)
          && dev_upload(&F->dX, (const double*) nullptr, (size_t) F->n * SOLVE_NRHS, st)

@@ -138,7 +138,7 @@ struct Plan {
   int64_t dinv_len = 0;            // doubles of diagonal-block inverses
   int n_blk = 0;                   // solve flags
   int64_t part_len = 0;            // doubles of partial sums: the backward ones, then the forward walk's
-  int64_t fpart_off = 0;           // start of the forward walk's partial sums (n_blk x 64 x SOLVE_NRHS)
+  int64_t fpart_off = 0;           // start of the walks' tagged pairs (2 x n_blk x 64 x SOLVE_NRHS, 8 bytes each)
   int64_t sp_len = 0;              // floats of the split arena (the largest level's split copies)
   // small fronts whose whole subtree is small, in device (level) order: one
   // persistent launch factors them all, taking them from a device-side queue
@@ -166,9 +166,10 @@ struct Plan {
   std::vector<uint8_t> gemm_choice[2];
 };
 
-// words of the solve's handshake array: a chain flag and a partial-sum flag
-// per 64-row block, and a walk progress word per front
-inline size_t solve_flag_words(const Plan& P) { return 2 * (size_t) P.n_blk + P.fronts.size(); }
+// words of the solve's handshake array cleared by every solve call: a chain
+// flag per 64-row block; one more word follows, the walks' call counter
+// (never cleared)
+inline size_t solve_flag_words(const Plan& P) { return (size_t) P.n_blk; }
 
 int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, Plan* P);
 

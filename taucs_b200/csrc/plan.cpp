@@ -376,9 +376,12 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
         F.part_off = -1;
       }
     }
-    // the forward walk's partial sums of every diagonal block follow
+    // the walks' tagged values follow, 8-byte aligned: per 64-row block
+    // the chain's 64 x 8 results, then the helpers' 64 x 8 partial sums, as
+    // (tag, value) pairs of 8 bytes (two FP32 elements each)
+    poff = (poff + 1) & ~int64_t(1);
     P.fpart_off = poff;
-    poff += (int64_t) P.n_blk * PANEL_NB * SOLVE_NRHS;
+    poff += (int64_t) P.n_blk * 2 * PANEL_NB * SOLVE_NRHS * 2;
     P.part_len = std::max<int64_t>(poff, 32);
     // split copies of the big fronts' panels for the FP32 tensor-core
     // products; the levels run one after another, so each level starts the

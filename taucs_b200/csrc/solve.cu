@@ -396,21 +396,6 @@ __device__ void wait_epoch(const int* flag, int epoch, int* status) {
   __syncthreads();
 }
 
-// A walk's progress word holds (epoch << 12) | blocks published.  Polls it
-// until at least count blocks of this epoch are published and returns the
-// number published (count itself after giving up, with SOLVE_TIMEOUT set).
-__device__ __forceinline__ int poll_progress(const int* p, int epoch, int count, int* status) {
-  const int want = ((epoch + g_solve_wait_skew) << 12) | count, limit = g_solve_wait_limit;
-  int it = 0, v;
-  while ((v = ld_acquire(p)) < want) {
-    if (++it > limit || ((it & 1023) == 0 && *(volatile int*) status == SOLVE_TIMEOUT)) {
-      atomicExch(status, SOLVE_TIMEOUT);
-      return count;
-    }
-    __nanosleep(32);
-  }
-  return v & 4095;
-}
 
 // Forward solve of big fronts.  Diagonal block r of L11 gives
 // y_r = L_rr^-1 (w_r - sum_{k<r} L_rk y_k), chained to block r-1 by
@@ -680,32 +665,37 @@ k_fwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 // y's in shared memory: consecutive steps are linked by barriers inside one
 // CTA, not by flags between CTAs.  Helper CTAs, one per diagonal block,
 // gather w_r and subtract the far terms k < r - WALK_D as the walker
-// publishes y_k (its progress word), then publish the partial p_r (pflags)
-// -- WALK_D steps ahead of the walker -- and pull the walker's tiles of
-// their block into L2; the walker at step r subtracts the WALK_D near terms
-// and applies the block's inverse.  Inside the walker eight compute warps
-// run the arithmetic while a ninth, communication warp takes the waits off
-// their path: it publishes each step's progress once the compute warps
-// signal that y_r is stored, and loads the partial two steps ahead, handing
-// both over through named barriers (one per direction and step parity).
-// The tiles of step r + 1 (L_{r+1,k} for the near k and the next inverse)
-// are loaded into registers while step r runs.  Walkers have the lowest CTA
-// indices and a helper waits only for the walker of its front, which waits
-// only for helpers of lower index, so in-order dispatch keeps every wait
-// finite; the waits are bounded all the same.  In the last diagonal block
-// rows >= s are update rows of the same front; the walker finishes them
-// too.  The update-row blocks follow in FWD_UPD.  Right-hand sides are
-// processed eight at a time (the layout of the partials).
+// publishes y_k, then publish the partial p_r -- WALK_D steps ahead of the
+// walker -- and pull the walker's tiles of their block into L2; the walker
+// at step r subtracts the WALK_D near terms and applies the block's inverse.
+// Every value crossing between CTAs travels as a tagged pair (tag in the
+// high word, value in the low word, one 8-byte relaxed store): a reader
+// knows a value is current when its tag is, so neither side fences or
+// polls a flag.  The tag is (call counter << 12) | epoch, the counter being
+// advanced on the device at the start of every solve call (recorded launch
+// sequences stay valid), so a slot never holds a current-looking stale pair.
+// Inside the walker eight compute warps run the arithmetic while a ninth
+// warp loads the partials two steps ahead, handing them over through named
+// barriers (one per direction and step parity).  The tiles of step r + 1
+// (L_{r+1,k} for the near k and the next inverse) are loaded into registers
+// while step r runs.  Walkers have the lowest CTA indices and a helper waits
+// only for the walker of its front, which waits only for helpers of lower
+// index, so in-order dispatch keeps every wait finite; the waits are bounded
+// all the same.  In the last diagonal block rows >= s are update rows of the
+// same front; the walker finishes them too.  The update-row blocks follow in
+// FWD_UPD (the walker also sets the blocks' flags for it).  Right-hand sides
+// are processed eight at a time (the layout of the pairs).
 constexpr int WALK_D = 2, WALK_T = WALK_D + 1;
 constexpr int WALK_PER = WALK_T * BR * BR / 256;   // staged tile entries per compute thread
-constexpr int WALK_THREADS = 288;                   // eight compute warps and a communication warp
+constexpr int WALK_THREADS = 288;                   // eight compute warps and a loader warp
+constexpr int WALK_PAIRS = BR * SOLVE_NRHS;         // tagged pairs per block: [row][right-hand side]
 // levels with more big fronts keep the flag-chained kernels: every walker
 // must be resident with room to spare for helpers (two CTAs per SM)
 constexpr int WALK_MAX_FRONTS = 64;
 // named barriers of the walker (0 is __syncthreads): the compute warps
-// among themselves; partial and tiles of a step ready (+ step parity);
-// y of a step stored (+ step parity)
-constexpr int WB_COMPUTE = 1, WB_READY = 2, WB_STORED = 4;
+// among themselves; partial of a step ready (+ step parity); partial buffer
+// of a step released (+ step parity)
+constexpr int WB_COMPUTE = 1, WB_READY = 2, WB_FREE = 4;
 
 // barrier ids are immediates, so that the kernel reserves only the ids it uses
 template <int ID, int N>
@@ -716,7 +706,6 @@ template <int ID, int N>
 __device__ __forceinline__ void nbar_arrive() {
   asm volatile("bar.arrive %0, %1;" ::"n"(ID), "n"(N) : "memory");
 }
-// the hand-over barriers of a step of parity par
 __device__ __forceinline__ void walk_ready_arrive(int par) {
   if (par) nbar_arrive<WB_READY + 1, WALK_THREADS>();
   else nbar_arrive<WB_READY, WALK_THREADS>();
@@ -725,16 +714,51 @@ __device__ __forceinline__ void walk_ready_sync(int par) {
   if (par) nbar_sync<WB_READY + 1, WALK_THREADS>();
   else nbar_sync<WB_READY, WALK_THREADS>();
 }
-__device__ __forceinline__ void walk_stored_arrive(int par) {
-  if (par) nbar_arrive<WB_STORED + 1, WALK_THREADS>();
-  else nbar_arrive<WB_STORED, WALK_THREADS>();
+__device__ __forceinline__ void walk_free_arrive(int par) {
+  if (par) nbar_arrive<WB_FREE + 1, WALK_THREADS>();
+  else nbar_arrive<WB_FREE, WALK_THREADS>();
 }
-__device__ __forceinline__ void walk_stored_sync(int par) {
-  if (par) nbar_sync<WB_STORED + 1, WALK_THREADS>();
-  else nbar_sync<WB_STORED, WALK_THREADS>();
+__device__ __forceinline__ void walk_free_sync(int par) {
+  if (par) nbar_sync<WB_FREE + 1, WALK_THREADS>();
+  else nbar_sync<WB_FREE, WALK_THREADS>();
 }
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// tagged pairs: one relaxed 8-byte access each (single-copy atomic)
+__device__ __forceinline__ void put_pair(unsigned long long* p, unsigned tag, float v) {
+  const unsigned long long x = ((unsigned long long) tag << 32) | __float_as_uint(v);
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
+}
+__device__ __forceinline__ unsigned long long get_pair(const unsigned long long* p) {
+  unsigned long long x;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
+  return x;
+}
+__device__ __forceinline__ bool pair_ok(unsigned long long x, unsigned tag) { return (unsigned) (x >> 32) == tag; }
+__device__ __forceinline__ float pair_value(unsigned long long x) { return __uint_as_float((unsigned) x); }
+
+// the tag of a walk: the solve call's counter and the epoch
+__device__ __forceinline__ unsigned walk_tag(const int* counter, int epoch) {
+  return ((unsigned) *counter << 12) | (unsigned) epoch;
+}
+
+// waits (bounded) until pair x at p carries tag, reloading it
+__device__ __forceinline__ unsigned long long wait_pair(const unsigned long long* p, unsigned long long x, unsigned tag,
+                                                        int* status) {
+  const int limit = g_solve_wait_limit;
+  const unsigned want = tag + (unsigned) (g_solve_wait_skew << 12);
+  int it = 0;
+  while (!pair_ok(x, want)) {
+    if (++it > limit || ((it & 1023) == 0 && *(volatile int*) status == SOLVE_TIMEOUT)) {
+      atomicExch(status, SOLVE_TIMEOUT);
+      break;
+    }
+    __nanosleep(32);
+    x = get_pair(p);
+  }
+  return x;
 }
 
 // dynamic shared memory of the walk: the walker's tiles of one step, its
@@ -752,55 +776,74 @@ constexpr size_t bwalk_smem() {
 }
 
 // The far terms of a walk's helper: blocks t = 0 .. n-1 of the chain in the
-// order the walker publishes them (its progress counts them), each adding
-// acc[q] += sum_jj load_l(t, jj) ys[qg * 16 + jj][q] with ys[i][q] =
-// load_y(t, i, q).  Every round takes all published blocks not used yet, up
-// to WALK_HB, and issues all of their loads before any waits.  Threads past
-// the first 256 (act false) only keep the barriers.
+// order the walker publishes them, each adding acc[q] += sum_jj
+// load_l(t, jj) ys[qg * 16 + jj][q] with ys[i][q] the value of pair
+// [i][q] of block pairs(t).  Every round loads up to WALK_HB blocks, all
+// loads in flight at once, and uses the leading blocks whose pairs all carry
+// the tag; a round that finds none waits (bounded) for the first.  Threads
+// past the first 256 (act false) only keep the barriers.
 constexpr int WALK_HB = 4;
-template <typename T, int NQ, typename LoadL, typename LoadY>
-__device__ __forceinline__ void walk_far_terms(const int* prog, int epoch, int* status, int n, LoadL load_l,
-                                               LoadY load_y, T (*ysb)[BR][NQ], T (&acc)[NQ], int qg, bool act) {
-  __shared__ int avail_s;
+template <int NQ, typename LoadL, typename Pairs>
+__device__ __forceinline__ void walk_far_terms(unsigned tag, int* status, int n, LoadL load_l, Pairs pairs,
+                                               float (*ysb)[BR][NQ], float (&acc)[NQ], int qg, bool act) {
+  __shared__ unsigned bad_s;
   constexpr int NY = WALK_HB * BR * NQ / 256;
-  int avail = 0;
   for (int t = 0; t < n;) {
-    if (t >= avail) {
-      if (threadIdx.x == 0) avail_s = poll_progress(prog, epoch, t + 1, status);
-      __syncthreads();
-      avail = max(min(avail_s, n), t + 1);
-    }
-    const int nb = min(avail - t, WALK_HB);
-    T lv[WALK_HB][BR / 4];
+    const int nb = min(n - t, WALK_HB);
+    if (threadIdx.x == 0) bad_s = 0;
+    __syncthreads();
+    float lv[WALK_HB][BR / 4];
+    unsigned long long yv[NY];
     if (act) {
 #pragma unroll
       for (int b = 0; b < WALK_HB; b++)
 #pragma unroll
-        for (int jj = 0; jj < BR / 4; jj++) lv[b][jj] = (b < nb) ? load_l(t + b, jj) : T(0);
-      T yv[NY];
+        for (int jj = 0; jj < BR / 4; jj++) lv[b][jj] = (b < nb) ? load_l(t + b, jj) : 0.0f;
 #pragma unroll
       for (int u = 0; u < NY; u++) {
-        const int e = threadIdx.x + 256 * u, b = e / (BR * NQ), i = e % BR, q = (e / BR) % NQ;
-        yv[u] = (b < nb) ? load_y(t + b, i, q) : T(0);
+        const int e = threadIdx.x + 256 * u, b = e / (BR * NQ);
+        yv[u] = (b < nb) ? get_pair(pairs(t + b) + e % (BR * NQ)) : 0ull;
       }
+      unsigned bad = 0;
 #pragma unroll
       for (int u = 0; u < NY; u++) {
-        const int e = threadIdx.x + 256 * u;
-        ysb[e / (BR * NQ)][e % BR][(e / BR) % NQ] = yv[u];
+        const int e = threadIdx.x + 256 * u, b = e / (BR * NQ);
+        if (b < nb && !pair_ok(yv[u], tag)) bad |= 1u << b;
+      }
+      if (bad) atomicOr(&bad_s, bad);
+    }
+    __syncthreads();
+    // the leading blocks whose pairs are all current; none: wait for the first
+    int ok = __ffs(bad_s | (1u << nb)) - 1;
+    if (ok == 0) {
+      if (act) {
+#pragma unroll
+        for (int u = 0; u < NY; u++) {
+          const int e = threadIdx.x + 256 * u, b = e / (BR * NQ);
+          if (b == 0) yv[u] = wait_pair(pairs(t) + e % (BR * NQ), yv[u], tag, status);
+        }
+      }
+      ok = 1;
+    }
+    if (act) {
+#pragma unroll
+      for (int u = 0; u < NY; u++) {
+        const int e = threadIdx.x + 256 * u, b = e / (BR * NQ), r = e % (BR * NQ);
+        ysb[b][r / NQ][r % NQ] = pair_value(yv[u]);
       }
     }
     __syncthreads();
     if (act) {
 #pragma unroll
       for (int b = 0; b < WALK_HB; b++)
-        if (b < nb)
+        if (b < ok)
 #pragma unroll
           for (int jj = 0; jj < BR / 4; jj++)
 #pragma unroll
             for (int q = 0; q < NQ; q++) acc[q] += lv[b][jj] * ysb[b][qg * (BR / 4) + jj][q];
     }
     __syncthreads();
-    t += nb;
+    t += ok;
   }
 }
 
@@ -809,8 +852,10 @@ __global__ void __maxnreg__(112)
 k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
            const FrontDesc* __restrict__ fronts, const int* __restrict__ children, const int* __restrict__ maps,
            const int* __restrict__ rows, const T* __restrict__ L, const T* __restrict__ Dinv,
-           const T* __restrict__ B, int ldb, T* __restrict__ W, T* __restrict__ fpart, int nrhs,
-           int* __restrict__ flags, int* __restrict__ pflags, int* __restrict__ progress, int epoch, int* status) {
+           const T* __restrict__ B, int ldb, T* __restrict__ W, unsigned long long* __restrict__ ypairs,
+           unsigned long long* __restrict__ ppairs, int nrhs, int* __restrict__ flags, const int* counter, int epoch,
+           int* status) {
+  static_assert(sizeof(T) == 4, "the tagged pairs carry FP32 values");
   constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
   static_assert(NQ % 4 == 0, "four thread groups share the right-hand sides");
   extern __shared__ __align__(16) unsigned char wsm[];
@@ -818,14 +863,15 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   __shared__ int rng[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int row = tid % BR, qg = tid / BR;
+  const unsigned tag = walk_tag(counter, epoch);
   if (blockIdx.x < nwalk) {
     // ---------------------------------------------------------------- walker
-    const int fi = walk_fronts[blockIdx.x];
-    const FrontDesc F = fronts[fi];
+    const FrontDesc F = fronts[walk_fronts[blockIdx.x]];
     const int f = F.f, s = F.s, nbs = (s + BR - 1) / BR;
     const T* P = L + F.l_off;
     T* Wf = W + F.v_off * WS;
-    const T* fp = fpart + (size_t) F.blk_off * BR * NQ;
+    unsigned long long* yp = ypairs + (size_t) F.blk_off * WALK_PAIRS;
+    const unsigned long long* pp = ppairs + (size_t) F.blk_off * WALK_PAIRS;
     // tl[j] for j < WALK_D: L_{r, r-WALK_D+j} (zero before the first block);
     // tl[WALK_D]: the inverse of block r, and in rows >= bw of the last
     // block the update rows' entries of L_{., r}; all column-major
@@ -833,32 +879,28 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     T (*yr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * BR * sizeof(T));
     T (*pvb)[BR][NQ + 1] = yr + WALK_T;   // [2]: the partials of even and odd steps
     if (warp == 8) {
-      // ---- communication warp
+      // ---- loader warp: the partials two steps ahead
       auto load_p = [&](int r, int buf) {
-        if (lane == 0) poll_epoch(pflags + F.blk_off + r, epoch, status);
-        __syncwarp();   // the lanes' loads below follow lane 0's acquire
-        constexpr int NV = BR * NQ / 32;
-        T v[NV];
+        constexpr int NV = WALK_PAIRS / 32;
+        unsigned long long v[NV];
+        const unsigned long long* src = pp + (size_t) r * WALK_PAIRS;
 #pragma unroll
-        for (int u = 0; u < NV; u++) v[u] = __ldcg(fp + (size_t) r * BR * NQ + lane + 32 * u);
+        for (int u = 0; u < NV; u++) v[u] = get_pair(src + lane + 32 * u);
 #pragma unroll
         for (int u = 0; u < NV; u++) {
+          v[u] = wait_pair(src + lane + 32 * u, v[u], tag, status);
           const int e = lane + 32 * u;
-          pvb[buf][e / NQ][e % NQ] = v[u];
+          pvb[buf][e / NQ][e % NQ] = pair_value(v[u]);
         }
         walk_ready_arrive(buf);
       };
       load_p(0, 0);
       if (nbs > 1) load_p(1, 1);
-      for (int r = 0; r < nbs; r++) {
-        walk_stored_sync(r & 1);
-        // y_r is stored: the block's own flag for the update-row blocks of
-        // the next launch, the progress word for the helpers
-        if (lane == 0) {
-          flags[F.blk_off + r] = epoch;
-          st_release(progress + fi, (epoch << 12) | (r + 1));
-        }
-        if (r + 2 < nbs) load_p(r + 2, r & 1);
+      // one wait per step of the compute warps (the last two complete the
+      // barriers of the final steps): step r - 2 released its buffer
+      for (int r = 2; r < nbs + 2; r++) {
+        walk_free_sync(r & 1);
+        if (r < nbs) load_p(r, r & 1);
       }
       return;
     }
@@ -894,8 +936,8 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
       const int r0 = r * BR, nr = min(BR, f - r0), bw = min(BR, s - r0);
       const int slot = r % WALK_T, buf = r & 1;
       T (*pv)[NQ + 1] = pvb[buf];
-      // p_r is in place (communication warp) and so are the tiles of step r
-      // (every compute thread put its share before arriving here)
+      // p_r is in place (loader warp) and so are the tiles of step r (every
+      // compute thread put its share before arriving here)
       walk_ready_sync(buf);
       if (r + 1 < nbs) fetch(r + 1);   // in flight during the step
       // near terms: p_r -= sum_j L_{r, r-WALK_D+j} y_{r-WALK_D+j}
@@ -934,6 +976,8 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] = (row < bw) ? y[c] : pv[row][qg * QG + c];
       }
       nbar_sync<WB_COMPUTE, 256>();
+      // the partial buffer of this step is free for the loader (step r + 2)
+      walk_free_arrive(buf);
       if (bw < nr) {
         // update rows inside the last diagonal block: w_i -= L[i, r] y_r
         // (reads rows < bw of the ring slot, writes rows >= bw)
@@ -951,31 +995,39 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         }
         nbar_sync<WB_COMPUTE, 256>();
       }
+      // y_r: tagged pairs for the helpers, plain values for later launches
+      {
+        unsigned long long* dst = yp + (size_t) r * WALK_PAIRS;
+#pragma unroll
+        for (int u = 0; u < WALK_PAIRS / 256; u++) {
+          const int e = tid + 256 * u;
+          put_pair(dst + e, tag, yr[slot][e / NQ][e % NQ]);
+        }
+      }
       for (int e = tid; e < nr * nrhs; e += 256) {
         const int i = e % nr, q = e / nr;
         Wf[r0 + i + (size_t) q * f] = yr[slot][i][q];
       }
-      // every read of this step's tiles is done before they are replaced;
-      // the stores of y_r come before the hand-over to the communication warp
+      if (tid == 0) flags[F.blk_off + r] = epoch;
+      // every read of this step's tiles is done before they are replaced
       nbar_sync<WB_COMPUTE, 256>();
-      walk_stored_arrive(buf);
       if (r + 1 < nbs) put();
     }
     return;
   }
   // ------------------------------------------------------------------ helper
-  // (the communication warp's threads only keep the barriers here)
+  // (the loader warp's threads only keep the barriers here)
   const bool act = tid < 256;
   const int2_ bk = blocks[blockIdx.x - nwalk];
   const FrontDesc F = fronts[bk.a];
   const int r = bk.b, f = F.f, s = F.s;
   const int r0 = r * BR, nr = min(BR, f - r0);
   const T* P = L + F.l_off;
-  const T* Wf = W + F.v_off * WS;
   const int* rw = rows + F.rows_off;
   T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);            // [4]
   T (*ysb)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm) + 4;         // [WALK_HB]
   const int kend = max(r - WALK_D, 0);
+  const unsigned long long* yp = ypairs + (size_t) F.blk_off * WALK_PAIRS;
   // the walker's tiles of this block into L2: the near blocks' 64 columns
   // (two 128-byte lines each, the second while it holds rows of the front)
   // and the block's inverse
@@ -1021,25 +1073,22 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
-  walk_far_terms<T, NQ>(
-      progress + bk.a, epoch, status, kend,
+  walk_far_terms<NQ>(
+      tag, status, kend,
       [&](int k, int jj) -> T {
         return (row < nr) ? P[(r0 + row) + (size_t) (k * BR + qg * (BR / 4) + jj) * f] : T(0);
       },
-      [&](int k, int j, int q) -> T { return (q < nrhs) ? __ldcg(Wf + k * BR + j + (size_t) q * f) : T(0); }, ysb,
-      acc, qg, act);
+      [&](int k) { return yp + (size_t) k * WALK_PAIRS; }, ysb, acc, qg, act);
   if (act) {
 #pragma unroll
     for (int q = 0; q < NQ; q++) red[qg][row][q] = acc[q];
   }
   __syncthreads();
-  T* dst = fpart + (size_t) (F.blk_off + r) * BR * NQ;
-  for (int e = tid; e < BR * NQ; e += WALK_THREADS) {
+  unsigned long long* dst = ppairs + (size_t) (F.blk_off + r) * WALK_PAIRS;
+  for (int e = tid; e < WALK_PAIRS; e += WALK_THREADS) {
     const int i = e / NQ, q = e % NQ;
-    dst[e] = hpv[i][q] - (red[0][i][q] + red[1][i][q] + red[2][i][q] + red[3][i][q]);
+    put_pair(dst + e, tag, hpv[i][q] - (red[0][i][q] + red[1][i][q] + red[2][i][q] + red[3][i][q]));
   }
-  __syncthreads();
-  if (tid == 0) st_release(pflags + F.blk_off + r, epoch);
 }
 
 // x at the update rows of every big front of a level, gathered once into the
@@ -1355,64 +1404,63 @@ k_bwd_big(const int2_* __restrict__ blocks, const FrontDesc* __restrict__ fronts
 // walk: the mirror of k_fwd_walk.  The walker of a front runs
 // x_k = L_kk^-T (v_k - sum_{j>k} L_jk^T x_j) from the last block to the
 // first, subtracting the WALK_D near terms j = k+1, k+2 itself, with the
-// same split into compute warps and a communication warp; helper CTAs, one
-// per diagonal block (listed last block first), form v_k = y_k - L21^T x2
-// from the chunk partial sums, subtract the far terms j > k + WALK_D as the
-// walker publishes x_j, publish the partial through the second flag array
-// and pull the walker's tiles of their block into L2.  The same in-order
-// dispatch argument as the forward walk keeps every wait finite.
+// same split into compute warps and a loader warp; helper CTAs, one per
+// diagonal block (listed last block first), form v_k = y_k - L21^T x2 from
+// the chunk partial sums, subtract the far terms j > k + WALK_D as the
+// walker publishes x_j, publish the partial and pull the walker's tiles of
+// their block into L2.  Values cross between CTAs as tagged pairs, as in
+// the forward walk, and the same in-order dispatch argument keeps every
+// wait finite.
 template <typename T, int WS>
 __global__ void __maxnreg__(112)
 k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restrict__ blocks,
            const FrontDesc* __restrict__ fronts, const int* __restrict__ rows, const T* __restrict__ L,
            const T* __restrict__ Dinv, T* __restrict__ X, int ldx, T* __restrict__ W,
-           const T* __restrict__ part, T* __restrict__ bpart, int nrhs, int* __restrict__ flags,
-           int* __restrict__ pflags, int* __restrict__ progress, int epoch, int* status) {
+           const T* __restrict__ part, unsigned long long* __restrict__ ypairs,
+           unsigned long long* __restrict__ ppairs, int nrhs, int* __restrict__ flags, const int* counter, int epoch,
+           int* status) {
+  static_assert(sizeof(T) == 4, "the tagged pairs carry FP32 values");
   constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
   extern __shared__ __align__(16) unsigned char wsm[];
   __shared__ T hpv[BR][NQ + 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int col = tid % BR, qg = tid / BR;
+  const unsigned tag = walk_tag(counter, epoch);
   if (blockIdx.x < nwalk) {
     // ---------------------------------------------------------------- walker
-    const int fi = walk_fronts[blockIdx.x];
-    const FrontDesc F = fronts[fi];
+    const FrontDesc F = fronts[walk_fronts[blockIdx.x]];
     const int f = F.f, s = F.s, nbs = (s + BR - 1) / BR;
     const T* P = L + F.l_off;
     T* Wf = W + F.v_off * WS;
     const int* rw = rows + F.rows_off;
-    const T* bp = bpart + (size_t) F.blk_off * BR * NQ;
+    unsigned long long* yp = ypairs + (size_t) F.blk_off * WALK_PAIRS;
+    const unsigned long long* pp = ppairs + (size_t) F.blk_off * WALK_PAIRS;
     // tl[j] for j < WALK_D: L_{k+1+j, k} (zero past the last block);
     // tl[WALK_D]: the inverse of block k; all [row][column]
     T (*tl)[BR][BR + 1] = reinterpret_cast<T (*)[BR][BR + 1]>(wsm);
     T (*xr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * (BR + 1) * sizeof(T));
     T (*pvb)[BR][NQ + 1] = xr + WALK_T;   // [2]: the partials by step parity
     if (warp == 8) {
-      // ---- communication warp; step t of the walk is block nbs - 1 - t
+      // ---- loader warp; step t of the walk is block nbs - 1 - t
       auto load_p = [&](int t, int buf) {
-        const int k = nbs - 1 - t;
-        if (lane == 0) poll_epoch(pflags + F.blk_off + k, epoch, status);
-        __syncwarp();   // the lanes' loads below follow lane 0's acquire
-        constexpr int NV = BR * NQ / 32;
-        T v[NV];
+        constexpr int NV = WALK_PAIRS / 32;
+        unsigned long long v[NV];
+        const unsigned long long* src = pp + (size_t) (nbs - 1 - t) * WALK_PAIRS;
 #pragma unroll
-        for (int u = 0; u < NV; u++) v[u] = __ldcg(bp + (size_t) k * BR * NQ + lane + 32 * u);
+        for (int u = 0; u < NV; u++) v[u] = get_pair(src + lane + 32 * u);
 #pragma unroll
         for (int u = 0; u < NV; u++) {
+          v[u] = wait_pair(src + lane + 32 * u, v[u], tag, status);
           const int e = lane + 32 * u;
-          pvb[buf][e / NQ][e % NQ] = v[u];
+          pvb[buf][e / NQ][e % NQ] = pair_value(v[u]);
         }
         walk_ready_arrive(buf);
       };
       load_p(0, 0);
       if (nbs > 1) load_p(1, 1);
-      for (int t = 0; t < nbs; t++) {
-        walk_stored_sync(t & 1);
-        if (lane == 0) {
-          flags[F.blk_off + nbs - 1 - t] = epoch;
-          st_release(progress + fi, (epoch << 12) | (t + 1));
-        }
-        if (t + 2 < nbs) load_p(t + 2, t & 1);
+      for (int t = 2; t < nbs + 2; t++) {
+        walk_free_sync(t & 1);
+        if (t < nbs) load_p(t, t & 1);
       }
       return;
     }
@@ -1450,7 +1498,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
       const int slot = k % WALK_T, buf = t & 1;
       T (*pv)[NQ + 1] = pvb[buf];
       walk_ready_sync(buf);   // p_k and the tiles of step k are in place
-      if (k > 0) fetch(k - 1);                     // in flight during the step
+      if (k > 0) fetch(k - 1);   // in flight during the step
       // near terms: p_k -= sum_j L_{k+1+j, k}^T x_{k+1+j}
       {
         T u[QG];
@@ -1486,22 +1534,30 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         for (int c = 0; c < QG; c++) xr[slot][col][qg * QG + c] = (col < bw) ? x[c] : T(0);
       }
       nbar_sync<WB_COMPUTE, 256>();
+      walk_free_arrive(buf);   // the partial buffer of this step is free
+      {
+        unsigned long long* dst = yp + (size_t) k * WALK_PAIRS;
+#pragma unroll
+        for (int u = 0; u < WALK_PAIRS / 256; u++) {
+          const int e = tid + 256 * u;
+          put_pair(dst + e, tag, xr[slot][e / NQ][e % NQ]);
+        }
+      }
       for (int e = tid; e < bw * nrhs; e += 256) {
         const int c = e % bw, q = e / bw;
         const T v = xr[slot][c][q];
         Wf[c0 + c + (size_t) q * f] = v;
         X[rw[c0 + c] + (size_t) q * ldx] = v;
       }
-      // every read of this step's tiles is done before they are replaced;
-      // the stores of x_k come before the hand-over to the communication warp
+      if (tid == 0) flags[F.blk_off + k] = epoch;
+      // every read of this step's tiles is done before they are replaced
       nbar_sync<WB_COMPUTE, 256>();
-      walk_stored_arrive(buf);
       if (k > 0) put();
     }
     return;
   }
   // ------------------------------------------------------------------ helper
-  // (the communication warp's threads only keep the barriers here)
+  // (the loader warp's threads only keep the barriers here)
   const bool act = tid < 256;
   const int2_ bk = blocks[blockIdx.x - nwalk];
   const FrontDesc F = fronts[bk.a];
@@ -1513,6 +1569,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
   T (*red)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm);            // [4]
   T (*ysb)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm) + 4;         // [WALK_HB]
   const int jlo = k + WALK_D + 1;   // far blocks j = nbs-1 .. jlo
+  const unsigned long long* yp = ypairs + (size_t) F.blk_off * WALK_PAIRS;
   // the walker's tiles of this block into L2: the near blocks' 64-row
   // column pieces of block column k (two 128-byte lines each, the second
   // while it holds rows of the near block) and the block's inverse
@@ -1544,35 +1601,32 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     }
     hpv[c][q] = v;
   }
-  // far terms: blocks j = nbs-1 down to jlo, taken as the walker publishes
-  // them (block t of the helper's order is j = nbs-1-t)
+  // far terms: blocks j = nbs-1 down to jlo (block t of the helper's order
+  // is j = nbs-1-t); rows past the block's last column are zero in the pairs
   T acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
-  walk_far_terms<T, NQ>(
-      progress + bk.a, epoch, status, max(nbs - jlo, 0),
+  walk_far_terms<NQ>(
+      tag, status, max(nbs - jlo, 0),
       [&](int t, int tt) -> T {
         const int j = nbs - 1 - t, i = qg * (BR / 4) + tt;
         return (col < bw && i < min(BR, s - j * BR)) ? __ldg(P + (size_t) (c0 + col) * f + j * BR + i) : T(0);
       },
-      [&](int t, int i, int q) -> T {
-        const int j = nbs - 1 - t;
-        return (i < min(BR, s - j * BR) && q < nrhs) ? __ldcg(Wf + j * BR + i + (size_t) q * f) : T(0);
-      },
-      ysb, acc, qg, act);
+      [&](int t) { return yp + (size_t) (nbs - 1 - t) * WALK_PAIRS; }, ysb, acc, qg, act);
   if (act) {
 #pragma unroll
     for (int q = 0; q < NQ; q++) red[qg][col][q] = acc[q];
   }
   __syncthreads();
-  T* dst = bpart + (size_t) (F.blk_off + k) * BR * NQ;
-  for (int e = tid; e < BR * NQ; e += WALK_THREADS) {
+  unsigned long long* dst = ppairs + (size_t) (F.blk_off + k) * WALK_PAIRS;
+  for (int e = tid; e < WALK_PAIRS; e += WALK_THREADS) {
     const int c = e / NQ, q = e % NQ;
-    dst[e] = hpv[c][q] - (red[0][c][q] + red[1][c][q] + red[2][c][q] + red[3][c][q]);
+    put_pair(dst + e, tag, hpv[c][q] - (red[0][c][q] + red[1][c][q] + red[2][c][q] + red[3][c][q]));
   }
-  __syncthreads();
-  if (tid == 0) st_release(pflags + F.blk_off + k, epoch);
 }
+
+// advances the walks' call counter (one thread)
+__global__ void k_walk_counter(int* counter) { *counter += 1; }
 
 }  // namespace
 
@@ -1614,8 +1668,12 @@ static void solve_attrs() {
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
     cudaFuncSetAttribute(k_bwd_big<T, 1, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 1>());
     cudaFuncSetAttribute(k_bwd_big<T, 8, SOLVE_NRHS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwd_smem<T, 8>());
-    cudaFuncSetAttribute(k_fwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) walk_smem<T>());
-    cudaFuncSetAttribute(k_bwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bwalk_smem<T>());
+    if constexpr (std::is_same<T, float>::value) {
+      cudaFuncSetAttribute(k_fwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int) walk_smem<T>());
+      cudaFuncSetAttribute(k_bwd_walk<T, SOLVE_NRHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int) bwalk_smem<T>());
+    }
     return true;
   });
 }
@@ -1642,8 +1700,22 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
   solve_attrs<T>();
   // the handshake flags restart from zero on every call, so the epochs of a
   // call are always 1, 2, ... and a recorded launch sequence stays valid
-  // (with the walks' partial-sum flags and progress words)
   cudaMemsetAsync(flags, 0, sizeof(int) * solve_flag_words(P), st);
+  // the walks: their tagged pairs, and the call counter in the word after
+  // the cleared ones, advanced on the device once per call
+  int* counter = flags + solve_flag_words(P);
+  unsigned long long* ypairs = reinterpret_cast<unsigned long long*>(part + P.fpart_off);
+  unsigned long long* ppairs = ypairs + (size_t) P.n_blk * WALK_PAIRS;
+  auto walk_level = [&](const LevelPlan& LP) {
+    return std::is_same<T, float>::value && walk_enabled() && LP.max_s_big >= FWD_CHAIN_MIN_S &&
+           (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR;
+  };
+  bool walks = false;
+  for (const LevelPlan& LP : P.levels) walks = walks || walk_level(LP);
+  if (walks) {
+    k_walk_counter<<<1, 1, 0, st>>>(counter);
+    count_launch();
+  }
   const int np = D.n_pers;
   if (np > 0) cudaMemsetAsync(D.pers_solve, 0, sizeof(int) * (size_t) (2 * np + 2), st);
   int ep = 0;
@@ -1695,12 +1767,12 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         // than a one-column instantiation (columns >= nrhs are skipped)
         auto run = [&](auto nqc) {
           constexpr int Q = decltype(nqc)::value;
-          if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
-            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR) {
+          if (walk_level(LP)) {
             const int nbig = (int) LP.big_fronts.size();
-            k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, WALK_THREADS, walk_smem<T>(), st>>>(
-                D.big_list + D.big_off[h], nbig, bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W,
-                part + P.fpart_off, nq, flags, flags + P.n_blk, flags + 2 * (size_t) P.n_blk, ef, status);
+            if constexpr (std::is_same<T, float>::value)
+              k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, WALK_THREADS, walk_smem<T>(), st>>>(
+                  D.big_list + D.big_off[h], nbig, bl, D.fronts, D.children, D.maps, D.rows, L, Dinv, Bq, ld, W, ypairs,
+                  ppairs, nq, flags, counter, ef, status);
             if (nu)
               k_fwd_big<T, Q, SOLVE_NRHS, FWD_UPD><<<nu, 128, 0, st>>>(bl + nd, D.fronts, D.children, D.maps, D.rows,
                                                                       L, Dinv, Bq, ld, W, nq, flags, ef, status);
@@ -1745,12 +1817,12 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
           count_launch();
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
-        if (LP.max_s_big >= FWD_CHAIN_MIN_S && std::is_same<T, float>::value && walk_enabled() &&
-            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR) {
+        if (walk_level(LP)) {
           const int nbig = (int) LP.big_fronts.size();
-          k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, WALK_THREADS, bwalk_smem<T>(), st>>>(
-              D.big_list + D.big_off[h], nbig, bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, part + P.fpart_off,
-              nq, flags, flags + P.n_blk, flags + 2 * (size_t) P.n_blk, eb, status);
+          if constexpr (std::is_same<T, float>::value)
+            k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, WALK_THREADS, bwalk_smem<T>(), st>>>(
+                D.big_list + D.big_off[h], nbig, bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, ypairs, ppairs, nq,
+                flags, counter, eb, status);
         } else if (nq <= 2)
           k_bwd_big<T, 2, SOLVE_NRHS, true><<<nb, 128, bwd_smem<T, 2>(), st>>>(bl, D.fronts, D.rows, L, Dinv, Xq, ld, W, part, nq, flags, eb, status);
         else if (nq <= 4)
