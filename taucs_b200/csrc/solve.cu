@@ -762,17 +762,18 @@ __device__ __forceinline__ unsigned long long wait_pair(const unsigned long long
 }
 
 // dynamic shared memory of the walk: the walker's tiles of one step, its
-// ring of y's and two partial buffers; the helpers use the first part for
-// their partial sums and staged y's
+// ring of y's, two partial buffers, the quarters' products and the reduced
+// partial; the helpers use the first part for their partial sums and staged
+// y's
 template <typename T>
 constexpr size_t walk_smem() {
-  return (WALK_T * BR * BR + (WALK_T + 2) * BR * (SOLVE_NRHS + 1)) * sizeof(T);
+  return (WALK_T * BR * BR + (WALK_T + 2 + 4 + 1) * BR * SOLVE_NRHS) * sizeof(T);
 }
 // the backward walker's tiles are [row][column], padded against bank
 // conflicts of the coalesced staging stores
 template <typename T>
 constexpr size_t bwalk_smem() {
-  return (WALK_T * BR * (BR + 1) + (WALK_T + 2) * BR * (SOLVE_NRHS + 1)) * sizeof(T);
+  return (WALK_T * BR * (BR + 1) + (WALK_T + 2 + 4 + 1) * BR * SOLVE_NRHS) * sizeof(T);
 }
 
 // The far terms of a walk's helper: blocks t = 0 .. n-1 of the chain in the
@@ -856,7 +857,7 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
            unsigned long long* __restrict__ ppairs, int nrhs, int* __restrict__ flags, const int* counter, int epoch,
            int* status) {
   static_assert(sizeof(T) == 4, "the tagged pairs carry FP32 values");
-  constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
+  constexpr int NQ = SOLVE_NRHS, TPT = BR * BR / 256;
   static_assert(NQ % 4 == 0, "four thread groups share the right-hand sides");
   extern __shared__ __align__(16) unsigned char wsm[];
   __shared__ T hpv[BR][NQ + 1];
@@ -874,10 +875,15 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     const unsigned long long* pp = ppairs + (size_t) F.blk_off * WALK_PAIRS;
     // tl[j] for j < WALK_D: L_{r, r-WALK_D+j} (zero before the first block);
     // tl[WALK_D]: the inverse of block r, and in rows >= bw of the last
-    // block the update rows' entries of L_{., r}; all column-major
+    // block the update rows' entries of L_{., r}; all column-major.  yr:
+    // the ring of the last y's; pvb: the partials of even and odd steps;
+    // red: the four j-quarters' partial products; pf: p_r after the near
+    // terms.  Rows of eight right-hand sides, 32 bytes, read as vectors.
     T (*tl)[BR][BR] = reinterpret_cast<T (*)[BR][BR]>(wsm);
-    T (*yr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * BR * sizeof(T));
-    T (*pvb)[BR][NQ + 1] = yr + WALK_T;   // [2]: the partials of even and odd steps
+    T (*yr)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm + WALK_T * BR * BR * sizeof(T));
+    T (*pvb)[BR][NQ] = yr + WALK_T;   // [2]
+    T (*red)[BR][NQ] = pvb + 2;        // [4]
+    T (*pf)[NQ] = red[4];
     if (warp == 8) {
       // ---- loader warp: the partials two steps ahead
       auto load_p = [&](int r, int buf) {
@@ -932,66 +938,79 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     };
     fetch(0);
     put();
+    // thread (row, j-quarter jq): the products of its row with 16 of the
+    // block's columns for all eight right-hand sides, reduced over the
+    // quarters in shared memory
+    const int jq = tid / BR, j0 = jq * (BR / 4);
     for (int r = 0; r < nbs; r++) {
       const int r0 = r * BR, nr = min(BR, f - r0), bw = min(BR, s - r0);
       const int slot = r % WALK_T, buf = r & 1;
-      T (*pv)[NQ + 1] = pvb[buf];
       // p_r is in place (loader warp) and so are the tiles of step r (every
       // compute thread put its share before arriving here)
       walk_ready_sync(buf);
       if (r + 1 < nbs) fetch(r + 1);   // in flight during the step
       // near terms: p_r -= sum_j L_{r, r-WALK_D+j} y_{r-WALK_D+j}
       {
-        T u[QG];
+        T u[NQ];
 #pragma unroll
-        for (int c = 0; c < QG; c++) u[c] = 0.0;
+        for (int q = 0; q < NQ; q++) u[q] = 0.0;
 #pragma unroll
         for (int jj = 0; jj < WALK_D; jj++) {
           const int k = r - WALK_D + jj;
           if (k < 0) continue;
           const int sl = k % WALK_T;
-#pragma unroll 8
-          for (int j = 0; j < BR; j++) {
+#pragma unroll 4
+          for (int j = j0; j < j0 + BR / 4; j++) {
             const T l = tl[jj][j][row];
 #pragma unroll
-            for (int c = 0; c < QG; c++) u[c] += l * yr[sl][j][qg * QG + c];
+            for (int q = 0; q < NQ; q++) u[q] += l * yr[sl][j][q];
           }
         }
 #pragma unroll
-        for (int c = 0; c < QG; c++) pv[row][qg * QG + c] -= u[c];
+        for (int q = 0; q < NQ; q++) red[jq][row][q] = u[q];
       }
       nbar_sync<WB_COMPUTE, 256>();
-      // y_r = L_rr^-1 p_r in rows < bw; the update rows keep p
-      {
-        T y[QG];
+      // thread (row, jq) finishes right-hand sides 2 jq and 2 jq + 1
 #pragma unroll
-        for (int c = 0; c < QG; c++) y[c] = 0.0;
-        if (row < bw)
-          for (int j = 0; j <= row; j++) {
-            const T d = tl[WALK_D][j][row];
-#pragma unroll
-            for (int c = 0; c < QG; c++) y[c] += d * pv[j][qg * QG + c];
-          }
-#pragma unroll
-        for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] = (row < bw) ? y[c] : pv[row][qg * QG + c];
+      for (int c = 0; c < 2; c++) {
+        const int q = 2 * jq + c;
+        pf[row][q] = pvb[buf][row][q] - (red[0][row][q] + red[1][row][q] + red[2][row][q] + red[3][row][q]);
       }
       nbar_sync<WB_COMPUTE, 256>();
       // the partial buffer of this step is free for the loader (step r + 2)
       walk_free_arrive(buf);
+      // y_r = L_rr^-1 p_r in rows < bw (the inverse is lower triangular)
+      {
+        T u[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) u[q] = 0.0;
+        const int je = min(j0 + BR / 4, min(row + 1, bw));
+        for (int j = j0; j < je; j++) {
+          const T d = tl[WALK_D][j][row];
+#pragma unroll
+          for (int q = 0; q < NQ; q++) u[q] += d * pf[j][q];
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; q++) red[jq][row][q] = u[q];
+      }
+      nbar_sync<WB_COMPUTE, 256>();
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int q = 2 * jq + c;
+        yr[slot][row][q] = (row < bw) ? red[0][row][q] + red[1][row][q] + red[2][row][q] + red[3][row][q] : pf[row][q];
+      }
+      nbar_sync<WB_COMPUTE, 256>();
       if (bw < nr) {
         // update rows inside the last diagonal block: w_i -= L[i, r] y_r
         // (reads rows < bw of the ring slot, writes rows >= bw)
         if (row >= bw) {
-          T v[QG];
 #pragma unroll
-          for (int c = 0; c < QG; c++) v[c] = 0.0;
-          for (int j = 0; j < bw; j++) {
-            const T l = tl[WALK_D][j][row];
-#pragma unroll
-            for (int c = 0; c < QG; c++) v[c] += l * yr[slot][j][qg * QG + c];
+          for (int c = 0; c < 2; c++) {
+            const int q = 2 * jq + c;
+            T v = 0.0;
+            for (int j = 0; j < bw; j++) v += tl[WALK_D][j][row] * yr[slot][j][q];
+            yr[slot][row][q] -= v;
           }
-#pragma unroll
-          for (int c = 0; c < QG; c++) yr[slot][row][qg * QG + c] -= v[c];
         }
         nbar_sync<WB_COMPUTE, 256>();
       }
@@ -1420,7 +1439,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
            unsigned long long* __restrict__ ppairs, int nrhs, int* __restrict__ flags, const int* counter, int epoch,
            int* status) {
   static_assert(sizeof(T) == 4, "the tagged pairs carry FP32 values");
-  constexpr int NQ = SOLVE_NRHS, QG = NQ / 4, TPT = BR * BR / 256;
+  constexpr int NQ = SOLVE_NRHS, TPT = BR * BR / 256;
   extern __shared__ __align__(16) unsigned char wsm[];
   __shared__ T hpv[BR][NQ + 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1438,8 +1457,10 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     // tl[j] for j < WALK_D: L_{k+1+j, k} (zero past the last block);
     // tl[WALK_D]: the inverse of block k; all [row][column]
     T (*tl)[BR][BR + 1] = reinterpret_cast<T (*)[BR][BR + 1]>(wsm);
-    T (*xr)[BR][NQ + 1] = reinterpret_cast<T (*)[BR][NQ + 1]>(wsm + WALK_T * BR * (BR + 1) * sizeof(T));
-    T (*pvb)[BR][NQ + 1] = xr + WALK_T;   // [2]: the partials by step parity
+    T (*xr)[BR][NQ] = reinterpret_cast<T (*)[BR][NQ]>(wsm + WALK_T * BR * (BR + 1) * sizeof(T));
+    T (*pvb)[BR][NQ] = xr + WALK_T;   // [2]: the partials by step parity
+    T (*red)[BR][NQ] = pvb + 2;        // [4]: the i-quarters' products
+    T (*pf)[NQ] = red[4];              // p_k after the near terms
     if (warp == 8) {
       // ---- loader warp; step t of the walk is block nbs - 1 - t
       auto load_p = [&](int t, int buf) {
@@ -1492,49 +1513,65 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
     };
     fetch(nbs - 1);
     put();
+    // thread (col, i-quarter iq): the products of its column with 16 of the
+    // block's rows for all eight right-hand sides, reduced over the quarters
+    // in shared memory
+    const int iq = tid / BR, i0 = iq * (BR / 4);
     for (int t = 0; t < nbs; t++) {
       const int k = nbs - 1 - t;
       const int c0 = k * BR, bw = min(BR, s - c0);
       const int slot = k % WALK_T, buf = t & 1;
-      T (*pv)[NQ + 1] = pvb[buf];
       walk_ready_sync(buf);   // p_k and the tiles of step k are in place
       if (k > 0) fetch(k - 1);   // in flight during the step
       // near terms: p_k -= sum_j L_{k+1+j, k}^T x_{k+1+j}
       {
-        T u[QG];
+        T u[NQ];
 #pragma unroll
-        for (int c = 0; c < QG; c++) u[c] = 0.0;
+        for (int q = 0; q < NQ; q++) u[q] = 0.0;
 #pragma unroll
         for (int jj = 0; jj < WALK_D; jj++) {
           const int j = k + 1 + jj;
           if (j >= nbs) continue;
           const int sl = j % WALK_T;
-#pragma unroll 8
-          for (int i = 0; i < BR; i++) {
+#pragma unroll 4
+          for (int i = i0; i < i0 + BR / 4; i++) {
             const T l = tl[jj][i][col];
 #pragma unroll
-            for (int c = 0; c < QG; c++) u[c] += l * xr[sl][i][qg * QG + c];
+            for (int q = 0; q < NQ; q++) u[q] += l * xr[sl][i][q];
           }
         }
 #pragma unroll
-        for (int c = 0; c < QG; c++) pv[col][qg * QG + c] -= u[c];
+        for (int q = 0; q < NQ; q++) red[iq][col][q] = u[q];
       }
       nbar_sync<WB_COMPUTE, 256>();
-      // x_k = L_kk^-T p_k (the inverse is lower triangular)
-      {
-        T x[QG];
 #pragma unroll
-        for (int c = 0; c < QG; c++) x[c] = 0.0;
-        for (int i = col; i < bw; i++) {
-          const T d = tl[WALK_D][i][col];
-#pragma unroll
-          for (int c = 0; c < QG; c++) x[c] += d * pv[i][qg * QG + c];
-        }
-#pragma unroll
-        for (int c = 0; c < QG; c++) xr[slot][col][qg * QG + c] = (col < bw) ? x[c] : T(0);
+      for (int c = 0; c < 2; c++) {
+        const int q = 2 * iq + c;
+        pf[col][q] = pvb[buf][col][q] - (red[0][col][q] + red[1][col][q] + red[2][col][q] + red[3][col][q]);
       }
       nbar_sync<WB_COMPUTE, 256>();
       walk_free_arrive(buf);   // the partial buffer of this step is free
+      // x_k = L_kk^-T p_k (the inverse is lower triangular)
+      {
+        T u[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) u[q] = 0.0;
+        const int ib = max(i0, col), ie = min(i0 + BR / 4, bw);
+        for (int i = ib; i < ie; i++) {
+          const T d = tl[WALK_D][i][col];
+#pragma unroll
+          for (int q = 0; q < NQ; q++) u[q] += d * pf[i][q];
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; q++) red[iq][col][q] = u[q];
+      }
+      nbar_sync<WB_COMPUTE, 256>();
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int q = 2 * iq + c;
+        xr[slot][col][q] = (col < bw) ? red[0][col][q] + red[1][col][q] + red[2][col][q] + red[3][col][q] : T(0);
+      }
+      nbar_sync<WB_COMPUTE, 256>();
       {
         unsigned long long* dst = yp + (size_t) k * WALK_PAIRS;
 #pragma unroll
