@@ -50,7 +50,9 @@ TOL = 1e-12
 SAMPLE_GRID = 56          # bounded CPU sample of the lognormal workload
 
 KC = dict(small_front=0, build=1, leaf=2, dinv=3, gemm_panel=4, gemm_u=5, solve_fwd=6, solve_bwd=7)
-TENSOR_KC = {"gemm_panel", "gemm_u", "dinv", "leaf"}
+# kernel classes whose roofline is the tensor pipe; the others (the panel
+# leaves among them: a latency-bound chain) are held against HBM
+TENSOR_KC = {"gemm_panel", "gemm_u"}
 # DRAM traffic per algorithmic byte of a kernel class, from one ncu capture
 # of a 56^3 update-matrix launch (FP32 fronts): dram read + write 109.7 MB
 # against 146.7 MB of L21 read once and U read and written once; the bench
@@ -819,13 +821,17 @@ def read_profile(tb, nsteps):
     return kern
 
 
-def roofline(kern, tensor_peak, tensor_src, hbm_peak, traffic_table=None):
-    """The dominant kernel's roofline.  traffic_table (kernel class ->
-    (DRAM bytes per algorithmic byte, source)) is passed only for the run whose
-    kernel and sizes the ncu capture matches (FP32 fronts at 80^3)."""
+def roofline(kern, tensor_peak, tensor_src, hbm_peak, traffic_table=None, dom=None):
+    """The roofline of kernel class dom (default: the dominant one by time).
+    traffic_table (kernel class -> (DRAM bytes per algorithmic byte, source))
+    is passed only for the run whose kernel and sizes the ncu capture matches
+    (FP32 fronts at 80^3)."""
     if not kern:
         return None
-    dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])[0]
+    if dom is None:
+        dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])[0]
+    if dom not in kern:
+        return None
     d = kern[dom]
     per_launch_ms = d["ms_per_step"] / max(d["launches_per_step"], 1)
     bytes_per_launch = d.get("gb_per_step", 0.0) / max(d["launches_per_step"], 1) * 1e9
@@ -1003,7 +1009,13 @@ def run_ours(args):
 
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
-    if mixed:
+    if mixed and args.split_format == 1 and peaks.get("bf16_tflops_sustained"):
+        bf16 = peaks["bf16_tflops_sustained"]
+        tensor_peak = bf16 / 3.0
+        tensor_src = (f"MEASURED_PEAKS.json bf16_tflops_sustained ({bf16:.0f} TF/s; the products run inside a "
+                      f"long step) / 3: the FP16x3 products do 3 FP16 MMAs (the bf16 rate) per FP32-accurate "
+                      f"product (of measured)")
+    elif mixed:
         tf32 = tf32_gemm_peak()
         tensor_peak = tf32 / 3.0
         tensor_src = (f"cuBLAS TF32 GEMM 8192^3 measured in this run ({tf32:.0f} TF/s) / 3: the TF32x3 "
@@ -1011,7 +1023,10 @@ def run_ours(args):
     else:
         tensor_peak = fp64_gemm_peak()
         tensor_src = "FP64: cuBLAS DGEMM 8192^3 measured in this run (of measured)"
-    roof = roofline(kern, tensor_peak, tensor_src, hbm_peak, TRAFFIC_PER_ALG_BYTE if mixed else None)
+    traffic = TRAFFIC_PER_ALG_BYTE if mixed else None
+    roof = roofline(kern, tensor_peak, tensor_src, hbm_peak, traffic)
+    # the update-matrix product, the dominant tensor-core kernel, beside it
+    roof_gemm = roofline(kern, tensor_peak, tensor_src, hbm_peak, traffic, dom="gemm_u")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1047,6 +1062,7 @@ def run_ours(args):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "roofline": roof,
+        "roofline_gemm_u": roof_gemm,
         "kernels": kern,
         "cpu_baseline": cpu,
         "scaled_residual": {"device": res_main, "e2e": res_e2e},

@@ -59,6 +59,12 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
     sb.insert(sb.end(), LP.solve_bwd_blocks.begin(), LP.solve_bwd_blocks.end());
     sl.insert(sl.end(), LP.solve_l21_tasks.begin(), LP.solve_l21_tasks.end());
   }
+  // each tile's child records follow one another, one per child of its front
+  int64_t nrec = 0;
+  for (Tile& t : tiles) {
+    t.ch_off = (int) nrec;
+    nrec += P.fronts[t.front].child_end - P.fronts[t.front].child_begin;
+  }
   std::vector<int2_> dblk;
   for (int i = 0; i < (int) P.fronts.size(); i++)
     if (P.fronts[i].dinv_off >= 0)
@@ -84,7 +90,10 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
          && dev_upload(&D->tiles, tiles.data(), tiles.size(), st)
          && dev_upload(&D->sfwd, sf.data(), sf.size(), st)
          && dev_upload(&D->sbwd, sb.data(), sb.size(), st)
-         && dev_upload(&D->sl21, sl.data(), sl.size(), st);
+         && dev_upload(&D->sl21, sl.data(), sl.size(), st)
+         && dev_upload(&D->tile_ch, (const TileChild*) nullptr, (size_t) std::max<int64_t>(nrec, 1), st);
+  // the records, found once per plan on the device
+  if (ok && !tiles.empty()) ok = cuda_ok((cudaError_t) launch_tile_ranges(*D, (int) tiles.size(), st), "tile ranges");
   if (ok) ok = cuda_ok(cudaStreamSynchronize(st), "plan upload");
   return ok ? 0 : -1;
 }
@@ -92,7 +101,7 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
 void devplan_free(DevPlan* D) {
   tb::dfree(D->fronts); tb::dfree(D->children); tb::dfree(D->rows); tb::dfree(D->maps);
   tb::dfree(D->acol_ptr); tb::dfree(D->a_rows); tb::dfree(D->a_idx);
-  tb::dfree(D->small_list); tb::dfree(D->big_list); tb::dfree(D->tiles);
+  tb::dfree(D->small_list); tb::dfree(D->big_list); tb::dfree(D->tiles); tb::dfree(D->tile_ch);
   tb::dfree(D->sfwd); tb::dfree(D->sbwd); tb::dfree(D->sl21); tb::dfree(D->dblk);
   tb::dfree(D->small_num); tb::dfree(D->pers_list); tb::dfree(D->pers_parent); tb::dfree(D->pers_pending0);
   tb::dfree(D->pers_work); tb::dfree(D->pers_solve);

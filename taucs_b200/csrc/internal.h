@@ -49,6 +49,16 @@ int mmd_order(int n, const int* colptr, const int* rowind, int* perm, int* invpe
 struct Tile {
   int front;   // device-order front index
   int r0, c0;
+  int ch_off;  // first of the tile's child records (one per child of the front)
+};
+
+// Where child ci of a front lands in one build tile, found once per plan:
+// the child's columns [ja, jb) and rows [ia, ib) (child-local indices) that
+// map into the tile, with the child's map offset, order m and update matrix.
+struct TileChild {
+  int ja, jb, ia, ib;
+  int map_off, mc;
+  int64_t u_off;
 };
 
 struct int2_ {

@@ -65,6 +65,7 @@ struct DevPlan {
   int* a_idx = nullptr;
   int* small_list = nullptr;   // all levels, concatenated
   int* big_list = nullptr;
+  TileChild* tile_ch = nullptr;   // per build tile, one record per child of its front
   Tile* tiles = nullptr;
   int2_* sfwd = nullptr;       // solve blocks, all levels concatenated
   int2_* sbwd = nullptr;
@@ -88,6 +89,8 @@ void devplan_free(DevPlan* D);
 // numeric factorization over all levels; vals = A's values (device);
 // status (device int) receives the smallest failing global column, or
 // INT_MAX; returns a cudaError_t code
+// the build tiles' child records (once per plan, after the upload)
+int launch_tile_ranges(const DevPlan& D, int ntiles, cudaStream_t st);
 int launch_numeric_fp64(const Plan& P, const DevPlan& D, const double* vals, double* L,
                         double* U, double* Dinv, int* status, cudaStream_t st);
 // the same factorization with FP32 fronts (TF32x3 tensor products)

@@ -184,19 +184,56 @@ k_small_persistent(const int* __restrict__ tasks, int ntask, const int* __restri
 
 // --------------------------------------------------------------- front build
 
-// threads of a build CTA: four warps (the four bounds of a child's ranges are
-// searched at once), sixteen CTAs resident per SM
+// threads of a build CTA: four warps, sixteen CTAs resident per SM
 constexpr int BUILD_THREADS = 128;
+
+// The child records of the build tiles, once per plan: CTA t (four warps)
+// finds for each child of tile t's front the child's columns and rows that
+// land in the tile, the four bounds searched at once (32-ary warp searches
+// of the child's increasing map).
+__global__ void __launch_bounds__(128)
+k_tile_ranges(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+              const int* __restrict__ maps, TileChild* __restrict__ rec) {
+  const Tile tl = tiles[blockIdx.x];
+  const FrontDesc F = fronts[tl.front];
+  const int f = F.f, s = F.s, m = f - s;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int R0, C0, nr, nc;
+  if (tl.c0 >= 0) {
+    R0 = tl.r0; C0 = tl.c0;
+    nr = min(BUILD_TR, f - R0); nc = min(BUILD_TC, s - C0);
+  } else {
+    const int uc0 = -1 - tl.c0;
+    R0 = s + tl.r0; C0 = s + uc0;
+    nr = min(BUILD_TR, m - tl.r0); nc = min(BUILD_TC, m - uc0);
+  }
+  for (int ci = F.child_begin; ci < F.child_end; ci++) {
+    const FrontDesc C = fronts[children[ci]];
+    const int mc = C.f - C.s;
+    const int key = warp == 0 ? C0 : warp == 1 ? C0 + nc : warp == 2 ? R0 : R0 + nr;
+    const int r = warp_lower_bound(maps + C.map_off, mc, key);
+    TileChild* out = rec + tl.ch_off + (ci - F.child_begin);
+    if (lane == 0) {
+      int* o = &out->ja;
+      o[warp] = r;   // ja, jb, ia, ib in warp order
+      if (warp == 0) {
+        out->map_off = C.map_off;
+        out->mc = mc;
+        out->u_off = C.u_off;
+      }
+    }
+  }
+}
+
 
 template <typename T>
 __global__ void __launch_bounds__(BUILD_THREADS)
-k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
-        const int* __restrict__ children, const int* __restrict__ maps,
+k_build(const Tile* __restrict__ tiles, const TileChild* __restrict__ tile_ch, const FrontDesc* __restrict__ fronts,
+        const int* __restrict__ maps,
         const int* __restrict__ acol_ptr, const int* __restrict__ a_rows,
         const int* __restrict__ a_idx, const T* __restrict__ vals,
         T* __restrict__ L, T* __restrict__ U, const int* status) {
   __shared__ T W[BUILD_TR * BUILD_TC];
-  __shared__ int rng[4];
   if (failed(status)) return;
   const Tile tl = tiles[blockIdx.x];
   const FrontDesc F = fronts[tl.front];
@@ -232,25 +269,20 @@ k_build(const Tile* __restrict__ tiles, const FrontDesc* __restrict__ fronts,
     }
     __syncthreads();
   }
-  for (int ci = F.child_begin; ci < F.child_end; ci++) {
-    const FrontDesc C = fronts[children[ci]];
-    const int mc = C.f - C.s;
-    const int* mp = maps + C.map_off;
-    // the child's columns and rows that land in this tile: four warps search
-    // the four bounds at once
-    if (warp < 4) {
-      const int key = warp == 0 ? C0 : warp == 1 ? C0 + nc : warp == 2 ? R0 : R0 + nr;
-      const int r = warp_lower_bound(mp, mc, key);
-      if (lane == 0) rng[warp] = r;
-    }
-    __syncthreads();
-    const int ja = rng[0], jb = rng[1], ia = rng[2], ib = rng[3];
-    __syncthreads();
+  // the children's shares, in child order, from the tile's records (found
+  // once per plan); every load of a child's share is issued before the
+  // first add (the children's update matrices were written by earlier
+  // launches)
+  const int nch = F.child_end - F.child_begin;
+  for (int c = 0; c < nch; c++) {
+    const TileChild R = tile_ch[tl.ch_off + c];
+    const int ja = R.ja, jb = R.jb, ia = R.ia, ib = R.ib;
     if (ja >= jb || ia >= ib) continue;
+    const int mc = R.mc;
+    const int* mp = maps + R.map_off;
+    const T* Uc = U + R.u_off;
     // warp w takes the child's columns ja + w + NW u, lane l its rows
-    // ia + l + 32v: every load of the tile's share is issued before the first
-    // add (the children's update matrices were written by earlier launches)
-    const T* Uc = U + C.u_off;
+    // ia + l + 32v
     constexpr int NW = BUILD_THREADS / 32, JU = (BUILD_TC + NW - 1) / NW, IU = BUILD_TR / 32;
     int pi[IU], pj[JU];
     T val[JU][IU];
@@ -1050,7 +1082,7 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
       if (prof_enabled())
         for (int fi : LP.big_fronts) by += build_bytes(P, P.fronts[fi], sizeof(T));
       prof_begin(KC_BUILD, st);
-      k_build<T><<<ntiles, BUILD_THREADS, 0, st>>>(D.tiles + D.tile_off[h], D.fronts, D.children, D.maps, D.acol_ptr,
+      k_build<T><<<ntiles, BUILD_THREADS, 0, st>>>(D.tiles + D.tile_off[h], D.tile_ch, D.fronts, D.maps, D.acol_ptr,
                                       D.a_rows, D.a_idx, vals, L, U, status);
       prof_end(KC_BUILD, st, 0.0, by);
       count_launch();
@@ -1153,6 +1185,11 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
              2.0 * sizeof(T) * D.n_dblk * PANEL_NB * PANEL_NB);
     count_launch();
   }
+  return (int) cudaGetLastError();
+}
+
+int launch_tile_ranges(const DevPlan& D, int ntiles, cudaStream_t st) {
+  k_tile_ranges<<<ntiles, 128, 0, st>>>(D.tiles, D.fronts, D.children, D.maps, D.tile_ch);
   return (int) cudaGetLastError();
 }
 

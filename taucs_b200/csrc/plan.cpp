@@ -423,11 +423,11 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
           // panel region: rows [0,f), columns [0,s); U region: m x m
           for (int c0 = 0; c0 < F.s; c0 += BUILD_TC)
             for (int r0 = (c0 / BUILD_TR) * BUILD_TR; r0 < F.f; r0 += BUILD_TR)
-              LP.build_tiles.push_back(Tile{i, r0, c0});
+              LP.build_tiles.push_back(Tile{i, r0, c0, 0});
           const int m = F.f - F.s;
           for (int c0 = 0; c0 < m; c0 += BUILD_TC)
             for (int r0 = (c0 / BUILD_TR) * BUILD_TR; r0 < m; r0 += BUILD_TR)
-              LP.build_tiles.push_back(Tile{i, r0, -1 - c0});
+              LP.build_tiles.push_back(Tile{i, r0, -1 - c0, 0});
           const int nrb = (F.f + PANEL_NB - 1) / PANEL_NB, nbs = (F.s + PANEL_NB - 1) / PANEL_NB;
           for (int r = 0; r < nbs; r++) LP.solve_fwd_blocks.push_back(int2_{i, r});
           for (int r = nbs; r < nrb; r++) fwd_upd.push_back(int2_{i, r});

@@ -101,6 +101,10 @@ size_t predict_bytes(const Plan& P) {
              + 8.0 * n * SOLVE_NRHS * 4 + 4.0 * n * SOLVE_NRHS + 16.0 * n  // R, Xr, Br, X, V32, scale
              + 4.0 * ((double) P.rows.size() + P.maps.size() + P.acol_ptr.size() + 2.0 * P.a_rows.size())
              + (double) sizeof(FrontDesc) * P.fronts.size() + 4.0 * (solve_flag_words(P) + 1);
+  // the build tiles and their child records
+  for (const LevelPlan& LP : P.levels)
+    for (const Tile& t : LP.build_tiles)
+      b += sizeof(Tile) + sizeof(TileChild) * (double) (P.fronts[t.front].child_end - P.fronts[t.front].child_begin);
   return (size_t) (b * 1.05) + (2u << 20);
 }
 
