@@ -534,11 +534,15 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       }
     }
     __syncthreads();
-    // the columns right of the piece: rw[c] -= sum_k x[k] L[c][c0 + k] (the
-    // diagonal block's rows also compute their upper part, never read)
+    // the columns right of the piece: rw[c] -= sum_k x[k] L[c][c0 + k].  A
+    // warp of the diagonal block stops at the last row it holds (the columns
+    // past it are upper-triangle entries of all its rows, never read): the
+    // warp that factors the next piece is on the chain and does the least
+    const int cmax = is_d ? (warp - 2) * 32 + 31 : PANEL_NB - 1;
     if (below) {
 #pragma unroll
       for (int c = c0 + LQ; c < PANEL_NB; c++) {
+        if (c > cmax) break;
         const T* xr = Xt[b & 1][c];
         T acc = rw[c];
 #pragma unroll

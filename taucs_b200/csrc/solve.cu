@@ -739,6 +739,17 @@ __device__ __forceinline__ unsigned long long get_pair(const unsigned long long*
 __device__ __forceinline__ bool pair_ok(unsigned long long x, unsigned tag) { return (unsigned) (x >> 32) == tag; }
 __device__ __forceinline__ float pair_value(unsigned long long x) { return __uint_as_float((unsigned) x); }
 
+// a row of eight FP32 values in shared memory (32-byte aligned), read as
+// two 128-bit vectors
+__device__ __forceinline__ void ld_row8(const float* p, float (&v)[8]) {
+  const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 4);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void st_row8(float* p, const float (&v)[8]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  *reinterpret_cast<float4*>(p + 4) = make_float4(v[4], v[5], v[6], v[7]);
+}
+
 // the tag of a walk: the solve call's counter and the epoch
 __device__ __forceinline__ unsigned walk_tag(const int* counter, int epoch) {
   return ((unsigned) *counter << 12) | (unsigned) epoch;
@@ -839,9 +850,12 @@ __device__ __forceinline__ void walk_far_terms(unsigned tag, int* status, int n,
       for (int b = 0; b < WALK_HB; b++)
         if (b < ok)
 #pragma unroll
-          for (int jj = 0; jj < BR / 4; jj++)
+          for (int jj = 0; jj < BR / 4; jj++) {
+            float yv[NQ];
+            ld_row8(ysb[b][qg * (BR / 4) + jj], yv);
 #pragma unroll
-            for (int q = 0; q < NQ; q++) acc[q] += lv[b][jj] * ysb[b][qg * (BR / 4) + jj][q];
+            for (int q = 0; q < NQ; q++) acc[q] += lv[b][jj] * yv[q];
+          }
     }
     __syncthreads();
     t += ok;
@@ -962,12 +976,13 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll 4
           for (int j = j0; j < j0 + BR / 4; j++) {
             const T l = tl[jj][j][row];
+            T yv[NQ];
+            ld_row8(yr[sl][j], yv);
 #pragma unroll
-            for (int q = 0; q < NQ; q++) u[q] += l * yr[sl][j][q];
+            for (int q = 0; q < NQ; q++) u[q] += l * yv[q];
           }
         }
-#pragma unroll
-        for (int q = 0; q < NQ; q++) red[jq][row][q] = u[q];
+        st_row8(red[jq][row], u);
       }
       nbar_sync<WB_COMPUTE, 256>();
       // thread (row, jq) finishes right-hand sides 2 jq and 2 jq + 1
@@ -987,11 +1002,12 @@ k_fwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         const int je = min(j0 + BR / 4, min(row + 1, bw));
         for (int j = j0; j < je; j++) {
           const T d = tl[WALK_D][j][row];
+          T pv8[NQ];
+          ld_row8(pf[j], pv8);
 #pragma unroll
-          for (int q = 0; q < NQ; q++) u[q] += d * pf[j][q];
+          for (int q = 0; q < NQ; q++) u[q] += d * pv8[q];
         }
-#pragma unroll
-        for (int q = 0; q < NQ; q++) red[jq][row][q] = u[q];
+        st_row8(red[jq][row], u);
       }
       nbar_sync<WB_COMPUTE, 256>();
 #pragma unroll
@@ -1536,12 +1552,13 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
 #pragma unroll 4
           for (int i = i0; i < i0 + BR / 4; i++) {
             const T l = tl[jj][i][col];
+            T xv[NQ];
+            ld_row8(xr[sl][i], xv);
 #pragma unroll
-            for (int q = 0; q < NQ; q++) u[q] += l * xr[sl][i][q];
+            for (int q = 0; q < NQ; q++) u[q] += l * xv[q];
           }
         }
-#pragma unroll
-        for (int q = 0; q < NQ; q++) red[iq][col][q] = u[q];
+        st_row8(red[iq][col], u);
       }
       nbar_sync<WB_COMPUTE, 256>();
 #pragma unroll
@@ -1559,11 +1576,12 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         const int ib = max(i0, col), ie = min(i0 + BR / 4, bw);
         for (int i = ib; i < ie; i++) {
           const T d = tl[WALK_D][i][col];
+          T pv8[NQ];
+          ld_row8(pf[i], pv8);
 #pragma unroll
-          for (int q = 0; q < NQ; q++) u[q] += d * pf[i][q];
+          for (int q = 0; q < NQ; q++) u[q] += d * pv8[q];
         }
-#pragma unroll
-        for (int q = 0; q < NQ; q++) red[iq][col][q] = u[q];
+        st_row8(red[iq][col], u);
       }
       nbar_sync<WB_COMPUTE, 256>();
 #pragma unroll
