@@ -54,11 +54,13 @@ KC = dict(small_front=0, build=1, leaf=2, dinv=3, gemm_panel=4, gemm_u=5, solve_
 # leaves among them: a latency-bound chain) are held against HBM
 TENSOR_KC = {"gemm_panel", "gemm_u"}
 # DRAM traffic per algorithmic byte of a kernel class, from one ncu capture
-# of a 56^3 update-matrix launch (FP32 fronts): dram read + write 109.7 MB
-# against 146.7 MB of L21 read once and U read and written once; the bench
-# scales it to its own per-launch algorithmic bytes
-TRAFFIC_PER_ALG_BYTE = {"gemm_u": (109.7 / 146.7, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 56^3 "
-                                                  "update-matrix launch, scaled by algorithmic bytes (L21 read once, "
+# of a 56^3 update-matrix launch (FP32 fronts, FP16x3 products, four fronts
+# of one level): dram read + write 265.0 MB against 314.0 MB of L21 read once
+# and U read and written once; the bench scales it to its own per-launch
+# algorithmic bytes
+TRAFFIC_PER_ALG_BYTE = {"gemm_u": (265.0 / 314.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 56^3 "
+                                                  "update-matrix launch (python -m taucs_b200.profile_case "
+                                                  "update-gemm 56), scaled by algorithmic bytes (L21 read once, "
                                                   "U read and written once) to this launch size")}
 
 
