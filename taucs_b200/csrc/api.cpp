@@ -206,6 +206,7 @@ static void free_device(Factor* F) {
   tb::dfree(F->dcsr_col); F->dcsr_col = nullptr;
   tb::dfree(F->dcsr_val); F->dcsr_val = nullptr;
   tb::dfree(F->dR); F->dR = nullptr;
+  tb::dfree(F->dXi); F->dXi = nullptr;
   tb::dfree(F->dseg); F->dseg = nullptr;
   tb::dfree(F->dXr); F->dXr = nullptr;
   tb::dfree(F->dBr); F->dBr = nullptr;

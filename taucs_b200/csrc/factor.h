@@ -57,6 +57,7 @@ struct Factor {
   int* dcsr_col = nullptr;
   int* dcsr_val = nullptr;     // index of each CSR entry in A's value array
   double* dR = nullptr;        // residual (n x SOLVE_NRHS)
+  double* dXi = nullptr;       // the iterate, row-interleaved (n rows of SOLVE_NRHS), for the residual's gathers
   double* dXr = nullptr;       // refined solution (n x SOLVE_NRHS)
   double* dBr = nullptr;       // right-hand sides (n x SOLVE_NRHS)
   unsigned long long* dnorm = nullptr;  // 2 x SOLVE_NRHS inf-norm bit patterns

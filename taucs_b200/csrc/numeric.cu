@@ -448,10 +448,13 @@ template <int CW>
 __device__ __forceinline__ void leaf_split_row(const double (&)[PANEL_NB], int, int, unsigned char*, int64_t, int64_t,
                                                int64_t, int) {}
 
-template <typename T>
+template <typename T, int SPF>
 __global__ void __launch_bounds__(128)
 k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows,
-       T* __restrict__ L, T* __restrict__ Dinv, float* __restrict__ sp, int sp_fmt, int kb, int* status) {
+       T* __restrict__ L, T* __restrict__ Dinv, float* __restrict__ sp, int kb, int* status) {
+  // SPF: the split format of the copy for the tensor-core products (one
+  // instantiation each: the fully unrolled row code is large)
+  constexpr int sp_fmt = SPF;
   // Xt[buf][c][k]: the new L[c][c0 + k] of the diagonal block's rows c below
   // the current piece (row-major, 16-byte aligned rows, two buffers by piece
   // parity); Lp, rinv: the factored piece and its reciprocal diagonal
@@ -573,8 +576,7 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       const int cw = sp_chunk_cols(sp_fmt);
       const int kc_end = (kb + w == s) ? (int) sp_kchunks(s, sp_fmt) : (kb + w) / cw;
       const int nch = kc_end - kb / cw;
-      if (sp_fmt == 0) leaf_split_row<4>(rw, w, nch, base, part, kb / 4, rg, r0 + i);
-      else leaf_split_row<8>(rw, w, nch, base, part, kb / 8, rg, r0 + i);
+      leaf_split_row<SPF ? 8 : 4>(rw, w, nch, base, part, kb / (SPF ? 8 : 4), rg, r0 + i);
     }
   }
 }
@@ -1113,8 +1115,10 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
         }
       }
       prof_begin(KC_LEAF, st);
-      k_leaf<T><<<dim3(gx, nb), 128, 0, st>>>(blst, D.fronts, D.rows, L, Dinv, sp, sp_fmt, kb,
-                                                           status);
+      if (sp_fmt)
+        k_leaf<T, 1><<<dim3(gx, nb), 128, 0, st>>>(blst, D.fronts, D.rows, L, Dinv, sp, kb, status);
+      else
+        k_leaf<T, 0><<<dim3(gx, nb), 128, 0, st>>>(blst, D.fronts, D.rows, L, Dinv, sp, kb, status);
       prof_end(KC_LEAF, st, fl, by);
       count_launch();
     };

@@ -112,6 +112,80 @@ __global__ void k_residual(int n, const int* __restrict__ rp, const int* __restr
   }
 }
 
+// the iterate's rows interleaved: Xi[i][q] = X[i + q ld] (zero past nrhs), so
+// that the residual gathers one 64-byte row per matrix entry instead of
+// eight scattered values
+__global__ void k_interleave(int n, const double* __restrict__ X, int ld, int nrhs, double* __restrict__ Xi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v[SOLVE_NRHS];
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs) ? X[i + (size_t) q * ld] : 0.0;
+  double2* o = reinterpret_cast<double2*>(Xi + (size_t) i * SOLVE_NRHS);
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q += 2) o[q / 2] = make_double2(v[q], v[q + 1]);
+}
+
+// k_residual over the interleaved iterate (same results, bit for bit: the
+// entries of a row are subtracted in the same order)
+__global__ void k_residual_i(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                             const int* __restrict__ vi, const double* __restrict__ vals,
+                             const double* __restrict__ Xi, const double* __restrict__ B, double* __restrict__ R,
+                             int ld, int ldr, int nrhs, const int* __restrict__ seg, unsigned long long* norms) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int sg = (seg && i < n) ? seg[i] : 0;
+  double acc[SOLVE_NRHS];
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = (i < n && q < nrhs) ? B[i + (size_t) q * ld] : 0.0;
+  const int e0 = (i < n) ? rp[i] : 0, e1 = (i < n) ? rp[i + 1] : 0;
+  for (int eb = e0; eb < e1; eb += 4) {
+    int c[4];
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) c[u] = (eb + u < e1) ? ci[eb + u] : -1;
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = (c[u] >= 0) ? vals[vi[eb + u]] : 0.0;
+    double2 xr[4][SOLVE_NRHS / 2];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const double2* row = reinterpret_cast<const double2*>(Xi + (size_t) max(c[u], 0) * SOLVE_NRHS);
+#pragma unroll
+      for (int h = 0; h < SOLVE_NRHS / 2; h++) xr[u][h] = (c[u] >= 0) ? row[h] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      if (c[u] >= 0) {
+#pragma unroll
+        for (int h = 0; h < SOLVE_NRHS / 2; h++) {
+          acc[2 * h] -= v[u] * xr[u][h].x;
+          acc[2 * h + 1] -= v[u] * xr[u][h].y;
+        }
+      }
+  }
+  double xs[SOLVE_NRHS];
+  {
+    const double2* row = reinterpret_cast<const double2*>(Xi + (size_t) (i < n ? i : 0) * SOLVE_NRHS);
+#pragma unroll
+    for (int h = 0; h < SOLVE_NRHS / 2; h++) {
+      const double2 t = row[h];
+      xs[2 * h] = t.x;
+      xs[2 * h + 1] = t.y;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < SOLVE_NRHS; q++) {
+    if (q >= nrhs) break;
+    double r = 0.0, x = 0.0;
+    if (i < n) {
+      R[i + (size_t) q * ldr] = acc[q];
+      r = fabs(acc[q]);
+      x = fabs(xs[q]);
+    }
+    seg_max(norms + 2 * q, sg, 2 * SOLVE_NRHS, r);
+    seg_max(norms + 2 * q + 1, sg, 2 * SOLVE_NRHS, x);
+  }
+}
+
 __global__ void k_scale_down(int n, const double* __restrict__ R, const double* __restrict__ scale,
                              float* __restrict__ out, int ld, int nrhs) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,6 +386,7 @@ static int ensure_refine(Factor* F) {
             up(&F->dcsr_val, cval) &&
             cuda_ok(tb::dmalloc(&F->dscale, sizeof(double) * std::max(n, 1)), "cudaMalloc") &&
             cuda_ok(tb::dmalloc(&F->dR, sizeof(double) * nv), "cudaMalloc") &&
+            cuda_ok(tb::dmalloc(&F->dXi, sizeof(double) * nv), "cudaMalloc") &&
             cuda_ok(tb::dmalloc(&F->dXr, sizeof(double) * nv), "cudaMalloc") &&
             cuda_ok(tb::dmalloc(&F->dBr, sizeof(double) * nv), "cudaMalloc") &&
             cuda_ok(tb::dmalloc(&F->dV32, sizeof(float) * nv), "cudaMalloc") &&
@@ -488,9 +563,10 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     // r = b - A x and the inf-norms of r and x per segment, read back
     auto residual = [&](cudaStream_t s) {
       cudaMemsetAsync(F->dnorm, 0, norm_bytes(F), s);
-      k_residual<<<nblk(n, 256), 256, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, X, B, F->dR,
-                                              ld, n, nq, F->dseg, F->dnorm);
-      count_launch();
+      k_interleave<<<nblk(n, 256), 256, 0, s>>>(n, X, ld, nq, F->dXi);
+      k_residual_i<<<nblk(n, 256), 256, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, F->dXi, B,
+                                                F->dR, ld, n, nq, F->dseg, F->dnorm);
+      count_launch(2);
       cudaMemcpyAsync(F->hnorm, F->dnorm, norm_bytes(F), cudaMemcpyDeviceToHost, s);
       return (int) cudaGetLastError();
     };
