@@ -983,26 +983,23 @@ static void launch_gemm(bool alt, int gx128, int gx64, int nb, const int* blst, 
 }
 
 // CTAs of the persistent small-front launch: all that fit on the device at
-// once with `smem` bytes each (computed once per device and type, at the
-// largest shared-memory size)
+// once with `smem` bytes each (the shared memory of the largest front in the
+// persistent set: a set of small fronts fits many more CTAs per SM)
 template <typename T>
 static int pers_grid(size_t smem) {
   static PerDeviceOnce pd;
-  static int per_sm[MAX_DEVICES], sms[MAX_DEVICES];
+  static int sms[MAX_DEVICES];
   per_device_once(pd, [] {
     int d = 0;
     cudaGetDevice(&d);
     cudaDeviceGetAttribute(&sms[d], cudaDevAttrMultiProcessorCount, d);
-    int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_small_persistent<T>, 128,
-                                                  (size_t) SMALL_F_MAX * SMALL_F_MAX * sizeof(T));
-    per_sm[d] = std::max(b, 1);
     return true;
   });
   int d = 0;
   cudaGetDevice(&d);
-  (void) smem;
-  return std::max(1, per_sm[d] * sms[d]);
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_small_persistent<T>, 128, smem) != cudaSuccess) b = 1;
+  return std::max(1, std::max(b, 1) * sms[d]);
 }
 
 template <typename T>
