@@ -76,7 +76,7 @@ int devplan_upload(const Plan& P, DevPlan* D, cudaStream_t st) {
          && dev_upload(&D->pers_list, P.pers_fronts.data(), P.pers_fronts.size(), st)
          && dev_upload(&D->pers_parent, P.pers_parent.data(), P.pers_parent.size(), st)
          && dev_upload(&D->pers_pending0, P.pers_pending.data(), P.pers_pending.size(), st)
-         && dev_upload(&D->pers_work, (const int*) nullptr, P.pers_fronts.size() + 1, st)
+         && dev_upload(&D->pers_work, (const int*) nullptr, P.pers_fronts.size() + 2, st)
          && dev_upload(&D->pers_solve, (const int*) nullptr, 2 * P.pers_fronts.size() + 2, st)
          && dev_upload(&D->dblk, dblk.data(), dblk.size(), st)
          && dev_upload(&D->children, P.children.data(), P.children.size(), st)

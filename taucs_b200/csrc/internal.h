@@ -150,13 +150,17 @@ struct Plan {
   int64_t part_len = 0;            // doubles of partial sums: the backward ones, then the forward walk's
   int64_t fpart_off = 0;           // start of the walks' tagged pairs (2 x n_blk x 64 x SOLVE_NRHS, 8 bytes each)
   int64_t sp_len = 0;              // floats of the split arena (the largest level's split copies)
-  // small fronts whose whole subtree is small, in device (level) order: one
-  // persistent launch factors them all, taking them from a device-side queue
-  // in this order, each once its children are done.  pers_parent: the task
-  // index of the front's parent when that parent is in the list too, else -1;
-  // pers_pending: the front's number of children (all of them in the list).
+  // small fronts whose whole subtree is small: first those whose subtree
+  // has only fronts of order <= SMALL_WARP_F (pers_nwarp of them, factored
+  // one front per warp), then the others, each part in device (level)
+  // order -- children always before their parent.  Two persistent launches
+  // (one per part) take them from device-side queues in this order, each
+  // once its children are done.  pers_parent: the task index of the front's
+  // parent when that parent is in the list too, else -1; pers_pending: the
+  // front's number of children (all of them in the list).
   std::vector<int> pers_fronts, pers_parent, pers_pending;
-  int pers_fmax = 0;               // largest order f among them
+  int pers_nwarp = 0;
+  int pers_fmax = 0;               // largest order f among the second part's fronts
   int64_t nnz = 0;
   std::vector<FrontDesc> fronts;
   std::vector<int> children;       // device-order child indices

@@ -13,6 +13,9 @@ namespace tb {
 // fronts of order <= SMALL_F_MAX are built and factored entirely in shared
 // memory by one CTA (k_small_front); larger ones go through the tiled path
 constexpr int SMALL_F_MAX = 96;
+// persistent fronts whose subtree has only fronts of order <= SMALL_WARP_F
+// are factored by one warp each, the front's rows in the lanes' registers
+constexpr int SMALL_WARP_F = 32;
 // front-build tile (rows x columns of one front held in shared memory)
 constexpr int BUILD_TR = 64;
 constexpr int BUILD_TC = 32;
@@ -76,7 +79,7 @@ struct DevPlan {
   int* pers_list = nullptr;    // Plan::pers_fronts, pers_parent, pers_pending
   int* pers_parent = nullptr;
   int* pers_pending0 = nullptr;
-  int* pers_work = nullptr;    // per factorization: pending counts (n_pers) + the queue head
+  int* pers_work = nullptr;    // per factorization: pending counts (n_pers) + the two queue heads
   int* pers_solve = nullptr;   // per solve: pending counts and done flags (n_pers each) + two queue heads
   int n_pers = 0;
   std::vector<int> small_off, big_off, tile_off, sfwd_off, sbwd_off, sl21_off, small_num_off;  // per level (host)

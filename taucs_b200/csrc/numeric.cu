@@ -69,43 +69,103 @@ __device__ void small_front(const FrontDesc& F, const FrontDesc* __restrict__ fr
 
   for (int k = tid; k < f * f; k += nt) W[k] = 0.0;
   __syncthreads();
+  // A's columns, one thread per column (duplicate rows add in order), the
+  // entries four at a time with their loads issued together
   for (int c = tid; c < s; c += nt) {
-    const int e1 = acol_ptr[F.acol_off + c + 1];
-    for (int e = acol_ptr[F.acol_off + c]; e < e1; e++) W[a_rows[e] + c * f] += vals[a_idx[e]];
+    int e = __ldg(acol_ptr + F.acol_off + c);
+    const int e1 = __ldg(acol_ptr + F.acol_off + c + 1);
+    for (; e < e1; e += 4) {
+      int r[4];
+      T v[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) r[q] = e + q < e1 ? __ldg(a_rows + e + q) : -1;
+#pragma unroll
+      for (int q = 0; q < 4; q++) v[q] = e + q < e1 ? __ldg(vals + __ldg(a_idx + e + q)) : T(0);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (r[q] >= 0) W[r[q] + c * f] += v[q];
+    }
   }
   __syncthreads();
+  // the children's update matrices in child order: warp w takes the child's
+  // columns w + nw u (eight per pass), lane l its rows l + 32 v; a pass
+  // issues all its loads before its adds
+  constexpr int SJ = 8, SV = (SMALL_F_MAX + 31) / 32;
   for (int ci = F.child_begin; ci < F.child_end; ci++) {
     const FrontDesc C = fronts[children[ci]];
     const int mc = C.f - C.s;
     const int* mp = maps + C.map_off;
     const T* Uc = U + C.u_off;
-    for (int j = warp; j < mc; j += nw) {
-      const int pj = mp[j] * f;
-      for (int i = j + lane; i < mc; i += 32) W[mp[i] + pj] += Uc[i + (size_t) j * mc];
+    int pi[SV];
+#pragma unroll
+    for (int v = 0; v < SV; v++) pi[v] = lane + 32 * v < mc ? __ldg(mp + lane + 32 * v) : -1;
+    for (int j0 = warp; j0 < mc; j0 += nw * SJ) {
+      int pj[SJ];
+      T val[SJ][SV];
+#pragma unroll
+      for (int u = 0; u < SJ; u++) {
+        const int j = j0 + nw * u;
+        pj[u] = j < mc ? __ldg(mp + j) * f : -1;
+#pragma unroll
+        for (int v = 0; v < SV; v++) {
+          const int i = lane + 32 * v;
+          val[u][v] = (j < mc && i >= j && i < mc) ? __ldg(Uc + i + (size_t) j * mc) : T(0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < SJ; u++) {
+        const int j = j0 + nw * u;
+#pragma unroll
+        for (int v = 0; v < SV; v++) {
+          const int i = lane + 32 * v;
+          if (pj[u] >= 0 && i >= j && i < mc) W[pi[v] + pj[u]] += val[u][v];
+        }
+      }
     }
     __syncthreads();
   }
+  // column j stays unscaled in W: its multipliers W[i][j] rj are formed
+  // where they are used (the same products as scaling it in place), and the
+  // panel is scaled by rjs[] on its way out -- one barrier per column
+  __shared__ T rjs[SMALL_F_MAX];
+  constexpr int KU = 4;
   for (int j = 0; j < s; j++) {
     const T d = W[j + j * f];
     if (!(d > 0.0)) {
       if (tid == 0) atomicMin(status, rows[F.rows_off + j]);
       return;
     }
-    __syncthreads();
     const T rj = rsqrt_t(d);
-    for (int i = j + 1 + tid; i < f; i += nt) W[i + j * f] *= rj;
-    if (tid == 0) W[j + j * f] = d * rj;
-    __syncthreads();
-    for (int k = j + 1 + warp; k < f; k += nw) {
-      const T lkj = W[k + j * f];
-      T* wk = W + k * f;
-      const T* wj = W + j * f;
-      for (int i = k + lane; i < f; i += 32) wk[i] -= wj[i] * lkj;
+    if (tid == 0) rjs[j] = rj;
+    // warp w takes columns k0 + nw u (u < KU) of the trailing part, lane l
+    // the rows from k0 + l; each pass loads before it stores
+    const T* wj = W + j * f;
+    for (int k0 = j + 1 + warp; k0 < f; k0 += nw * KU) {
+      T lk[KU];
+#pragma unroll
+      for (int u = 0; u < KU; u++) {
+        const int k = k0 + nw * u;
+        lk[u] = k < f ? wj[k] * rj : T(0);
+      }
+      for (int i = k0 + lane; i < f; i += 32) {
+        const T li = wj[i] * rj;
+        T w[KU];
+#pragma unroll
+        for (int u = 0; u < KU; u++) {
+          const int k = k0 + nw * u;
+          w[u] = (k < f && i >= k) ? W[i + k * f] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < KU; u++) {
+          const int k = k0 + nw * u;
+          if (k < f && i >= k) W[i + k * f] = w[u] - li * lk[u];
+        }
+      }
     }
     __syncthreads();
   }
   T* Lp = L + F.l_off;
-  for (int k = tid; k < f * s; k += nt) Lp[k] = W[k];
+  for (int k = tid; k < f * s; k += nt) Lp[k] = W[k] * rjs[k / f];
   if (m > 0) {
     T* Up = U + F.u_off;
     for (int k = tid; k < m * m; k += nt) {
@@ -135,6 +195,146 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
   return v;
 }
 
+// One front of order f <= SMALL_WARP_F by one warp: the front is assembled
+// in the warp's shared rows Ws (row-major, one padded row per front row),
+// then lane i holds row i in registers for the partial Cholesky of the first
+// s columns (column j's multipliers passed by shuffles; the same operations
+// as small_front), and writes the panel and the update matrix with zeros
+// above the diagonal.  On a nonpositive pivot the front's global column is
+// recorded and the warp returns early.
+template <typename T>
+__device__ void warp_front(const FrontDesc& F, const FrontDesc* __restrict__ fronts, T (*Ws)[SMALL_WARP_F + 1],
+                           const int* __restrict__ children, const int* __restrict__ maps,
+                           const int* __restrict__ rows, const int* __restrict__ acol_ptr,
+                           const int* __restrict__ a_rows, const int* __restrict__ a_idx,
+                           const T* __restrict__ vals, T* __restrict__ L, T* __restrict__ U, int* status) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int WF = SMALL_WARP_F;
+  const int f = F.f, s = F.s, m = f - s;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < WF; c++) Ws[lane][c] = T(0);
+  __syncwarp();
+  // A's column `lane` (one lane per column: duplicate rows add in order)
+  if (lane < s) {
+    int e = __ldg(acol_ptr + F.acol_off + lane);
+    const int e1 = __ldg(acol_ptr + F.acol_off + lane + 1);
+    for (; e + 4 <= e1; e += 4) {
+      int r[4];
+      T v[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) r[q] = __ldg(a_rows + e + q);
+#pragma unroll
+      for (int q = 0; q < 4; q++) v[q] = __ldg(vals + __ldg(a_idx + e + q));
+#pragma unroll
+      for (int q = 0; q < 4; q++) Ws[r[q]][lane] += v[q];
+    }
+    for (; e < e1; e++) Ws[__ldg(a_rows + e)][lane] += __ldg(vals + __ldg(a_idx + e));
+  }
+  // the children's update matrices in child order: lane i takes the child's
+  // row i, all its loads before its adds (distinct rows: no conflicts)
+  for (int ci = F.child_begin; ci < F.child_end; ci++) {
+    const FrontDesc C = fronts[children[ci]];
+    const int mc = C.f - C.s;
+    const T* Uc = U + C.u_off;
+    const int pi = lane < mc ? __ldg(maps + C.map_off + lane) : 0;
+    T v[WF];
+#pragma unroll
+    for (int j = 0; j < WF; j++) v[j] = (j <= lane && lane < mc) ? __ldg(Uc + lane + (size_t) j * mc) : T(0);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < WF; j++) {
+      if (j >= mc) break;
+      const int pj = __shfl_sync(FULL, pi, j);
+      if (j <= lane && lane < mc) Ws[pi][pj] += v[j];
+    }
+  }
+  __syncwarp();
+  T w[WF];
+#pragma unroll
+  for (int c = 0; c < WF; c++) w[c] = Ws[lane][c];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < WF; j++) {
+    if (j >= s) break;
+    const T d = __shfl_sync(FULL, w[j], j);
+    if (!(d > T(0))) {
+      if (lane == 0) atomicMin(status, rows[F.rows_off + j]);
+      return;
+    }
+    const T rj = rsqrt_t(d);
+    const T lij = lane > j ? w[j] * rj : (lane == j ? d * rj : T(0));
+    w[j] = lij;
+#pragma unroll
+    for (int k = j + 1; k < WF; k++) {
+      if (k >= f) break;
+      const T lkj = __shfl_sync(FULL, lij, k);
+      if (lane >= k) w[k] -= lij * lkj;
+    }
+  }
+  if (lane < f) {
+    T* Lp = L + F.l_off;
+#pragma unroll
+    for (int c = 0; c < WF; c++) {
+      if (c >= s) break;
+      Lp[lane + (size_t) c * f] = w[c];
+    }
+    if (lane >= s) {
+      T* Up = U + F.u_off;
+#pragma unroll
+      for (int k = 0; k < WF; k++)
+        if (k >= s && k < f) Up[(lane - s) + (size_t) (k - s) * m] = k <= lane ? w[k] : T(0);
+    }
+  }
+}
+
+// The first part of the persistent set (fronts whose subtree has only
+// fronts of order <= SMALL_WARP_F), in one launch of resident CTAs of four
+// warps: each warp takes the next front from a device-side queue (tasks
+// t0 .. t1-1 in level order), waits until the front's children are done
+// (pending count), factors it (warp_front) and counts itself off at its
+// parent -- also when the parent is in the second part, whose launch runs
+// after this one.  Waits are bounded (NUMERIC_TIMEOUT); after a nonpositive
+// pivot anywhere the remaining fronts are only counted off.
+template <typename T>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4)
+k_small_warp(const int* __restrict__ tasks, int t0, int t1, const int* __restrict__ parent_task, int* pending,
+             int* next, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
+             const int* __restrict__ maps, const int* __restrict__ rows, const int* __restrict__ acol_ptr,
+             const int* __restrict__ a_rows, const int* __restrict__ a_idx, const T* __restrict__ vals,
+             T* __restrict__ L, T* __restrict__ U, int* status) {
+  __shared__ T Ws_all[4][SMALL_WARP_F][SMALL_WARP_F + 1];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = t0 + atomicAdd(next, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= t1) break;
+    int skip = 0;
+    if (lane == 0) {
+      int it = 0;
+      while (ld_acquire_gpu(pending + t) != 0) {
+        if (++it > (1 << 22)) {
+          atomicMin(status, NUMERIC_TIMEOUT);
+          break;
+        }
+        __nanosleep(32);
+      }
+      skip = failed(status);
+    }
+    skip = __shfl_sync(0xffffffffu, skip, 0);
+    if (!skip)
+      warp_front<T>(fronts[tasks[t]], fronts, Ws_all[wi], children, maps, rows, acol_ptr, a_rows, a_idx, vals, L,
+                    U, status);
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      const int pt = parent_task[t];
+      if (pt >= 0) atomicSub(pending + pt, 1);
+    }
+  }
+}
+
 // The small fronts whose whole subtree is small (Plan::pers_fronts), in one
 // launch of resident CTAs: each CTA takes the next front from a device-side
 // queue (an atomic counter over the fronts in level order), waits until the
@@ -146,7 +346,7 @@ __device__ __forceinline__ int ld_acquire_gpu(const int* p) {
 // remaining fronts are only marked done.
 template <typename T>
 __global__ void __launch_bounds__(128)
-k_small_persistent(const int* __restrict__ tasks, int ntask, const int* __restrict__ parent_task, int* pending,
+k_small_persistent(const int* __restrict__ tasks, int t0, int t1, const int* __restrict__ parent_task, int* pending,
                    int* next, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
                    const int* __restrict__ maps, const int* __restrict__ rows, const int* __restrict__ acol_ptr,
                    const int* __restrict__ a_rows, const int* __restrict__ a_idx, const T* __restrict__ vals,
@@ -155,10 +355,10 @@ k_small_persistent(const int* __restrict__ tasks, int ntask, const int* __restri
   __shared__ int t_s, skip_s;
   T* W = reinterpret_cast<T*>(smraw);
   for (;;) {
-    if (threadIdx.x == 0) t_s = atomicAdd(next, 1);
+    if (threadIdx.x == 0) t_s = t0 + atomicAdd(next, 1);
     __syncthreads();
     const int t = t_s;
-    if (t >= ntask) break;
+    if (t >= t1) break;
     if (threadIdx.x == 0) {
       int it = 0;
       while (ld_acquire_gpu(pending + t) != 0) {
@@ -1002,6 +1202,18 @@ static int pers_grid(size_t smem) {
   return std::max(1, std::max(b, 1) * sms[d]);
 }
 
+// CTAs (four warps) of the one-warp-per-front persistent launch: all that
+// fit on the device at once
+template <typename T>
+static int warp_grid() {
+  int d = 0;
+  cudaGetDevice(&d);
+  int sms = 0, b = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_small_warp<T>, 128, 0) != cudaSuccess) b = 1;
+  return std::max(1, std::max(b, 1) * sms);
+}
+
 template <typename T>
 static void set_smem_attrs() {
   // once per device and type (request-server workers reach this concurrently)
@@ -1027,23 +1239,43 @@ static int launch_numeric(const Plan& P, const DevPlan& D, const T* vals, T* L, 
   k_init_status<<<1, 1, 0, st>>>(status);
   count_launch();
   if (D.n_pers > 0) {
-    // every small front with only small fronts below it, in one launch
-    cudaMemcpyAsync(D.pers_work, D.pers_pending0, sizeof(int) * D.n_pers, cudaMemcpyDeviceToDevice, st);
-    cudaMemsetAsync(D.pers_work + D.n_pers, 0, sizeof(int), st);
-    const size_t smem = (size_t) P.pers_fmax * P.pers_fmax * sizeof(T);
-    const int grid = std::min(D.n_pers, pers_grid<T>(smem));
-    double fl = 0.0, by = 0.0;
-    if (prof_enabled())
-      for (int i : P.pers_fronts) {
-        fl += front_flops(P.fronts[i]);
-        by += front_bytes(P, P.fronts[i], sizeof(T));
-      }
-    prof_begin(KC_SMALL, st);
-    k_small_persistent<T><<<grid, 128, smem, st>>>(D.pers_list, D.n_pers, D.pers_parent, D.pers_work,
-                                                   D.pers_work + D.n_pers, D.fronts, D.children, D.maps, D.rows,
-                                                   D.acol_ptr, D.a_rows, D.a_idx, vals, L, U, status);
-    prof_end(KC_SMALL, st, fl, by);
-    count_launch();
+    // every small front with only small fronts below it, in two launches:
+    // one warp per front for the subtrees of fronts of order <= SMALL_WARP_F
+    // (tasks 0 .. nw-1), then one CTA per front for the rest (their children
+    // in the first part counted themselves off in the first launch)
+    const int nw = P.pers_nwarp, np = D.n_pers;
+    cudaMemcpyAsync(D.pers_work, D.pers_pending0, sizeof(int) * np, cudaMemcpyDeviceToDevice, st);
+    cudaMemsetAsync(D.pers_work + np, 0, 2 * sizeof(int), st);
+    auto prof_range = [&](int t0, int t1, double& fl, double& by) {
+      fl = by = 0.0;
+      if (prof_enabled())
+        for (int t = t0; t < t1; t++) {
+          fl += front_flops(P.fronts[P.pers_fronts[t]]);
+          by += front_bytes(P, P.fronts[P.pers_fronts[t]], sizeof(T));
+        }
+    };
+    double fl, by;
+    if (nw > 0) {
+      const int grid = std::min((nw + 3) / 4, warp_grid<T>());
+      prof_range(0, nw, fl, by);
+      prof_begin(KC_SMALL, st);
+      k_small_warp<T><<<grid, 128, 0, st>>>(D.pers_list, 0, nw, D.pers_parent, D.pers_work, D.pers_work + np,
+                                            D.fronts, D.children, D.maps, D.rows, D.acol_ptr, D.a_rows, D.a_idx,
+                                            vals, L, U, status);
+      prof_end(KC_SMALL, st, fl, by);
+      count_launch();
+    }
+    if (np > nw) {
+      const size_t smem = (size_t) P.pers_fmax * P.pers_fmax * sizeof(T);
+      const int grid = std::min(np - nw, pers_grid<T>(smem));
+      prof_range(nw, np, fl, by);
+      prof_begin(KC_SMALL, st);
+      k_small_persistent<T><<<grid, 128, smem, st>>>(D.pers_list, nw, np, D.pers_parent, D.pers_work,
+                                                     D.pers_work + np + 1, D.fronts, D.children, D.maps, D.rows,
+                                                     D.acol_ptr, D.a_rows, D.a_idx, vals, L, U, status);
+      prof_end(KC_SMALL, st, fl, by);
+      count_launch();
+    }
   }
   for (int h = 0; h < P.n_levels; h++) {
     const LevelPlan& LP = P.levels[h];

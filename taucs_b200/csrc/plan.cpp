@@ -448,16 +448,25 @@ int build_plan(const Symbolic& S, int n, const int* colptr, const int* rowind, P
     }
   }
 
-  // the persistent set, in device (level) order
+  // the persistent set: the fronts whose subtree has only fronts of order
+  // <= SMALL_WARP_F, then the others, each part in device (level) order
   {
-    std::vector<int> task(nf, -1);
+    std::vector<int> task(nf, -1), smax(nf, 0);
     for (int i = 0; i < nf; i++) {
       const FrontDesc& F = P.fronts[i];
-      if (!pure[i]) continue;
-      task[i] = (int) P.pers_fronts.size();
-      P.pers_fronts.push_back(i);
-      P.pers_pending.push_back(F.child_end - F.child_begin);
-      P.pers_fmax = std::max(P.pers_fmax, F.f);
+      smax[i] = F.f;
+      for (int ci = F.child_begin; ci < F.child_end; ci++) smax[i] = std::max(smax[i], smax[P.children[ci]]);
+    }
+    for (int part = 0; part < 2; part++) {
+      for (int i = 0; i < nf; i++) {
+        const FrontDesc& F = P.fronts[i];
+        if (!pure[i] || (smax[i] <= SMALL_WARP_F) != (part == 0)) continue;
+        task[i] = (int) P.pers_fronts.size();
+        P.pers_fronts.push_back(i);
+        P.pers_pending.push_back(F.child_end - F.child_begin);
+        if (part == 1) P.pers_fmax = std::max(P.pers_fmax, F.f);
+      }
+      if (part == 0) P.pers_nwarp = (int) P.pers_fronts.size();
     }
     P.pers_parent.assign(P.pers_fronts.size(), -1);
     for (size_t t = 0; t < P.pers_fronts.size(); t++) {

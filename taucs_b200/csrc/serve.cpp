@@ -94,7 +94,7 @@ size_t predict_bytes(const Plan& P) {
   const double n = P.n, nnz = P.nnz;
   double b = 4.0 * (P.l_len + P.u_len + P.dinv_len + P.part_len)      // FP32 factor, partial sums
              + 4.0 * P.sp_len                                           // split arena
-             + 4.0 * 4.0 * P.pers_fronts.size()                         // persistent queues
+             + 4.0 * (6.0 * P.pers_fronts.size() + 4.0)                 // persistent queues
              + 8.0 * P.part_len                                         // FP64 partial sums
              + 12.0 * P.v_len * SOLVE_NRHS                              // work vectors (FP64 + FP32)
              + 8.0 * nnz * 2 + 4.0 * nnz * 6                            // A (FP64, FP32), pattern, CSR

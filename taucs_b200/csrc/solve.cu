@@ -251,6 +251,112 @@ __device__ __forceinline__ int ld_acquire_i(const int* p) {
   return v;
 }
 
+// One-warp form of the backward small-front step for the persistent launch
+// (fronts of order f <= SMALL_F_MAX): the front's vector is kept in the
+// warp's shared rows ws[nrhs][f]; each lane holds the L entries it needs for
+// the substitution chain in registers, loaded together (in groups of eight,
+// as far as the block is wide) before the arithmetic, so that the chain
+// waits for memory once per 32-column block instead of once per column.
+// (The same form of the forward step measured slower than fwd_small.)
+constexpr int PW_SLOTS = (SMALL_F_MAX + 31) / 32;   // rows per lane
+
+// backward step of one small front by one warp: x at the update rows, then
+// per diagonal block from the last: r = y - L[below, block]^T x_below (lane
+// j takes column jb + j, the rows in batches of eight loads), and the L11^T
+// substitution chain from registers
+template <typename T, int WS>
+__device__ void bwd_warp(const FrontDesc& F, const int* __restrict__ rows, const T* __restrict__ L,
+                         T* __restrict__ X, int ldx, const T* __restrict__ W, int nrhs, T (*ws)[SMALL_F_MAX]) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int f = F.f, s = F.s, lane = threadIdx.x & 31;
+  const T* Wf = W + F.v_off * WS;
+  const int* rw = rows + F.rows_off;
+  const T* P = L + F.l_off;
+  {
+    int g[PW_SLOTS];
+#pragma unroll
+    for (int sl = 0; sl < PW_SLOTS; sl++) {
+      const int r = lane + 32 * sl;
+      g[sl] = (r >= s && r < f) ? __ldg(rw + r) : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < SOLVE_NRHS; q++) {
+      if (q >= nrhs) break;
+      T v[PW_SLOTS];
+#pragma unroll
+      for (int sl = 0; sl < PW_SLOTS; sl++) {
+        const int r = lane + 32 * sl;
+        v[sl] = g[sl] >= 0 ? X[g[sl] + (size_t) q * ldx] : r < s ? Wf[r + q * f] : T(0);
+      }
+#pragma unroll
+      for (int sl = 0; sl < PW_SLOTS; sl++)
+        if (lane + 32 * sl < f) ws[q][lane + 32 * sl] = v[sl];
+    }
+  }
+  __syncwarp();
+  const int nblk = (s + SB - 1) / SB;
+  for (int b = nblk - 1; b >= 0; b--) {
+    const int jb = b * SB, bw = min(SB, s - jb), je = jb + bw;
+    const bool own = lane < bw;
+    const T* pj = P + (size_t) (jb + lane) * f;
+    // the solved rows below the block: x in rows [je, f)
+    T acc[SOLVE_NRHS];
+#pragma unroll
+    for (int q = 0; q < SOLVE_NRHS; q++) acc[q] = T(0);
+    for (int i0 = je; i0 < f; i0 += 8) {
+      T l[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) l[u] = (own && i0 + u < f) ? pj[i0 + u] : T(0);
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        if (i0 + u >= f) break;
+#pragma unroll
+        for (int q = 0; q < SOLVE_NRHS; q++)
+          if (q < nrhs) acc[q] += l[u] * ws[q][i0 + u];
+      }
+    }
+    // lane l: column jb + l of the diagonal block
+    T lc[SB];
+#pragma unroll
+    for (int k0 = 0; k0 < SB; k0 += 8) {
+      if (k0 >= bw) break;
+#pragma unroll
+      for (int k = k0; k < k0 + 8; k++) lc[k] = (own && k > lane && k < bw) ? pj[jb + k] : T(0);
+    }
+    const T rd = own ? T(1) / pj[jb + lane] : T(0);
+    T v[SOLVE_NRHS];
+#pragma unroll
+    for (int q = 0; q < SOLVE_NRHS; q++) v[q] = (q < nrhs && own) ? ws[q][jb + lane] - acc[q] : T(0);
+#pragma unroll
+    for (int j = SB - 1; j >= 0; j--) {
+      if (j >= bw) continue;
+      const T rj = __shfl_sync(FULL, rd, j);
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++) {
+        if (q >= nrhs) break;
+        const T xj = __shfl_sync(FULL, v[q], j) * rj;
+        if (lane == j) v[q] = xj;
+        else v[q] -= lc[j] * xj;
+      }
+    }
+    if (own)
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++)
+        if (q < nrhs) ws[q][jb + lane] = v[q];
+    __syncwarp();
+  }
+#pragma unroll
+  for (int sl = 0; sl < PW_SLOTS; sl++) {
+    const int r = lane + 32 * sl;
+    if (r < s) {
+      const int g = __ldg(rw + r);
+#pragma unroll
+      for (int q = 0; q < SOLVE_NRHS; q++)
+        if (q < nrhs) X[g + (size_t) q * ldx] = ws[q][r];
+    }
+  }
+}
+
 // The small fronts with only small fronts below them (Plan::pers_fronts), in
 // one launch per direction; each warp takes the next front from a device-
 // side queue.  Forward, in level order: a front waits until its children's
@@ -294,11 +400,11 @@ k_fwd_pers(const int* __restrict__ tasks, int ntask, const int* __restrict__ par
 }
 
 template <typename T, int WS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 k_bwd_pers(const int* __restrict__ tasks, int ntask, const int* __restrict__ parent_task, int* done, int* next,
            int epoch, const FrontDesc* __restrict__ fronts, const int* __restrict__ rows, const T* __restrict__ L,
            T* __restrict__ X, int ldx, T* __restrict__ W, int nrhs, int* status) {
-  __shared__ T xs_all[8][SB][SOLVE_NRHS];
+  __shared__ T ws_all[8][SOLVE_NRHS][SMALL_F_MAX];
   const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
   for (;;) {
     int q = 0;
@@ -318,7 +424,7 @@ k_bwd_pers(const int* __restrict__ tasks, int ntask, const int* __restrict__ par
       }
     }
     __syncwarp();
-    bwd_small<T, WS, 32>(fronts[tasks[t]], rows, L, X, ldx, W, nrhs, xs_all[wi]);
+    bwd_warp<T, WS>(fronts[tasks[t]], rows, L, X, ldx, W, nrhs, ws_all[wi]);
     __syncwarp();
     if (lane == 0) {
       __threadfence();

@@ -178,11 +178,12 @@ def test_rows_and_maps(tb, case):
 
 
 def check_persistent(F):
-    """The persistent set and its device-side queue: every task is a small
-    front (f <= 96) whose children are all tasks, queued after them (level
-    order, so a task is only taken after everything it waits for was taken);
-    every small front whose subtree is small is in the set; parent links and
-    child counts agree with the tree."""
+    """The persistent set and its device-side queues: every task is a small
+    front (f <= 96) whose children are all tasks, queued after them (so a
+    task is only taken after everything it waits for was taken); the fronts
+    whose subtree has only fronts of order <= 32 come first (the one-warp
+    launch), each part in level order; every small front whose subtree is
+    small is in the set; parent links and child counts agree with the tree."""
     import ctypes as C
     lib = __import__("taucs_b200").lib()
     fr, _ = F.layout()
@@ -197,7 +198,14 @@ def check_persistent(F):
     task_of[tasks] = np.arange(n)
     nchild = np.bincount(parent[parent >= 0], minlength=fr.shape[0])
     assert np.all(f[tasks] <= 96)
-    assert np.all(np.diff(level[tasks]) >= 0), "queue in level order"
+    smax = f.copy()
+    for i in np.argsort(level, kind="stable"):
+        if parent[i] >= 0:
+            smax[parent[i]] = max(smax[parent[i]], smax[i])
+    nw = int(np.sum(smax[tasks] <= 32))
+    assert np.all(smax[tasks[:nw]] <= 32) and np.all(smax[tasks[nw:]] > 32), "one-warp part first"
+    assert np.all(np.diff(level[tasks[:nw]]) >= 0) and np.all(np.diff(level[tasks[nw:]]) >= 0), \
+        "each part in level order"
     for t, i in enumerate(tasks):
         assert pend[t] == nchild[i]
         kids = np.nonzero(parent == i)[0]
