@@ -13,6 +13,15 @@ a capture command needs to know.
                                                        among the panel-leaf launches, of the first
                                                        leaf of the root front's level (the root
                                                        front's supernode is the largest)
+    python -m taucs_b200.profile_case batch K           one FP32-front factorization and refinement
+                                                       (1 right-hand side each) of a batch of K
+                                                       systems: half 2D 5-point grids of side
+                                                       U{8..96}, half 3D 7-point grids of side
+                                                       U{4..24}, lognormal(0, 1) conductances
+                                                       (system i: generator seed i); the launch
+                                                       order starts with the two persistent
+                                                       small-front launches (one warp per front,
+                                                       then one CTA per front)
 
 The lognormal systems are the bench's (sigma 2, anisotropy 1:1:100, seed 0,
 AMD ordering).  Profiling mode (per-launch CUDA events) is used only where an
@@ -28,6 +37,20 @@ def _system(tb, g):
     A = tb.lognormal(g, g, g, 2.0, (1, 1, 100), 0)
     p, ip = tb.order(A, "amd")
     return A.permute(p, ip)
+
+
+def _batch(tb, count, seed=0):
+    rng = np.random.default_rng(seed)
+    systems = []
+    for i in range(count):
+        if i < count // 2:
+            k = int(rng.integers(8, 97))
+            systems.append(tb.lognormal(k, k, 0, 1.0, (1, 1, 1), i))
+        else:
+            k = int(rng.integers(4, 25))
+            systems.append(tb.lognormal(k, k, k, 1.0, (1, 1, 1), i))
+    bs = [rng.uniform(-1, 1, A.n) for A in systems]
+    return systems, bs
 
 
 def _factor(tb, torch, P, profile):
@@ -54,6 +77,18 @@ def main(argv):
     import torch
     import taucs_b200 as tb
     case, g = argv[1], int(argv[2])
+    if case == "batch":
+        systems, bs = _batch(tb, g)
+        B = tb.Batch(systems)
+        B.set_precision(1)
+        dv = torch.from_numpy(B.combined_values()).cuda()
+        db = torch.from_numpy(B.combined_rhs(bs)).cuda()
+        dx = torch.zeros_like(db)
+        assert tb.lib().taucs_b200_factor_numeric_device(B.h, C.c_void_p(dv.data_ptr())) == 0, tb.last_error()
+        its, res = B.solve_refine_device(1, dx.data_ptr(), db.data_ptr(), B.n)
+        torch.cuda.synchronize()
+        print("systems", B.count, "rows", B.n, "refinement steps", its, "worst scaled residual", max(res))
+        return
     P = _system(tb, g)
     if case == "factor-refine":
         F, _, _ = _factor(tb, torch, P, False)
