@@ -798,6 +798,7 @@ constexpr int WALK_PAIRS = BR * SOLVE_NRHS;         // tagged pairs per block: [
 // levels with more big fronts keep the flag-chained kernels: every walker
 // must be resident with room to spare for helpers (two CTAs per SM)
 constexpr int WALK_MAX_FRONTS = 64;
+constexpr int BWD_WALK_MIN_S = 512;
 // named barriers of the walker (0 is __syncthreads): the compute warps
 // among themselves; partial of a step ready (+ step parity); partial buffer
 // of a step released (+ step parity)
@@ -1867,12 +1868,14 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
   int* counter = flags + solve_flag_words(P);
   unsigned long long* ypairs = reinterpret_cast<unsigned long long*>(part + P.fpart_off);
   unsigned long long* ppairs = ypairs + (size_t) P.n_blk * WALK_PAIRS;
-  auto walk_level = [&](const LevelPlan& LP) {
-    return std::is_same<T, float>::value && walk_enabled() && LP.max_s_big >= FWD_CHAIN_MIN_S &&
+  // the forward walk pays off on chains of 32 blocks or more, the backward
+  // one from 8 (both measured on the 80^3 lognormal system)
+  auto walk_level = [&](const LevelPlan& LP, bool fwd) {
+    return std::is_same<T, float>::value && walk_enabled() && LP.max_s_big >= (fwd ? FWD_CHAIN_MIN_S : BWD_WALK_MIN_S) &&
            (int) LP.big_fronts.size() <= WALK_MAX_FRONTS && LP.max_s_big < 4095 * BR;
   };
   bool walks = false;
-  for (const LevelPlan& LP : P.levels) walks = walks || walk_level(LP);
+  for (const LevelPlan& LP : P.levels) walks = walks || walk_level(LP, true) || walk_level(LP, false);
   if (walks) {
     k_walk_counter<<<1, 1, 0, st>>>(counter);
     count_launch();
@@ -1928,7 +1931,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
         // than a one-column instantiation (columns >= nrhs are skipped)
         auto run = [&](auto nqc) {
           constexpr int Q = decltype(nqc)::value;
-          if (walk_level(LP)) {
+          if (walk_level(LP, true)) {
             const int nbig = (int) LP.big_fronts.size();
             if constexpr (std::is_same<T, float>::value)
               k_fwd_walk<T, SOLVE_NRHS><<<nbig + nd, WALK_THREADS, walk_smem<T>(), st>>>(
@@ -1978,7 +1981,7 @@ static int launch_solve(const Plan& P, const DevPlan& D, const T* L, const T* Di
           count_launch();
         }
         const int2_* bl = D.sbwd + D.sbwd_off[h];
-        if (walk_level(LP)) {
+        if (walk_level(LP, false)) {
           const int nbig = (int) LP.big_fronts.size();
           if constexpr (std::is_same<T, float>::value)
             k_bwd_walk<T, SOLVE_NRHS><<<nbig + nb, WALK_THREADS, bwalk_smem<T>(), st>>>(
