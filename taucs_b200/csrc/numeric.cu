@@ -687,7 +687,12 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       rw[c] = in ? P[g + (size_t) (kb + c) * f] : ((is_d && c == i) ? T(1) : T(0));
     }
   }
-#pragma unroll
+  // the four 16-column pieces in a rolled loop over one body: the row is
+  // rotated left by 16 entries after each piece, so the current piece is
+  // always rw[0..15] and its trailing columns rw[16..63 - c0] (after the
+  // fourth rotation the row is back in column order); one copy of the row
+  // code instead of four keeps the kernel's instructions cache-resident
+#pragma unroll 1
   for (int b = 0; b < PANEL_NB / LQ; b++) {
     const int c0 = b * LQ;
     // the piece's 16 rows are lanes base .. base + 15 of warp 2 + c0 / 32
@@ -696,14 +701,14 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
       const int ii = lane - base;
       T a[LQ];
 #pragma unroll
-      for (int k = 0; k < LQ; k++) a[k] = (k <= ii) ? rw[c0 + k] : T(0);
+      for (int k = 0; k < LQ; k++) a[k] = (k <= ii) ? rw[k] : T(0);
       int bad = -1;
       CholStep<T, 0>::run(a, ii, base, bad);
       if (ii >= 0 && ii < LQ) {
         T dg = T(1);
 #pragma unroll
         for (int k = 0; k < LQ; k++) {
-          if (k <= ii) rw[c0 + k] = a[k];
+          if (k <= ii) rw[k] = a[k];
           Lp[ii][k] = (k <= ii) ? a[k] : T(0);
           if (k == ii) dg = a[k];
         }
@@ -721,7 +726,7 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
     const bool below = !is_d || i >= c0 + LQ;
     T x[LQ];
 #pragma unroll
-    for (int c = 0; c < LQ; c++) x[c] = rw[c0 + c];
+    for (int c = 0; c < LQ; c++) x[c] = rw[c];
     if (below) {
 #pragma unroll
       for (int c = 0; c < LQ; c++) {
@@ -730,29 +735,37 @@ k_leaf(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, const
         for (int c2 = c + 1; c2 < LQ; c2++) x[c2] -= x[c] * Lp[c2][c];
       }
 #pragma unroll
-      for (int c = 0; c < LQ; c++) rw[c0 + c] = x[c];
+      for (int c = 0; c < LQ; c++) rw[c] = x[c];
       if (is_d) {
 #pragma unroll
         for (int c = 0; c < LQ; c++) Xt[b & 1][i][c] = x[c];
       }
     }
     __syncthreads();
-    // the columns right of the piece: rw[c] -= sum_k x[k] L[c][c0 + k].  A
-    // warp of the diagonal block stops at the last row it holds (the columns
-    // past it are upper-triangle entries of all its rows, never read): the
-    // warp that factors the next piece is on the chain and does the least
-    const int cmax = is_d ? (warp - 2) * 32 + 31 : PANEL_NB - 1;
+    // the columns right of the piece: rw[c] -= sum_k x[k] L[c0 + c][c0 + k].
+    // A warp of the diagonal block stops at the last row it holds (the
+    // columns past it are upper-triangle entries of all its rows, never
+    // read): the warp that factors the next piece is on the chain and does
+    // the least
+    const int cmax = (is_d ? (warp - 2) * 32 + 31 : PANEL_NB - 1) - c0;
     if (below) {
 #pragma unroll
-      for (int c = c0 + LQ; c < PANEL_NB; c++) {
+      for (int c = LQ; c < PANEL_NB; c++) {
         if (c > cmax) break;
-        const T* xr = Xt[b & 1][c];
+        const T* xr = Xt[b & 1][c0 + c];
         T acc = rw[c];
 #pragma unroll
         for (int k = 0; k < LQ; k++) acc -= x[k] * xr[k];
         rw[c] = acc;
       }
     }
+    // rotate left by one piece
+#pragma unroll
+    for (int k = 0; k < LQ; k++) x[k] = rw[k];
+#pragma unroll
+    for (int k = 0; k < PANEL_NB - LQ; k++) rw[k] = rw[k + LQ];
+#pragma unroll
+    for (int k = 0; k < LQ; k++) rw[PANEL_NB - LQ + k] = x[k];
   }
   if (is_d) {
     if (blockIdx.x == 0) {
