@@ -754,7 +754,8 @@ def run_batch(args):
         F = tb.factor_symbolic(P)
         F.set_precision(0)
         pre.append((F, P, np.ascontiguousarray(bs[i][p])))
-    for F, P, b in pre[:4]:
+    # (every system once untimed: its first call also uploads its plan)
+    for F, P, b in pre:
         F.numeric(P)
         F.solve(b)
     t0 = time.perf_counter()
@@ -797,8 +798,8 @@ def run_batch(args):
         "fp64": {"value": K * count / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64 / K,
                  "worst_system_scaled_residual": res64},
         "one_at_a_time_fp64_gpu": {"value": 1.0 / t_one, "unit": UNIT,
-                                   "sample": "128 evenly spaced systems, FP64 factor + solve each, "
-                                             "patterns analysed beforehand"},
+                                   "sample": "128 evenly spaced systems, FP64 factor + solve each from host "
+                                             "arrays, patterns analysed and every system run once beforehand"},
     }
     return out
 

@@ -1219,12 +1219,19 @@ static int pers_grid(size_t smem) {
 // fit on the device at once
 template <typename T>
 static int warp_grid() {
+  static PerDeviceOnce pd;
+  static int grid[MAX_DEVICES];
+  per_device_once(pd, [] {
+    int d = 0, sms = 0, b = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_small_warp<T>, 128, 0) != cudaSuccess) b = 1;
+    grid[d] = std::max(1, std::max(b, 1) * sms);
+    return true;
+  });
   int d = 0;
   cudaGetDevice(&d);
-  int sms = 0, b = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_small_warp<T>, 128, 0) != cudaSuccess) b = 1;
-  return std::max(1, std::max(b, 1) * sms);
+  return grid[d];
 }
 
 template <typename T>
