@@ -1646,6 +1646,9 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
       const int slot = k % WALK_T, buf = t & 1;
       walk_ready_sync(buf);   // p_k and the tiles of step k are in place
       if (k > 0) fetch(k - 1);   // in flight during the step
+      // the global row of this thread's x entry (full blocks), loaded now so
+      // that the scatter at the end of the step does not wait for it
+      const int gx = (bw == BR) ? __ldg(rw + c0 + tid % BR) : 0;
       // near terms: p_k -= sum_j L_{k+1+j, k}^T x_{k+1+j}
       {
         T u[NQ];
@@ -1680,13 +1683,15 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         T u[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; q++) u[q] = 0.0;
-        const int ib = max(i0, col), ie = min(i0 + BR / 4, bw);
-        for (int i = ib; i < ie; i++) {
+#pragma unroll
+        for (int ii = 0; ii < BR / 4; ii++) {
+          const int i = i0 + ii;
+          const bool ok = i >= col && i < bw;
           const T d = tl[WALK_D][i][col];
           T pv8[NQ];
           ld_row8(pf[i], pv8);
 #pragma unroll
-          for (int q = 0; q < NQ; q++) u[q] += d * pv8[q];
+          for (int q = 0; q < NQ; q++) u[q] += ok ? d * pv8[q] : T(0);
         }
         st_row8(red[iq][col], u);
       }
@@ -1709,7 +1714,7 @@ k_bwd_walk(const int* __restrict__ walk_fronts, int nwalk, const int2_* __restri
         const int c = e % bw, q = e / bw;
         const T v = xr[slot][c][q];
         Wf[c0 + c + (size_t) q * f] = v;
-        X[rw[c0 + c] + (size_t) q * ldx] = v;
+        X[(bw == BR ? gx : rw[c0 + c]) + (size_t) q * ldx] = v;
       }
       if (tid == 0) flags[F.blk_off + k] = epoch;
       // every read of this step's tiles is done before they are replaced
