@@ -534,13 +534,10 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
     // done fires once every MMA issued above has completed
     tc_commit(done);
   }
-  // ---- epilogue: warp w owns TMEM lanes (tile rows) 32 w .. 32 w + 31
-  int gd = 1;
-  if (lane == 0) gd = mbar_wait(done, 0);
-  const bool got = __shfl_sync(0xffffffffu, gd, 0) != 0;
-  __syncwarp();
-  if (!got && lane == 0) record_timeout(status);
-  tc_fence_after();
+  // ---- epilogue: warp w owns TMEM lanes (tile rows) 32 w .. 32 w + 31.
+  // The first 32 columns of the old C rows are loaded before the wait for
+  // the products (they do not depend on them), and each later group while
+  // the group before it is stored
   const int er = warp * 32 + lane;
   const int row = R0 + er;
   const bool rv = er < nr && row >= lo;
@@ -554,10 +551,32 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
     ldc = m;
   }
   const int coff = (mode == 0) ? 0 : s;
+  // all 32 loads of a group are issued before the first store: interleaved,
+  // each load would wait for the store before it (the compiler cannot rule
+  // out that they alias), one memory latency per element
+  auto load_old = [&](int cb, float (&o)[32]) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+      const int col = C0 + cb + j;
+      o[j] = (rv && cb + j < nc && col >= lo && row >= col) ? Cp[(int64_t) (col - coff) * ldc] : 0.0f;
+    }
+  };
+  float oldn[32];
+  load_old(0, oldn);
+  int gd = 1;
+  if (lane == 0) gd = mbar_wait(done, 0);
+  const bool got = __shfl_sync(0xffffffffu, gd, 0) != 0;
+  __syncwarp();
+  if (!got && lane == 0) record_timeout(status);
+  tc_fence_after();
   // tcgen05.ld is warp-collective: the decision must be warp-uniform
   if (__all_sync(0xffffffffu, got && !*(volatile int*) &abort_cta)) {
     const unsigned tl = tmem + ((unsigned) (warp * 32) << 16);
     for (int cb = 0; cb < nc; cb += 32) {
+      float old[32];
+#pragma unroll
+      for (int j = 0; j < 32; j++) old[j] = oldn[j];
+      if (cb + 32 < nc) load_old(cb + 32, oldn);
       unsigned v[32];
       tmem_ld32(tl + cb, v);
       if (FMT) {
@@ -568,15 +587,6 @@ k_gemm_sp(const int* __restrict__ list, const FrontDesc* __restrict__ fronts, co
           v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(v1[j]) * (1.0f / 2048.0f));
       }
       if (rv) {
-        // all 32 loads are issued before the first store: interleaved, each
-        // load would wait for the store before it (the compiler cannot rule
-        // out that they alias), one memory latency per element
-        float old[32];
-#pragma unroll
-        for (int j = 0; j < 32; j++) {
-          const int col = C0 + cb + j;
-          old[j] = (cb + j < nc && col >= lo && row >= col) ? Cp[(int64_t) (col - coff) * ldc] : 0.0f;
-        }
 #pragma unroll
         for (int j = 0; j < 32; j++) {
           const int col = C0 + cb + j;
