@@ -254,37 +254,36 @@ __device__ void warp_front(const FrontDesc& F, const FrontDesc* __restrict__ fro
 #pragma unroll
   for (int c = 0; c < WF; c++) w[c] = Ws[lane][c];
   __syncwarp();
-#pragma unroll
-  for (int j = 0; j < WF; j++) {
-    if (j >= s) break;
-    const T d = __shfl_sync(FULL, w[j], j);
+  // pivot j in a rolled loop: the row is rotated left by one entry per
+  // pivot, so column j is always w[0] and column j + k is w[k] (one body of
+  // row code instead of one per pivot keeps the kernel cache-resident); the
+  // finished column goes straight to the panel
+  T* Lp = L + F.l_off;
+#pragma unroll 1
+  for (int j = 0; j < s; j++) {
+    const T d = __shfl_sync(FULL, w[0], j);
     if (!(d > T(0))) {
       if (lane == 0) atomicMin(status, rows[F.rows_off + j]);
       return;
     }
     const T rj = rsqrt_t(d);
-    const T lij = lane > j ? w[j] * rj : (lane == j ? d * rj : T(0));
-    w[j] = lij;
+    const T lij = lane > j ? w[0] * rj : (lane == j ? d * rj : T(0));
+    if (lane < f) Lp[lane + (size_t) j * f] = lij;
 #pragma unroll
-    for (int k = j + 1; k < WF; k++) {
-      if (k >= f) break;
-      const T lkj = __shfl_sync(FULL, lij, k);
-      if (lane >= k) w[k] -= lij * lkj;
+    for (int k = 1; k < WF; k++) {
+      const T lkj = __shfl_sync(FULL, lij, (j + k) & (WF - 1));
+      if (lane >= j + k && j + k < f) w[k] -= lij * lkj;
     }
+#pragma unroll
+    for (int k = 0; k < WF - 1; k++) w[k] = w[k + 1];
+    w[WF - 1] = T(0);
   }
-  if (lane < f) {
-    T* Lp = L + F.l_off;
+  // after s rotations w[k] is the row's column s + k
+  if (lane < f && lane >= s) {
+    T* Up = U + F.u_off;
 #pragma unroll
-    for (int c = 0; c < WF; c++) {
-      if (c >= s) break;
-      Lp[lane + (size_t) c * f] = w[c];
-    }
-    if (lane >= s) {
-      T* Up = U + F.u_off;
-#pragma unroll
-      for (int k = 0; k < WF; k++)
-        if (k >= s && k < f) Up[(lane - s) + (size_t) (k - s) * m] = k <= lane ? w[k] : T(0);
-    }
+    for (int k = 0; k < WF; k++)
+      if (k < m) Up[(lane - s) + (size_t) k * m] = k <= lane - s ? w[k] : T(0);
   }
 }
 
@@ -297,7 +296,7 @@ __device__ void warp_front(const FrontDesc& F, const FrontDesc* __restrict__ fro
 // after this one.  Waits are bounded (NUMERIC_TIMEOUT); after a nonpositive
 // pivot anywhere the remaining fronts are only counted off.
 template <typename T>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 4)
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4)
 k_small_warp(const int* __restrict__ tasks, int t0, int t1, const int* __restrict__ parent_task, int* pending,
              int* next, const FrontDesc* __restrict__ fronts, const int* __restrict__ children,
              const int* __restrict__ maps, const int* __restrict__ rows, const int* __restrict__ acol_ptr,
