@@ -6,7 +6,7 @@ Default workload (--workload mixed80): the precision configuration -- a 3D
 exp(2 N(0,1)) times an anisotropy of 1:1:100 in x:y:z (seeded generator,
 taucs_b200_generate_lognormal), AMD ordering, 8 right-hand sides ~ U(-1,1)
 (seed 0).  One STEP factors the analysed pattern with FP32 fronts (diagonal
-scaling, tcgen05 TF32x3 products) and refines all 8 solutions in FP64 to a
+scaling, tcgen05 FP16x3 products; --split-format 0 for TF32x3) and refines all 8 solutions in FP64 to a
 scaled residual ||Ax-b||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-12 --
 the FP32+refinement form.  The plain FP64 path (FP64 fronts, one solve of the
 8 right-hand sides) is timed beside it on the same inputs and reported as
@@ -54,11 +54,11 @@ KC = dict(small_front=0, build=1, leaf=2, dinv=3, gemm_panel=4, gemm_u=5, solve_
 # leaves among them: a latency-bound chain) are held against HBM
 TENSOR_KC = {"gemm_panel", "gemm_u"}
 # DRAM traffic per algorithmic byte of a kernel class, from one ncu capture
-# of a 56^3 update-matrix launch (FP32 fronts, FP16x3 products, four fronts
-# of one level): dram read + write 265.0 MB against 314.0 MB of L21 read once
-# and U read and written once; the bench scales it to its own per-launch
-# algorithmic bytes
-TRAFFIC_PER_ALG_BYTE = {"gemm_u": (265.0 / 314.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 56^3 "
+# of a 56^3 update-matrix launch (FP32 fronts, FP16x3 products, the largest
+# update product of the 56^3 factorization: one front, 630 tiles): dram read
+# + write 101.1 + 11.0 MB against 129.9 MB of L21 read once and U read and
+# written once; the bench scales it to its own per-launch algorithmic bytes
+TRAFFIC_PER_ALG_BYTE = {"gemm_u": (112.1 / 129.9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 56^3 "
                                                   "update-matrix launch (python -m taucs_b200.profile_case "
                                                   "update-gemm 56), scaled by algorithmic bytes (L21 read once, "
                                                   "U read and written once) to this launch size")}

@@ -5,14 +5,17 @@ a capture command needs to know.
     python -m taucs_b200.profile_case factor-refine G   one FP32-front numeric factorization of the
                                                        G^3 lognormal system and its refinement
                                                        (8 right-hand sides): one bench step
-    python -m taucs_b200.profile_case update-gemm G     one FP32-front factorization of the G^3
-                                                       system; prints the launch index, among the
-                                                       tcgen05 GEMM launches, of the largest
-                                                       update-matrix product (for ncu -k/-s)
-    python -m taucs_b200.profile_case leaf G            the same factorization; prints the index,
-                                                       among the panel-leaf launches, of the first
-                                                       leaf of the root front's level (the root
-                                                       front's supernode is the largest)
+    python -m taucs_b200.profile_case update-gemm G     two FP32-front factorizations of the G^3
+                                                       system (the first unprofiled); prints the
+                                                       launch index, among the tcgen05 GEMM
+                                                       launches of the process, of the second
+                                                       one's largest update-matrix product (for
+                                                       ncu -k/-s)
+    python -m taucs_b200.profile_case leaf G            the same two factorizations; prints the
+                                                       index, among the panel-leaf launches of the
+                                                       process, of the second one's first leaf of
+                                                       the root front's level (the root front's
+                                                       supernode is the largest)
     python -m taucs_b200.profile_case batch K           one FP32-front factorization and refinement
                                                        (1 right-hand side each) of a batch of K
                                                        systems: half 2D 5-point grids of side
@@ -59,6 +62,10 @@ def _factor(tb, torch, P, profile):
     dv = torch.from_numpy(P.values).cuda()
     lib = tb.lib()
     if profile:
+        # one factorization first, unprofiled: the first launch of each
+        # kernel carries one-time costs that would skew the per-launch times
+        assert lib.taucs_b200_factor_numeric_device(F.h, C.c_void_p(dv.data_ptr())) == 0, tb.last_error()
+        torch.cuda.synchronize()
         lib.taucs_b200_profile(1)
     assert lib.taucs_b200_factor_numeric_device(F.h, C.c_void_p(dv.data_ptr())) == 0, tb.last_error()
     torch.cuda.synchronize()
@@ -102,7 +109,8 @@ def main(argv):
         _, _, (kc, ms) = _factor(tb, torch, P, True)
         g = [(int(k), float(t)) for k, t in zip(kc, ms) if k in (4, 5)]   # panel and update products
         best = max(range(len(g)), key=lambda j: g[j][1] if g[j][0] == 5 else -1.0)
-        print("tcgen05 GEMM launches", len(g), "largest update-matrix launch: index", best, "ms", g[best][1])
+        # the index counts the unprofiled factorization's launches too
+        print("tcgen05 GEMM launches", len(g), "largest update-matrix launch: index", len(g) + best, "ms", g[best][1])
     elif case == "leaf":
         F, _, (kc, ms) = _factor(tb, torch, P, True)
         leaves = [float(t) for k, t in zip(kc, ms) if k == 2]
@@ -110,7 +118,7 @@ def main(argv):
         # the first of the final run of leaf launches of the root's width
         s_root = int(F.info().max_sn_size)
         first = max(0, len(leaves) - (s_root + 63) // 64)
-        print("leaf launches", len(leaves), "first leaf of the root level: index", first,
+        print("leaf launches", len(leaves), "first leaf of the root level: index", len(leaves) + first,
               "ms", leaves[first] if leaves else 0.0)
     else:
         raise SystemExit(__doc__)
