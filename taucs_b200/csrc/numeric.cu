@@ -902,10 +902,6 @@ __device__ __forceinline__ void cp_async_t(float* smem, const float* gmem, bool 
 }
 
 // FP64 fronts: one DMMA per fragment pair
-__device__ __forceinline__ void mma_tile(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
-  dmma16888(c, a, b);
-}
-
 // FP32 fronts: three TF32 products per fragment pair (hi*hi + hi*lo + lo*hi,
 // the operands split as x = tf32(x) + tf32(x - tf32(x))), which keeps close
 // to FP32 accuracy on the TF32 tensor path (same m16n8k8 fragment layout as
@@ -921,17 +917,6 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4], 
       "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-__device__ __forceinline__ void mma_tile(float (&c)[4], const float (&a)[4], const float (&b)[2]) {
-  unsigned ah[4], al[4], bh[2], bl[2];
-#pragma unroll
-  for (int i = 0; i < 4; i++) split_tf32(a[i], ah[i], al[i]);
-#pragma unroll
-  for (int i = 0; i < 2; i++) split_tf32(b[i], bh[i], bl[i]);
-  mma_tf32(c, al, bh);
-  mma_tf32(c, ah, bl);
-  mma_tf32(c, ah, bh);
 }
 
 // MI x NI fragment products of one k8 step.  FP32: every A and B fragment is
