@@ -128,7 +128,9 @@ __global__ void k_interleave(int n, const double* __restrict__ X, int ld, int nr
 
 // k_residual over the interleaved iterate (same results, bit for bit: the
 // entries of a row are subtracted in the same order)
-__global__ void k_residual_i(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+constexpr int RES_THREADS = 256;   // the block size k_residual_i is launched with
+
+__global__ void __launch_bounds__(RES_THREADS) k_residual_i(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                              const int* __restrict__ vi, const double* __restrict__ vals,
                              const double* __restrict__ Xi, const double* __restrict__ B, double* __restrict__ R,
                              int ld, int ldr, int nrhs, const int* __restrict__ seg, unsigned long long* norms) {
@@ -172,6 +174,15 @@ __global__ void k_residual_i(int n, const int* __restrict__ rp, const int* __res
       xs[2 * h + 1] = t.y;
     }
   }
+  // the norms: when every row of the block lies in one segment (the usual
+  // case) the block reduces them first and issues one atomic per norm --
+  // one per warp would queue thousands of atomics on the same few words
+  __shared__ int sg_blk;
+  __shared__ double red[RES_THREADS / 32][2 * SOLVE_NRHS];
+  if (threadIdx.x == 0) sg_blk = sg;
+  __syncthreads();
+  const bool uni = __syncthreads_and(sg == sg_blk) != 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < SOLVE_NRHS; q++) {
     if (q >= nrhs) break;
@@ -181,8 +192,29 @@ __global__ void k_residual_i(int n, const int* __restrict__ rp, const int* __res
       r = fabs(acc[q]);
       x = fabs(xs[q]);
     }
-    seg_max(norms + 2 * q, sg, 2 * SOLVE_NRHS, r);
-    seg_max(norms + 2 * q + 1, sg, 2 * SOLVE_NRHS, x);
+    if (uni) {
+      for (int o = 16; o > 0; o >>= 1) {
+        r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+        x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+      }
+      if (lane == 0) {
+        red[warp][2 * q] = r;
+        red[warp][2 * q + 1] = x;
+      }
+    } else {
+      seg_max(norms + 2 * q, sg, 2 * SOLVE_NRHS, r);
+      seg_max(norms + 2 * q + 1, sg, 2 * SOLVE_NRHS, x);
+    }
+  }
+  if (uni) {
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < 2 * nrhs) {
+      double m = 0.0;
+#pragma unroll
+      for (int w = 0; w < RES_THREADS / 32; w++) m = fmax(m, red[w][t]);
+      max_abs(norms + (size_t) sg_blk * 2 * SOLVE_NRHS + t, m);
+    }
   }
 }
 
@@ -564,7 +596,7 @@ static int refine_device(Factor* F, int nrhs, double* dX, const double* dB, int 
     auto residual = [&](cudaStream_t s) {
       cudaMemsetAsync(F->dnorm, 0, norm_bytes(F), s);
       k_interleave<<<nblk(n, 256), 256, 0, s>>>(n, X, ld, nq, F->dXi);
-      k_residual_i<<<nblk(n, 256), 256, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, F->dXi, B,
+      k_residual_i<<<nblk(n, RES_THREADS), RES_THREADS, 0, s>>>(n, F->dcsr_ptr, F->dcsr_col, F->dcsr_val, F->dvals_cur, F->dXi, B,
                                                 F->dR, ld, n, nq, F->dseg, F->dnorm);
       count_launch(2);
       cudaMemcpyAsync(F->hnorm, F->dnorm, norm_bytes(F), cudaMemcpyDeviceToHost, s);
