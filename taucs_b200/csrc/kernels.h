@@ -17,7 +17,7 @@ constexpr int SMALL_F_MAX = 96;
 // are factored by one warp each, the front's rows in the lanes' registers
 constexpr int SMALL_WARP_F = 32;
 // front-build tile (rows x columns of one front held in shared memory)
-constexpr int BUILD_TR = 64;
+constexpr int BUILD_TR = 128;
 constexpr int BUILD_TC = 32;
 // block column width of the blocked partial Cholesky of large fronts
 constexpr int PANEL_NB = 64;

@@ -13,7 +13,7 @@
 //                   factors it (right-looking partial Cholesky of the first s
 //                   columns, i.e. POTRF+TRSM+SYRK fused) and writes the panel
 //                   and the update matrix once;
-//   k_build         larger fronts: one CTA per 64x32 tile of the front's lower
+//   k_build         larger fronts: one CTA per 128x32 tile of the front's lower
 //                   part gathers A's entries and the children's update
 //                   matrices into shared memory in a fixed child order
 //                   (deterministic, no atomics) and writes the tile once;
