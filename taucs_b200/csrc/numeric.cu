@@ -14,9 +14,10 @@
 //                   columns, i.e. POTRF+TRSM+SYRK fused) and writes the panel
 //                   and the update matrix once;
 //   k_build         larger fronts: one CTA per 128x32 tile of the front's lower
-//                   part gathers A's entries and the children's update
-//                   matrices into shared memory in a fixed child order
-//                   (deterministic, no atomics) and writes the tile once;
+//                   part gathers A's entries (shared-memory atomic adds:
+//                   duplicate entries are summed) and the children's update
+//                   matrices in a fixed child order into shared memory and
+//                   writes the tile once;
 //   k_leaf          blocked partial Cholesky, step kb: one launch factors
 //                   the 64x64 diagonal block and applies it to every row
 //                   below it (one CTA per 64-row slab, each factoring the
